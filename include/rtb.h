@@ -1,0 +1,283 @@
+/*
+ * rtb.h -- C ABI of the B200 ray-tracing engine (librtb200.so).
+ *
+ * The library replaces the CUDA engine of amirych/rt behind the engine API of
+ * common-lib/rt_engine_func.h:25-104.  Two families of entry points:
+ *
+ *  1. Drop-in calls (rtb_<reference name>): one per function of
+ *     rt_engine_func.h, same arguments and semantics, host arrays in and out,
+ *     synchronous.  rt_b200/shim/rt_engine_b200.cpp implements the reference's
+ *     C++ prototypes on top of them, so Beam, Surface, TabulatedFunction,
+ *     Scheme and ccd_frame link against this library unchanged.
+ *  2. Device-resident calls (rtb_trace*, rtb_generate_beams, rtb_ccd_frame,
+ *     rtb_adjoint_*): a whole scheme over many beams in one call, rays kept in
+ *     HBM, asynchronous on a caller stream.
+ *
+ * Every function returns an int status: 0..4 equal RT_engine_error
+ * (common-lib/rt_engine_errors.h:4-5); larger values name the exception the
+ * reference would have thrown.  No function throws across the ABI.
+ * Arrays are plain pointers; "host" arguments may be pageable or pinned
+ * memory, "device" arguments must be device memory of the current device.
+ */
+#ifndef RTB_H
+#define RTB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+enum {
+    RTB_OK = 0,               /* ENGINE_ERROR_OK */
+    RTB_INIT_FAILED = 1,      /* ENGINE_ERROR_INIT_FAILED */
+    RTB_BAD_ALLOC = 2,        /* ENGINE_ERROR_BAD_ALLOC */
+    RTB_FAILED = 3,           /* ENGINE_ERROR_FAILED */
+    RTB_BAD_VALUE = 4,        /* ENGINE_ERROR_BAD_VALUE */
+    RTB_NO_INTERSECTIONS = 5, /* a stage lost every remaining ray (Surface::NoIntersections, surface.cpp:256,318) */
+    RTB_NO_GOOD_RAYS = 6,     /* an action lost every remaining ray (Surface::NoGoodRays, surface.cpp:469,581) */
+    RTB_OUT_OF_RANGE = 7      /* a wavelength outside a table (TabulatedFunction::OutOfRange, tabulated_function.cpp:179-181) */
+};
+
+/* ---- enumerations with the reference's numbering ------------------------ */
+enum { RTB_PLANE = 0, RTB_CONIC = 1, RTB_TORIC = 2, RTB_AUX_CLASS = 3 };          /* surface.h:130 */
+enum { RTB_MIRROR = 0, RTB_LENS = 1, RTB_GRATING = 2, RTB_STOP = 3,
+       RTB_SHADE = 4, RTB_DETECTOR = 5, RTB_AUX_TYPE = 6 };                     /* surface.h:131 */
+enum { RTB_CIRCLE = 0, RTB_RECTANGLE = 1 };                                    /* surface.h:132, beam.h:32 */
+enum { RTB_REFLECTIVE = 0, RTB_TRANSPARENT = 1 };                              /* surface.h:241 */
+
+/* ---- engine options ----------------------------------------------------- */
+enum { RTB_ENGINE_PER_SURFACE = 0, RTB_ENGINE_FUSED = 1 };
+enum { RTB_FP64 = 0, RTB_MIXED = 1 };
+/* Quirk fixes: 0 reproduces the reference; each bit selects the correct form. */
+enum {
+    RTB_FIX_TORIC_SIGN = 1,   /* iter_toric's 1+k1c^2Y^2 becomes 1-k1c^2Y^2 (cuda_engine/rt_cuda_engine_surface.cu:350) */
+    RTB_FIX_TORIC_STEP = 2    /* iter_toric's Steffensen step divides by Fzn-Fxn == 0 once converged and
+                                 sends the ray to inf/NaN (surface.cu:390); the fix stops there instead */
+};
+
+#define RTB_MAX_POLY 10           /* MAX_POLY_COEFFS, surface.h:14 */
+#define RTB_MAX_PARAMS 16         /* c, k, N, a1..a10, cR */
+#define RTB_MAX_SURFACES 32
+#define RTB_MAX_GRATINGS 8
+#define RTB_MAX_KNOTS 1024
+#define RTB_NOT_LOST 0xFF         /* lost_stage of a ray that reached the end */
+
+/* A tabulated function (TabulatedFunction, tabulated_function.h:30-66):
+ * n == 1 is a single value y[0] valid for any argument; n >= 4 knots x
+ * strictly increasing with natural-spline second derivatives y2 (from
+ * rtb_spline_init).  Pointers are host memory. */
+typedef struct rtb_table {
+    size_t n;
+    const double* x;
+    const double* y;
+    const double* y2;
+} rtb_table;
+
+/* One surface, as Scheme::load_from_file builds it (common-lib/scheme.cpp:416-664). */
+typedef struct rtb_surface {
+    int32_t cls;                    /* RTB_PLANE .. RTB_AUX_CLASS */
+    int32_t type;                   /* RTB_MIRROR .. RTB_AUX_TYPE */
+    int32_t shape;                  /* RTB_CIRCLE / RTB_RECTANGLE */
+    int32_t grating_type;           /* RTB_REFLECTIVE / RTB_TRANSPARENT */
+    int64_t order;                  /* Grating::Order[0] (surface.h:277) */
+    double gr_const;                /* grating constant, microns (surface.h:278) */
+    double params[RTB_MAX_PARAMS];  /* Surface::Params: c, k, N, a1..aN [, cR] (surface.cpp:49-83) */
+    double size[2];                 /* Surface::Size: radius, or width and height */
+    double center[2];               /* Surface::Center */
+    double distance[3];             /* Surface::Distance, mm */
+    double angles_deg[3];           /* scheme angles, degrees, about y, x, z */
+    rtb_table n1, n2;               /* refractive index before / after */
+} rtb_surface;
+
+/* One beam (one wavelength range of Scheme::run, scheme.cpp:966-1067): a
+ * contiguous segment of the ray arrays plus what generates it. */
+typedef struct rtb_beam {
+    uint64_t first_ray;             /* index of the first ray in the ray arrays */
+    uint64_t n_rays;
+    int64_t orders[RTB_MAX_GRATINGS];  /* order of each grating in scheme order (range-file columns, scheme.cpp:1026-1032) */
+    int32_t n_orders;               /* 0: every grating uses its own order */
+    int32_t shape;                  /* RTB_CIRCLE (disk) */
+    double disk[3];                 /* Beam::Params: rays per wavelength, R_in, R_out (beam.cpp:219-245) */
+    double center[3];               /* Beam::Center */
+    double range[2];                /* wavelength range, microns */
+    uint64_t n_lambda;              /* composite beam: ray i takes lambda_(i mod n_lambda) (beam.cpp:470-484) */
+    double field[2];                /* field angles, radians: direction (tan fx, tan fy, 1)/norm */
+    uint64_t seed;                  /* Philox4x32-10 key of this beam's positions */
+} rtb_beam;
+
+/* Ray arrays (SoA, common-lib/beam.h:96-99).  Device memory for the
+ * device-resident calls, host memory for rtb_trace_host. */
+typedef struct rtb_rays {
+    double *X, *Y, *Z, *cX, *cY, *cZ, *lambda;
+    char* flag;                     /* 1 good, 0 lost */
+    uint8_t* lost_stage;            /* 3*surface + {0 intersection, 1 aperture, 2 action}; RTB_NOT_LOST */
+    size_t n;
+} rtb_rays;
+
+typedef struct rtb_trace_opts {
+    int32_t engine;                 /* RTB_ENGINE_PER_SURFACE / RTB_ENGINE_FUSED */
+    int32_t precision;              /* RTB_FP64 / RTB_MIXED */
+    uint32_t fixes;                 /* RTB_FIX_* bits */
+    int32_t renormalize_lost;       /* apply the reference's trailing Normalize calls to lost rays (beam.cpp:527-571) */
+    int32_t block_size;             /* 0: tuned default */
+    int32_t rays_per_thread;        /* 0: tuned default */
+    int32_t state_out;              /* fused: 1 writes X..cZ back, 0 writes only the CCD-plane X,Y */
+    int32_t reserved;
+} rtb_trace_opts;
+
+/* Per-call statistics of a trace. */
+typedef struct rtb_trace_stats {
+    uint64_t ray_surfaces;          /* sum over rays of non-Aux surfaces reached (lost rays count their losing surface) */
+    uint64_t n_good;                /* rays that reached the end */
+    int32_t failed_beam;            /* first beam whose stage lost every remaining ray, -1 if none */
+    int32_t failed_stage;           /* that stage, -1 if none */
+} rtb_trace_stats;
+
+/* CCD geometry (ccd/ccd_frame.cpp:46-68): light-sensitive area in mm, pixel
+ * counts, pixel size in mm. */
+typedef struct rtb_ccd {
+    double xsize, ysize;
+    uint64_t xdim, ydim;
+    double xpix, ypix;
+} rtb_ccd;
+
+/* =========================================================================
+ * 1. Drop-in calls: rt_engine_func.h, host arrays, synchronous.
+ * ========================================================================= */
+
+/* rt_engine_init (rt_engine_func.h:25): selects device 0, creates the stream
+ * and the device arena.  Idempotent. */
+int rtb_init(void);
+
+/* rt_engine_info (rt_engine_func.h:26): newline-separated info lines into buf. */
+int rtb_info(char* buf, size_t buflen);
+
+/* beam_random (rt_engine_func.h:30-31): uniform disk, params = [N, R_in, R_out],
+ * center = [x, y, z].  Positions come from Philox4x32-10 keyed by `seed`, ray
+ * `first_ray + i`, in place of the reference's clock-seeded cuRAND. */
+int rtb_beam_random(int shape, const double* params, const double* center, size_t n,
+                    double* X, double* Y, double* Z, uint64_t seed, uint64_t first_ray);
+
+/* beam_conic_cosins (rt_engine_func.h:33); conic_angle in radians. */
+int rtb_beam_conic_cosins(size_t n, double conic_angle, const double* X, const double* Y,
+                          double* cX, double* cY, double* cZ);
+
+/* beam_gauss_cosins (rt_engine_func.h:35); fwhm in arcsec. */
+int rtb_beam_gauss_cosins(size_t n, double fwhm, double* cX, double* cY, double* cZ, uint64_t seed);
+
+/* uniform_range_beam (rt_engine_func.h:37). */
+int rtb_uniform_range_beam(size_t n, const double* range, double* lambda);
+
+/* random_range_beam (rt_engine_func.h:39). */
+int rtb_random_range_beam(size_t n, const double* range, double* lambda, uint64_t seed);
+
+/* beam_transform (rt_engine_func.h:41-42); angles in radians. */
+int rtb_beam_transform(size_t n, const double* angles, const double* dist,
+                       double* X, double* Y, double* Z, double* cX, double* cY, double* cZ);
+
+/* surface_intersection (rt_engine_func.h:46-49).  *n_bad is incremented. */
+int rtb_surface_intersection(int cls, const double* params, size_t n,
+                             double* X, double* Y, double* Z, double* cX, double* cY, double* cZ,
+                             size_t* n_bad, char* flag);
+
+/* surface_reflection (rt_engine_func.h:52-54). */
+int rtb_surface_reflection(int cls, const double* params, size_t n,
+                           double* X, double* Y, double* Z, double* cX, double* cY, double* cZ);
+
+/* surface_refraction (rt_engine_func.h:57-61). */
+int rtb_surface_refraction(int cls, const double* params, size_t n,
+                           double* X, double* Y, double* Z, double* cX, double* cY, double* cZ,
+                           const double* lambda, const rtb_table* n1, const rtb_table* n2,
+                           size_t* n_bad, char* flag);
+
+/* surface_diffration (rt_engine_func.h:64-70). */
+int rtb_surface_diffration(int cls, int gr_type, const double* params, long diff_order,
+                           double gr_constant, size_t n,
+                           double* X, double* Y, double* Z, double* cX, double* cY, double* cZ,
+                           const double* lambda, const rtb_table* n1, const rtb_table* n2,
+                           size_t* n_bad, char* flag);
+
+/* surface_QE (rt_engine_func.h:73): spec[i] *= QE(lambda[i]). */
+int rtb_surface_QE(size_t n, const double* lambda, double* spec, const rtb_table* qe);
+
+/* grating_energy_distr (rt_engine_func.h:75-78); angles in radians. */
+int rtb_grating_energy_distr(size_t n, const double* lambda, long order, double blaze_angle,
+                             double alpha, double gamma, double gr_const, double rule_start,
+                             double rule_stop, double* energy_distr);
+
+/* rt_engine_free_vector / rt_engine_alocate_vector (rt_engine_func.h:84-86):
+ * page-locked host vectors, so the drop-in copies run at full PCIe rate. */
+void rtb_free_vector(double* data);
+double* rtb_alocate_vector(size_t n_elem);
+
+/* spline_init (rt_engine_func.h:91): natural cubic spline second derivatives. */
+int rtb_spline_init(size_t n, const double* x, const double* y, double* y2);
+
+/* ccd_coordinates (rt_engine_func.h:96-99). */
+int rtb_ccd_coordinates(size_t n, const double* X, const double* Y, double ccd_xsize,
+                        double ccd_ysize, double ccd_xpix, double ccd_ypix,
+                        unsigned int* ccd_X, unsigned int* ccd_Y);
+
+/* compute_ccd_image (rt_engine_func.h:101-104): image += spec(l)*l/hc*QE(l)*pix_area
+ * per ray; rays whose pixel lies outside xdim x ydim are skipped and counted
+ * in *n_outside (may be NULL). */
+int rtb_compute_ccd_image(size_t n, const unsigned int* ccd_X, const unsigned int* ccd_Y,
+                          const double* lambda, const rtb_table* qe, const rtb_table* spec,
+                          size_t xdim, size_t ydim, double xpix, double ypix, double* image,
+                          uint64_t* n_outside);
+
+/* Host loops of Beam and Surface run on the device.
+ * Beam::Normalize (beam.cpp:527-571). */
+int rtb_normalize(size_t n, double* cX, double* cY, double* cZ);
+/* Surface::ApplyConstrains / Shade::ApplyConstrains (surface.cpp:264-321,652-699);
+ * shade != 0 selects the inverted test.  *n_bad is incremented. */
+int rtb_apply_constrains(int shade, int shape, const double* size, const double* center, size_t n,
+                         const double* X, const double* Y, char* flag, size_t* n_bad);
+/* Beam::Rearrange (beam.cpp:574-598) over the good prefix [0, *n_good) of the
+ * seven arrays; *n_good is updated. */
+int rtb_rearrange(size_t* n_good, double* X, double* Y, double* Z, double* cX, double* cY,
+                  double* cZ, double* lambda, char* flag);
+
+/* =========================================================================
+ * 2. Device-resident calls.  `stream` is a cudaStream_t (NULL: the library's
+ *    own stream).  Each call is ordered on that stream.
+ * ========================================================================= */
+
+/* Fill rays[first_ray, first_ray+n_rays) of every beam: uniform disk positions
+ * (Philox4x32-10), parallel cosines turned by the field angles, composite
+ * uniform wavelengths, flag 1, lost_stage RTB_NOT_LOST. */
+int rtb_generate_beams(const rtb_beam* beams, size_t n_beams, const rtb_rays* rays, void* stream);
+
+/* Trace every beam through the scheme, in place (Scheme::run's per-surface
+ * loop, scheme.cpp:983-1055).  Rays keep their index; lost rays carry
+ * flag 0 and lost_stage.  stats may be NULL. */
+int rtb_trace(const rtb_surface* surfaces, size_t n_surfaces, const rtb_beam* beams, size_t n_beams,
+              const rtb_trace_opts* opts, const rtb_rays* rays, rtb_trace_stats* stats, void* stream);
+
+/* rtb_trace on host arrays: copies in, traces and copies out, overlapping the
+ * copies of one chunk with the trace of another.  Synchronous. */
+int rtb_trace_host(const rtb_surface* surfaces, size_t n_surfaces, const rtb_beam* beams,
+                   size_t n_beams, const rtb_trace_opts* opts, const rtb_rays* host_rays,
+                   rtb_trace_stats* stats);
+
+/* Frame counts: counts[iy*xdim + ix] += 1 for every good ray whose pixel
+ * (ccd_coordinates, ccd.cu:30-45) lies on the CCD; *n_outside (device, may be
+ * NULL) counts the good rays that do not.  counts is not cleared. */
+int rtb_ccd_frame(const rtb_rays* rays, const rtb_ccd* ccd, uint32_t* counts, uint64_t* n_outside,
+                  void* stream);
+
+/* Order of the rays as the reference's Rearrange calls leave them
+ * (beam.cpp:574-598), from lost_stage: order[k] is the index of the ray at
+ * position k of the reference's arrays for beam b; positions [0, n_good) are
+ * the good rays.  order is device memory of rays->n entries. */
+int rtb_reference_order(const rtb_beam* beams, size_t n_beams, size_t n_stages, const rtb_rays* rays,
+                        uint32_t* order, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RTB_H */

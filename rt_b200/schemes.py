@@ -1,0 +1,356 @@
+"""Spectrograph schemes and synthetic beams of the benchmark configurations.
+
+A scheme is a list of `SurfaceSpec`, the fields of one <surface> element of
+the reference's scheme XML (common-lib/scheme.cpp:416-664); `to_c()` turns it
+into the rtb_surface array of include/rtb.h.  The geometry BASELINE leaves
+open (distances, tilts, apertures, the glass and QE tables) is fixed here,
+seeded, and written out as scheme XML + range/table files by `write_xml` so
+the reference's own ray-tracing program reads the same scheme.
+
+Configurations:
+  * C0  `littrow_free()`: parabolic collimator R=-800 (k=-1) at z=400, plane
+        600 l/mm grating order +1 tilted 10 deg about x, spherical camera
+        R=-600, plane CCD 2048^2 x 15 um; 5 wavelengths 0.400..0.700 um.
+  * C1  `echelle()`: off-axis parabola R=-1600 (k=-1), echelle 31.6 l/mm
+        (orders 30..60, one range per order), cross-disperser 300 l/mm order 1
+        turned 90 deg about z, toric fold Rx=-2000 Ry=-2100, even-asphere lens
+        R=150/-400 with A4..A10 ~ N(0, 1e-7*10^-3k) and a 61-knot glass n(l),
+        plane CCD 4096^2 x 15 um; 64 wavelengths 0.380..0.900 um.
+  * C4  `littrow_free_asphere()`: C0 plus one even-asphere mirror.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+from typing import Callable, Sequence
+
+import numpy as np
+
+from . import ffi
+
+SEED = 20141203  # master seed of every synthetic table and beam
+
+
+# ---------------------------------------------------------------------------
+# tables
+
+def qe_table(seed: int = SEED) -> tuple[np.ndarray, np.ndarray]:
+    """CCD QE: 41 knots over 0.35..0.75 um, values uniform in [0.6, 0.95]."""
+    rng = np.random.default_rng(seed)
+    x = np.linspace(0.35, 0.75, 41)
+    return x, rng.uniform(0.6, 0.95, size=41)
+
+
+def glass_table() -> tuple[np.ndarray, np.ndarray]:
+    """Camera-lens glass n(lambda): 61 knots over 0.35..0.95 um, a Cauchy law
+    n = 1.5046 + 0.00420/l^2 (a borosilicate crown)."""
+    x = np.linspace(0.35, 0.95, 61)
+    return x, 1.5046 + 0.00420 / (x * x)
+
+
+# ---------------------------------------------------------------------------
+# surfaces
+
+@dataclass
+class SurfaceSpec:
+    cls: int
+    type: int
+    shape: int = ffi.CIRCLE
+    params: Sequence[float] = (0.0, 0.0, 0.0)
+    size: Sequence[float] = (1000.0, 1000.0)
+    center: Sequence[float] = (0.0, 0.0)
+    distance: Sequence[float] = (0.0, 0.0, 0.0)
+    angles: Sequence[float] = (0.0, 0.0, 0.0)      # degrees about y, x, z
+    grating_type: int = ffi.REFLECTIVE
+    order: int = 0
+    gr_const: float = 0.0                          # microns
+    n1: object = 1.0                               # float or (x, y) table
+    n2: object = 1.0
+    comment: str = ""
+
+
+def frame_towards(p: Sequence[float], v: Sequence[float]) -> tuple[list, list]:
+    """Distance and angles (deg) of a surface frame whose origin is p and whose
+    +z axis is the unit direction v, both given in the current frame, for the
+    reference's transform (translation, then rotations about y, x, z,
+    cuda_engine/rt_cuda_engine_beam.cu:416-579)."""
+    vx, vy, vz = v
+    rho = math.hypot(vx, vz)
+    ay = math.degrees(math.atan2(vx, vz))
+    ax = math.degrees(math.atan2(vy, rho))
+    return [float(p[0]), float(p[1]), float(p[2])], [ay, ax, 0.0]
+
+
+SplineFn = Callable[[np.ndarray, np.ndarray], np.ndarray]
+
+
+class CScheme:
+    """rtb_surface array built from specs; owns the table arrays."""
+
+    def __init__(self, specs: Sequence[SurfaceSpec], spline: SplineFn):
+        self.specs = list(specs)
+        self.holders = []
+        self.array = (ffi.Surface * len(self.specs))()
+        for k, s in enumerate(self.specs):
+            c = self.array[k]
+            c.cls, c.type, c.shape, c.grating_type = s.cls, s.type, s.shape, s.grating_type
+            c.order, c.gr_const = int(s.order), float(s.gr_const)
+            if len(s.params) > ffi.MAX_PARAMS:
+                raise ValueError("too many surface parameters")
+            for i, v in enumerate(s.params):
+                c.params[i] = float(v)
+            c.size[0], c.size[1] = (float(s.size[0]), float(s.size[1] if len(s.size) > 1 else 0.0))
+            c.center[0], c.center[1] = float(s.center[0]), float(s.center[1])
+            for i in range(3):
+                c.distance[i] = float(s.distance[i])
+                c.angles_deg[i] = float(s.angles[i])
+            c.n1 = self._table(s.n1, spline)
+            c.n2 = self._table(s.n2, spline)
+
+    def _table(self, t, spline: SplineFn) -> ffi.Table:
+        if isinstance(t, (int, float)):
+            h = ffi.TableHolder(value=float(t))
+        else:
+            h = ffi.TableHolder(x=t[0], y=t[1])
+            h.y2[:] = spline(h.x, h.y)
+        self.holders.append(h)
+        return h.table
+
+    def __len__(self) -> int:
+        return len(self.specs)
+
+    @property
+    def surfaces(self):
+        return list(self.array)
+
+    def n_gratings(self) -> int:
+        return sum(1 for s in self.specs if s.type == ffi.GRATING)
+
+    def non_aux(self) -> int:
+        return sum(1 for s in self.specs if s.type != ffi.AUX_TYPE)
+
+
+def to_c(specs: Sequence[SurfaceSpec], spline: SplineFn) -> CScheme:
+    return CScheme(specs, spline)
+
+
+# ---------------------------------------------------------------------------
+# beams
+
+def make_beam(first_ray: int, n_per_lambda: int, n_lambda: int, radius: float, lam_range,
+              seed: int, orders: Sequence[int] = (), field=(0.0, 0.0), center=(0.0, 0.0, 0.0)) -> ffi.Beam:
+    b = ffi.Beam()
+    b.first_ray = first_ray
+    b.n_rays = n_per_lambda * n_lambda
+    b.n_orders = len(orders)
+    for i, o in enumerate(orders):
+        b.orders[i] = int(o)
+    b.shape = ffi.CIRCLE
+    b.disk[0], b.disk[1], b.disk[2] = float(n_per_lambda), 0.0, float(radius)
+    for i in range(3):
+        b.center[i] = float(center[i])
+    b.range[0], b.range[1] = float(lam_range[0]), float(lam_range[1])
+    b.n_lambda = n_lambda
+    b.field[0], b.field[1] = float(field[0]), float(field[1])
+    b.seed = seed
+    return b
+
+
+# ---------------------------------------------------------------------------
+# C0: Littrow-free single-beam spectrograph
+
+C0_LAMBDA = (0.400, 0.700)
+C0_NLAMBDA = 5
+C0_RADIUS = 10.0
+C0_CCD = dict(xsize=30.72, ysize=30.72, xdim=2048, ydim=2048, xpix=0.015, ypix=0.015)
+
+
+def littrow_free() -> list[SurfaceSpec]:
+    """C0 scheme.  The beam (disk r=10 mm at z=0, along +z) meets the
+    parabola (R=-800, k=-1) at z=400, converges through its focus 400 mm
+    back, meets the grating 700 mm after the parabola (tilted 10 deg about x),
+    the camera mirror 600 mm further on and the CCD in the camera's image of
+    the focus.  Distances along the chief ray of 0.55 um."""
+    par = SurfaceSpec(ffi.CONIC, ffi.MIRROR, params=(-1 / 800.0, -1.0, 0), size=(40.0, 0.0),
+                      distance=(0.0, 0.0, 400.0), comment="collimator")
+    gr = SurfaceSpec(ffi.PLANE, ffi.GRATING, shape=ffi.RECTANGLE, size=(80.0, 80.0),
+                     distance=(0.0, 0.0, -700.0), angles=(180.0, 10.0, 0.0), order=1,
+                     gr_const=1.0 / 0.6, comment="grating 600 l/mm")
+    cam_d, cam_a = C0_FRAMES["camera"]
+    cam = SurfaceSpec(ffi.CONIC, ffi.MIRROR, params=(-1 / 600.0, 0.0, 0), size=(80.0, 0.0),
+                      distance=cam_d, angles=cam_a, comment="camera")
+    ccd_d, ccd_a = C0_FRAMES["ccd"]
+    ccd = SurfaceSpec(ffi.PLANE, ffi.DETECTOR, shape=ffi.RECTANGLE, size=(30.72, 30.72),
+                      distance=ccd_d, angles=ccd_a, comment="CCD 2048x2048 15um")
+    return [par, gr, cam, ccd]
+
+
+def littrow_free_asphere() -> list[SurfaceSpec]:
+    """C4 scheme: C0 with the camera mirror made an even asphere
+    (A4, A6, A8 of small seeded values)."""
+    s = littrow_free()
+    rng = np.random.default_rng(SEED + 4)
+    a = [0.0, float(rng.normal(0, 1e-10)), float(rng.normal(0, 1e-13)), float(rng.normal(0, 1e-16))]
+    s[2].params = (-1 / 600.0, 0.0, len(a), *a)
+    s[2].comment = "camera (even asphere)"
+    return s
+
+
+def c0_beams(n_per_lambda: int = 20000, seed: int = SEED, first_ray: int = 0) -> list[ffi.Beam]:
+    return [make_beam(first_ray, n_per_lambda, C0_NLAMBDA, C0_RADIUS, C0_LAMBDA, seed)]
+
+
+# Frames of C0's camera and CCD (distance, angles) in the frame of the
+# previous surface, found by tracing the chief ray (see design_frames()).
+C0_FRAMES = {
+    "camera": ([-198.0, -104.188907, -556.723155], [-160.421942, -4.0, 0.0]),
+    "ccd": ([0.0, -47.560451, -452.507462], [180.0, -6.0, 0.0]),
+}
+
+# ---------------------------------------------------------------------------
+# C1: cross-dispersed echelle
+
+C1_LAMBDA = (0.380, 0.900)
+C1_NLAMBDA = 64
+C1_RADIUS = 25.0
+C1_ORDERS = tuple(range(30, 61))
+C1_CCD = dict(xsize=61.44, ysize=61.44, xdim=4096, ydim=4096, xpix=0.015, ypix=0.015)
+# Frames (distance, angles) of C1's surfaces, each in the frame of the previous
+# one, aimed along the chief ray of order 45 at 0.6284 um.
+C1_FRAMES: dict = {
+    "oap": ([0.0, -80.0, 1000.0], [0.0, 0.0, 0.0]),
+    "echelle": ([0.0, 65.037406, -151.25187], [116.385776, -2.550993, 5.126721]),
+    "xdisp": ([0.202434, 0.0, -149.999863], [179.922676, 0.0, 90.0]),
+    "fold": ([-28.278, 0.0, -147.310403], [-169.133574, 12.0, 0.0]),
+    "lens1": ([0.0, -31.186754, -146.72214], [180.0, -12.0, 0.0]),
+    "lens2": ([0.0, 0.0, 12.0], [0.0, 0.0, 0.0]),
+    "ccd": ([0.0, 0.0, 145.0], [0.0, 0.0, 0.0]),
+}
+
+
+def lens_asphere_coeffs(seed: int = SEED + 1) -> list[float]:
+    """A4..A10 ~ N(0, 1e-7 * 10^-3k), k = 1..4, as polynomial terms a2..a5
+    (a1, the r^2 term, is 0)."""
+    rng = np.random.default_rng(seed)
+    return [float(rng.normal(0.0, 1e-7 * 10.0 ** (-3 * k))) for k in range(1, 5)]
+
+
+def echelle(glass=None) -> list[SurfaceSpec]:
+    g = glass_table() if glass is None else glass
+    a1 = lens_asphere_coeffs(SEED + 1)
+    a2 = lens_asphere_coeffs(SEED + 2)
+    f = C1_FRAMES
+    return [
+        SurfaceSpec(ffi.CONIC, ffi.MIRROR, params=(-1 / 1600.0, -1.0, 0), size=(140.0, 0.0),
+                    distance=f["oap"][0], angles=f["oap"][1], comment="off-axis parabola"),
+        SurfaceSpec(ffi.PLANE, ffi.GRATING, shape=ffi.RECTANGLE, size=(260.0, 120.0),
+                    distance=f["echelle"][0], angles=f["echelle"][1], order=45, gr_const=1000.0 / 31.6,
+                    comment="echelle 31.6 l/mm, blaze 63.5 deg"),
+        SurfaceSpec(ffi.PLANE, ffi.GRATING, shape=ffi.RECTANGLE, size=(160.0, 160.0),
+                    distance=f["xdisp"][0], angles=f["xdisp"][1], order=1, gr_const=1000.0 / 300.0,
+                    comment="cross-disperser 300 l/mm"),
+        SurfaceSpec(ffi.TORIC, ffi.MIRROR, params=(-1 / 2100.0, 0.0, 0, -1 / 2000.0), size=(110.0, 0.0),
+                    distance=f["fold"][0], angles=f["fold"][1], comment="toric fold"),
+        SurfaceSpec(ffi.CONIC, ffi.LENS, params=(1 / 150.0, 0.0, 5, 0.0, *a1), size=(75.0, 0.0),
+                    distance=f["lens1"][0], angles=f["lens1"][1], n1=1.0, n2=g, comment="camera lens front"),
+        SurfaceSpec(ffi.CONIC, ffi.LENS, params=(-1 / 400.0, 0.0, 5, 0.0, *a2), size=(75.0, 0.0),
+                    distance=f["lens2"][0], angles=f["lens2"][1], n1=g, n2=1.0, comment="camera lens back"),
+        SurfaceSpec(ffi.PLANE, ffi.DETECTOR, shape=ffi.RECTANGLE, size=(61.44, 61.44),
+                    distance=f["ccd"][0], angles=f["ccd"][1], comment="CCD 4096x4096 15um"),
+    ]
+
+
+def c1_rays_per_lambda(total: int = 100_000_000) -> int:
+    """Rays per wavelength per order range: ceil(total / 31 / 64)."""
+    return -(-total // (len(C1_ORDERS) * C1_NLAMBDA))
+
+
+def c1_beams(n_per_lambda: int | None = None, seed: int = SEED, orders=C1_ORDERS) -> list[ffi.Beam]:
+    """One beam per echelle order (range rows "0.38 0.90 m 1")."""
+    n = c1_rays_per_lambda() if n_per_lambda is None else n_per_lambda
+    beams, first = [], 0
+    for i, m in enumerate(orders):
+        beams.append(make_beam(first, n, C1_NLAMBDA, C1_RADIUS, C1_LAMBDA, seed + 1000 + i, orders=(m, 1)))
+        first += n * C1_NLAMBDA
+    return beams
+
+
+def total_rays(beams: Sequence[ffi.Beam]) -> int:
+    return int(max(b.first_ray + b.n_rays for b in beams))
+
+
+def ccd(cfg: dict) -> ffi.CCD:
+    return ffi.CCD(cfg["xsize"], cfg["ysize"], cfg["xdim"], cfg["ydim"], cfg["xpix"], cfg["ypix"])
+
+
+# ---------------------------------------------------------------------------
+# Coverage schemes: small schemes that between them reach every surface
+# class, type, aperture shape, intersection kind and action of the engine,
+# with losses at every kind of stage.  Used by the parity tests.
+
+def _glass_n():
+    x, y = glass_table()
+    return (x, y)
+
+
+def coverage_schemes() -> dict[str, list[SurfaceSpec]]:
+    g = _glass_n()
+    mirrors = [
+        SurfaceSpec(ffi.CONIC, ffi.MIRROR, params=(-1 / 500.0, 0.0, 0), size=(9.0, 0.0),
+                    distance=(0.0, 0.0, 100.0), comment="spherical mirror, clips the beam edge"),
+        SurfaceSpec(ffi.AUX_CLASS, ffi.AUX_TYPE, distance=(0.0, 0.0, -60.0), angles=(180.0, 0.0, 0.0)),
+        SurfaceSpec(ffi.TORIC, ffi.MIRROR, params=(-1 / 900.0, 0.2, 0, -1 / 800.0), size=(30.0, 0.0),
+                    distance=(0.0, 0.0, 40.0), angles=(3.0, -2.0, 0.0), comment="toric mirror"),
+        SurfaceSpec(ffi.PLANE, ffi.MIRROR, shape=ffi.RECTANGLE, size=(40.0, 40.0),
+                    distance=(0.0, 0.0, -80.0), angles=(160.0, 5.0, 0.0), comment="plane fold"),
+        SurfaceSpec(ffi.PLANE, ffi.STOP, shape=ffi.RECTANGLE, size=(16.0, 14.0), center=(3.47, -0.3),
+                    distance=(11.714761, -1.364972, -27.584438), angles=(156.989684, -2.607805, 10.0),
+                    comment="rectangular stop"),
+        SurfaceSpec(ffi.PLANE, ffi.SHADE, size=(0.5, 0.0), center=(-4.6, 2.3),
+                    distance=(0.0, 0.0, 20.0), comment="central obscuration"),
+        SurfaceSpec(ffi.PLANE, ffi.SHADE, shape=ffi.RECTANGLE, size=(0.4, 30.0), center=(-4.0, 0.0),
+                    distance=(0.0, 0.0, 5.0), comment="spider vane"),
+        SurfaceSpec(ffi.PLANE, ffi.DETECTOR, shape=ffi.RECTANGLE, size=(30.72, 30.72),
+                    distance=(0.0, 0.0, 60.0), comment="detector"),
+    ]
+    lenses = [
+        SurfaceSpec(ffi.CONIC, ffi.LENS, params=(1 / 100.0, -0.5, 0), size=(12.0, 0.0),
+                    distance=(0.0, 0.0, 50.0), n1=1.0, n2=1.5, comment="conic front, scalar indices"),
+        SurfaceSpec(ffi.CONIC, ffi.LENS, params=(-1 / 200.0, 0.0, 3, 0.0, 2e-7, -1e-10), size=(12.0, 0.0),
+                    distance=(0.0, 0.0, 8.0), n1=1.5, n2=g, comment="asphere, tabulated glass after"),
+        SurfaceSpec(ffi.CONIC, ffi.LENS, params=(0.0, 0.0, 2, 1e-4, -3e-8), size=(12.0, 0.0),
+                    distance=(0.0, 0.0, 6.0), n1=g, n2=1.0, comment="polynomial-only surface"),
+        SurfaceSpec(ffi.PLANE, ffi.LENS, size=(30.0, 0.0), distance=(0.0, 0.0, 20.0), n1=1.0, n2=g,
+                    comment="plane window front"),
+        SurfaceSpec(ffi.PLANE, ffi.LENS, size=(30.0, 0.0), distance=(0.0, 0.0, 5.0), angles=(0.0, 41.0, 0.0),
+                    n1=g, n2=1.0, comment="tilted window back (total internal reflection for part)"),
+        SurfaceSpec(ffi.PLANE, ffi.DETECTOR, shape=ffi.RECTANGLE, size=(60.0, 60.0),
+                    distance=(0.0, -34.79, 19.74), angles=(0.0, -60.4, 0.0), comment="detector"),
+    ]
+    gratings = [
+        SurfaceSpec(ffi.PLANE, ffi.GRATING, size=(30.0, 0.0), distance=(0.0, 0.0, 30.0),
+                    grating_type=ffi.TRANSPARENT, order=1, gr_const=2.0, n1=1.0, n2=g,
+                    comment="transmission grating into glass"),
+        SurfaceSpec(ffi.PLANE, ffi.LENS, size=(30.0, 0.0), distance=(0.0, 0.0, 5.0), n1=g, n2=1.0,
+                    comment="glass back"),
+        SurfaceSpec(ffi.CONIC, ffi.GRATING, params=(-1 / 400.0, 0.0, 0), size=(40.0, 0.0),
+                    distance=(0.0, 0.0, 50.0), angles=(8.0, 0.0, 0.0), order=-1, gr_const=3.0,
+                    comment="concave reflective grating"),
+        SurfaceSpec(ffi.AUX_CLASS, ffi.AUX_TYPE, distance=(0.0, 0.0, -40.0), angles=(180.0, 0.0, 0.0)),
+        SurfaceSpec(ffi.CONIC, ffi.GRATING, params=(1 / 300.0, 0.0, 0), size=(40.0, 0.0),
+                    distance=(0.0, 0.0, 0.0), grating_type=ffi.TRANSPARENT, order=1, gr_const=4.0,
+                    n1=1.0, n2=1.0, comment="convex transmission grating"),
+        SurfaceSpec(ffi.TORIC, ffi.GRATING, params=(-1 / 600.0, 0.0, 0, -1 / 500.0), size=(50.0, 0.0),
+                    distance=(0.0, 0.0, 40.0), angles=(2.0, 0.0, 0.0), order=1, gr_const=5.0,
+                    comment="toric reflective grating"),
+        SurfaceSpec(ffi.AUX_CLASS, ffi.AUX_TYPE, distance=(0.0, 0.0, -30.0), angles=(180.0, 0.0, 0.0)),
+        SurfaceSpec(ffi.TORIC, ffi.GRATING, params=(1 / 700.0, 0.0, 0, 1 / 650.0), size=(60.0, 0.0),
+                    distance=(0.0, 0.0, 0.0), grating_type=ffi.TRANSPARENT, order=1, gr_const=6.0,
+                    n1=1.0, n2=1.0, comment="toric transmission grating"),
+        SurfaceSpec(ffi.PLANE, ffi.GRATING, size=(80.0, 0.0), distance=(0.0, 0.0, 30.0), order=2,
+                    gr_const=1.3, comment="plane reflective grating, order 2 evanescent for red"),
+        SurfaceSpec(ffi.PLANE, ffi.DETECTOR, shape=ffi.RECTANGLE, size=(80.0, 80.0),
+                    distance=(-20.850663, 0.0, -21.569651), angles=(-135.971022, 0.0, 0.0), comment="detector"),
+    ]
+    return {"mirrors": mirrors, "lenses": lenses, "gratings": gratings}
