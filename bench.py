@@ -1,0 +1,322 @@
+#!/usr/bin/env python3
+"""Benchmark: ray-surfaces/s of the cross-dispersed echelle (1e8 rays) on B200.
+
+Workload (one step): the C1 scheme -- off-axis parabola, echelle (orders
+30..60, one beam per order), cross-disperser, toric fold, two-surface
+even-asphere lens, CCD 4096^2 -- traced for 31 x 64 x 50,404 = 1.0e8 rays
+resident in HBM (5.7 GB of input, far larger than the 126 MB L2), with the
+CCD frame counts accumulated.  A ray-surface is one ray through one non-Aux
+surface; lost rays count up to the surface that loses them.
+
+Engines timed: the plain FP64 per-surface engine (one kernel per surface),
+the fused FP64 kernel and the fused mixed-precision kernel (the headline
+`value`).  `e2e` runs the same trace through rtb_trace_host on page-locked
+host arrays (copies in and out inside the timed region).  `cpu_baseline` is
+the CPU oracle on the host cores over a bounded sample of the same rays.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "ray·surfaces/s on 1 B200, fused mixed vs plain FP64 at ≤0.05µm CCD error"
+UNIT = "ray·surfaces/s"
+WORKLOAD = ("C1 cross-dispersed echelle: 1.0e8 rays (31 echelle orders 30..60 x 64 wavelengths 0.38-0.90 um "
+            "x 50404 rays, disk r=25 mm), OAP + echelle + cross-disperser + toric fold + 2 even-asphere lens "
+            "surfaces + CCD 4096^2, frame counts accumulated")
+FIXES = 3  # RTB_FIX_TORIC_SIGN | RTB_FIX_TORIC_STEP (the toric fold's Steffensen 0/0)
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--rays-per-lambda", type=int, default=0, help="override (default: 1e8 rays total)")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--engines", default="per_surface,fused_fp64,fused_mixed")
+    return p.parse_args()
+
+
+def dist_init(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+class Clocks:
+    """Samples SM clocks and throttle reasons with nvidia-smi during a region."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.f = None
+
+    def __enter__(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None or self.f is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.strip().split(",") for r in self.f.read().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[0]))
+                mx.append(float(r[1]))
+                for nm, v in zip(names, r[4:8]):
+                    if v.strip().lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(specs_fn, beams_all, budget_s=6.0):
+    """CPU oracle on all host threads over a bounded sample: the first m rays
+    of every beam, m sized for ~budget_s seconds."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as O
+    from rt_b200 import schemes as S
+    lib = O.load()
+    threads = lib.oracle_num_threads()
+    cs = S.to_c(specs_fn(), O.spline_init)
+
+    def run(m):
+        beams, first = [], 0
+        for b in beams_all:
+            nb = S.make_beam(first, 1, 1, 1.0, (0.5, 0.5), 0)
+            nb.first_ray, nb.n_rays = first, min(m, int(b.n_rays))
+            for i in range(b.n_orders):
+                nb.orders[i] = b.orders[i]
+            nb.n_orders = b.n_orders
+            nb.disk[:] = b.disk[:]
+            nb.range[:] = b.range[:]
+            nb.n_lambda = b.n_lambda
+            nb.seed = b.seed
+            beams.append(nb)
+            first += nb.n_rays
+        rays = O.generate(beams, first)
+        t0 = time.perf_counter()
+        st, stats, _ = O.trace(cs.surfaces, beams, rays, fixes=FIXES)
+        dt = time.perf_counter() - t0
+        return first, stats.ray_surfaces, dt
+
+    n, rs, dt = run(2000)
+    rate = rs / dt
+    m = int(min(max(2000, budget_s * rate / (len(beams_all) * 5.3)), int(beams_all[0].n_rays)))
+    n, rs, dt = run(m)
+    return {"value": rs / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"first {m} rays of each of the {len(beams_all)} order beams ({n} rays, {rs} ray-surfaces), "
+                      f"CPU oracle (C++, OpenMP, FP64), {dt:.2f} s"}
+
+
+def reference_arm(args):
+    world, rank, _ = dist_init(args)
+    if rank != 0:
+        return
+    from rt_b200 import schemes as S
+    beams = S.c1_beams()
+    res = cpu_baseline(S.echelle, beams, budget_s=max(2.0, 0.5 * args.steps))
+    line = {"impl": "reference", "metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "engine": "CPU oracle (restatement of cuda_engine math; the reference's "
+                       "CPU engine simd_engine is a non-functional stub)"},
+            "cpu_baseline": res,
+            "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return reference_arm(args)
+    import torch
+    world, rank, local = dist_init(args)
+    torch.cuda.set_device(local)
+    from rt_b200 import engine as E
+    from rt_b200 import ffi, schemes as S
+
+    npl = args.rays_per_lambda or S.c1_rays_per_lambda()
+    beams = S.c1_beams(n_per_lambda=npl, seed=S.SEED + 7919 * rank)
+    n = S.total_rays(beams)
+    cs = S.to_c(S.echelle(), E.spline_init)
+    surf = cs.surfaces
+    rays_in = E.generate(beams, n)
+    out = E.DeviceRays(n)
+    ccd = S.ccd(S.C1_CCD)
+    counts = torch.zeros(int(ccd.xdim) * int(ccd.ydim), dtype=torch.int32, device="cuda")
+    outside = torch.zeros(1, dtype=torch.int64, device="cuda")
+    import ctypes as C
+    L = E.lib()
+    L.rtb_trace_out.argtypes = [C.POINTER(ffi.Surface), C.c_size_t, C.POINTER(ffi.Beam), C.c_size_t,
+                                C.POINTER(ffi.TraceOpts), C.POINTER(ffi.Rays), C.POINTER(ffi.Rays),
+                                C.POINTER(ffi.TraceStats), C.c_void_p]
+    s_arr = (ffi.Surface * len(surf))(*surf)
+    b_arr = (ffi.Beam * len(beams))(*beams)
+    rin, rout = rays_in.struct(), out.struct()
+    stream = torch.cuda.current_stream()
+
+    def step(o):
+        stats = ffi.TraceStats()
+        st = L.rtb_trace_out(s_arr, len(surf), b_arr, len(beams), C.byref(o), C.byref(rin), C.byref(rout),
+                             C.byref(stats), C.c_void_p(stream.cuda_stream))
+        ffi.check(st, "rtb_trace_out")
+        return stats
+
+    def timed(o, K, W):
+        for _ in range(W):
+            stats = step(o)
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(K):
+            stats = step(o)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        if world > 1:
+            t = torch.tensor([ms], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms / K, stats
+
+    engines = {}
+    mk = lambda eng, prec: E.opts(engine=eng, precision=prec, fixes=FIXES, state_out=0, ccd=ccd, counts=counts,
+                                  n_outside=outside)
+    plan = [("per_surface", ffi.ENGINE_PER_SURFACE, ffi.FP64), ("fused_fp64", ffi.ENGINE_FUSED, ffi.FP64),
+            ("fused_mixed", ffi.ENGINE_FUSED, ffi.MIXED)]
+    want = set(args.engines.split(","))
+    head = None
+    clocks = None
+    for name, eng, prec in plan:
+        if name not in want:
+            continue
+        o = mk(eng, prec)
+        try:
+            step(o)
+        except RuntimeError as e:
+            engines[name] = {"error": str(e)}
+            continue
+        if name == "fused_mixed" or (head is None and name == "fused_fp64"):
+            with Clocks(local) as ck:
+                ms, stats = timed(o, args.steps, args.warmup)
+            clocks = ck.summary()
+        else:
+            ms, stats = timed(o, max(2, args.steps // 2), 1)
+        rate = stats.ray_surfaces * world / (ms * 1e-3)
+        engines[name] = {"ms_per_step": ms, "value": rate, "ray_surfaces_per_step": stats.ray_surfaces,
+                         "n_good": stats.n_good}
+        if name in ("fused_mixed", "fused_fp64"):
+            head = name if (head is None or name == "fused_mixed") else head
+    if head is None:
+        raise SystemExit("no engine ran")
+    hv = engines[head]
+
+    # roofline of the headline kernel (HBM view): algorithmic bytes per launch
+    # = 57 B read (X,Y,Z,cX,cY,cZ,lambda,flag) + 18 B written (X,Y,flag,
+    # lost_stage) per ray + 4 B per ray counted on the frame.
+    alg_bytes = n * (57 + 18) + hv["n_good"] * 4
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = alg_bytes / (hv["ms_per_step"] * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": None, "kernel": "k_fused_mixed" if head == "fused_mixed" else "k_fused_fp64",
+                "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
+
+    e2e = None
+    if not args.no_e2e and rank == 0:
+        h = E.PinnedRays(n)
+        src_cpu = {f: getattr(rays_in, f).cpu().numpy() for f in E.FIELDS}
+        o = mk(ffi.ENGINE_FUSED, ffi.MIXED if head == "fused_mixed" else ffi.FP64)
+        times = []
+        for it in range(2 + max(1, args.steps // 3)):
+            for f in E.FIELDS:
+                np.copyto(getattr(h, f), src_cpu[f])
+            h.flag[:] = 1
+            t0 = time.perf_counter()
+            st, stats = E.trace_host(surf, beams, h, o)
+            times.append(time.perf_counter() - t0)
+            ffi.check(st, "rtb_trace_host")
+        t = float(np.median(times[2:]))
+        e2e = {"value": stats.ray_surfaces / t, "unit": UNIT, "h2d_bytes_per_step": n * 57,
+               "d2h_bytes_per_step": n * 18, "seconds_per_step": t,
+               "how": "rtb_trace_host on page-locked host arrays, wall clock, median of steps"}
+        h.free()
+
+    cpu = None
+    if not args.no_cpu and rank == 0:
+        cpu = cpu_baseline(S.echelle, beams)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": hv["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": hv["ms_per_step"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if head == "fused_mixed" else "f64",
+                "data": "synthetic",
+                "config": {"workload": WORKLOAD, "n_rays": n, "engine": head, "beams": len(beams),
+                           "l2": "inputs (5.7 GB) larger than L2", "toric_fixes": FIXES},
+                "engines": engines,
+                "speedup_vs_plain_fp64": (hv["value"] / engines["per_surface"]["value"])
+                if "per_surface" in engines and "value" in engines["per_surface"] else None,
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+                "gpu_launches": args.steps * 1}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -25,6 +25,12 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#if defined(__GNUC__)
+#define RTB_API __attribute__((visibility("default")))
+#else
+#define RTB_API
+#endif
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -117,6 +123,14 @@ typedef struct rtb_rays {
     size_t n;
 } rtb_rays;
 
+/* CCD geometry (ccd/ccd_frame.cpp:46-68): light-sensitive area in mm, pixel
+ * counts, pixel size in mm. */
+typedef struct rtb_ccd {
+    double xsize, ysize;
+    uint64_t xdim, ydim;
+    double xpix, ypix;
+} rtb_ccd;
+
 typedef struct rtb_trace_opts {
     int32_t engine;                 /* RTB_ENGINE_PER_SURFACE / RTB_ENGINE_FUSED */
     int32_t precision;              /* RTB_FP64 / RTB_MIXED */
@@ -126,6 +140,9 @@ typedef struct rtb_trace_opts {
     int32_t rays_per_thread;        /* 0: tuned default */
     int32_t state_out;              /* fused: 1 writes X..cZ back, 0 writes only the CCD-plane X,Y */
     int32_t reserved;
+    const rtb_ccd* ccd;             /* optional: add good rays to frame counts (see rtb_ccd_frame) */
+    uint32_t* counts;               /* device, ccd->xdim*ccd->ydim pixels; not cleared */
+    uint64_t* n_outside;            /* device, may be NULL */
 } rtb_trace_opts;
 
 /* Per-call statistics of a trace. */
@@ -136,13 +153,6 @@ typedef struct rtb_trace_stats {
     int32_t failed_stage;           /* that stage, -1 if none */
 } rtb_trace_stats;
 
-/* CCD geometry (ccd/ccd_frame.cpp:46-68): light-sensitive area in mm, pixel
- * counts, pixel size in mm. */
-typedef struct rtb_ccd {
-    double xsize, ysize;
-    uint64_t xdim, ydim;
-    double xpix, ypix;
-} rtb_ccd;
 
 /* =========================================================================
  * 1. Drop-in calls: rt_engine_func.h, host arrays, synchronous.
@@ -150,95 +160,99 @@ typedef struct rtb_ccd {
 
 /* rt_engine_init (rt_engine_func.h:25): selects device 0, creates the stream
  * and the device arena.  Idempotent. */
-int rtb_init(void);
+RTB_API int rtb_init(void);
 
 /* rt_engine_info (rt_engine_func.h:26): newline-separated info lines into buf. */
-int rtb_info(char* buf, size_t buflen);
+RTB_API int rtb_info(char* buf, size_t buflen);
 
 /* beam_random (rt_engine_func.h:30-31): uniform disk, params = [N, R_in, R_out],
  * center = [x, y, z].  Positions come from Philox4x32-10 keyed by `seed`, ray
  * `first_ray + i`, in place of the reference's clock-seeded cuRAND. */
-int rtb_beam_random(int shape, const double* params, const double* center, size_t n,
+RTB_API int rtb_beam_random(int shape, const double* params, const double* center, size_t n,
                     double* X, double* Y, double* Z, uint64_t seed, uint64_t first_ray);
 
 /* beam_conic_cosins (rt_engine_func.h:33); conic_angle in radians. */
-int rtb_beam_conic_cosins(size_t n, double conic_angle, const double* X, const double* Y,
+RTB_API int rtb_beam_conic_cosins(size_t n, double conic_angle, const double* X, const double* Y,
                           double* cX, double* cY, double* cZ);
 
 /* beam_gauss_cosins (rt_engine_func.h:35); fwhm in arcsec. */
-int rtb_beam_gauss_cosins(size_t n, double fwhm, double* cX, double* cY, double* cZ, uint64_t seed);
+RTB_API int rtb_beam_gauss_cosins(size_t n, double fwhm, double* cX, double* cY, double* cZ, uint64_t seed);
 
 /* uniform_range_beam (rt_engine_func.h:37). */
-int rtb_uniform_range_beam(size_t n, const double* range, double* lambda);
+RTB_API int rtb_uniform_range_beam(size_t n, const double* range, double* lambda);
 
 /* random_range_beam (rt_engine_func.h:39). */
-int rtb_random_range_beam(size_t n, const double* range, double* lambda, uint64_t seed);
+RTB_API int rtb_random_range_beam(size_t n, const double* range, double* lambda, uint64_t seed);
 
 /* beam_transform (rt_engine_func.h:41-42); angles in radians. */
-int rtb_beam_transform(size_t n, const double* angles, const double* dist,
+RTB_API int rtb_beam_transform(size_t n, const double* angles, const double* dist,
                        double* X, double* Y, double* Z, double* cX, double* cY, double* cZ);
 
 /* surface_intersection (rt_engine_func.h:46-49).  *n_bad is incremented. */
-int rtb_surface_intersection(int cls, const double* params, size_t n,
+RTB_API int rtb_surface_intersection(int cls, const double* params, size_t n,
                              double* X, double* Y, double* Z, double* cX, double* cY, double* cZ,
                              size_t* n_bad, char* flag);
+/* surface_intersection with quirk fixes (RTB_FIX_* bits); no reference counterpart. */
+RTB_API int rtb_surface_intersection_fix(int cls, const double* params, size_t n, double* X, double* Y, double* Z,
+                                         double* cX, double* cY, double* cZ, size_t* n_bad, char* flag,
+                                         uint32_t fixes);
 
 /* surface_reflection (rt_engine_func.h:52-54). */
-int rtb_surface_reflection(int cls, const double* params, size_t n,
+RTB_API int rtb_surface_reflection(int cls, const double* params, size_t n,
                            double* X, double* Y, double* Z, double* cX, double* cY, double* cZ);
 
 /* surface_refraction (rt_engine_func.h:57-61). */
-int rtb_surface_refraction(int cls, const double* params, size_t n,
+RTB_API int rtb_surface_refraction(int cls, const double* params, size_t n,
                            double* X, double* Y, double* Z, double* cX, double* cY, double* cZ,
                            const double* lambda, const rtb_table* n1, const rtb_table* n2,
                            size_t* n_bad, char* flag);
 
 /* surface_diffration (rt_engine_func.h:64-70). */
-int rtb_surface_diffration(int cls, int gr_type, const double* params, long diff_order,
+RTB_API int rtb_surface_diffration(int cls, int gr_type, const double* params, long diff_order,
                            double gr_constant, size_t n,
                            double* X, double* Y, double* Z, double* cX, double* cY, double* cZ,
                            const double* lambda, const rtb_table* n1, const rtb_table* n2,
                            size_t* n_bad, char* flag);
 
 /* surface_QE (rt_engine_func.h:73): spec[i] *= QE(lambda[i]). */
-int rtb_surface_QE(size_t n, const double* lambda, double* spec, const rtb_table* qe);
+RTB_API int rtb_surface_QE(size_t n, const double* lambda, double* spec, const rtb_table* qe);
 
 /* grating_energy_distr (rt_engine_func.h:75-78); angles in radians. */
-int rtb_grating_energy_distr(size_t n, const double* lambda, long order, double blaze_angle,
+RTB_API int rtb_grating_energy_distr(size_t n, const double* lambda, long order, double blaze_angle,
                              double alpha, double gamma, double gr_const, double rule_start,
                              double rule_stop, double* energy_distr);
 
 /* rt_engine_free_vector / rt_engine_alocate_vector (rt_engine_func.h:84-86):
  * page-locked host vectors, so the drop-in copies run at full PCIe rate. */
-void rtb_free_vector(double* data);
-double* rtb_alocate_vector(size_t n_elem);
+RTB_API void rtb_free_vector(double* data);
+RTB_API double* rtb_alocate_vector(size_t n_elem);
 
 /* spline_init (rt_engine_func.h:91): natural cubic spline second derivatives. */
-int rtb_spline_init(size_t n, const double* x, const double* y, double* y2);
+RTB_API int rtb_spline_init(size_t n, const double* x, const double* y, double* y2);
 
 /* ccd_coordinates (rt_engine_func.h:96-99). */
-int rtb_ccd_coordinates(size_t n, const double* X, const double* Y, double ccd_xsize,
+RTB_API int rtb_ccd_coordinates(size_t n, const double* X, const double* Y, double ccd_xsize,
                         double ccd_ysize, double ccd_xpix, double ccd_ypix,
                         unsigned int* ccd_X, unsigned int* ccd_Y);
 
 /* compute_ccd_image (rt_engine_func.h:101-104): image += spec(l)*l/hc*QE(l)*pix_area
  * per ray; rays whose pixel lies outside xdim x ydim are skipped and counted
  * in *n_outside (may be NULL). */
-int rtb_compute_ccd_image(size_t n, const unsigned int* ccd_X, const unsigned int* ccd_Y,
+RTB_API int rtb_compute_ccd_image(size_t n, const unsigned int* ccd_X, const unsigned int* ccd_Y,
                           const double* lambda, const rtb_table* qe, const rtb_table* spec,
                           size_t xdim, size_t ydim, double xpix, double ypix, double* image,
                           uint64_t* n_outside);
 
 /* Host loops of Beam and Surface run on the device.
  * Beam::Normalize (beam.cpp:527-571). */
-int rtb_normalize(size_t n, double* cX, double* cY, double* cZ);
+RTB_API int rtb_normalize(size_t n, double* cX, double* cY, double* cZ);
 /* Surface::ApplyConstrains / Shade::ApplyConstrains (surface.cpp:264-321,652-699);
  * shade != 0 selects the inverted test.  *n_bad is incremented. */
-int rtb_apply_constrains(int shade, int shape, const double* size, const double* center, size_t n,
+RTB_API int rtb_apply_constrains(int shade, int shape, const double* size, const double* center, size_t n,
                          const double* X, const double* Y, char* flag, size_t* n_bad);
 /* Beam::Rearrange (beam.cpp:574-598) over the good prefix [0, *n_good) of the
  * seven arrays; *n_good is updated. */
-int rtb_rearrange(size_t* n_good, double* X, double* Y, double* Z, double* cX, double* cY,
+RTB_API int rtb_rearrange(size_t* n_good, double* X, double* Y, double* Z, double* cX, double* cY,
                   double* cZ, double* lambda, char* flag);
 
 /* =========================================================================
@@ -249,31 +263,38 @@ int rtb_rearrange(size_t* n_good, double* X, double* Y, double* Z, double* cX, d
 /* Fill rays[first_ray, first_ray+n_rays) of every beam: uniform disk positions
  * (Philox4x32-10), parallel cosines turned by the field angles, composite
  * uniform wavelengths, flag 1, lost_stage RTB_NOT_LOST. */
-int rtb_generate_beams(const rtb_beam* beams, size_t n_beams, const rtb_rays* rays, void* stream);
+RTB_API int rtb_generate_beams(const rtb_beam* beams, size_t n_beams, const rtb_rays* rays, void* stream);
 
 /* Trace every beam through the scheme, in place (Scheme::run's per-surface
  * loop, scheme.cpp:983-1055).  Rays keep their index; lost rays carry
  * flag 0 and lost_stage.  stats may be NULL. */
-int rtb_trace(const rtb_surface* surfaces, size_t n_surfaces, const rtb_beam* beams, size_t n_beams,
+RTB_API int rtb_trace(const rtb_surface* surfaces, size_t n_surfaces, const rtb_beam* beams, size_t n_beams,
               const rtb_trace_opts* opts, const rtb_rays* rays, rtb_trace_stats* stats, void* stream);
+
+/* rtb_trace reading `in` and writing `out` (in may equal out).  `in` keeps
+ * its contents; out->lambda is not written.  With opts->state_out == 0 only
+ * X, Y, flag and lost_stage of `out` are written. */
+RTB_API int rtb_trace_out(const rtb_surface* surfaces, size_t n_surfaces, const rtb_beam* beams, size_t n_beams,
+                          const rtb_trace_opts* opts, const rtb_rays* in, const rtb_rays* out,
+                          rtb_trace_stats* stats, void* stream);
 
 /* rtb_trace on host arrays: copies in, traces and copies out, overlapping the
  * copies of one chunk with the trace of another.  Synchronous. */
-int rtb_trace_host(const rtb_surface* surfaces, size_t n_surfaces, const rtb_beam* beams,
+RTB_API int rtb_trace_host(const rtb_surface* surfaces, size_t n_surfaces, const rtb_beam* beams,
                    size_t n_beams, const rtb_trace_opts* opts, const rtb_rays* host_rays,
                    rtb_trace_stats* stats);
 
 /* Frame counts: counts[iy*xdim + ix] += 1 for every good ray whose pixel
  * (ccd_coordinates, ccd.cu:30-45) lies on the CCD; *n_outside (device, may be
  * NULL) counts the good rays that do not.  counts is not cleared. */
-int rtb_ccd_frame(const rtb_rays* rays, const rtb_ccd* ccd, uint32_t* counts, uint64_t* n_outside,
+RTB_API int rtb_ccd_frame(const rtb_rays* rays, const rtb_ccd* ccd, uint32_t* counts, uint64_t* n_outside,
                   void* stream);
 
 /* Order of the rays as the reference's Rearrange calls leave them
  * (beam.cpp:574-598), from lost_stage: order[k] is the index of the ray at
  * position k of the reference's arrays for beam b; positions [0, n_good) are
  * the good rays.  order is device memory of rays->n entries. */
-int rtb_reference_order(const rtb_beam* beams, size_t n_beams, size_t n_stages, const rtb_rays* rays,
+RTB_API int rtb_reference_order(const rtb_beam* beams, size_t n_beams, size_t n_stages, const rtb_rays* rays,
                         uint32_t* order, void* stream);
 
 #ifdef __cplusplus

@@ -1,0 +1,89 @@
+// common.cuh -- device-side definitions shared by the engine's kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/rtb.h"
+
+namespace rtb {
+
+// Constants of the reference (common-lib/num_defs.h:20,31;
+// cuda_engine/rt_cuda_engine_beam.cu:41; rt_cuda_engine_ccd.cu:19;
+// rt_cuda_engine_surface.cu:667-668).
+constexpr double K_RT_PI = 3.14159265359;
+constexpr double K_DEG2RAD = K_RT_PI / 180.0;   // value of `deg2rad` after *= or /=
+constexpr double K_PI2 = 6.28318531;
+constexpr double K_HC = 1.98644560233e-12;
+constexpr double K_ITER_EPS = 1.0e-7;
+constexpr unsigned K_ITER_MAX = 100000;
+
+// Intersection algorithm of a surface, as engine_intersection_cycle picks it
+// (rt_cuda_engine_surface.cu:593-636).
+enum IsectKind : int32_t { IS_NONE = 0, IS_PLANE, IS_PARABOLOID, IS_CONIC, IS_ITER_POLY, IS_ITER_CONIC, IS_TORIC };
+
+// Error bits a kernel raises for the host (the reference throws instead).
+enum DevError : uint32_t { DEV_ERR_OUT_OF_RANGE = 1u, DEV_ERR_BAD_VALUE = 2u };
+
+// One surface as the kernels consume it: everything the reference's host
+// code derives before a kernel launch (copy_surf_params, the transform's
+// sin/cos, grating/lens constants) is precomputed on the host.
+struct DevSurface {
+    int32_t cls, type, shape, gr_type;
+    int32_t kind;           // IsectKind
+    int32_t grating_index;  // -1 unless a grating
+    int32_t non_aux;
+    int32_t renorm_after;   // Normalize calls that follow this surface's action
+    int32_t surfaces_upto;  // non-Aux surfaces up to and including this one
+    int32_t n_poly;
+    int32_t translate;
+    int32_t rot_mask;       // bit i: rotation i (about y, x, z) applies
+    int64_t order;
+    double gr_const;
+    double c, k1, cR;
+    double poly[RTB_MAX_POLY];
+    double dist[3];
+    double sinA[3], cosA[3];
+    double size[2], center[2];
+    int32_t n1_off, n1_n, n2_off, n2_n;  // tables: offset/count into the knot buffer (count 1 = single value)
+};
+
+// Scheme passed by value as a kernel parameter (lands in the constant bank;
+// CUDA 12.1+ allows 32 KB of parameters).
+struct DevScheme {
+    int32_t n_surfaces;
+    int32_t n_knots;        // doubles per array in the knot buffer
+    uint32_t fixes;
+    int32_t renorm_lost;
+    DevSurface s[RTB_MAX_SURFACES];
+};
+
+// Beam table on the device (first ray and orders of each beam).
+struct DevBeam {
+    uint64_t first_ray;
+    uint64_t n_rays;
+    int64_t orders[RTB_MAX_GRATINGS];
+    int32_t n_orders;
+    int32_t pad;
+};
+
+struct DevRays {
+    double *X, *Y, *Z, *cX, *cY, *cZ, *lambda;
+    char* flag;
+    uint8_t* lost_stage;
+    uint64_t n;
+};
+
+}  // namespace rtb
+
+#define RTB_CUDA_TRY(expr)                              \
+    do {                                                \
+        cudaError_t _e = (expr);                        \
+        if (_e != cudaSuccess) return rtb::cuda_status(_e); \
+    } while (0)
+
+namespace rtb {
+inline int cuda_status(cudaError_t e) {
+    return (e == cudaErrorMemoryAllocation) ? RTB_BAD_ALLOC : RTB_FAILED;
+}
+}  // namespace rtb

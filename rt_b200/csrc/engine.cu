@@ -1,0 +1,682 @@
+// engine.cu -- C ABI: engine state, scheme preparation and the drop-in calls
+// of common-lib/rt_engine_func.h (host arrays in and out, synchronous).
+//
+// Each drop-in call copies the arrays it reads to the device, runs one
+// kernel and copies back what the reference's call returns; the copies and
+// the kernel are ordered on the library stream, the temporaries come from the
+// stream-ordered pool (no cudaMalloc/cudaFree per call as in
+// rt_cuda_engine_common.cu:72-155).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "engine.cuh"
+
+namespace rtb {
+
+Engine& engine() {
+    static Engine e;
+    return e;
+}
+
+int ensure_init() {
+    Engine& e = engine();
+    if (e.inited) return RTB_OK;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return RTB_INIT_FAILED;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return RTB_INIT_FAILED;
+    if (prop.major < 10) return RTB_INIT_FAILED;  // built for sm_100a only
+    e.device = dev;
+    e.sm_count = prop.multiProcessorCount;
+    e.max_smem_optin = (int)prop.sharedMemPerBlockOptin;
+    if (cudaStreamCreateWithFlags(&e.stream, cudaStreamNonBlocking) != cudaSuccess) return RTB_INIT_FAILED;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t keep = ~0ull;  // keep freed blocks for reuse instead of returning them to the driver
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    e.inited = true;
+    return RTB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Scheme preparation
+
+double scheme_angle_rad(double deg) {
+    double rad = deg * K_DEG2RAD;   // Surface::SetAngles (surface.cpp:201)
+    double back = rad / K_DEG2RAD;  // Surface::GetAngles (surface.cpp:227)
+    return back * K_DEG2RAD;        // Beam::Transform (beam.cpp:609-611)
+}
+
+// Translation and the rotations' host sin/cos (rt_cuda_engine_beam.cu:431-533).
+void transform_constants(const double ang[3], const double dist[3], DevSurface& s) {
+    for (int i = 0; i < 3; ++i) s.dist[i] = dist[i];
+    s.translate = (dist[2] != 0.0) || (dist[0] != 0.0) || (dist[1] != 0.0);
+    s.rot_mask = 0;
+    for (int i = 0; i < 3; ++i) {
+        if (ang[i] != 0) {
+            s.rot_mask |= 1 << i;
+            s.sinA[i] = std::sin(ang[i]);
+            s.cosA[i] = std::cos(ang[i]);
+        } else {
+            s.sinA[i] = 0.0;
+            s.cosA[i] = 1.0;
+        }
+    }
+}
+
+// copy_surf_params (rt_cuda_engine_surface.cu:108-148) and the dispatch of
+// engine_intersection_cycle (surface.cu:593-636).
+int surface_from_params(int cls, const double* params, DevSurface& s) {
+    std::memset(&s, 0, sizeof(s));
+    s.cls = cls;
+    s.grating_index = -1;
+    if (cls == RTB_AUX_CLASS) {
+        s.kind = IS_NONE;
+        s.k1 = 1.0;
+        return RTB_OK;
+    }
+    if (cls != RTB_PLANE && cls != RTB_CONIC && cls != RTB_TORIC) return RTB_BAD_VALUE;
+    if (!params) return RTB_BAD_VALUE;
+    s.c = params[0];
+    s.k1 = params[1] + 1;
+    double nn = params[2];
+    if (!(nn >= 0) || nn > RTB_MAX_POLY) return RTB_BAD_VALUE;
+    s.n_poly = (int)(size_t)nn;
+    for (int i = 0; i < s.n_poly; ++i) s.poly[i] = params[3 + i];
+    s.cR = (cls == RTB_TORIC) ? params[3 + s.n_poly] : 0.0;
+    if (cls == RTB_PLANE) {
+        s.kind = IS_PLANE;
+    } else if (cls == RTB_CONIC) {
+        size_t NN = (size_t)params[2];
+        if (NN == 0) {
+            if (params[0] == 0) s.kind = IS_PLANE;
+            else if (params[1] == -1) s.kind = IS_PARABOLOID;
+            else s.kind = IS_CONIC;
+        } else {
+            s.kind = (params[0] == 0) ? IS_ITER_POLY : IS_ITER_CONIC;
+        }
+    } else {
+        s.kind = IS_TORIC;
+    }
+    return RTB_OK;
+}
+
+// Append a table to the knot buffer: [x(n) y(n) y2(n)], or [0, y0] for a
+// single value.
+int add_table(const rtb_table* t, std::vector<double>& knots, int32_t& off, int32_t& cnt) {
+    if (!t || t->n == 0 || !t->y) return RTB_BAD_VALUE;
+    off = (int32_t)knots.size();
+    if (t->n == 1) {
+        cnt = 1;
+        knots.push_back(0.0);
+        knots.push_back(t->y[0]);
+        knots.push_back(0.0);
+        return RTB_OK;
+    }
+    if (t->n < 4 || t->n > RTB_MAX_KNOTS || !t->x || !t->y2) return RTB_BAD_VALUE;
+    cnt = (int32_t)t->n;
+    knots.insert(knots.end(), t->x, t->x + t->n);
+    knots.insert(knots.end(), t->y, t->y + t->n);
+    knots.insert(knots.end(), t->y2, t->y2 + t->n);
+    return RTB_OK;
+}
+
+int prepare_surface(const rtb_surface& in, DevSurface& s, std::vector<double>& knots) {
+    bool non_aux = in.type != RTB_AUX_TYPE;
+    int st = surface_from_params(non_aux ? in.cls : RTB_AUX_CLASS, in.params, s);
+    if (st != RTB_OK) return st;
+    s.cls = in.cls;
+    s.type = in.type;
+    s.shape = in.shape;
+    s.gr_type = in.grating_type;
+    s.non_aux = non_aux;
+    if (!non_aux) s.kind = IS_NONE;
+    s.order = in.order;
+    s.gr_const = in.gr_const;
+    if (in.type < RTB_MIRROR || in.type > RTB_AUX_TYPE) return RTB_BAD_VALUE;
+    if (in.shape != RTB_CIRCLE && in.shape != RTB_RECTANGLE) return RTB_BAD_VALUE;
+    if (in.type == RTB_GRATING && in.grating_type != RTB_REFLECTIVE && in.grating_type != RTB_TRANSPARENT)
+        return RTB_BAD_VALUE;
+    double ang[3];
+    for (int i = 0; i < 3; ++i) ang[i] = scheme_angle_rad(in.angles_deg[i]);
+    transform_constants(ang, in.distance, s);
+    for (int i = 0; i < 2; ++i) {
+        s.size[i] = in.size[i];
+        s.center[i] = in.center[i];
+    }
+    s.n1_off = s.n2_off = 0;
+    s.n1_n = s.n2_n = 1;
+    if (in.type == RTB_LENS || in.type == RTB_GRATING) {
+        st = add_table(&in.n2, knots, s.n2_off, s.n2_n);
+        if (st != RTB_OK) return st;
+        if (in.type == RTB_LENS || in.grating_type == RTB_TRANSPARENT) {
+            st = add_table(&in.n1, knots, s.n1_off, s.n1_n);
+            if (st != RTB_OK) return st;
+        }
+    }
+    return RTB_OK;
+}
+
+int prepare_scheme(const rtb_surface* surf, size_t n, uint32_t fixes, int renorm_lost, PreparedScheme& out) {
+    if (!surf || n == 0 || n > RTB_MAX_SURFACES) return RTB_BAD_VALUE;
+    std::memset(&out.sch, 0, sizeof(out.sch));
+    out.knots.clear();
+    out.knots.push_back(0.0);  // offset 0: a harmless single value for unused tables
+    out.knots.push_back(1.0);
+    out.knots.push_back(0.0);
+    int ng = 0, nonaux = 0;
+    for (size_t k = 0; k < n; ++k) {
+        DevSurface& s = out.sch.s[k];
+        int st = prepare_surface(surf[k], s, out.knots);
+        if (st != RTB_OK) return st;
+        s.grating_index = (s.type == RTB_GRATING) ? ng++ : -1;
+        if (s.non_aux) ++nonaux;
+        s.surfaces_upto = nonaux;
+    }
+    if (ng > RTB_MAX_GRATINGS) return RTB_BAD_VALUE;
+    for (size_t k = 0; k < n; ++k) {
+        int cnt = out.sch.s[k].non_aux ? 1 : 0;
+        for (size_t j = k + 1; j < n; ++j) cnt += 1 + (out.sch.s[j].non_aux ? 1 : 0);
+        out.sch.s[k].renorm_after = cnt;
+    }
+    out.sch.n_surfaces = (int32_t)n;
+    out.sch.n_knots = (int32_t)out.knots.size();
+    out.sch.fixes = fixes;
+    out.sch.renorm_lost = renorm_lost;
+    return RTB_OK;
+}
+
+// Natural cubic spline second derivatives: the sequential algorithm of
+// Numerical Recipes that rt_cuda_engine_spline.cu:43-145 intends (its
+// kernel runs the recurrence in parallel and races); 4..1024 knots run in
+// well under a microsecond on the host.
+static void spline_second_derivatives(size_t N, const double* x, const double* y, double* y2) {
+    std::vector<double> u(N, 0.0);
+    y2[0] = 0.0;
+    y2[N - 1] = 0.0;
+    for (size_t i = 1; i + 1 < N; ++i) {
+        double sig = (x[i] - x[i - 1]) / (x[i + 1] - x[i - 1]);
+        double p = sig * y2[i - 1] + 2.0;
+        y2[i] = (sig - 1.0) / p;
+        u[i] = (y[i + 1] - y[i]) / (x[i + 1] - x[i]) - (y[i] - y[i - 1]) / (x[i] - x[i - 1]);
+        u[i] = (6.0 * u[i] / (x[i + 1] - x[i - 1]) - sig * u[i - 1]) / p;
+    }
+    for (size_t k = N - 2; k > 0; --k) y2[k] = y2[k] * y2[k + 1] + u[k];
+}
+
+// ---------------------------------------------------------------------------
+// Drop-in helpers
+
+namespace {
+
+struct Lock {
+    std::lock_guard<std::mutex> g;
+    Lock() : g(engine().mu) {}
+};
+
+// Device copies of up to 8 double arrays and one flag array, from one pool
+// allocation.
+struct Staged {
+    DevBuf buf;
+    double* d[8] = {nullptr};
+    char* flag = nullptr;
+    unsigned long long* counter = nullptr;
+    unsigned* err = nullptr;
+    int init(size_t n, int n_double, bool with_flag, cudaStream_t st) {
+        size_t bytes = 64 + n_double * n * sizeof(double) + (with_flag ? n + 16 : 0);
+        int s = buf.alloc(bytes, st);
+        if (s != RTB_OK) return s;
+        char* p = buf.as<char>();
+        counter = reinterpret_cast<unsigned long long*>(p);
+        err = reinterpret_cast<unsigned*>(p + 8);
+        p += 64;
+        for (int i = 0; i < n_double; ++i) {
+            d[i] = reinterpret_cast<double*>(p);
+            p += n * sizeof(double);
+        }
+        if (with_flag) flag = p;
+        RTB_CUDA_TRY(cudaMemsetAsync(buf.p, 0, 64, st));
+        return RTB_OK;
+    }
+};
+
+int h2d(void* dst, const void* src, size_t bytes, cudaStream_t st) {
+    if (bytes == 0) return RTB_OK;
+    RTB_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
+    return RTB_OK;
+}
+
+int d2h(void* dst, const void* src, size_t bytes, cudaStream_t st) {
+    if (bytes == 0) return RTB_OK;
+    RTB_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st));
+    return RTB_OK;
+}
+
+int finish(cudaStream_t st, const unsigned* d_err, size_t* n_bad, const unsigned long long* d_counter) {
+    unsigned long long cnt = 0;
+    unsigned err = 0;
+    if (d_counter) RTB_CUDA_TRY(cudaMemcpyAsync(&cnt, d_counter, sizeof(cnt), cudaMemcpyDeviceToHost, st));
+    if (d_err) RTB_CUDA_TRY(cudaMemcpyAsync(&err, d_err, sizeof(err), cudaMemcpyDeviceToHost, st));
+    RTB_CUDA_TRY(cudaStreamSynchronize(st));
+    RTB_CUDA_TRY(cudaGetLastError());
+    if (err & DEV_ERR_OUT_OF_RANGE) return RTB_OUT_OF_RANGE;
+    if (err) return RTB_BAD_VALUE;
+    if (n_bad) *n_bad += (size_t)cnt;
+    return RTB_OK;
+}
+
+}  // namespace
+
+}  // namespace rtb
+
+using namespace rtb;
+
+extern "C" {
+
+int rtb_init(void) {
+    Lock l;
+    return ensure_init();
+}
+
+int rtb_info(char* buf, size_t buflen) {
+    Lock l;
+    int st = ensure_init();
+    if (st != RTB_OK) return st;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, engine().device) != cudaSuccess) return RTB_FAILED;
+    std::string s = "B200 ray-tracing engine (sm_100a)\n";
+    s += std::string("Device name: ") + prop.name + "\n";
+    s += "Computing ability: " + std::to_string(prop.major) + "." + std::to_string(prop.minor) + "\n";
+    s += "Global memory: " + std::to_string(prop.totalGlobalMem) + "\n";
+    s += "Number of multiprocessors: " + std::to_string(prop.multiProcessorCount) + "\n";
+    if (!buf || buflen == 0) return RTB_BAD_VALUE;
+    std::snprintf(buf, buflen, "%s", s.c_str());
+    return RTB_OK;
+}
+
+int rtb_spline_init(size_t n, const double* x, const double* y, double* y2) {
+    if (n < 4 || !x || !y || !y2) return RTB_BAD_VALUE;
+    spline_second_derivatives(n, x, y, y2);
+    return RTB_OK;
+}
+
+double* rtb_alocate_vector(size_t n_elem) {
+    void* p = nullptr;
+    if (cudaHostAlloc(&p, sizeof(double) * (n_elem ? n_elem : 1), cudaHostAllocPortable) != cudaSuccess) return nullptr;
+    return static_cast<double*>(p);
+}
+
+void rtb_free_vector(double* data) {
+    if (data) cudaFreeHost(data);
+}
+
+int rtb_beam_random(int shape, const double* params, const double* center, size_t n, double* X, double* Y, double* Z,
+                    uint64_t seed, uint64_t first_ray) {
+    if (shape != RTB_CIRCLE || !params || !center) return RTB_BAD_VALUE;
+    if (n == 0) return RTB_OK;
+    Lock l;
+    int st = ensure_init();
+    if (st != RTB_OK) return st;
+    cudaStream_t s = engine().stream;
+    Staged g;
+    if ((st = g.init(n, 3, false, s)) != RTB_OK) return st;
+    k_beam_random<<<grid_for(n, 256, 8), 256, 0, s>>>(n, params[1], params[2], center[0], center[1], center[2], seed,
+                                                        first_ray, g.d[0], g.d[1], g.d[2]);
+    double* out[3] = {X, Y, Z};
+    for (int i = 0; i < 3; ++i)
+        if ((st = d2h(out[i], g.d[i], n * sizeof(double), s)) != RTB_OK) return st;
+    return finish(s, nullptr, nullptr, nullptr);
+}
+
+// conic_cosins_kernel (rt_cuda_engine_beam.cu:586-611): cZ = cos(a/2),
+// (cX, cY) = sin(a/2) (cos, sin)(atan2(Y, X)).  Evaluated on the host: it is
+// not on the benchmark path and uses transcendental functions per ray.
+int rtb_beam_conic_cosins(size_t n, double conic_angle, const double* X, const double* Y, double* cX, double* cY,
+                          double* cZ) {
+    if (n && (!X || !Y || !cX || !cY || !cZ)) return RTB_BAD_VALUE;
+    double cc = std::cos(conic_angle / 2.0), sc = std::sin(conic_angle / 2.0);
+    for (size_t i = 0; i < n; ++i) {
+        double phi = std::atan2(Y[i], X[i]);
+        cZ[i] = cc;
+        cX[i] = sc * std::cos(phi);
+        cY[i] = sc * std::sin(phi);
+    }
+    return RTB_OK;
+}
+
+// gauss_cosins_kernel (rt_cuda_engine_beam.cu:952-991) re-derived: two
+// rotations by normal deviates of standard deviation tan(sigma), sigma the
+// FWHM in arcsec converted to radians (beam.cu:1099).  Host-side, seeded.
+int rtb_beam_gauss_cosins(size_t n, double fwhm, double* cX, double* cY, double* cZ, uint64_t seed) {
+    if (n && (!cX || !cY || !cZ)) return RTB_BAD_VALUE;
+    double stddev = fwhm / 2.35482 * K_RT_PI / 180 / 3600;
+    double tg = std::tan(stddev);
+    uint64_t state = seed * 0x9E3779B97F4A7C15ull + 1;
+    auto next_u = [&]() {
+        state ^= state >> 12;
+        state ^= state << 25;
+        state ^= state >> 27;
+        return ((state * 0x2545F4914F6CDD1Dull) >> 11) * (1.0 / 9007199254740992.0) + 1e-300;
+    };
+    for (size_t i = 0; i < n; ++i) {
+        double u1 = next_u(), u2 = next_u();
+        double rad = std::sqrt(-2.0 * std::log(u1));
+        double gx = tg * rad * std::cos(6.283185307179586 * u2);
+        double gy = tg * rad * std::sin(6.283185307179586 * u2);
+        double x = 0.0, y = 0.0, z = 1.0;
+        double cs = 1.0 / std::sqrt(1.0 + gx * gx);
+        double sn = (std::signbit(gx) ? -1.0 : 1.0) * (gx == 0 ? 0.0 : 1.0 / std::sqrt(1.0 + 1.0 / gx / gx));
+        y = -sn * z;
+        z = cs * z;
+        cs = 1.0 / std::sqrt(1.0 + gy * gy);
+        sn = (std::signbit(gy) ? -1.0 : 1.0) * (gy == 0 ? 0.0 : 1.0 / std::sqrt(1.0 + 1.0 / gy / gy));
+        x = -sn * z;
+        z = cs * z;
+        cX[i] = x;
+        cY[i] = y;
+        cZ[i] = z;
+    }
+    return RTB_OK;
+}
+
+int rtb_uniform_range_beam(size_t n, const double* range, double* lambda) {
+    if (!range || (n && !lambda)) return RTB_BAD_VALUE;
+    if (n == 0) return RTB_OK;
+    Lock l;
+    int st = ensure_init();
+    if (st != RTB_OK) return st;
+    cudaStream_t s = engine().stream;
+    double d_l = (range[1] - range[0]) / (n - 1);  // rt_cuda_engine_beam.cu:726
+    Staged g;
+    if ((st = g.init(n, 1, false, s)) != RTB_OK) return st;
+    k_uniform_range<<<grid_for(n, 256, 8), 256, 0, s>>>(n, range[0], d_l, g.d[0]);
+    if ((st = d2h(lambda, g.d[0], n * sizeof(double), s)) != RTB_OK) return st;
+    return finish(s, nullptr, nullptr, nullptr);
+}
+
+int rtb_random_range_beam(size_t n, const double* range, double* lambda, uint64_t seed) {
+    if (!range || (n && !lambda)) return RTB_BAD_VALUE;
+    if (n == 0) return RTB_OK;
+    Lock l;
+    int st = ensure_init();
+    if (st != RTB_OK) return st;
+    cudaStream_t s = engine().stream;
+    Staged g;
+    if ((st = g.init(n, 1, false, s)) != RTB_OK) return st;
+    k_random_range<<<grid_for(n, 256, 8), 256, 0, s>>>(n, range[0], range[1], seed, g.d[0]);
+    if ((st = d2h(lambda, g.d[0], n * sizeof(double), s)) != RTB_OK) return st;
+    return finish(s, nullptr, nullptr, nullptr);
+}
+
+int rtb_beam_transform(size_t n, const double* angles, const double* dist, double* X, double* Y, double* Z,
+                       double* cX, double* cY, double* cZ) {
+    if (!angles || !dist) return RTB_BAD_VALUE;
+    if (n == 0) return RTB_OK;
+    Lock l;
+    int st = ensure_init();
+    if (st != RTB_OK) return st;
+    cudaStream_t s = engine().stream;
+    DevSurface ds;
+    std::memset(&ds, 0, sizeof(ds));
+    transform_constants(angles, dist, ds);
+    Staged g;
+    if ((st = g.init(n, 6, false, s)) != RTB_OK) return st;
+    double* a[6] = {X, Y, Z, cX, cY, cZ};
+    for (int i = 0; i < 6; ++i)
+        if ((st = h2d(g.d[i], a[i], n * sizeof(double), s)) != RTB_OK) return st;
+    k_transform<<<grid_for(n, 256, 8), 256, 0, s>>>(n, ds, g.d[0], g.d[1], g.d[2], g.d[3], g.d[4], g.d[5]);
+    for (int i = 0; i < 6; ++i)
+        if ((st = d2h(a[i], g.d[i], n * sizeof(double), s)) != RTB_OK) return st;
+    return finish(s, nullptr, nullptr, nullptr);
+}
+
+static int intersection_impl(int cls, const double* params, size_t n, double* X, double* Y, double* Z, double* cX,
+                             double* cY, double* cZ, size_t* n_bad, char* flag, uint32_t fixes) {
+    if (!n_bad) return RTB_BAD_VALUE;
+    if (cls == RTB_AUX_CLASS || n == 0) return RTB_OK;  // surface.cu:634-635
+    DevSurface ds;
+    int st = surface_from_params(cls, params, ds);
+    if (st != RTB_OK) return st;
+    Lock l;
+    if ((st = ensure_init()) != RTB_OK) return st;
+    cudaStream_t s = engine().stream;
+    Staged g;
+    if ((st = g.init(n, 6, true, s)) != RTB_OK) return st;
+    double* a[6] = {X, Y, Z, cX, cY, cZ};
+    for (int i = 0; i < 6; ++i)
+        if ((st = h2d(g.d[i], a[i], n * sizeof(double), s)) != RTB_OK) return st;
+    if ((st = h2d(g.flag, flag, n, s)) != RTB_OK) return st;
+    k_intersect<<<grid_for(n, 256, 8), 256, 0, s>>>(n, ds, fixes, g.d[0], g.d[1], g.d[2], g.d[3], g.d[4], g.d[5],
+                                                      g.flag, g.counter);
+    for (int i = 0; i < 3; ++i)
+        if ((st = d2h(a[i], g.d[i], n * sizeof(double), s)) != RTB_OK) return st;
+    if ((st = d2h(flag, g.flag, n, s)) != RTB_OK) return st;
+    return finish(s, g.err, n_bad, g.counter);
+}
+
+int rtb_surface_intersection(int cls, const double* params, size_t n, double* X, double* Y, double* Z, double* cX,
+                             double* cY, double* cZ, size_t* n_bad, char* flag) {
+    return intersection_impl(cls, params, n, X, Y, Z, cX, cY, cZ, n_bad, flag, 0);
+}
+
+int rtb_surface_intersection_fix(int cls, const double* params, size_t n, double* X, double* Y, double* Z,
+                                 double* cX, double* cY, double* cZ, size_t* n_bad, char* flag, uint32_t fixes) {
+    return intersection_impl(cls, params, n, X, Y, Z, cX, cY, cZ, n_bad, flag, fixes);
+}
+
+int rtb_surface_reflection(int cls, const double* params, size_t n, double* X, double* Y, double* Z, double* cX,
+                           double* cY, double* cZ) {
+    if (n == 0) return RTB_OK;
+    DevSurface ds;
+    int st = surface_from_params(cls, params, ds);
+    if (st != RTB_OK) return st;
+    Lock l;
+    if ((st = ensure_init()) != RTB_OK) return st;
+    cudaStream_t s = engine().stream;
+    Staged g;
+    if ((st = g.init(n, 6, false, s)) != RTB_OK) return st;
+    double* a[6] = {X, Y, Z, cX, cY, cZ};
+    for (int i = 0; i < 6; ++i)
+        if ((st = h2d(g.d[i], a[i], n * sizeof(double), s)) != RTB_OK) return st;
+    k_reflect<<<grid_for(n, 256, 8), 256, 0, s>>>(n, ds, g.d[0], g.d[1], g.d[2], g.d[3], g.d[4], g.d[5]);
+    for (int i = 3; i < 6; ++i)
+        if ((st = d2h(a[i], g.d[i], n * sizeof(double), s)) != RTB_OK) return st;
+    return finish(s, nullptr, nullptr, nullptr);
+}
+
+// Refraction (type Lens) or diffraction (type Grating) over host arrays.
+static int action_impl(int type, int cls, int gr_type, const double* params, long order, double gr_const, size_t n,
+                       double* X, double* Y, double* Z, double* cX, double* cY, double* cZ, const double* lambda,
+                       const rtb_table* n1, const rtb_table* n2, size_t* n_bad, char* flag) {
+    if (!n_bad) return RTB_BAD_VALUE;
+    if (n == 0) return RTB_OK;
+    DevSurface ds;
+    int st = surface_from_params(cls, params, ds);
+    if (st != RTB_OK) return st;
+    ds.type = type;
+    ds.gr_type = gr_type;
+    ds.gr_const = gr_const;
+    std::vector<double> knots = {0.0, 1.0, 0.0};
+    if ((st = add_table(n2, knots, ds.n2_off, ds.n2_n)) != RTB_OK) return st;
+    if (type == RTB_LENS || gr_type == RTB_TRANSPARENT) {
+        if ((st = add_table(n1, knots, ds.n1_off, ds.n1_n)) != RTB_OK) return st;
+    }
+    Lock l;
+    if ((st = ensure_init()) != RTB_OK) return st;
+    cudaStream_t s = engine().stream;
+    Staged g;
+    if ((st = g.init(n, 7, true, s)) != RTB_OK) return st;
+    DevBuf kb;
+    if ((st = kb.alloc(knots.size() * sizeof(double), s)) != RTB_OK) return st;
+    if ((st = h2d(kb.p, knots.data(), knots.size() * sizeof(double), s)) != RTB_OK) return st;
+    double* a[6] = {X, Y, Z, cX, cY, cZ};
+    for (int i = 0; i < 6; ++i)
+        if ((st = h2d(g.d[i], a[i], n * sizeof(double), s)) != RTB_OK) return st;
+    if ((st = h2d(g.d[6], lambda, n * sizeof(double), s)) != RTB_OK) return st;
+    if ((st = h2d(g.flag, flag, n, s)) != RTB_OK) return st;
+    k_action<<<grid_for(n, 256, 8), 256, 0, s>>>(n, ds, kb.as<double>(), (long long)order, g.d[6], g.d[0], g.d[1],
+                                                   g.d[2], g.d[3], g.d[4], g.d[5], g.flag, g.counter, g.err);
+    for (int i = 3; i < 6; ++i)
+        if ((st = d2h(a[i], g.d[i], n * sizeof(double), s)) != RTB_OK) return st;
+    if ((st = d2h(flag, g.flag, n, s)) != RTB_OK) return st;
+    return finish(s, g.err, n_bad, g.counter);
+}
+
+int rtb_surface_refraction(int cls, const double* params, size_t n, double* X, double* Y, double* Z, double* cX,
+                           double* cY, double* cZ, const double* lambda, const rtb_table* n1, const rtb_table* n2,
+                           size_t* n_bad, char* flag) {
+    return action_impl(RTB_LENS, cls, RTB_REFLECTIVE, params, 0, 0.0, n, X, Y, Z, cX, cY, cZ, lambda, n1, n2, n_bad,
+                       flag);
+}
+
+int rtb_surface_diffration(int cls, int gr_type, const double* params, long diff_order, double gr_constant, size_t n,
+                           double* X, double* Y, double* Z, double* cX, double* cY, double* cZ, const double* lambda,
+                           const rtb_table* n1, const rtb_table* n2, size_t* n_bad, char* flag) {
+    if (gr_type != RTB_REFLECTIVE && gr_type != RTB_TRANSPARENT) return RTB_BAD_VALUE;  // surface.cu:1637,1706
+    return action_impl(RTB_GRATING, cls, gr_type, params, diff_order, gr_constant, n, X, Y, Z, cX, cY, cZ, lambda, n1,
+                       n2, n_bad, flag);
+}
+
+int rtb_surface_QE(size_t n, const double* lambda, double* spec, const rtb_table* qe) {
+    if (n == 0) return RTB_OK;
+    std::vector<double> knots;
+    int32_t off, cnt;
+    int st = add_table(qe, knots, off, cnt);
+    if (st != RTB_OK) return st;
+    Lock l;
+    if ((st = ensure_init()) != RTB_OK) return st;
+    cudaStream_t s = engine().stream;
+    Staged g;
+    if ((st = g.init(n, 2, false, s)) != RTB_OK) return st;
+    DevBuf kb;
+    if ((st = kb.alloc(knots.size() * sizeof(double), s)) != RTB_OK) return st;
+    if ((st = h2d(kb.p, knots.data(), knots.size() * sizeof(double), s)) != RTB_OK) return st;
+    if ((st = h2d(g.d[0], lambda, n * sizeof(double), s)) != RTB_OK) return st;
+    if ((st = h2d(g.d[1], spec, n * sizeof(double), s)) != RTB_OK) return st;
+    k_surface_qe<<<grid_for(n, 256, 8), 256, 0, s>>>(n, g.d[0], g.d[1], kb.as<double>(), off, cnt, g.err);
+    if ((st = d2h(spec, g.d[1], n * sizeof(double), s)) != RTB_OK) return st;
+    return finish(s, g.err, nullptr, nullptr);
+}
+
+int rtb_normalize(size_t n, double* cX, double* cY, double* cZ) {
+    if (n == 0) return RTB_OK;
+    Lock l;
+    int st = ensure_init();
+    if (st != RTB_OK) return st;
+    cudaStream_t s = engine().stream;
+    Staged g;
+    if ((st = g.init(n, 3, false, s)) != RTB_OK) return st;
+    double* a[3] = {cX, cY, cZ};
+    for (int i = 0; i < 3; ++i)
+        if ((st = h2d(g.d[i], a[i], n * sizeof(double), s)) != RTB_OK) return st;
+    k_normalize<<<grid_for(n, 256, 8), 256, 0, s>>>(n, g.d[0], g.d[1], g.d[2]);
+    for (int i = 0; i < 3; ++i)
+        if ((st = d2h(a[i], g.d[i], n * sizeof(double), s)) != RTB_OK) return st;
+    return finish(s, nullptr, nullptr, nullptr);
+}
+
+int rtb_apply_constrains(int shade, int shape, const double* size, const double* center, size_t n, const double* X,
+                         const double* Y, char* flag, size_t* n_bad) {
+    if (!size || !center || !n_bad) return RTB_BAD_VALUE;
+    if (shape != RTB_CIRCLE && shape != RTB_RECTANGLE) return RTB_BAD_VALUE;
+    if (n == 0) return RTB_OK;
+    Lock l;
+    int st = ensure_init();
+    if (st != RTB_OK) return st;
+    cudaStream_t s = engine().stream;
+    Staged g;
+    if ((st = g.init(n, 2, true, s)) != RTB_OK) return st;
+    if ((st = h2d(g.d[0], X, n * sizeof(double), s)) != RTB_OK) return st;
+    if ((st = h2d(g.d[1], Y, n * sizeof(double), s)) != RTB_OK) return st;
+    if ((st = h2d(g.flag, flag, n, s)) != RTB_OK) return st;
+    k_aperture<<<grid_for(n, 256, 8), 256, 0, s>>>(n, shade, shape, size[0], shape == RTB_RECTANGLE ? size[1] : 0.0,
+                                                     center[0], center[1], g.d[0], g.d[1], g.flag, g.counter);
+    if ((st = d2h(flag, g.flag, n, s)) != RTB_OK) return st;
+    return finish(s, nullptr, n_bad, g.counter);
+}
+
+int rtb_ccd_coordinates(size_t n, const double* X, const double* Y, double xsize, double ysize, double xpix,
+                        double ypix, unsigned int* ccd_X, unsigned int* ccd_Y) {
+    if (n == 0) return RTB_OK;
+    Lock l;
+    int st = ensure_init();
+    if (st != RTB_OK) return st;
+    cudaStream_t s = engine().stream;
+    Staged g;
+    if ((st = g.init(n, 3, false, s)) != RTB_OK) return st;
+    if ((st = h2d(g.d[0], X, n * sizeof(double), s)) != RTB_OK) return st;
+    if ((st = h2d(g.d[1], Y, n * sizeof(double), s)) != RTB_OK) return st;
+    unsigned* ix = reinterpret_cast<unsigned*>(g.d[2]);
+    unsigned* iy = ix + n;
+    k_ccd_coords<<<grid_for(n, 256, 8), 256, 0, s>>>(n, g.d[0], g.d[1], xsize, ysize, xpix, ypix, ix, iy);
+    if ((st = d2h(ccd_X, ix, n * sizeof(unsigned), s)) != RTB_OK) return st;
+    if ((st = d2h(ccd_Y, iy, n * sizeof(unsigned), s)) != RTB_OK) return st;
+    return finish(s, nullptr, nullptr, nullptr);
+}
+
+int rtb_compute_ccd_image(size_t n, const unsigned int* ccd_X, const unsigned int* ccd_Y, const double* lambda,
+                          const rtb_table* qe, const rtb_table* spec, size_t xdim, size_t ydim, double xpix,
+                          double ypix, double* image, uint64_t* n_outside) {
+    if (!image || xdim == 0 || ydim == 0) return RTB_BAD_VALUE;
+    if (xdim * ydim > 0xFFFFFFFFull) return RTB_BAD_VALUE;  // 32-bit pixel index (ccd.cu:224)
+    std::vector<double> knots;
+    int32_t qo, qn, so, sn;
+    int st = add_table(qe, knots, qo, qn);
+    if (st != RTB_OK) return st;
+    if ((st = add_table(spec, knots, so, sn)) != RTB_OK) return st;
+    Lock l;
+    if ((st = ensure_init()) != RTB_OK) return st;
+    cudaStream_t s = engine().stream;
+    size_t npix = xdim * ydim;
+    DevBuf img, kb;
+    if ((st = img.alloc(npix * sizeof(double), s)) != RTB_OK) return st;
+    if ((st = kb.alloc(knots.size() * sizeof(double), s)) != RTB_OK) return st;
+    if ((st = h2d(kb.p, knots.data(), knots.size() * sizeof(double), s)) != RTB_OK) return st;
+    if ((st = h2d(img.p, image, npix * sizeof(double), s)) != RTB_OK) return st;
+    Staged g;
+    if ((st = g.init(n ? n : 1, 2, false, s)) != RTB_OK) return st;
+    if (n) {
+        unsigned* ix = reinterpret_cast<unsigned*>(g.d[1]);
+        unsigned* iy = ix + n;
+        if ((st = h2d(g.d[0], lambda, n * sizeof(double), s)) != RTB_OK) return st;
+        if ((st = h2d(ix, ccd_X, n * sizeof(unsigned), s)) != RTB_OK) return st;
+        if ((st = h2d(iy, ccd_Y, n * sizeof(unsigned), s)) != RTB_OK) return st;
+        double pix_area = xpix * ypix * 1.0E-2;  // ccd.cu:360
+        k_ccd_image<<<grid_for(n, 256, 8), 256, 0, s>>>(n, ix, iy, g.d[0], kb.as<double>(), qo, qn, so, sn, xdim, ydim,
+                                                          pix_area, img.as<double>(), g.counter, g.err);
+    }
+    if ((st = d2h(image, img.p, npix * sizeof(double), s)) != RTB_OK) return st;
+    size_t outside = 0;
+    st = finish(s, g.err, &outside, g.counter);
+    if (st == RTB_OK && n_outside) *n_outside += outside;
+    return st;
+}
+
+}  // extern "C"
+
+namespace rtb {
+__global__ void k_grating_energy(size_t n, const double* lambda, long long order, double blaze, double alpha,
+                                 double gamma, double gr_const, double rule_start, double rule_stop, double* energy);
+}
+
+extern "C" int rtb_grating_energy_distr(size_t n, const double* lambda, long order, double blaze_angle, double alpha,
+                                        double gamma, double gr_const, double rule_start, double rule_stop,
+                                        double* energy_distr) {
+    if (n == 0) return RTB_OK;
+    if (!lambda || !energy_distr) return RTB_BAD_VALUE;
+    Lock l;
+    int st = ensure_init();
+    if (st != RTB_OK) return st;
+    cudaStream_t s = engine().stream;
+    Staged g;
+    if ((st = g.init(n, 2, false, s)) != RTB_OK) return st;
+    if ((st = h2d(g.d[0], lambda, n * sizeof(double), s)) != RTB_OK) return st;
+    if ((st = h2d(g.d[1], energy_distr, n * sizeof(double), s)) != RTB_OK) return st;
+    k_grating_energy<<<grid_for(n, 256, 8), 256, 0, s>>>(n, g.d[0], (long long)order, blaze_angle, alpha, gamma,
+                                                          gr_const, rule_start, rule_stop, g.d[1]);
+    if ((st = d2h(energy_distr, g.d[1], n * sizeof(double), s)) != RTB_OK) return st;
+    return finish(s, nullptr, nullptr, nullptr);
+}

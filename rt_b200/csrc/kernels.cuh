@@ -1,0 +1,80 @@
+// kernels.cuh -- kernel declarations and their argument structs.
+#pragma once
+
+#include "common.cuh"
+
+namespace rtb {
+
+// One beam for the generator (rtb_generate_beams).
+struct GenBeam {
+    uint64_t first_ray, n_rays, n_lambda;
+    uint64_t seed;
+    double disk[3];     // N, R_in, R_out
+    double center[3];
+    double range[2];
+    double d_lambda;    // (range[1]-range[0])/(n_lambda-1) (rt_cuda_engine_beam.cu:726)
+    double c0[3];       // direction cosines of the field angle, normalised
+};
+
+// CCD frame accumulation arguments.
+struct FrameArgs {
+    double xsize, ysize, xpix, ypix;
+    uint64_t xdim, ydim;
+    unsigned* counts;               // device; NULL disables the frame
+    unsigned long long* n_outside;  // device; may be NULL
+};
+
+// Size of the dynamic shared memory the fused kernels use.
+inline size_t fused_smem_bytes(int n_knots) {
+    return ((sizeof(DevScheme) + 15) / 16) * 16 + sizeof(double) * (size_t)n_knots;
+}
+
+// ---- drop-in kernels (kernels_fp64.cu) ----
+__global__ void k_transform(size_t n, DevSurface s, double* X, double* Y, double* Z, double* cX, double* cY,
+                            double* cZ);
+__global__ void k_intersect(size_t n, DevSurface s, uint32_t fixes, double* X, double* Y, double* Z,
+                            const double* cX, const double* cY, const double* cZ, char* flag,
+                            unsigned long long* n_bad);
+__global__ void k_reflect(size_t n, DevSurface s, const double* X, const double* Y, const double* Z, double* cX,
+                          double* cY, double* cZ);
+__global__ void k_action(size_t n, DevSurface s, const double* knots, long long order, const double* lambda,
+                         const double* X, const double* Y, const double* Z, double* cX, double* cY, double* cZ,
+                         char* flag, unsigned long long* n_bad, unsigned* err);
+__global__ void k_normalize(size_t n, double* cX, double* cY, double* cZ);
+__global__ void k_aperture(size_t n, int shade, int shape, double sz0, double sz1, double c0, double c1,
+                           const double* X, const double* Y, char* flag, unsigned long long* n_bad);
+__global__ void k_ccd_coords(size_t n, const double* X, const double* Y, double xsize, double ysize, double xpix,
+                             double ypix, unsigned* ix, unsigned* iy);
+__global__ void k_ccd_image(size_t n, const unsigned* ix, const unsigned* iy, const double* lambda,
+                            const double* knots, int qe_off, int qe_n, int sp_off, int sp_n, size_t xdim, size_t ydim,
+                            double pix_area, double* image, unsigned long long* n_outside, unsigned* err);
+__global__ void k_surface_qe(size_t n, const double* lambda, double* spec, const double* knots, int off, int cnt,
+                             unsigned* err);
+__global__ void k_beam_random(size_t n, double p1, double p2, double cx, double cy, double cz, uint64_t seed,
+                              uint64_t first, double* X, double* Y, double* Z);
+__global__ void k_uniform_range(size_t n, double l0, double d_l, double* lambda);
+__global__ void k_random_range(size_t n, double l0, double l1, uint64_t seed, double* lambda);
+__global__ void k_generate(const GenBeam* beams, int n_beams, uint64_t total, DevRays rays);
+__global__ void k_ccd_frame(DevRays rays, FrameArgs f);
+
+// ---- trace kernels ----
+// counts: [n_beams][3*n_surfaces + 1] -- rays lost per stage, then rays that
+// reached the end.
+// Rays are read from `in` and written to `out` (which may be `in`); a lost
+// ray's flag and lost_stage are written to `out`.
+__global__ void k_surface_step(const DevScheme* sch, int k, const double* knots, const DevBeam* beams, int n_beams,
+                               DevRays in, DevRays out, unsigned long long* counts, unsigned* err);
+__global__ void k_fused_fp64(const DevScheme* sch, const double* knots, const DevBeam* beams, int n_beams,
+                             DevRays in, DevRays out, unsigned long long* counts, unsigned* err, int state_out,
+                             FrameArgs frame);
+// kernels_mixed.cu
+__global__ void k_fused_mixed(const DevScheme* sch, const double* knots, const DevBeam* beams, int n_beams,
+                              DevRays in, DevRays out, unsigned long long* counts, unsigned* err, int state_out,
+                              FrameArgs frame);
+
+// ---- ordering (order.cu) ----
+int reference_order(const DevBeam* h_beams, int n_beams, int n_stages, const DevRays& rays, uint32_t* order,
+                    cudaStream_t stream);
+int rearrange_device(size_t n_good, double* arrays[7], char* flag, size_t* n_good_out, cudaStream_t stream);
+
+}  // namespace rtb

@@ -1,0 +1,466 @@
+// kernels_fp64.cu -- plain FP64 kernels of the engine.
+//
+// Compiled with --fmad=false: every kernel here is bit-identical to the CPU
+// oracle (see ray_fp64.cuh).  Three groups:
+//   * drop-in kernels, one per engine call of common-lib/rt_engine_func.h;
+//   * the per-surface trace kernel (one launch per surface, ray state in HBM);
+//   * the fused FP64 trace kernel (whole scheme per ray, state in registers).
+#include "kernels.cuh"
+#include "ray_fp64.cuh"
+#include "philox.cuh"
+
+namespace rtb {
+
+using f64::Ray;
+
+__device__ __forceinline__ size_t gtid() { return (size_t)blockIdx.x * blockDim.x + threadIdx.x; }
+__device__ __forceinline__ size_t gstride() { return (size_t)blockDim.x * gridDim.x; }
+
+// Count one event per lane that has `pred`, one atomic per warp.
+__device__ __forceinline__ void warp_count(bool pred, unsigned long long* counter) {
+    unsigned mask = __ballot_sync(__activemask(), pred);
+    if (pred && (threadIdx.x & 31) == (unsigned)(__ffs(mask) - 1)) atomicAdd(counter, (unsigned long long)__popc(mask));
+}
+
+// ===========================================================================
+// Drop-in kernels
+// ===========================================================================
+
+__global__ void k_transform(size_t n, DevSurface s, double* X, double* Y, double* Z, double* cX, double* cY,
+                            double* cZ) {
+    for (size_t i = gtid(); i < n; i += gstride()) {
+        Ray r{X[i], Y[i], Z[i], cX[i], cY[i], cZ[i]};
+        f64::transform(s, r);
+        X[i] = r.X; Y[i] = r.Y; Z[i] = r.Z; cX[i] = r.cX; cY[i] = r.cY; cZ[i] = r.cZ;
+    }
+}
+
+__global__ void k_intersect(size_t n, DevSurface s, uint32_t fixes, double* X, double* Y, double* Z,
+                            const double* cX, const double* cY, const double* cZ, char* flag,
+                            unsigned long long* n_bad) {
+    for (size_t i0 = (size_t)blockIdx.x * blockDim.x; i0 < n; i0 += gstride()) {
+        size_t i = i0 + threadIdx.x;
+        bool lost = false;
+        if (i < n) {
+            Ray r{X[i], Y[i], Z[i], cX[i], cY[i], cZ[i]};
+            lost = !f64::intersect(s, fixes, r);
+            X[i] = r.X; Y[i] = r.Y; Z[i] = r.Z;
+            if (lost) flag[i] = 0;
+        }
+        warp_count(lost, n_bad);
+    }
+}
+
+__global__ void k_reflect(size_t n, DevSurface s, const double* X, const double* Y, const double* Z, double* cX,
+                          double* cY, double* cZ) {
+    for (size_t i = gtid(); i < n; i += gstride()) {
+        Ray r{X[i], Y[i], Z[i], cX[i], cY[i], cZ[i]};
+        f64::reflect(s, r);
+        cX[i] = r.cX; cY[i] = r.cY; cZ[i] = r.cZ;
+    }
+}
+
+// Refraction or diffraction (the action of a Lens or Grating surface).
+__global__ void k_action(size_t n, DevSurface s, const double* knots, long long order, const double* lambda,
+                         const double* X, const double* Y, const double* Z, double* cX, double* cY, double* cZ,
+                         char* flag, unsigned long long* n_bad, unsigned* err) {
+    for (size_t i0 = (size_t)blockIdx.x * blockDim.x; i0 < n; i0 += gstride()) {
+        size_t i = i0 + threadIdx.x;
+        bool lost = false;
+        if (i < n) {
+            Ray r{X[i], Y[i], Z[i], cX[i], cY[i], cZ[i]};
+            int a = f64::action(s, knots, order, lambda[i], r);
+            if (a == f64::ACT_RANGE) {
+                atomicOr(err, DEV_ERR_OUT_OF_RANGE);
+            } else {
+                lost = a == f64::ACT_LOST;
+                cX[i] = r.cX; cY[i] = r.cY; cZ[i] = r.cZ;
+                if (lost) flag[i] = 0;
+            }
+        }
+        warp_count(lost, n_bad);
+    }
+}
+
+__global__ void k_normalize(size_t n, double* cX, double* cY, double* cZ) {
+    for (size_t i = gtid(); i < n; i += gstride()) {
+        double a = cX[i], b = cY[i], c = cZ[i];
+        f64::normalize(a, b, c);
+        cX[i] = a; cY[i] = b; cZ[i] = c;
+    }
+}
+
+__global__ void k_aperture(size_t n, int shade, int shape, double sz0, double sz1, double c0, double c1,
+                           const double* X, const double* Y, char* flag, unsigned long long* n_bad) {
+    const double size[2] = {sz0, sz1}, center[2] = {c0, c1};
+    for (size_t i0 = (size_t)blockIdx.x * blockDim.x; i0 < n; i0 += gstride()) {
+        size_t i = i0 + threadIdx.x;
+        bool lost = false;
+        if (i < n) {
+            lost = !f64::aperture_pass(shade != 0, shape, size, center, X[i], Y[i]);
+            if (lost) flag[i] = 0;
+        }
+        warp_count(lost, n_bad);
+    }
+}
+
+// __double2uint_rz: round toward zero, saturating, NaN -> 0 (rt_cuda_engine_ccd.cu:37-38).
+__device__ __forceinline__ void ccd_coords(double X, double Y, double xsize, double ysize, double xpix, double ypix,
+                                           unsigned& ix, unsigned& iy) {
+    ix = __double2uint_rz((X + xsize / 2.0) / xpix);
+    iy = __double2uint_rz((Y + ysize / 2.0) / ypix);
+}
+
+__global__ void k_ccd_coords(size_t n, const double* X, const double* Y, double xsize, double ysize, double xpix,
+                             double ypix, unsigned* ix, unsigned* iy) {
+    for (size_t i = gtid(); i < n; i += gstride()) {
+        unsigned a, b;
+        ccd_coords(X[i], Y[i], xsize, ysize, xpix, ypix, a, b);
+        ix[i] = a;
+        iy[i] = b;
+    }
+}
+
+// compute_ccd_image_kernel (rt_cuda_engine_ccd.cu:219-232, 280-288) with the
+// spline evaluations on the device, a bounds check, and atomic accumulation.
+__global__ void k_ccd_image(size_t n, const unsigned* ix, const unsigned* iy, const double* lambda,
+                            const double* knots, int qe_off, int qe_n, int sp_off, int sp_n, size_t xdim, size_t ydim,
+                            double pix_area, double* image, unsigned long long* n_outside, unsigned* err) {
+    for (size_t i0 = (size_t)blockIdx.x * blockDim.x; i0 < n; i0 += gstride()) {
+        size_t i = i0 + threadIdx.x;
+        bool outside = false;
+        if (i < n) {
+            double q, sp, l = lambda[i];
+            if (!f64::table_eval(knots + qe_off, qe_n, l, q) || !f64::table_eval(knots + sp_off, sp_n, l, sp)) {
+                atomicOr(err, DEV_ERR_OUT_OF_RANGE);
+            } else {
+                sp = sp * l;
+                if (ix[i] >= xdim || iy[i] >= ydim) {
+                    outside = true;
+                } else {
+                    unsigned index = iy[i] * (unsigned)xdim + ix[i];
+                    atomicAdd(image + index, sp / K_HC * q * pix_area);
+                }
+            }
+        }
+        warp_count(outside, n_outside);
+    }
+}
+
+__global__ void k_surface_qe(size_t n, const double* lambda, double* spec, const double* knots, int off, int cnt,
+                             unsigned* err) {
+    for (size_t i = gtid(); i < n; i += gstride()) {
+        double q;
+        if (!f64::table_eval(knots + off, cnt, lambda[i], q)) {
+            atomicOr(err, DEV_ERR_OUT_OF_RANGE);
+            continue;
+        }
+        spec[i] *= q;
+    }
+}
+
+__global__ void k_beam_random(size_t n, double p1, double p2, double cx, double cy, double cz, uint64_t seed,
+                              uint64_t first, double* X, double* Y, double* Z) {
+    const double params[3] = {0.0, p1, p2}, center[3] = {cx, cy, cz};
+    for (size_t i = gtid(); i < n; i += gstride()) {
+        double u1, u2;
+        ray_uniforms(seed, 0, first + i, u1, u2);
+        disk_position(params, center, u1, u2, X[i], Y[i], Z[i]);
+    }
+}
+
+__global__ void k_uniform_range(size_t n, double l0, double d_l, double* lambda) {
+    for (size_t i = gtid(); i < n; i += gstride()) lambda[i] = l0 + (double)i * d_l;
+}
+
+__global__ void k_random_range(size_t n, double l0, double l1, uint64_t seed, double* lambda) {
+    for (size_t i = gtid(); i < n; i += gstride()) {
+        double u1, u2;
+        ray_uniforms(seed, 1, i, u1, u2);
+        lambda[i] = (l1 - l0) * u1 + l0;
+    }
+}
+
+// rtb_generate_beams: disk positions, field-turned parallel cosines,
+// composite wavelengths lambda_(i mod n_lambda).
+__global__ void k_generate(const GenBeam* beams, int n_beams, uint64_t total, DevRays rays) {
+    for (size_t i = gtid(); i < total; i += gstride()) {
+        int lo = 0, hi = n_beams - 1;
+        while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if (beams[mid].first_ray <= i) lo = mid; else hi = mid - 1;
+        }
+        const GenBeam& b = beams[lo];
+        uint64_t j = i - b.first_ray;
+        if (j >= b.n_rays) continue;
+        double u1, u2;
+        ray_uniforms(b.seed, 0, j, u1, u2);
+        disk_position(b.disk, b.center, u1, u2, rays.X[i], rays.Y[i], rays.Z[i]);
+        rays.cX[i] = b.c0[0];
+        rays.cY[i] = b.c0[1];
+        rays.cZ[i] = b.c0[2];
+        uint64_t k = j % b.n_lambda;
+        rays.lambda[i] = (b.n_lambda == 1) ? b.range[0] : b.range[0] + (double)k * b.d_lambda;
+        if (rays.flag) rays.flag[i] = 1;
+        if (rays.lost_stage) rays.lost_stage[i] = RTB_NOT_LOST;
+    }
+}
+
+// ===========================================================================
+// Trace kernels
+// ===========================================================================
+
+__device__ __forceinline__ int beam_of(const DevBeam* beams, int n_beams, uint64_t i) {
+    int lo = 0, hi = n_beams - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (beams[mid].first_ray <= i) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Count one event per lane (a loss at a stage, or reaching the end), one
+// atomic per distinct counter in the warp.
+__device__ __forceinline__ void count_event(bool ev, int key, unsigned long long* counts) {
+    unsigned active = __activemask();
+    unsigned em = __ballot_sync(active, ev);
+    if (!ev) return;
+    unsigned same = __match_any_sync(em, key);
+    if ((threadIdx.x & 31) == (unsigned)(__ffs(same) - 1)) atomicAdd(counts + key, (unsigned long long)__popc(same));
+}
+
+// One surface of the per-surface engine.  Live rays (flag 1) are read, moved
+// through the transform, Normalize, intersection, aperture, action and
+// Normalize of surface k, and written back; a ray lost here gets
+// lost_stage, flag 0 and the Normalize calls the reference would still
+// apply to it.  After the last surface the survivors are counted.
+__global__ void __launch_bounds__(256) k_surface_step(const DevScheme* __restrict__ sch, int k, const double* knots,
+                                                      const DevBeam* beams, int n_beams, DevRays in, DevRays out,
+                                                      unsigned long long* counts, unsigned* err) {
+    const DevSurface& s = sch->s[k];
+    const int n_stages = 3 * sch->n_surfaces;
+    const bool last = k == sch->n_surfaces - 1;
+    for (size_t i0 = (size_t)blockIdx.x * blockDim.x; i0 < in.n; i0 += gstride()) {
+        size_t i = i0 + threadIdx.x;
+        bool ev = false;
+        int key = 0;
+        if (i < in.n && in.flag[i] == 1) {
+            Ray r{in.X[i], in.Y[i], in.Z[i], in.cX[i], in.cY[i], in.cZ[i]};
+            f64::transform(s, r);
+            f64::normalize(r.cX, r.cY, r.cZ);
+            int stage = -1;
+            if (s.non_aux) {
+                if (!f64::intersect(s, sch->fixes, r)) {
+                    stage = 3 * k;
+                } else if (!f64::aperture_pass(s.type == RTB_SHADE, s.shape, s.size, s.center, r.X, r.Y)) {
+                    stage = 3 * k + 1;
+                } else {
+                    long long order = s.order;
+                    if (s.type == RTB_GRATING) {
+                        int b = beam_of(beams, n_beams, i);
+                        if (beams[b].n_orders > 0) order = beams[b].orders[s.grating_index];
+                    }
+                    double lam = (s.type == RTB_LENS || s.type == RTB_GRATING) ? in.lambda[i] : 0.0;
+                    int a = f64::action(s, knots, order, lam, r);
+                    if (a == f64::ACT_RANGE) atomicOr(err, DEV_ERR_OUT_OF_RANGE);
+                    else if (a == f64::ACT_LOST) stage = 3 * k + 2;
+                    else f64::normalize(r.cX, r.cY, r.cZ);
+                }
+            }
+            if (stage >= 0) {
+                ev = true;
+                if (sch->renorm_lost) f64::renormalize(r, s.renorm_after);
+                out.flag[i] = 0;
+                out.lost_stage[i] = (uint8_t)stage;
+                key = beam_of(beams, n_beams, i) * (n_stages + 1) + stage;
+            } else if (last) {
+                ev = true;
+                key = beam_of(beams, n_beams, i) * (n_stages + 1) + n_stages;
+            }
+            if (in.flag != out.flag) {
+                if (stage < 0) out.flag[i] = 1;
+                if (stage < 0) out.lost_stage[i] = RTB_NOT_LOST;
+            }
+            out.X[i] = r.X; out.Y[i] = r.Y; out.Z[i] = r.Z;
+            out.cX[i] = r.cX; out.cY[i] = r.cY; out.cZ[i] = r.cZ;
+        } else if (i < in.n && in.flag != out.flag) {
+            out.flag[i] = in.flag[i];
+        }
+        count_event(ev, key, counts);
+    }
+}
+
+// Frame counts of one good ray at the detector: warp-aggregated increments
+// of the pixel it lands on.  Non-finite coordinates count as outside.
+__device__ __forceinline__ void frame_add(bool good, double X, double Y, const FrameArgs& f) {
+    unsigned active = __activemask();
+    long long pix = -1;
+    if (good) {
+        if (isfinite(X) && isfinite(Y)) {
+            unsigned ix, iy;
+            ccd_coords(X, Y, f.xsize, f.ysize, f.xpix, f.ypix, ix, iy);
+            if (ix < f.xdim && iy < f.ydim) pix = (long long)iy * (long long)f.xdim + ix;
+        }
+    }
+    bool in = pix >= 0;
+    unsigned im = __ballot_sync(active, in);
+    if (in) {
+        unsigned same = __match_any_sync(im, pix);
+        if ((threadIdx.x & 31) == (unsigned)(__ffs(same) - 1)) atomicAdd(f.counts + pix, (unsigned)__popc(same));
+    }
+    bool out = good && !in;
+    unsigned om = __ballot_sync(active, out);
+    if (out && f.n_outside && (threadIdx.x & 31) == (unsigned)(__ffs(om) - 1))
+        atomicAdd(f.n_outside, (unsigned long long)__popc(om));
+}
+
+// Frame counts over all good rays (rtb_ccd_frame).
+__global__ void k_ccd_frame(DevRays rays, FrameArgs f) {
+    for (size_t i0 = (size_t)blockIdx.x * blockDim.x; i0 < rays.n; i0 += gstride()) {
+        size_t i = i0 + threadIdx.x;
+        bool good = false;
+        double X = 0, Y = 0;
+        if (i < rays.n && rays.flag[i] == 1) {
+            good = true;
+            X = rays.X[i];
+            Y = rays.Y[i];
+        }
+        frame_add(good, X, Y, f);
+    }
+}
+
+// Copy the scheme and the knot tables into shared memory (fused kernels).
+__device__ __forceinline__ const DevScheme* stage_scheme(const DevScheme* sch, const double* knots,
+                                                         const double*& s_knots) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    DevScheme* s_sch = reinterpret_cast<DevScheme*>(smem);
+    double* kn = reinterpret_cast<double*>(smem + ((sizeof(DevScheme) + 15) / 16) * 16);
+    const int4* src = reinterpret_cast<const int4*>(sch);
+    int4* dst = reinterpret_cast<int4*>(smem);
+    for (int j = threadIdx.x; j < (int)(sizeof(DevScheme) / 16); j += blockDim.x) dst[j] = src[j];
+    int nk = sch->n_knots;
+    for (int j = threadIdx.x; j < nk; j += blockDim.x) kn[j] = knots[j];
+    __syncthreads();
+    s_knots = kn;
+    return s_sch;
+}
+
+// Fused FP64 trace: the whole surface sequence per ray in registers, the
+// scheme and knot tables in shared memory, a persistent grid striding over
+// the rays.  Bit-identical to k_surface_step.  With a frame, good rays add
+// their pixel with warp-aggregated atomics.
+__global__ void __launch_bounds__(256) k_fused_fp64(const DevScheme* __restrict__ g_sch, const double* knots,
+                                                    const DevBeam* beams, int n_beams, DevRays in, DevRays out,
+                                                    unsigned long long* counts, unsigned* err, int state_out,
+                                                    FrameArgs frame) {
+    const double* s_knots;
+    const DevScheme* sch = stage_scheme(g_sch, knots, s_knots);
+    const int ns = sch->n_surfaces;
+    const int n_stages = 3 * ns;
+    for (size_t i0 = (size_t)blockIdx.x * blockDim.x; i0 < in.n; i0 += gstride()) {
+        size_t i = i0 + threadIdx.x;
+        bool ev = false, good = false;
+        int key = 0;
+        double outX = 0, outY = 0;
+        if (i < in.n && in.flag[i] == 1) {
+            Ray r{in.X[i], in.Y[i], in.Z[i], in.cX[i], in.cY[i], in.cZ[i]};
+            const double lam = in.lambda[i];
+            const int b = beam_of(beams, n_beams, i);
+            int stage = -1;
+            for (int k = 0; k < ns; ++k) {
+                const DevSurface& s = sch->s[k];
+                f64::transform(s, r);
+                f64::normalize(r.cX, r.cY, r.cZ);
+                if (!s.non_aux) continue;
+                if (!f64::intersect(s, sch->fixes, r)) { stage = 3 * k; break; }
+                if (!f64::aperture_pass(s.type == RTB_SHADE, s.shape, s.size, s.center, r.X, r.Y)) {
+                    stage = 3 * k + 1;
+                    break;
+                }
+                long long order = s.order;
+                if (s.type == RTB_GRATING && beams[b].n_orders > 0) order = beams[b].orders[s.grating_index];
+                int a = f64::action(s, s_knots, order, lam, r);
+                if (a == f64::ACT_RANGE) { atomicOr(err, DEV_ERR_OUT_OF_RANGE); stage = -2; break; }
+                if (a == f64::ACT_LOST) { stage = 3 * k + 2; break; }
+                f64::normalize(r.cX, r.cY, r.cZ);
+            }
+            if (stage >= 0) {
+                ev = true;
+                if (sch->renorm_lost) f64::renormalize(r, sch->s[stage / 3].renorm_after);
+                out.flag[i] = 0;
+                out.lost_stage[i] = (uint8_t)stage;
+                key = b * (n_stages + 1) + stage;
+            } else if (stage == -1) {
+                ev = good = true;
+                key = b * (n_stages + 1) + n_stages;
+                if (in.flag != out.flag) {
+                    out.flag[i] = 1;
+                    out.lost_stage[i] = RTB_NOT_LOST;
+                }
+            }
+            if (stage != -2) {
+                out.X[i] = r.X;
+                out.Y[i] = r.Y;
+                if (state_out) {
+                    out.Z[i] = r.Z;
+                    out.cX[i] = r.cX;
+                    out.cY[i] = r.cY;
+                    out.cZ[i] = r.cZ;
+                }
+            }
+            outX = r.X;
+            outY = r.Y;
+        }
+        else if (i < in.n && in.flag != out.flag) {
+            out.flag[i] = in.flag[i];
+        }
+        count_event(ev, key, counts);
+        if (frame.counts) frame_add(good, outX, outY, frame);
+    }
+}
+
+}  // namespace rtb
+
+namespace rtb {
+
+// I1 of the blaze function after Tarasov (rt_cuda_engine_surface.cu:1988-2019):
+// blaze angle c, incidence k1 (alpha), grating constant eps, relative rule
+// length rule_size.
+__device__ __forceinline__ double i1_tarasov(double c, double k1, double eps, double rule_size, double lambda,
+                                             double beta) {
+    double I1 = K_RT_PI * eps * rule_size / lambda * cos(beta) / cos(c - beta) * (sin(c - k1) + sin(c - beta));
+    double term = cos(beta) * cos(c - k1) / cos(c - beta);
+    if (fabs(I1) < K_RT_PI / 2.0) {
+        I1 *= I1;
+        I1 = (0.00761 * I1 - 0.16605) * I1 + 1;
+    } else {
+        I1 = sin(I1) / (I1);
+    }
+    I1 *= term;
+    I1 *= I1;
+    return I1;
+}
+
+// grating_energy_distr_kernel (rt_cuda_engine_surface.cu:2098-2153): the
+// energy in `order`, normalised over all propagating orders.
+__global__ void k_grating_energy(size_t n, const double* lambda, long long order, double blaze, double alpha,
+                                 double gamma, double gr_const, double rule_start, double rule_stop, double* energy) {
+    const double rule_size = rule_stop - rule_start;
+    for (size_t i = gtid(); i < n; i += gstride()) {
+        double l = lambda[i];
+        double sin_alpha = sin(alpha);
+        double cos_gamma = cos(gamma);
+        long long order_min = __double2ll_rz(gr_const / l * (sin_alpha - 1) * cos_gamma);
+        long long order_max = __double2ll_rz(gr_const / l * (sin_alpha + 1) * cos_gamma);
+        double norm = 0.0;
+        for (long long m = order_min; m <= order_max; ++m) {
+            double beta = asin(m * l / gr_const / cos_gamma - sin_alpha);
+            norm += i1_tarasov(blaze, alpha, gr_const, rule_size, l, beta);
+        }
+        double beta = asin(order * l / (gr_const * cos_gamma) - sin_alpha);
+        double I1 = i1_tarasov(blaze, alpha, gr_const, rule_size, l, beta);
+        energy[i] *= I1 / norm;
+    }
+}
+
+}  // namespace rtb

@@ -65,20 +65,21 @@ class Rays(C.Structure):
                 ("lost_stage", C.c_void_p), ("n", C.c_size_t)]
 
 
+class CCD(C.Structure):
+    _fields_ = [("xsize", C.c_double), ("ysize", C.c_double), ("xdim", C.c_uint64), ("ydim", C.c_uint64),
+                ("xpix", C.c_double), ("ypix", C.c_double)]
+
+
 class TraceOpts(C.Structure):
     _fields_ = [("engine", C.c_int32), ("precision", C.c_int32), ("fixes", C.c_uint32),
                 ("renormalize_lost", C.c_int32), ("block_size", C.c_int32), ("rays_per_thread", C.c_int32),
-                ("state_out", C.c_int32), ("reserved", C.c_int32)]
+                ("state_out", C.c_int32), ("reserved", C.c_int32), ("ccd", C.POINTER(CCD)),
+                ("counts", C.c_void_p), ("n_outside", C.c_void_p)]
 
 
 class TraceStats(C.Structure):
     _fields_ = [("ray_surfaces", C.c_uint64), ("n_good", C.c_uint64), ("failed_beam", C.c_int32),
                 ("failed_stage", C.c_int32)]
-
-
-class CCD(C.Structure):
-    _fields_ = [("xsize", C.c_double), ("ysize", C.c_double), ("xdim", C.c_uint64), ("ydim", C.c_uint64),
-                ("xpix", C.c_double), ("ypix", C.c_double)]
 
 
 def dptr(a: np.ndarray) -> C.POINTER(C.c_double):
