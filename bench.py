@@ -262,6 +262,24 @@ def main():
         raise SystemExit("no engine ran")
     hv = engines[head]
 
+    # accuracy of the mixed kernel against the FP64 engine on the same rays
+    accuracy = None
+    if "value" in engines.get("fused_mixed", {}) and "value" in engines.get("fused_fp64", {}):
+        from rt_b200 import metrics
+        ref = E.DeviceRays(n)
+        rref = ref.struct()
+        o64 = E.opts(engine=ffi.ENGINE_FUSED, precision=ffi.FP64, fixes=FIXES, state_out=0)
+        omx = E.opts(engine=ffi.ENGINE_FUSED, precision=ffi.MIXED, fixes=FIXES, state_out=0)
+        stats = ffi.TraceStats()
+        ffi.check(L.rtb_trace_out(s_arr, len(surf), b_arr, len(beams), C.byref(o64), C.byref(rin), C.byref(rref),
+                                  C.byref(stats), C.c_void_p(stream.cuda_stream)))
+        ffi.check(L.rtb_trace_out(s_arr, len(surf), b_arr, len(beams), C.byref(omx), C.byref(rin), C.byref(rout),
+                                  C.byref(stats), C.c_void_p(stream.cuda_stream)))
+        torch.cuda.synchronize()
+        accuracy = metrics.ccd_error(out.X, out.Y, out.flag, ref.X, ref.Y, ref.flag, ccd.xsize, ccd.ysize,
+                                     ccd.xpix, ccd.ypix)
+        del ref
+
     # roofline of the headline kernel (HBM view): algorithmic bytes per launch
     # = 57 B read (X,Y,Z,cX,cY,cZ,lambda,flag) + 18 B written (X,Y,flag,
     # lost_stage) per ray + 4 B per ray counted on the frame.
@@ -311,6 +329,7 @@ def main():
                 "engines": engines,
                 "speedup_vs_plain_fp64": (hv["value"] / engines["per_surface"]["value"])
                 if "per_surface" in engines and "value" in engines["per_surface"] else None,
+                "accuracy_vs_fp64": accuracy,
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
                 "gpu_launches": args.steps * 1}
         print(json.dumps(line), flush=True)

@@ -5,22 +5,13 @@
 //   * drop-in kernels, one per engine call of common-lib/rt_engine_func.h;
 //   * the per-surface trace kernel (one launch per surface, ray state in HBM);
 //   * the fused FP64 trace kernel (whole scheme per ray, state in registers).
-#include "kernels.cuh"
+#include "trace_common.cuh"
 #include "ray_fp64.cuh"
 #include "philox.cuh"
 
 namespace rtb {
 
 using f64::Ray;
-
-__device__ __forceinline__ size_t gtid() { return (size_t)blockIdx.x * blockDim.x + threadIdx.x; }
-__device__ __forceinline__ size_t gstride() { return (size_t)blockDim.x * gridDim.x; }
-
-// Count one event per lane that has `pred`, one atomic per warp.
-__device__ __forceinline__ void warp_count(bool pred, unsigned long long* counter) {
-    unsigned mask = __ballot_sync(__activemask(), pred);
-    if (pred && (threadIdx.x & 31) == (unsigned)(__ffs(mask) - 1)) atomicAdd(counter, (unsigned long long)__popc(mask));
-}
 
 // ===========================================================================
 // Drop-in kernels
@@ -102,13 +93,6 @@ __global__ void k_aperture(size_t n, int shade, int shape, double sz0, double sz
         }
         warp_count(lost, n_bad);
     }
-}
-
-// __double2uint_rz: round toward zero, saturating, NaN -> 0 (rt_cuda_engine_ccd.cu:37-38).
-__device__ __forceinline__ void ccd_coords(double X, double Y, double xsize, double ysize, double xpix, double ypix,
-                                           unsigned& ix, unsigned& iy) {
-    ix = __double2uint_rz((X + xsize / 2.0) / xpix);
-    iy = __double2uint_rz((Y + ysize / 2.0) / ypix);
 }
 
 __global__ void k_ccd_coords(size_t n, const double* X, const double* Y, double xsize, double ysize, double xpix,
@@ -210,25 +194,6 @@ __global__ void k_generate(const GenBeam* beams, int n_beams, uint64_t total, De
 // Trace kernels
 // ===========================================================================
 
-__device__ __forceinline__ int beam_of(const DevBeam* beams, int n_beams, uint64_t i) {
-    int lo = 0, hi = n_beams - 1;
-    while (lo < hi) {
-        int mid = (lo + hi + 1) >> 1;
-        if (beams[mid].first_ray <= i) lo = mid; else hi = mid - 1;
-    }
-    return lo;
-}
-
-// Count one event per lane (a loss at a stage, or reaching the end), one
-// atomic per distinct counter in the warp.
-__device__ __forceinline__ void count_event(bool ev, int key, unsigned long long* counts) {
-    unsigned active = __activemask();
-    unsigned em = __ballot_sync(active, ev);
-    if (!ev) return;
-    unsigned same = __match_any_sync(em, key);
-    if ((threadIdx.x & 31) == (unsigned)(__ffs(same) - 1)) atomicAdd(counts + key, (unsigned long long)__popc(same));
-}
-
 // One surface of the per-surface engine.  Live rays (flag 1) are read, moved
 // through the transform, Normalize, intersection, aperture, action and
 // Normalize of surface k, and written back; a ray lost here gets
@@ -290,30 +255,6 @@ __global__ void __launch_bounds__(256) k_surface_step(const DevScheme* __restric
     }
 }
 
-// Frame counts of one good ray at the detector: warp-aggregated increments
-// of the pixel it lands on.  Non-finite coordinates count as outside.
-__device__ __forceinline__ void frame_add(bool good, double X, double Y, const FrameArgs& f) {
-    unsigned active = __activemask();
-    long long pix = -1;
-    if (good) {
-        if (isfinite(X) && isfinite(Y)) {
-            unsigned ix, iy;
-            ccd_coords(X, Y, f.xsize, f.ysize, f.xpix, f.ypix, ix, iy);
-            if (ix < f.xdim && iy < f.ydim) pix = (long long)iy * (long long)f.xdim + ix;
-        }
-    }
-    bool in = pix >= 0;
-    unsigned im = __ballot_sync(active, in);
-    if (in) {
-        unsigned same = __match_any_sync(im, pix);
-        if ((threadIdx.x & 31) == (unsigned)(__ffs(same) - 1)) atomicAdd(f.counts + pix, (unsigned)__popc(same));
-    }
-    bool out = good && !in;
-    unsigned om = __ballot_sync(active, out);
-    if (out && f.n_outside && (threadIdx.x & 31) == (unsigned)(__ffs(om) - 1))
-        atomicAdd(f.n_outside, (unsigned long long)__popc(om));
-}
-
 // Frame counts over all good rays (rtb_ccd_frame).
 __global__ void k_ccd_frame(DevRays rays, FrameArgs f) {
     for (size_t i0 = (size_t)blockIdx.x * blockDim.x; i0 < rays.n; i0 += gstride()) {
@@ -327,22 +268,6 @@ __global__ void k_ccd_frame(DevRays rays, FrameArgs f) {
         }
         frame_add(good, X, Y, f);
     }
-}
-
-// Copy the scheme and the knot tables into shared memory (fused kernels).
-__device__ __forceinline__ const DevScheme* stage_scheme(const DevScheme* sch, const double* knots,
-                                                         const double*& s_knots) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    DevScheme* s_sch = reinterpret_cast<DevScheme*>(smem);
-    double* kn = reinterpret_cast<double*>(smem + ((sizeof(DevScheme) + 15) / 16) * 16);
-    const int4* src = reinterpret_cast<const int4*>(sch);
-    int4* dst = reinterpret_cast<int4*>(smem);
-    for (int j = threadIdx.x; j < (int)(sizeof(DevScheme) / 16); j += blockDim.x) dst[j] = src[j];
-    int nk = sch->n_knots;
-    for (int j = threadIdx.x; j < nk; j += blockDim.x) kn[j] = knots[j];
-    __syncthreads();
-    s_knots = kn;
-    return s_sch;
 }
 
 // Fused FP64 trace: the whole surface sequence per ray in registers, the

@@ -1,11 +1,476 @@
-// kernels_mixed.cu -- fused mixed-precision trace kernel (see below).
-#include "kernels.cuh"
+// kernels_mixed.cu -- fused mixed-precision trace kernel.
+//
+// Same per-ray algorithm as the plain engine (ray_fp64.cuh) with the
+// precision of each step chosen for cost against its effect on the CCD
+// position:
+//   * ray state, transforms, intersection roots (quadratic in a
+//     cancellation-safe form, Newton on the asphere sag to 1e-12 mm in at most
+//     six steps from the base-conic root, the toric Steffensen iteration),
+//     the grating equation and the detector coordinate: FP64, contracted to FMA;
+//   * every division and square root: a MUFU seed (rcp/rsqrt.approx.f64)
+//     refined by Newton steps in FP64 instead of the IEEE FP64 division and
+//     square root sequences of the plain engine;
+//   * surface normals and their polynomial terms (the sqrt/div-heavy
+//     derivatives of conic_derivs / toric_derivs, surface.cu:45-94): FP32,
+//     promoted to FP64 before they act on the direction cosines.  Their
+//     transverse components are small, so the FP32 rounding moves a direction
+//     by ~1e-9 rad.
+// Compiled with FMA contraction.  Accuracy is measured against the FP64
+// oracle (median, p99.9 and max CCD error in um; target p99.9 <= 0.05 um).
+#include "trace_common.cuh"
+#include "ray_fp64.cuh"
 
 namespace rtb {
+namespace mx {
 
-__global__ void k_fused_mixed(const DevScheme*, const double*, const DevBeam*, int, DevRays, DevRays, unsigned long long*,
-                              unsigned* err, int, FrameArgs) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(err, DEV_ERR_BAD_VALUE);
+struct Ray {
+    double X, Y, Z, cX, cY, cZ;
+};
+
+// 1/x: rcp.approx.ftz.f64 seed (~2^-22) and two Newton steps.
+__device__ __forceinline__ double rcp(double x) {
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+    double e = fma(-x, r, 1.0);
+    r = fma(r, e, r);
+    e = fma(-x, r, 1.0);
+    return fma(r, e, r);
+}
+
+// 1/sqrt(x): rsqrt.approx.f64 seed and `steps` Newton steps.
+__device__ __forceinline__ double rsqrt_n(double x, int steps) {
+    double y;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    double h = 0.5 * x;
+    for (int i = 0; i < steps; ++i) y = y * fma(-h * y, y, 1.5);
+    return y;
+}
+
+// sqrt(x) to FP64 accuracy; NaN for x < 0, 0 for x == 0.
+__device__ __forceinline__ double sqrt_(double x) {
+    if (!(x > 0.0)) return (x == 0.0) ? 0.0 : __longlong_as_double(0x7ff8000000000000ll);
+    double y = rsqrt_n(x, 2);
+    double s = x * y;
+    return fma(0.5 * y, fma(-s, s, x), s);  // one correction of the product
+}
+
+__device__ __forceinline__ void normalize(Ray& r) {
+    double s = fma(r.cX, r.cX, fma(r.cY, r.cY, r.cZ * r.cZ));
+    double k = rsqrt_n(s, 2);
+    r.cX *= k;
+    r.cY *= k;
+    r.cZ *= k;
+}
+
+__device__ __forceinline__ void transform(const DevSurface& s, Ray& r) {
+    if (s.translate) {
+        r.X -= s.dist[0];
+        r.Y -= s.dist[1];
+        r.Z -= s.dist[2];
+    }
+    auto rot = [](double sA, double cA, double& v1, double& v2) {
+        double e = fma(v1, cA, -v2 * sA);
+        v2 = fma(v1, sA, v2 * cA);
+        v1 = e;
+    };
+    if (s.rot_mask & 1) { rot(s.sinA[0], s.cosA[0], r.X, r.Z); rot(s.sinA[0], s.cosA[0], r.cX, r.cZ); }
+    if (s.rot_mask & 2) { rot(s.sinA[1], s.cosA[1], r.Y, r.Z); rot(s.sinA[1], s.cosA[1], r.cY, r.cZ); }
+    if (s.rot_mask & 4) { rot(s.sinA[2], s.cosA[2], r.X, r.Y); rot(s.sinA[2], s.cosA[2], r.cX, r.cY); }
+}
+
+// ---- surface normals in FP32 -------------------------------------------------
+
+// (dF/dX, dF/dY) of the conic + even polynomial; dF/dZ = 1 (conic_derivs).
+__device__ __forceinline__ void conic_normal(const DevSurface& s, double X, double Y, double& nx, double& ny) {
+    float x = (float)X, y = (float)Y;
+    float r2 = fmaf(x, x, y * y);
+    float c = (float)s.c, k1 = (float)s.k1;
+    float E = c * rsqrtf(fmaf(-k1 * c * c, r2, 1.0f));
+    float sum = 0.0f, rr = 1.0f;
+    for (int i = 1; i <= s.n_poly; ++i, rr *= r2) sum = fmaf((float)i * (float)s.poly[i - 1], rr, sum);
+    E = fmaf(2.0f, sum, E);
+    nx = (double)(-E * x);
+    ny = (double)(-E * y);
+}
+
+// (dF/dX, dF/dY, dF/dZ) of the toric surface (toric_derivs).
+__device__ __forceinline__ void toric_normal(const DevSurface& s, double X, double Y, double Z, double& nx, double& ny,
+                                             double& nz) {
+    float y = (float)Y;
+    float Y2 = y * y;
+    float c = (float)s.c, k1 = (float)s.k1, cR = (float)s.cR;
+    float q = fmaf(-k1 * c * c, Y2, 1.0f);
+    float rq = rsqrtf(q);
+    float Fy = c * Y2 / (1.0f + q * rq);
+    float sum = 0.0f, rr = Y2;
+    for (int i = 0; i < s.n_poly; ++i, rr *= Y2) sum = fmaf((float)s.poly[i], rr, sum);
+    Fy += sum;
+    float dFy = c * y * rq;
+    sum = 0.0f;
+    rr = 1.0f;
+    for (int i = 1; i <= s.n_poly; ++i, rr *= Y2) sum = fmaf((float)i * (float)s.poly[i - 1], rr, sum);
+    dFy = fmaf(2.0f, sum, dFy);
+    nx = (double)(-cR * (float)X);
+    ny = (double)((cR * Fy - 1.0f) * dFy);
+    nz = 1.0 - s.cR * Z;
+}
+
+__device__ __forceinline__ void normal(const DevSurface& s, const Ray& r, double& nx, double& ny, double& nz) {
+    if (s.cls == RTB_TORIC) {
+        toric_normal(s, r.X, r.Y, r.Z, nx, ny, nz);
+    } else {
+        conic_normal(s, r.X, r.Y, nx, ny);
+        nz = 1.0;
+    }
+}
+
+// ---- intersections (FP64) ----------------------------------------------------
+
+__device__ __forceinline__ bool plane_isect(Ray& r) {
+    double s0 = -r.Z * rcp(r.cZ);
+    if (s0 < 0.0) return false;
+    r.X = fma(r.cX, s0, r.X);
+    r.Y = fma(r.cY, s0, r.Y);
+    r.Z = 0.0;
+    return true;
+}
+
+// Paraboloid with the reference's linear root (surface.cu:183-213).
+__device__ __forceinline__ bool paraboloid_isect(const DevSurface& s, Ray& r) {
+    double ic = rcp(s.c);
+    double B = 2.0 * (fma(s.k1 * r.Z, r.cZ, fma(r.X, r.cX, r.Y * r.cY)) - r.cZ * ic);
+    double C = fma(s.k1 * r.Z, r.Z, fma(r.X, r.X, r.Y * r.Y)) - 2.0 * r.Z * ic;
+    double t = -C * rcp(B);
+    if (t < 0.0) return false;
+    r.X = fma(t, r.cX, r.X);
+    r.Y = fma(t, r.cY, r.Y);
+    r.Z = fma(t, r.cZ, r.Z);
+    return true;
+}
+
+// Root of the base conic (c, k1) chosen as conic_intersection chooses it
+// (surface.cu:240-244), evaluated without cancellation.  False if D < 0.
+__device__ __forceinline__ bool conic_root(double c, double k1, const Ray& r, double& t) {
+    double ic = rcp(c);
+    double A = fma(k1 * r.cZ, r.cZ, fma(r.cX, r.cX, r.cY * r.cY));
+    double B = 2.0 * (fma(k1 * r.Z, r.cZ, fma(r.X, r.cX, r.Y * r.cY)) - r.cZ * ic);
+    double C = fma(k1 * r.Z, r.Z, fma(r.X, r.X, r.Y * r.Y)) - 2.0 * r.Z * ic;
+    double D = fma(B, B, -4.0 * A * C);
+    if (D < 0.0) return false;
+    double sq = sqrt_(D);
+    double q_pick = (c > 0) ? (-B - sq) : (-B + sq);
+    double q_other = (c > 0) ? (-B + sq) : (-B - sq);
+    // q_pick cancels when its two terms have opposite signs; then use
+    // t = 2C / q_other (q_pick * q_other = 4AC).
+    bool cancels = (c > 0) ? (B < 0) : (B > 0);
+    t = cancels ? 2.0 * C * rcp(q_other) : q_pick * rcp(2.0 * A);
+    return true;
+}
+
+__device__ __forceinline__ bool conic_isect(const DevSurface& s, Ray& r) {
+    double t;
+    if (!conic_root(s.c, s.k1, r, t)) return false;
+    r.X = fma(t, r.cX, r.X);
+    r.Y = fma(t, r.cY, r.Y);
+    r.Z = fma(t, r.cZ, r.Z);
+    return true;
+}
+
+// Even asphere (iterative_conic_intersection / iterative_poly_intersection,
+// surface.cu:257-333,497-561): the same surface and the same loss tests
+// (plane point behind the ray, grazing |dF| < 1e-7), with Newton started at
+// the base-conic root and run to |dt| < 1e-12 mm.
+__device__ __forceinline__ bool asphere_isect(const DevSurface& s, Ray& r) {
+    double s0 = -r.Z * rcp(r.cZ);
+    bool poly_only = s.c == 0.0;
+    if (poly_only ? !(s0 > 0) : !(s0 >= 0)) return false;
+    double t = s0;
+    if (!poly_only) {
+        double tc;
+        if (conic_root(s.c, s.k1, r, tc)) t = tc;
+    }
+    for (int it = 0; it < 6; ++it) {
+        double x = fma(t, r.cX, r.X), y = fma(t, r.cY, r.Y), z = fma(t, r.cZ, r.Z);
+        double r2 = fma(x, x, y * y);
+        double sag = 0.0, E = 0.0;
+        if (!poly_only) {
+            double q = fma(-s.k1 * s.c * s.c, r2, 1.0);
+            if (!(q > 0.0)) break;  // outside the conic: keep the current point, as the reference does
+            double sq = sqrt_(q);
+            sag = s.c * r2 * rcp(1.0 + sq);
+            E = s.c * rcp(sq);
+        }
+        double psum = 0.0, dsum = 0.0, rr = 1.0;
+        for (int i = 1; i <= s.n_poly; ++i) {
+            dsum = fma((double)i * s.poly[i - 1], rr, dsum);
+            rr *= r2;
+            psum = fma(s.poly[i - 1], rr, psum);
+        }
+        sag += psum;
+        E = fma(2.0, dsum, E);
+        double F = z - sag;
+        double dF = fma(-E, fma(x, r.cX, y * r.cY), r.cZ);
+        if (fabs(dF) < K_ITER_EPS) return false;
+        double dt = F * rcp(dF);
+        t -= dt;
+        if (fabs(dt) < 1e-12) break;
+    }
+    r.X = fma(t, r.cX, r.X);
+    r.Y = fma(t, r.cY, r.Y);
+    r.Z = fma(t, r.cZ, r.Z);
+    return true;
+}
+
+__device__ __forceinline__ double toric_func(const DevSurface& s, bool fix_sign, double t, const Ray& r) {
+    double X = fma(t, r.cX, r.X), Y = fma(t, r.cY, r.Y), Z = fma(t, r.cZ, r.Z);
+    double Y2 = Y * Y;
+    double k = s.k1 * s.c * s.c * Y2;
+    double FY = s.c * Y2 * rcp(1.0 + sqrt_(fix_sign ? 1.0 - k : 1.0 + k));
+    return Z - FY - 0.5 * s.cR * (fma(X, X, Z * Z) - FY * FY);
+}
+
+// iter_toric (surface.cu:359-410) in FP64 with fast divisions.
+__device__ __forceinline__ bool toric_isect(const DevSurface& s, uint32_t fixes, Ray& r) {
+    const bool fix_sign = (fixes & RTB_FIX_TORIC_SIGN) != 0;
+    const bool fix_step = (fixes & RTB_FIX_TORIC_STEP) != 0;
+    double sn1 = -r.Z * rcp(r.cZ);
+    if (!(sn1 >= 0)) return false;
+    unsigned niter = 0;
+    double Fyn = 0.0, sn;
+    do {
+        sn = sn1;
+        double Fxn = toric_func(s, fix_sign, sn, r);
+        if (fabs(Fyn - Fxn) <= K_ITER_EPS) break;
+        double Fzn = toric_func(s, fix_sign, sn + Fxn, r);
+        double den = Fzn - Fxn;
+        if (fix_step && den == 0.0) { sn1 = sn; break; }
+        sn1 = sn - Fxn * Fxn / den;
+        Fyn = Fxn;
+        ++niter;
+    } while ((fabs(sn1 - sn) >= K_ITER_EPS) && (niter <= K_ITER_MAX));
+    r.X = fma(sn1, r.cX, r.X);
+    r.Y = fma(sn1, r.cY, r.Y);
+    r.Z = fma(sn1, r.cZ, r.Z);
+    return true;
+}
+
+__device__ __forceinline__ bool intersect(const DevSurface& s, uint32_t fixes, Ray& r) {
+    switch (s.kind) {
+        case IS_PLANE: return plane_isect(r);
+        case IS_PARABOLOID: return paraboloid_isect(s, r);
+        case IS_CONIC: return conic_isect(s, r);
+        case IS_ITER_POLY:
+        case IS_ITER_CONIC: return asphere_isect(s, r);
+        case IS_TORIC: return toric_isect(s, fixes, r);
+        default: return true;
+    }
+}
+
+// ---- actions -------------------------------------------------------------------
+
+__device__ __forceinline__ void reflect(const DevSurface& s, Ray& r) {
+    if (s.cls == RTB_PLANE) {
+        r.cZ = -r.cZ;
+        return;
+    }
+    double nx, ny, nz;
+    normal(s, r, nx, ny, nz);
+    double a2 = 2.0 * fma(r.cX, nx, fma(r.cY, ny, r.cZ * nz)) * rcp(fma(nx, nx, fma(ny, ny, nz * nz)));
+    r.cX = fma(-a2, nx, r.cX);
+    r.cY = fma(-a2, ny, r.cY);
+    r.cZ = fma(-a2, nz, r.cZ);
+}
+
+__device__ __forceinline__ bool refract(const DevSurface& s, double mu, Ray& r) {
+    double nx = 0.0, ny = 0.0, nz = 1.0;
+    if (s.cls != RTB_PLANE) normal(s, r, nx, ny, nz);
+    double iG = rcp(fma(nx, nx, fma(ny, ny, nz * nz)));
+    double a = mu * fma(r.cX, nx, fma(r.cY, ny, r.cZ * nz)) * iG;
+    double b = fma(mu, mu, -1.0) * iG;
+    double a2 = a * a;
+    if (b > a2) return false;
+    double G = -a + sqrt_(a2 - b);
+    r.cX = fma(mu, r.cX, G * nx);
+    r.cY = fma(mu, r.cY, G * ny);
+    r.cZ = fma(mu, r.cZ, G * nz);
+    return true;
+}
+
+// Grating equation (surface.cu:1247-1520) in FP64.
+__device__ __forceinline__ bool diffract(const DevSurface& s, double mu, double L, Ray& r) {
+    const bool trans = s.gr_type == RTB_TRANSPARENT;
+    if (s.cls == RTB_PLANE) {
+        double a = trans ? mu * r.cZ : r.cZ;
+        double b = trans ? fma(mu, mu, -1.0) + fma(L, L, -2.0 * mu * L * r.cX) : fma(L, L, -2.0 * L * r.cX);
+        double a2 = a * a;
+        if (b > a2) return false;
+        double sq = sqrt_(a2 - b);
+        if (trans) {
+            r.cX = fma(mu, r.cX, -L);
+            r.cY *= mu;
+            r.cZ = fma(mu, r.cZ, -a + sq);
+        } else {
+            r.cX -= L;
+            r.cZ += -a - sq;
+        }
+        return true;
+    }
+    double nx, ny, nz;
+    normal(s, r, nx, ny, nz);
+    // rule direction p = (u, v, w), as the reference builds it (including its
+    // L^2+M+M for the toric, surface.cu:1438,1487)
+    double den = (s.cls == RTB_TORIC) ? fma(ny, ny, nz + nz) : fma(ny, ny, 1.0);
+    double G = nx * rcp(den);
+    double u = rsqrt_n(fma(nx, G, 1.0), 2);
+    double v = -ny * u * G;
+    double w = (s.cls == RTB_TORIC) ? -nz * u * G : -u * G;
+    double iG = rcp(fma(nx, nx, fma(ny, ny, nz * nz)));
+    double kn = fma(r.cX, nx, fma(r.cY, ny, r.cZ * nz));
+    double kp = fma(r.cX, u, fma(r.cY, v, r.cZ * w));
+    double a, b;
+    if (trans) {
+        a = mu * kn * iG;
+        b = (fma(mu, mu, -1.0) + fma(L, L, -2.0 * L * mu * kp)) * iG;
+    } else {
+        a = kn * iG;
+        b = fma(L, L, -2.0 * L * kp) * iG;
+    }
+    double a2 = a * a;
+    if (b > a2) return false;
+    double sq = sqrt_(a2 - b);
+    double g = trans ? -a + sq : -a - sq;
+    double m = trans ? mu : 1.0;
+    r.cX = fma(m, r.cX, fma(-L, u, g * nx));
+    r.cY = fma(m, r.cY, fma(-L, v, g * ny));
+    r.cZ = fma(m, r.cZ, fma(-L, w, g * nz));
+    return true;
+}
+
+// Tabulated function with the divisions by the knot spacing replaced by a
+// reciprocal; same bisection and exact-knot rule as the plain engine.
+__device__ __forceinline__ bool table_eval(const double* tab, int n, double xval, double& out) {
+    if (n == 1) {
+        out = tab[1];
+        return true;
+    }
+    const double* x = tab;
+    const double* y = tab + n;
+    const double* y2 = tab + 2 * n;
+    if ((xval < x[0]) || (xval > x[n - 1])) return false;
+    int il = 0, ir = n;
+    while ((ir - il) > 1) {
+        int i = (il + ir) >> 1;
+        if (x[i] == xval) {
+            out = y[i];
+            return true;
+        }
+        if (x[i] > xval) ir = i; else il = i;
+    }
+    double h = x[ir] - x[il];
+    double ih = rcp(h);
+    double a = (x[ir] - xval) * ih;
+    double b = (xval - x[il]) * ih;
+    double cub = fma(fma(a, a * a, -a), y2[il], fma(b, b * b, -b) * y2[ir]);
+    out = fma(a, y[il], fma(b, y[ir], cub * (h * h) * (1.0 / 6.0)));
+    return true;
+}
+
+__device__ __forceinline__ int action(const DevSurface& s, const double* knots, long long order, double lambda,
+                                      Ray& r) {
+    if (s.type == RTB_MIRROR) {
+        reflect(s, r);
+        return 0;
+    }
+    if (s.type == RTB_LENS) {
+        double a, b;
+        if (!table_eval(knots + s.n1_off, s.n1_n, lambda, a) || !table_eval(knots + s.n2_off, s.n2_n, lambda, b))
+            return 2;
+        return refract(s, a * rcp(b), r) ? 0 : 1;
+    }
+    if (s.type == RTB_GRATING) {
+        double n2v, mu = 0.0;
+        if (!table_eval(knots + s.n2_off, s.n2_n, lambda, n2v)) return 2;
+        double in2 = rcp(n2v);
+        if (s.gr_type == RTB_TRANSPARENT) {
+            double n1v;
+            if (!table_eval(knots + s.n1_off, s.n1_n, lambda, n1v)) return 2;
+            mu = n1v * in2;
+        }
+        double L = (double)order * lambda * in2 * rcp(s.gr_const);
+        return diffract(s, mu, L, r) ? 0 : 1;
+    }
+    return 0;
+}
+
+}  // namespace mx
+
+__global__ void __launch_bounds__(256) k_fused_mixed(const DevScheme* __restrict__ g_sch, const double* knots,
+                                                     const DevBeam* beams, int n_beams, DevRays in, DevRays out,
+                                                     unsigned long long* counts, unsigned* err, int state_out,
+                                                     FrameArgs frame) {
+    const double* s_knots;
+    const DevScheme* sch = stage_scheme(g_sch, knots, s_knots);
+    const int ns = sch->n_surfaces;
+    const int n_stages = 3 * ns;
+    for (size_t i0 = (size_t)blockIdx.x * blockDim.x; i0 < in.n; i0 += gstride()) {
+        size_t i = i0 + threadIdx.x;
+        bool ev = false, good = false;
+        int key = 0;
+        double outX = 0, outY = 0;
+        if (i < in.n && in.flag[i] == 1) {
+            mx::Ray r{in.X[i], in.Y[i], in.Z[i], in.cX[i], in.cY[i], in.cZ[i]};
+            const double lam = in.lambda[i];
+            const int b = beam_of(beams, n_beams, i);
+            int stage = -1;
+            for (int k = 0; k < ns; ++k) {
+                const DevSurface& s = sch->s[k];
+                mx::transform(s, r);
+                mx::normalize(r);
+                if (!s.non_aux) continue;
+                if (!mx::intersect(s, sch->fixes, r)) { stage = 3 * k; break; }
+                if (!f64::aperture_pass(s.type == RTB_SHADE, s.shape, s.size, s.center, r.X, r.Y)) {
+                    stage = 3 * k + 1;
+                    break;
+                }
+                long long order = s.order;
+                if (s.type == RTB_GRATING && beams[b].n_orders > 0) order = beams[b].orders[s.grating_index];
+                int a = mx::action(s, s_knots, order, lam, r);
+                if (a == 2) { atomicOr(err, DEV_ERR_OUT_OF_RANGE); stage = -2; break; }
+                if (a == 1) { stage = 3 * k + 2; break; }
+                mx::normalize(r);
+            }
+            if (stage >= 0) {
+                ev = true;
+                if (sch->renorm_lost) mx::normalize(r);
+                out.flag[i] = 0;
+                out.lost_stage[i] = (uint8_t)stage;
+                key = b * (n_stages + 1) + stage;
+            } else if (stage == -1) {
+                ev = good = true;
+                key = b * (n_stages + 1) + n_stages;
+                if (in.flag != out.flag) {
+                    out.flag[i] = 1;
+                    out.lost_stage[i] = RTB_NOT_LOST;
+                }
+            }
+            if (stage != -2) {
+                out.X[i] = r.X;
+                out.Y[i] = r.Y;
+                if (state_out) {
+                    out.Z[i] = r.Z;
+                    out.cX[i] = r.cX;
+                    out.cY[i] = r.cY;
+                    out.cZ[i] = r.cZ;
+                }
+            }
+            outX = r.X;
+            outY = r.Y;
+        } else if (i < in.n && in.flag != out.flag) {
+            out.flag[i] = in.flag[i];
+        }
+        count_event(ev, key, counts);
+        if (frame.counts) frame_add(good, outX, outY, frame);
+    }
 }
 
 }  // namespace rtb

@@ -419,6 +419,10 @@ int trace_host_impl(const rtb_surface* surfaces, size_t n_surfaces, const rtb_be
         for (int j = 0; j < 7; ++j)
             RTB_CUDA_TRY(cudaMemcpyAsync((&sl.r.X)[j], hin[j] + start, cnt * sizeof(double), cudaMemcpyHostToDevice, s));
         RTB_CUDA_TRY(cudaMemcpyAsync(sl.r.flag, h->flag + start, cnt, cudaMemcpyHostToDevice, s));
+        if (h->lost_stage)
+            RTB_CUDA_TRY(cudaMemcpyAsync(sl.r.lost_stage, h->lost_stage + start, cnt, cudaMemcpyHostToDevice, s));
+        else
+            RTB_CUDA_TRY(cudaMemsetAsync(sl.r.lost_stage, RTB_NOT_LOST, cnt, s));
         if ((st = sl.args.init(ps, sl.beams, s)) != RTB_OK) break;
         if ((st = launch_trace(ps, sl.args, (int)sl.beams.size(), o, sl.r, sl.r, frame, s)) != RTB_OK) break;
         int nout = o.state_out ? 6 : 2;

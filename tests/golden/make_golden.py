@@ -43,6 +43,21 @@ def scalarize(specs, value=1.5):
     return out
 
 
+def sphere_fold(specs):
+    """C1 with the toric fold replaced by a sphere of the mean radius: the
+    reference's toric iteration divides 0/0 for rays that converge exactly
+    (surface.cu:390), and which rays do depends on FMA contraction, so the
+    toric-free variant pins everything else ray by ray."""
+    out = []
+    for s in specs:
+        s = S.SurfaceSpec(**s.__dict__)
+        if s.cls == ffi.TORIC:
+            s.cls = ffi.CONIC
+            s.params = (-1 / 2050.0, 0.0, 0)
+        out.append(s)
+    return out
+
+
 def cases():
     cov = S.coverage_schemes()
     c0 = dict(n_lambda=5, radius=10.0, lam_range=(0.4, 0.7))
@@ -53,7 +68,10 @@ def cases():
         "c4": (S.littrow_free_asphere(), c0, (), 400),
         "c1_m38": (scalarize(S.echelle()), c1, (38, 1), 40),
         "c1_m52": (scalarize(S.echelle()), c1, (52, 1), 40),
+        "c1_sphere_m38": (sphere_fold(scalarize(S.echelle())), c1, (38, 1), 40),
+        "c1_sphere_m52": (sphere_fold(scalarize(S.echelle())), c1, (52, 1), 40),
         "mirrors": (cov["mirrors"], small, (), 400),
+        "mirrors_tagged": (cov["mirrors"], small, (), 400),
         "lenses": (scalarize(cov["lenses"]), small, (), 400),
         "gratings": (scalarize(cov["gratings"]), small, (), 400),
     }
@@ -77,6 +95,9 @@ def main(out_dir=HERE):
     for name, (specs, kw, orders, n_per) in cases().items():
         beam = S.make_beam(0, n_per, kw["n_lambda"], kw["radius"], kw["lam_range"], 20141203, orders=orders)
         rays = O.generate([beam], beam.n_rays)
+        if name.endswith("_tagged"):
+            # mirrors only: the wavelength is free, so it carries the ray index
+            rays.lambda_[:] = 0.4 + 1e-7 * np.arange(rays.n)
         rc, out = H.run_trace("refgpu", specs, list(orders), rays)
         inp = np.stack([rays.X, rays.Y, rays.Z, rays.cX, rays.cY, rays.cZ, rays.lambda_])
         payload = dict(rc=rc, input=inp, scheme=spec_arrays(specs), orders=np.array(orders, dtype=np.int64))
