@@ -258,6 +258,8 @@ def main():
                          "n_good": stats.n_good}
         if name in ("fused_mixed", "fused_fp64"):
             head = name if (head is None or name == "fused_mixed") else head
+    if head is None and "value" in engines.get("per_surface", {}):
+        head = "per_surface"
     if head is None:
         raise SystemExit("no engine ran")
     hv = engines[head]

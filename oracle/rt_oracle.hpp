@@ -662,9 +662,12 @@ inline bool table_eval(size_t n, const double* x, const double* y, const double*
 // CCD (cuda_engine/rt_cuda_engine_ccd.cu)
 // ===========================================================================
 
-// __double2uint_rz: truncation toward zero, saturating, NaN -> 0.
+// __double2uint_rz as the device converts: truncation toward zero,
+// saturating (negative -> 0, >= 2^32 -> 0xFFFFFFFF), NaN -> 0x80000000
+// (measured on B200: tests/test_gpu_parity.py).
 inline uint32_t double2uint_rz(double v) {
-    if (!(v > 0.0)) return 0u;            // negative, zero, NaN
+    if (v != v) return 0x80000000u;
+    if (!(v > 0.0)) return 0u;
     if (v >= 4294967296.0) return 0xFFFFFFFFu;
     return (uint32_t)v;                   // C++ conversion truncates toward zero
 }

@@ -37,7 +37,7 @@ __global__ void k_mark_stage(uint64_t n, const Seg* segs, int n_segs, const uint
     for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < n; k += (uint64_t)blockDim.x * gridDim.x) {
         int s = seg_of(segs, n_segs, k);
         bool in = k < segs[s].start + segs[s].ng;
-        mark[k] = (in && lost_stage[order[k]] == stage) ? 1u : 0u;
+        mark[k] = (in && lost_stage[segs[s].start + order[k]] == stage) ? 1u : 0u;
     }
 }
 

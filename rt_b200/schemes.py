@@ -122,7 +122,12 @@ class CScheme:
 
     @property
     def surfaces(self):
-        return list(self.array)
+        """The rtb_surface structs; each keeps this scheme (and so the table
+        arrays its pointers refer to) alive."""
+        out = list(self.array)
+        for s in out:
+            s._owner = self
+        return out
 
     def n_gratings(self) -> int:
         return sum(1 for s in self.specs if s.type == ffi.GRATING)

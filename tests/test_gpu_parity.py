@@ -334,7 +334,7 @@ def test_dropin_transform_normalize_aperture_rearrange_ccd():
                   C.c_double(0.015), C.c_double(0.015), ffi.vptr(ix), ffi.vptr(iy)) == 0
         out.append((ix, iy))
     assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
-    assert out[0][0][0] == 0 and out[0][0][1] == 0 and out[0][0][2] == 0xFFFFFFFF
+    assert out[0][0][0] == 0x80000000 and out[0][0][1] == 0 and out[0][0][2] == 0xFFFFFFFF
 
 
 def test_dropin_ccd_image_and_qe():
