@@ -278,6 +278,23 @@ RTB_API int rtb_trace_out(const rtb_surface* surfaces, size_t n_surfaces, const 
                           const rtb_trace_opts* opts, const rtb_rays* in, const rtb_rays* out,
                           rtb_trace_stats* stats, void* stream);
 
+/* rtb_trace_out for callers that cannot allocate memory (no counterpart in
+ * the reference).  Runs the fused kernel (opts->engine must be
+ * RTB_ENGINE_FUSED) with its scratch -- prepared scheme, tables, beam table,
+ * loss counters -- in a file-scope device array of RTB_NOALLOC_SCRATCH_BYTES
+ * per device and host-side staging in file-scope host arrays: no cudaMalloc,
+ * cudaFree, pool or heap allocation.  Requests that do not fit (more than
+ * RTB_NOALLOC_MAX_KNOTS table values, or too many beams x stages for the
+ * counters) return RTB_BAD_VALUE before any work is queued.  The first call on
+ * a device looks up the array's address with that device current; make it
+ * before any stream capture.  All calls share the array: calls that overlap
+ * on the GPU race.  Synchronous on `stream`. */
+#define RTB_NOALLOC_SCRATCH_BYTES 1048576
+#define RTB_NOALLOC_MAX_KNOTS 8192
+RTB_API int rtb_trace_out_noalloc(const rtb_surface* surfaces, size_t n_surfaces, const rtb_beam* beams,
+                                  size_t n_beams, const rtb_trace_opts* opts, const rtb_rays* in,
+                                  const rtb_rays* out, rtb_trace_stats* stats, void* stream);
+
 /* rtb_trace on host arrays: copies in, traces and copies out, overlapping the
  * copies of one chunk with the trace of another.  Synchronous. */
 RTB_API int rtb_trace_host(const rtb_surface* surfaces, size_t n_surfaces, const rtb_beam* beams,

@@ -24,6 +24,7 @@ SOURCES = {
     "trace.cu": ["--fmad=false"],
     "order.cu": [],
     "kernels_mixed.cu": ["--fmad=true"],
+    "noalloc.cu": ["--fmad=false"],
 }
 
 
