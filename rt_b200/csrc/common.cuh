@@ -48,15 +48,17 @@ struct DevSurface {
     int32_t n1_off, n1_n, n2_off, n2_n;  // tables: offset/count into the knot buffer (count 1 = single value)
 };
 
-// Scheme passed by value as a kernel parameter (lands in the constant bank;
-// CUDA 12.1+ allows 32 KB of parameters).
+// A prepared scheme in device memory; the fused kernels copy it to shared
+// memory, the per-surface kernel reads its one surface from global memory.
 struct DevScheme {
     int32_t n_surfaces;
     int32_t n_knots;        // doubles per array in the knot buffer
     uint32_t fixes;
     int32_t renorm_lost;
+    int32_t pad[4];
     DevSurface s[RTB_MAX_SURFACES];
 };
+static_assert(sizeof(DevScheme) % 16 == 0, "DevScheme is copied to shared memory in 16-byte words");
 
 // Beam table on the device (first ray and orders of each beam).
 struct DevBeam {

@@ -29,6 +29,14 @@ inline size_t fused_smem_bytes(int n_knots) {
     return ((sizeof(DevScheme) + 15) / 16) * 16 + sizeof(double) * (size_t)n_knots;
 }
 
+// Scheduling of the persistent fused kernels: `next` is a counter of
+// 32*rpt-ray tiles handed out to warps (zeroed before each launch).
+struct TileSched {
+    unsigned long long* next;
+    int rpt;
+};
+constexpr int kDefaultRpt = 2;
+
 // ---- drop-in kernels (kernels_fp64.cu) ----
 __global__ void k_transform(size_t n, DevSurface s, double* X, double* Y, double* Z, double* cX, double* cY,
                             double* cZ);
@@ -66,11 +74,11 @@ __global__ void k_surface_step(const DevScheme* sch, int k, const double* knots,
                                DevRays in, DevRays out, unsigned long long* counts, unsigned* err);
 __global__ void k_fused_fp64(const DevScheme* sch, const double* knots, const DevBeam* beams, int n_beams,
                              DevRays in, DevRays out, unsigned long long* counts, unsigned* err, int state_out,
-                             FrameArgs frame);
+                             FrameArgs frame, TileSched ts);
 // kernels_mixed.cu
 __global__ void k_fused_mixed(const DevScheme* sch, const double* knots, const DevBeam* beams, int n_beams,
                               DevRays in, DevRays out, unsigned long long* counts, unsigned* err, int state_out,
-                              FrameArgs frame);
+                              FrameArgs frame, TileSched ts);
 
 // ---- ordering (order.cu) ----
 int reference_order(const DevBeam* h_beams, int n_beams, int n_stages, const DevRays& rays, uint32_t* order,

@@ -271,76 +271,81 @@ __global__ void k_ccd_frame(DevRays rays, FrameArgs f) {
 }
 
 // Fused FP64 trace: the whole surface sequence per ray in registers, the
-// scheme and knot tables in shared memory, a persistent grid striding over
-// the rays.  Bit-identical to k_surface_step.  With a frame, good rays add
+// scheme and knot tables in shared memory, a persistent grid whose warps take
+// tiles of rays (next_tile).  Bit-identical to k_surface_step.  With a frame, good rays add
 // their pixel with warp-aggregated atomics.
 __global__ void __launch_bounds__(256) k_fused_fp64(const DevScheme* __restrict__ g_sch, const double* knots,
                                                     const DevBeam* beams, int n_beams, DevRays in, DevRays out,
                                                     unsigned long long* counts, unsigned* err, int state_out,
-                                                    FrameArgs frame) {
+                                                    FrameArgs frame, TileSched ts) {
     const double* s_knots;
     const DevScheme* sch = stage_scheme(g_sch, knots, s_knots);
     const int ns = sch->n_surfaces;
     const int n_stages = 3 * ns;
-    for (size_t i0 = (size_t)blockIdx.x * blockDim.x; i0 < in.n; i0 += gstride()) {
-        size_t i = i0 + threadIdx.x;
-        bool ev = false, good = false;
-        int key = 0;
-        double outX = 0, outY = 0;
-        if (i < in.n && in.flag[i] == 1) {
-            Ray r{in.X[i], in.Y[i], in.Z[i], in.cX[i], in.cY[i], in.cZ[i]};
-            const double lam = in.lambda[i];
-            const int b = beam_of(beams, n_beams, i);
-            int stage = -1;
-            for (int k = 0; k < ns; ++k) {
-                const DevSurface& s = sch->s[k];
-                f64::transform(s, r);
-                f64::normalize(r.cX, r.cY, r.cZ);
-                if (!s.non_aux) continue;
-                if (!f64::intersect(s, sch->fixes, r)) { stage = 3 * k; break; }
-                if (!f64::aperture_pass(s.type == RTB_SHADE, s.shape, s.size, s.center, r.X, r.Y)) {
-                    stage = 3 * k + 1;
-                    break;
+    const uint64_t tile_rays = 32ull * (uint64_t)ts.rpt;
+    const uint64_t n_tiles = (in.n + tile_rays - 1) / tile_rays;
+    uint64_t tile;
+    while (next_tile(ts, n_tiles, tile)) {
+        for (int j = 0; j < ts.rpt; ++j) {
+            const size_t i = tile * tile_rays + (size_t)j * 32 + (threadIdx.x & 31);
+            bool ev = false, good = false;
+            int key = 0;
+            double outX = 0, outY = 0;
+            if (i < in.n && in.flag[i] == 1) {
+                Ray r{in.X[i], in.Y[i], in.Z[i], in.cX[i], in.cY[i], in.cZ[i]};
+                const double lam = in.lambda[i];
+                const int b = beam_of(beams, n_beams, i);
+                int stage = -1;
+                for (int k = 0; k < ns; ++k) {
+                    const DevSurface& s = sch->s[k];
+                    f64::transform(s, r);
+                    f64::normalize(r.cX, r.cY, r.cZ);
+                    if (!s.non_aux) continue;
+                    if (!f64::intersect(s, sch->fixes, r)) { stage = 3 * k; break; }
+                    if (!f64::aperture_pass(s.type == RTB_SHADE, s.shape, s.size, s.center, r.X, r.Y)) {
+                        stage = 3 * k + 1;
+                        break;
+                    }
+                    long long order = s.order;
+                    if (s.type == RTB_GRATING && beams[b].n_orders > 0) order = beams[b].orders[s.grating_index];
+                    int a = f64::action(s, s_knots, order, lam, r);
+                    if (a == f64::ACT_RANGE) { atomicOr(err, DEV_ERR_OUT_OF_RANGE); stage = -2; break; }
+                    if (a == f64::ACT_LOST) { stage = 3 * k + 2; break; }
+                    f64::normalize(r.cX, r.cY, r.cZ);
                 }
-                long long order = s.order;
-                if (s.type == RTB_GRATING && beams[b].n_orders > 0) order = beams[b].orders[s.grating_index];
-                int a = f64::action(s, s_knots, order, lam, r);
-                if (a == f64::ACT_RANGE) { atomicOr(err, DEV_ERR_OUT_OF_RANGE); stage = -2; break; }
-                if (a == f64::ACT_LOST) { stage = 3 * k + 2; break; }
-                f64::normalize(r.cX, r.cY, r.cZ);
-            }
-            if (stage >= 0) {
-                ev = true;
-                if (sch->renorm_lost) f64::renormalize(r, sch->s[stage / 3].renorm_after);
-                out.flag[i] = 0;
-                out.lost_stage[i] = (uint8_t)stage;
-                key = b * (n_stages + 1) + stage;
-            } else if (stage == -1) {
-                ev = good = true;
-                key = b * (n_stages + 1) + n_stages;
-                if (in.flag != out.flag) {
-                    out.flag[i] = 1;
-                    out.lost_stage[i] = RTB_NOT_LOST;
+                if (stage >= 0) {
+                    ev = true;
+                    if (sch->renorm_lost) f64::renormalize(r, sch->s[stage / 3].renorm_after);
+                    out.flag[i] = 0;
+                    out.lost_stage[i] = (uint8_t)stage;
+                    key = b * (n_stages + 1) + stage;
+                } else if (stage == -1) {
+                    ev = good = true;
+                    key = b * (n_stages + 1) + n_stages;
+                    if (in.flag != out.flag) {
+                        out.flag[i] = 1;
+                        out.lost_stage[i] = RTB_NOT_LOST;
+                    }
                 }
-            }
-            if (stage != -2) {
-                out.X[i] = r.X;
-                out.Y[i] = r.Y;
-                if (state_out) {
-                    out.Z[i] = r.Z;
-                    out.cX[i] = r.cX;
-                    out.cY[i] = r.cY;
-                    out.cZ[i] = r.cZ;
+                if (stage != -2) {
+                    out.X[i] = r.X;
+                    out.Y[i] = r.Y;
+                    if (state_out) {
+                        out.Z[i] = r.Z;
+                        out.cX[i] = r.cX;
+                        out.cY[i] = r.cY;
+                        out.cZ[i] = r.cZ;
+                    }
                 }
+                outX = r.X;
+                outY = r.Y;
             }
-            outX = r.X;
-            outY = r.Y;
+            else if (i < in.n && in.flag != out.flag) {
+                out.flag[i] = in.flag[i];
+            }
+            count_event(ev, key, counts);
+            if (frame.counts) frame_add(good, outX, outY, frame);
         }
-        else if (i < in.n && in.flag != out.flag) {
-            out.flag[i] = in.flag[i];
-        }
-        count_event(ev, key, counts);
-        if (frame.counts) frame_add(good, outX, outY, frame);
     }
 }
 

@@ -221,36 +221,33 @@ __device__ __forceinline__ bool asphere_isect(const DevSurface& s, Ray& r) {
     return true;
 }
 
-__device__ __forceinline__ double toric_func(const DevSurface& s, bool fix_sign, double t, const Ray& r) {
-    double X = fma(t, r.cX, r.X), Y = fma(t, r.cY, r.Y), Z = fma(t, r.cZ, r.Z);
-    double Y2 = Y * Y;
-    double k = s.k1 * s.c * s.c * Y2;
-    double FY = s.c * Y2 * rcp(1.0 + sqrt_(fix_sign ? 1.0 - k : 1.0 + k));
-    return Z - FY - 0.5 * s.cR * (fma(X, X, Z * Z) - FY * FY);
-}
-
-// iter_toric (surface.cu:359-410) in FP64 with fast divisions.
+// Toric surface (iter_toric, surface.cu:359-410): the same function F of the
+// reference (with its 1+k1c^2Y^2 unless RTB_FIX_TORIC_SIGN), solved by
+// Newton from the Z=0 plane point with the analytic derivative
+//   dF/dt = cZ - FY' cY - cR (X cX + Z cZ - FY FY' cY),  FY' = c Y / s,
+// s = sqrt(1 -+ k1 c^2 Y^2) (FY = c Y^2 / (1 + s) has this derivative for
+// either sign), to |dt| < 1e-12 mm in at most six steps.  As in the
+// reference, a ray is lost only when the plane point lies behind it.
 __device__ __forceinline__ bool toric_isect(const DevSurface& s, uint32_t fixes, Ray& r) {
-    const bool fix_sign = (fixes & RTB_FIX_TORIC_SIGN) != 0;
-    const bool fix_step = (fixes & RTB_FIX_TORIC_STEP) != 0;
-    double sn1 = -r.Z * rcp(r.cZ);
-    if (!(sn1 >= 0)) return false;
-    unsigned niter = 0;
-    double Fyn = 0.0, sn;
-    do {
-        sn = sn1;
-        double Fxn = toric_func(s, fix_sign, sn, r);
-        if (fabs(Fyn - Fxn) <= K_ITER_EPS) break;
-        double Fzn = toric_func(s, fix_sign, sn + Fxn, r);
-        double den = Fzn - Fxn;
-        if (fix_step && den == 0.0) { sn1 = sn; break; }
-        sn1 = sn - Fxn * Fxn / den;
-        Fyn = Fxn;
-        ++niter;
-    } while ((fabs(sn1 - sn) >= K_ITER_EPS) && (niter <= K_ITER_MAX));
-    r.X = fma(sn1, r.cX, r.X);
-    r.Y = fma(sn1, r.cY, r.Y);
-    r.Z = fma(sn1, r.cZ, r.Z);
+    const double sgn = (fixes & RTB_FIX_TORIC_SIGN) ? -1.0 : 1.0;
+    double t = -r.Z * rcp(r.cZ);
+    if (!(t >= 0)) return false;
+    const double kc2 = sgn * s.k1 * s.c * s.c;
+    for (int it = 0; it < 6; ++it) {
+        double X = fma(t, r.cX, r.X), Y = fma(t, r.cY, r.Y), Z = fma(t, r.cZ, r.Z);
+        double Y2 = Y * Y;
+        double sq = sqrt_(fma(kc2, Y2, 1.0));
+        double FY = s.c * Y2 * rcp(1.0 + sq);
+        double dFY = s.c * Y * rcp(sq);
+        double F = Z - FY - 0.5 * s.cR * (fma(X, X, Z * Z) - FY * FY);
+        double dF = r.cZ - dFY * r.cY - s.cR * (fma(X, r.cX, Z * r.cZ) - FY * dFY * r.cY);
+        double dt = F * rcp(dF);
+        t -= dt;
+        if (!(fabs(dt) >= 1e-12)) break;
+    }
+    r.X = fma(t, r.cX, r.X);
+    r.Y = fma(t, r.cY, r.Y);
+    r.Z = fma(t, r.cZ, r.Z);
     return true;
 }
 
@@ -404,72 +401,85 @@ __device__ __forceinline__ int action(const DevSurface& s, const double* knots, 
 
 }  // namespace mx
 
-__global__ void __launch_bounds__(256) k_fused_mixed(const DevScheme* __restrict__ g_sch, const double* knots,
+// One surface of the mixed engine on one ray: -1 survived, a stage >= 0 that
+// lost it, -2 a wavelength outside a table.  The reference normalises the
+// direction cosines after every transform and action (beam.cpp:527-571);
+// rotations and the reflection, refraction and grating formulas preserve a
+// unit vector, so here the cosines are normalised once, when a ray is loaded.
+__device__ __forceinline__ int mx_surface(const DevSurface& s, int k, uint32_t fixes, const double* knots,
+                                          const DevBeam* beams, int b, double lam, mx::Ray& r) {
+    mx::transform(s, r);
+    if (!s.non_aux) return -1;
+    if (!mx::intersect(s, fixes, r)) return 3 * k;
+    if (!f64::aperture_pass(s.type == RTB_SHADE, s.shape, s.size, s.center, r.X, r.Y)) return 3 * k + 1;
+    long long order = s.order;
+    if (s.type == RTB_GRATING && beams[b].n_orders > 0) order = beams[b].orders[s.grating_index];
+    int a = mx::action(s, knots, order, lam, r);
+    if (a == 2) return -2;
+    if (a == 1) return 3 * k + 2;
+    return -1;
+}
+
+// Fused mixed-precision trace: one ray per thread at a time, the whole scheme
+// in registers, the scheme and knot tables in shared memory, a persistent
+// grid whose warps take tiles of rays (next_tile).  Blocks of up to 512
+// threads.
+__global__ void __maxnreg__(80) k_fused_mixed(const DevScheme* __restrict__ g_sch, const double* knots,
                                                      const DevBeam* beams, int n_beams, DevRays in, DevRays out,
                                                      unsigned long long* counts, unsigned* err, int state_out,
-                                                     FrameArgs frame) {
+                                                     FrameArgs frame, TileSched ts) {
     const double* s_knots;
     const DevScheme* sch = stage_scheme(g_sch, knots, s_knots);
     const int ns = sch->n_surfaces;
     const int n_stages = 3 * ns;
-    for (size_t i0 = (size_t)blockIdx.x * blockDim.x; i0 < in.n; i0 += gstride()) {
-        size_t i = i0 + threadIdx.x;
-        bool ev = false, good = false;
-        int key = 0;
-        double outX = 0, outY = 0;
-        if (i < in.n && in.flag[i] == 1) {
-            mx::Ray r{in.X[i], in.Y[i], in.Z[i], in.cX[i], in.cY[i], in.cZ[i]};
-            const double lam = in.lambda[i];
-            const int b = beam_of(beams, n_beams, i);
-            int stage = -1;
-            for (int k = 0; k < ns; ++k) {
-                const DevSurface& s = sch->s[k];
-                mx::transform(s, r);
+    const uint64_t tile_rays = 32ull * (uint64_t)ts.rpt;
+    const uint64_t n_tiles = (in.n + tile_rays - 1) / tile_rays;
+    uint64_t tile;
+    while (next_tile(ts, n_tiles, tile)) {
+        for (int j = 0; j < ts.rpt; ++j) {
+            const size_t i = tile * tile_rays + (size_t)j * 32 + (threadIdx.x & 31);
+            bool ev = false, good = false;
+            int key = 0;
+            double outX = 0, outY = 0;
+            if (i < in.n && in.flag[i] == 1) {
+                mx::Ray r{in.X[i], in.Y[i], in.Z[i], in.cX[i], in.cY[i], in.cZ[i]};
                 mx::normalize(r);
-                if (!s.non_aux) continue;
-                if (!mx::intersect(s, sch->fixes, r)) { stage = 3 * k; break; }
-                if (!f64::aperture_pass(s.type == RTB_SHADE, s.shape, s.size, s.center, r.X, r.Y)) {
-                    stage = 3 * k + 1;
-                    break;
+                const double lam = in.lambda[i];
+                const int b = beam_of(beams, n_beams, i);
+                int stage = -1;
+                for (int k = 0; k < ns && stage == -1; ++k) stage = mx_surface(sch->s[k], k, sch->fixes, s_knots, beams, b, lam, r);
+                if (stage == -2) atomicOr(err, DEV_ERR_OUT_OF_RANGE);
+                if (stage >= 0) {
+                    ev = true;
+                    out.flag[i] = 0;
+                    out.lost_stage[i] = (uint8_t)stage;
+                    key = b * (n_stages + 1) + stage;
+                } else if (stage == -1) {
+                    ev = good = true;
+                    key = b * (n_stages + 1) + n_stages;
+                    if (in.flag != out.flag) {
+                        out.flag[i] = 1;
+                        out.lost_stage[i] = RTB_NOT_LOST;
+                    }
                 }
-                long long order = s.order;
-                if (s.type == RTB_GRATING && beams[b].n_orders > 0) order = beams[b].orders[s.grating_index];
-                int a = mx::action(s, s_knots, order, lam, r);
-                if (a == 2) { atomicOr(err, DEV_ERR_OUT_OF_RANGE); stage = -2; break; }
-                if (a == 1) { stage = 3 * k + 2; break; }
-                mx::normalize(r);
-            }
-            if (stage >= 0) {
-                ev = true;
-                if (sch->renorm_lost) mx::normalize(r);
-                out.flag[i] = 0;
-                out.lost_stage[i] = (uint8_t)stage;
-                key = b * (n_stages + 1) + stage;
-            } else if (stage == -1) {
-                ev = good = true;
-                key = b * (n_stages + 1) + n_stages;
-                if (in.flag != out.flag) {
-                    out.flag[i] = 1;
-                    out.lost_stage[i] = RTB_NOT_LOST;
+                if (stage != -2) {
+                    out.X[i] = r.X;
+                    out.Y[i] = r.Y;
+                    if (state_out) {
+                        out.Z[i] = r.Z;
+                        out.cX[i] = r.cX;
+                        out.cY[i] = r.cY;
+                        out.cZ[i] = r.cZ;
+                    }
                 }
+                outX = r.X;
+                outY = r.Y;
+            } else if (i < in.n && in.flag != out.flag) {
+                out.flag[i] = in.flag[i];
             }
-            if (stage != -2) {
-                out.X[i] = r.X;
-                out.Y[i] = r.Y;
-                if (state_out) {
-                    out.Z[i] = r.Z;
-                    out.cX[i] = r.cX;
-                    out.cY[i] = r.cY;
-                    out.cZ[i] = r.cZ;
-                }
-            }
-            outX = r.X;
-            outY = r.Y;
-        } else if (i < in.n && in.flag != out.flag) {
-            out.flag[i] = in.flag[i];
+            count_event(ev, key, counts);
+            if (frame.counts) frame_add(good, outX, outY, frame);
         }
-        count_event(ev, key, counts);
-        if (frame.counts) frame_add(good, outX, outY, frame);
     }
 }
 

@@ -204,9 +204,10 @@ extern "C" RTB_API int rtb_trace_out_noalloc(const rtb_surface* surfaces, size_t
     RTB_CUDA_TRY(cudaMemcpyAsync(d, h_stage, l.counts, cudaMemcpyHostToDevice, s));
     RTB_CUDA_TRY(cudaMemsetAsync(d + l.counts, 0, l.total - l.counts, s));
 
+    const bool mixed = opts->precision == RTB_MIXED;
     size_t smem = fused_smem_bytes((int)n_knots);
     if (smem > (size_t)engine().max_smem_optin) return RTB_BAD_VALUE;
-    auto kern = (opts->precision == RTB_MIXED) ? k_fused_mixed : k_fused_fp64;
+    auto kern = mixed ? k_fused_mixed : k_fused_fp64;
     RTB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
     RTB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem));
@@ -230,11 +231,12 @@ extern "C" RTB_API int rtb_trace_out_noalloc(const rtb_surface* surfaces, size_t
     ro.lambda = out->lambda; ro.flag = out->flag; ro.lost_stage = out->lost_stage; ro.n = out->n;
     unsigned long long* counts_d = reinterpret_cast<unsigned long long*>(d + l.counts);
     unsigned* err_d = reinterpret_cast<unsigned*>(d + l.err);
-    kern<<<grid_for(in->n, 256, per_sm), 256, smem, s>>>(reinterpret_cast<const DevScheme*>(d),
-                                                         reinterpret_cast<const double*>(d + l.knots),
-                                                         reinterpret_cast<const DevBeam*>(d + l.beams),
-                                                         (int)n_beams, ri, ro, counts_d, err_d,
-                                                         opts->state_out ? 1 : 0, frame);
+    // the tile counter shares the zeroed 256-byte error slot
+    unsigned long long* tiles_d = reinterpret_cast<unsigned long long*>(d + l.err + 64);
+    kern<<<grid_for(in->n, 256 * kDefaultRpt, per_sm), 256, smem, s>>>(
+        reinterpret_cast<const DevScheme*>(d), reinterpret_cast<const double*>(d + l.knots),
+        reinterpret_cast<const DevBeam*>(d + l.beams), (int)n_beams, ri, ro, counts_d, err_d,
+        opts->state_out ? 1 : 0, frame, TileSched{tiles_d, kDefaultRpt});
     RTB_CUDA_TRY(cudaGetLastError());
     unsigned long long* counts_h = reinterpret_cast<unsigned long long*>(h_stage + l.counts);
     unsigned err = 0;

@@ -17,6 +17,49 @@ struct Ray {
     double X, Y, Z, cX, cY, cZ;
 };
 
+// The reference's root iterations stop only on convergence or after
+// K_ITER_MAX steps.  A few rays never converge: their iterate falls into an
+// exact cycle (on the C1 echelle's toric fold, 5 of 8.7e7 rays enter a
+// 2-cycle after 5 Steffensen steps) and would hold their warp for 1e5 steps.
+// Each iteration is a pure function of a small state, so once the state's
+// bit pattern repeats after `lam` steps it repeats forever: the remaining
+// steps up to the cap can be skipped in whole periods, and the loop then runs
+// the last (< lam) steps as usual.  The result is the same bits as running
+// every step.  Cycles are found with Brent's algorithm (R. P. Brent, "An
+// improved Monte Carlo factorization algorithm", BIT 20, 1980), armed only
+// after K_CYCLE_FROM steps so converging rays pay one compare per step.
+constexpr unsigned K_CYCLE_FROM = 8;
+
+struct CycleSkip {
+    unsigned long long a = 0, b = 0;  // saved state (bit patterns)
+    unsigned power = 1, lam = 0;
+    bool armed = false;
+
+    // Call after the step that brought the counter to `niter`, with the
+    // state (x, y) the next step starts from; may advance `niter`.
+    __device__ __forceinline__ void step(double x, double y, unsigned& niter) {
+        if (niter < K_CYCLE_FROM) return;
+        const unsigned long long xb = (unsigned long long)__double_as_longlong(x);
+        const unsigned long long yb = (unsigned long long)__double_as_longlong(y);
+        if (!armed) {
+            armed = true;
+            a = xb;
+            b = yb;
+            return;
+        }
+        ++lam;
+        if (xb == a && yb == b) {
+            const unsigned left = K_ITER_MAX + 1 - niter;  // steps until the cap ends the loop
+            niter += left - left % lam;
+        } else if (lam == power) {
+            a = xb;
+            b = yb;
+            power <<= 1;
+            lam = 0;
+        }
+    }
+};
+
 // conic_derivs (rt_cuda_engine_surface.cu:45-61)
 __device__ __forceinline__ void conic_derivs(const DevSurface& s, double X, double Y, double& dFdX, double& dFdY) {
     double r2 = X * X + Y * Y;
@@ -94,6 +137,7 @@ __device__ __forceinline__ bool iter_conic_isect(const DevSurface& s, Ray& r) {
     double s1, s2 = 0.0, Xi = 0, Yi = 0, Zi = 0;
     unsigned niter = 0;
     bool good = true;
+    CycleSkip cyc;
     do {
         s1 = s2;
         Xi = r.X + (s1 + s0) * r.cX;
@@ -113,6 +157,7 @@ __device__ __forceinline__ bool iter_conic_isect(const DevSurface& s, Ray& r) {
         if (fabs(dF) < K_ITER_EPS) { good = false; break; }
         s2 = s1 - F / dF;
         ++niter;
+        cyc.step(s2, 0.0, niter);
     } while ((fabs(s2 - s1) >= K_ITER_EPS) && (niter <= K_ITER_MAX));
     r.X = Xi;
     r.Y = Yi;
@@ -128,6 +173,7 @@ __device__ __forceinline__ bool iter_poly_isect(const DevSurface& s, Ray& r) {
     double s1, s2 = 0.0, Xi = 0, Yi = 0, Zi = 0;
     unsigned niter = 0;
     bool good = true;
+    CycleSkip cyc;
     do {
         s1 = s2;
         Xi = r.X + (s1 + s0) * r.cX;
@@ -144,6 +190,7 @@ __device__ __forceinline__ bool iter_poly_isect(const DevSurface& s, Ray& r) {
         if (fabs(dF) < K_ITER_EPS) { good = false; break; }
         s2 = s1 - F / dF;
         ++niter;
+        cyc.step(s2, 0.0, niter);
     } while ((fabs(s2 - s1) >= K_ITER_EPS) && (niter <= K_ITER_MAX));
     r.X = Xi;
     r.Y = Yi;
@@ -171,6 +218,7 @@ __device__ __forceinline__ bool toric_isect(const DevSurface& s, uint32_t fixes,
     if (!(sn1 >= 0)) return false;
     unsigned niter = 0;
     double Fyn = 0.0, sn;
+    CycleSkip cyc;
     do {
         sn = sn1;
         double Fxn = toric_func(s, fix_sign, sn, r);
@@ -181,6 +229,7 @@ __device__ __forceinline__ bool toric_isect(const DevSurface& s, uint32_t fixes,
         sn1 = sn - Fxn * Fxn / (Fzn - Fxn);
         Fyn = Fxn;
         ++niter;
+        cyc.step(sn1, Fyn, niter);
     } while ((fabs(sn1 - sn) >= K_ITER_EPS) && (niter <= K_ITER_MAX));
     r.X += sn1 * r.cX;
     r.Y += sn1 * r.cY;

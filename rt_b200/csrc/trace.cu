@@ -52,6 +52,7 @@ struct TraceArgs {
     DevBeam* beams;
     unsigned long long* counts;
     unsigned* err;
+    unsigned long long* tiles;  // tile counter of the fused kernels
     size_t counts_len;
     int init(const PreparedScheme& ps, const std::vector<DevBeam>& beams_h, cudaStream_t st) {
         size_t n_beams = beams_h.size();
@@ -68,11 +69,12 @@ struct TraceArgs {
         beams = reinterpret_cast<DevBeam*>(p + off_beams);
         counts = reinterpret_cast<unsigned long long*>(p + off_counts);
         err = reinterpret_cast<unsigned*>(p + off_err);
+        tiles = reinterpret_cast<unsigned long long*>(p + off_err + 64);
         RTB_CUDA_TRY(cudaMemcpyAsync(sch, &ps.sch, sizeof(DevScheme), cudaMemcpyHostToDevice, st));
         RTB_CUDA_TRY(cudaMemcpyAsync(knots, ps.knots.data(), ps.knots.size() * sizeof(double), cudaMemcpyHostToDevice, st));
         RTB_CUDA_TRY(cudaMemcpyAsync(beams, beams_h.data(), n_beams * sizeof(DevBeam), cudaMemcpyHostToDevice, st));
         RTB_CUDA_TRY(cudaMemsetAsync(counts, 0, counts_len * 8, st));
-        RTB_CUDA_TRY(cudaMemsetAsync(err, 0, 4, st));
+        RTB_CUDA_TRY(cudaMemsetAsync(err, 0, 256, st));  // err and the tile counter
         return RTB_OK;
     }
 };
@@ -93,21 +95,11 @@ FrameArgs frame_args(const rtb_trace_opts* o) {
     return f;
 }
 
-int configure_fused(int n_knots) {
-    size_t smem = fused_smem_bytes(n_knots);
-    if (smem > (size_t)engine().max_smem_optin) return RTB_BAD_VALUE;
-    RTB_CUDA_TRY(cudaFuncSetAttribute(k_fused_fp64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    RTB_CUDA_TRY(cudaFuncSetAttribute(k_fused_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    return RTB_OK;
-}
-
 }  // namespace
 
 // Launch the trace kernels of one call (no synchronisation).
 int launch_trace(const PreparedScheme& ps, TraceArgs& a, int n_beams, const rtb_trace_opts& o, const DevRays& in,
                  const DevRays& out, const FrameArgs& frame, cudaStream_t st) {
-    const int threads = (o.block_size > 0) ? o.block_size : 256;
-    if (threads != 128 && threads != 256) return RTB_BAD_VALUE;
     if (o.engine == RTB_ENGINE_PER_SURFACE) {
         if (o.precision != RTB_FP64) return RTB_BAD_VALUE;
         unsigned grid = grid_for(in.n, 256, 8);
@@ -118,17 +110,22 @@ int launch_trace(const PreparedScheme& ps, TraceArgs& a, int n_beams, const rtb_
                                                  a.counts, a.err);
         if (frame.counts) k_ccd_frame<<<grid, 256, 0, st>>>(out, frame);
     } else if (o.engine == RTB_ENGINE_FUSED) {
-        int st2 = configure_fused(ps.sch.n_knots);
-        if (st2 != RTB_OK) return st2;
-        size_t smem = fused_smem_bytes(ps.sch.n_knots);
+        const bool mixed = o.precision == RTB_MIXED;
+        if (!mixed && o.precision != RTB_FP64) return RTB_BAD_VALUE;
+        const int threads = (o.block_size > 0) ? o.block_size : 256;
+        if (threads != 128 && threads != 256 && !(mixed && threads == 512)) return RTB_BAD_VALUE;
+        const int rpt = (o.rays_per_thread > 0) ? o.rays_per_thread : kDefaultRpt;
+        if (rpt < 1 || rpt > 64) return RTB_BAD_VALUE;
+        const size_t smem = fused_smem_bytes(ps.sch.n_knots);
+        if (smem > (size_t)engine().max_smem_optin) return RTB_BAD_VALUE;
+        auto kern = mixed ? k_fused_mixed : k_fused_fp64;
+        RTB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int per_sm = 0;
-        auto kern = (o.precision == RTB_MIXED) ? k_fused_mixed : k_fused_fp64;
-        if (o.precision != RTB_MIXED && o.precision != RTB_FP64) return RTB_BAD_VALUE;
         RTB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
         if (per_sm < 1) per_sm = 1;
-        unsigned grid = grid_for(in.n, threads, per_sm);
+        unsigned grid = grid_for(in.n, threads * rpt, per_sm);
         kern<<<grid, threads, smem, st>>>(a.sch, a.knots, a.beams, n_beams, in, out, a.counts, a.err,
-                                          o.state_out ? 1 : 0, frame);
+                                          o.state_out ? 1 : 0, frame, TileSched{a.tiles, rpt});
     } else {
         return RTB_BAD_VALUE;
     }

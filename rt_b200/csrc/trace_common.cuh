@@ -21,6 +21,18 @@ __device__ __forceinline__ void ccd_coords(double X, double Y, double xsize, dou
     iy = __double2uint_rz((Y + ysize / 2.0) / ypix);
 }
 
+// Work distribution of the persistent fused kernels: a warp takes the next
+// tile of 32*rpt consecutive rays from a global counter (zeroed before the
+// launch) until the rays run out, so warps whose rays were lost early take
+// more tiles and the grid drains evenly.  Ray j*32 + lane of a tile belongs
+// to lane `lane`, which keeps every load and store of the tile coalesced.
+__device__ __forceinline__ bool next_tile(const TileSched& ts, uint64_t n_tiles, uint64_t& tile) {
+    unsigned long long t = 0;
+    if ((threadIdx.x & 31) == 0) t = atomicAdd(ts.next, 1ull);
+    tile = __shfl_sync(0xffffffffu, t, 0);
+    return tile < n_tiles;
+}
+
 __device__ __forceinline__ int beam_of(const DevBeam* beams, int n_beams, uint64_t i) {
     int lo = 0, hi = n_beams - 1;
     while (lo < hi) {

@@ -6,6 +6,7 @@ payloads aside) on the same inputs: positions, direction cosines,
 wavelengths, lost flags, lost stages, counts.
 """
 import ctypes as C
+import os
 
 import numpy as np
 import pytest
@@ -103,6 +104,52 @@ def test_trace_matches_oracle(name, engine, fixes):
     assert (stats_d.ray_surfaces, stats_d.n_good, stats_d.failed_beam, stats_d.failed_stage) == \
         (stats_o.ray_surfaces, stats_o.n_good, stats_o.failed_beam, stats_o.failed_stage)
     assert_rays_equal(dev.to_host(O.HostRays), ora)
+
+
+def _cycle_rays():
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "toric_cycles.npz"))
+    st = z["state"]
+    r = O.HostRays(st.shape[1])
+    for f, row in zip(E.FIELDS[:6], st):
+        getattr(r, f)[:] = row
+    r.lambda_[:] = 0.5
+    return r, z
+
+
+@pytest.mark.parametrize("fixes", FIXES)
+def test_toric_cycles_match_oracle(fixes):
+    """Rays of the C1 fold whose toric iteration falls into a cycle and runs
+    to the iteration cap: the CUDA engine skips whole periods of the cycle,
+    the oracle runs every step; results must be the same bits."""
+    rays, z = _cycle_rays()
+    assert z["cycling_fixed"].sum() >= 1 and z["cycling_literal"].sum() >= 1
+    p = np.zeros(16)
+    p[:4] = z["params"][:4]
+    out = []
+    for fn in _pair("surface_intersection_fix"):
+        r = rays.copy()
+        nb = C.c_size_t(0)
+        st = fn(ffi.TORIC, ffi.dptr(p), C.c_size_t(r.n), *(ffi.dptr(getattr(r, f)) for f in E.FIELDS[:6]),
+                C.byref(nb), ffi.vptr(r.flag), C.c_uint(fixes))
+        assert st == ffi.OK
+        out.append((r, nb.value))
+    (a, na), (b, nb_) = out
+    assert na == nb_
+    for f in ("X", "Y", "Z"):
+        assert same_bits(getattr(a, f), getattr(b, f)), f
+    assert np.array_equal(a.flag, b.flag)
+    # the same rays through the trace engines, as a one-surface scheme
+    specs = [S.SurfaceSpec(ffi.TORIC, ffi.MIRROR, params=tuple(z["params"][:4]), size=(1000.0, 0.0))]
+    beams = [S.make_beam(0, rays.n, 1, 1.0, (0.5, 0.5), 1)]
+    cs_o, cs_d = S.to_c(specs, O.spline_init), S.to_c(specs, E.spline_init)
+    ora = rays.copy()
+    st_o, stats_o, _ = O.trace(cs_o.surfaces, beams, ora, fixes=fixes)
+    for engine in (ffi.ENGINE_PER_SURFACE, ffi.ENGINE_FUSED):
+        dev = E.DeviceRays.from_host(rays)
+        st_d, stats_d = E.trace(cs_d.surfaces, beams, dev, E.opts(engine=engine, fixes=fixes))
+        assert st_d == st_o
+        assert stats_d.ray_surfaces == stats_o.ray_surfaces
+        assert_rays_equal(dev.to_host(O.HostRays), ora)
 
 
 def test_fused_writes_only_xy_when_asked():

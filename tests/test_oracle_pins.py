@@ -109,3 +109,85 @@ def test_no_intersections_status():
     if H.harness("cpu") is not None:
         rc, _ = H.run_trace("cpu", specs, [], rays)
         assert rc == ffi.NO_INTERSECTIONS
+
+
+def _toric_with_cycle_skip(r, c, k1, cR, fix_sign, fix_step):
+    """Scalar restatement of the CUDA engine's toric iteration: the
+    reference's Steffensen loop (rt_cuda_engine_surface.cu:359-410) plus the
+    engine's exact skip of whole periods once the state (sn1, Fyn) repeats
+    bit for bit (Brent's cycle finding, armed after 8 steps)."""
+    import math
+    import struct
+    X0, Y0, Z0, cX, cY, cZ = r
+    sgn = -1.0 if fix_sign else 1.0
+
+    def F(t):
+        X, Y, Z = X0 + t * cX, Y0 + t * cY, Z0 + t * cZ
+        Y2 = Y * Y
+        FY = c * Y2 / (1.0 + math.sqrt(1.0 + sgn * k1 * c * c * Y2))
+        return Z - FY - 0.5 * cR * (X * X + Z * Z - FY * FY)
+
+    bits = lambda v: struct.pack("<d", v)  # noqa: E731
+    sn1 = -Z0 / cZ
+    if not sn1 >= 0:
+        return None, 0
+    niter, Fyn, skipped = 0, 0.0, 0
+    saved, power, lam, armed = None, 1, 0, False
+    while True:
+        sn = sn1
+        Fxn = F(sn)
+        if abs(Fyn - Fxn) <= 1e-7:
+            break
+        Fzn = F(sn + Fxn)
+        if fix_step and Fzn - Fxn == 0.0:
+            sn1 = sn
+            break
+        sn1 = sn - Fxn * Fxn / (Fzn - Fxn)
+        Fyn = Fxn
+        niter += 1
+        if niter >= 8:
+            key = bits(sn1) + bits(Fyn)
+            if not armed:
+                armed, saved = True, key
+            else:
+                lam += 1
+                if key == saved:
+                    left = 100000 + 1 - niter
+                    niter += left - left % lam
+                    skipped += left - left % lam
+                elif lam == power:
+                    saved, power, lam = key, power * 2, 0
+        if not (abs(sn1 - sn) >= 1e-7 and niter <= 100000):
+            break
+    return (X0 + sn1 * cX, Y0 + sn1 * cY, Z0 + sn1 * cZ), skipped
+
+
+@pytest.mark.parametrize("fixes", [0, ffi.FIX_TORIC_SIGN | ffi.FIX_TORIC_STEP])
+def test_toric_cycle_skip_equals_full_iteration(fixes):
+    """The rays of the C1 fold that cycle until the iteration cap
+    (tests/golden/toric_cycles.npz): skipping whole periods gives the bits of
+    the oracle's full 1e5-step loop."""
+    import ctypes as C
+    import os
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "toric_cycles.npz"))
+    st = z["state"]
+    n = st.shape[1]
+    r = O.HostRays(n)
+    for f, row in zip(O.HostRays.FIELDS[:6], st):
+        getattr(r, f)[:] = row
+    p = np.zeros(16)
+    p[:4] = z["params"][:4]
+    nb = C.c_size_t(0)
+    assert O.load().oracle_surface_intersection_fix(
+        ffi.TORIC, ffi.dptr(p), C.c_size_t(n), *(ffi.dptr(getattr(r, f)) for f in O.HostRays.FIELDS[:6]),
+        C.byref(nb), ffi.vptr(r.flag), C.c_uint(fixes)) == ffi.OK
+    c, k, _, cR = z["params"][:4]
+    n_skipped = 0
+    for i in range(n):
+        xyz, skipped = _toric_with_cycle_skip(st[:, i], c, k + 1.0, cR, bool(fixes & ffi.FIX_TORIC_SIGN),
+                                              bool(fixes & ffi.FIX_TORIC_STEP))
+        n_skipped += skipped > 0
+        assert xyz is not None and r.flag[i] == 1
+        assert same_bits(np.array(xyz), np.array([r.X[i], r.Y[i], r.Z[i]])), i
+    cyc = z["cycling_fixed"] if fixes else z["cycling_literal"]
+    assert n_skipped == int(cyc.sum()) >= 1
