@@ -8,11 +8,15 @@ resident in HBM (5.7 GB of input, far larger than the 126 MB L2), with the
 CCD frame counts accumulated.  A ray-surface is one ray through one non-Aux
 surface; lost rays count up to the surface that loses them.
 
-Engines timed: the plain FP64 per-surface engine (one kernel per surface),
-the fused FP64 kernel and the fused mixed-precision kernel (the headline
-`value`).  `e2e` runs the same trace through rtb_trace_host on page-locked
-host arrays (copies in and out inside the timed region).  `cpu_baseline` is
-the CPU oracle on the host cores over a bounded sample of the same rays.
+Engines timed: the plain FP64 per-surface engine (one kernel per surface,
+rtb_trace_out), the fused FP64 kernel and the fused mixed-precision kernel
+(the headline `value`), each fused kernel as a plan (rtb_plan_*: rays
+resident in HBM, one CUDA graph launch per step, launch configuration chosen
+by the autotuner first).  `e2e` runs the same trace through rtb_trace_host on
+page-locked host arrays (copies in and out inside the timed region).
+`cpu_baseline` is the CPU oracle on the host cores over a bounded sample of
+the same rays.  `c3_batched` is C3: 512 beams of uneven size, wavelength,
+field angle and order through the same scheme in one graph launch.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 """
@@ -43,12 +47,13 @@ FIXES = 3  # RTB_FIX_TORIC_SIGN | RTB_FIX_TORIC_STEP (the toric f
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--rays-per-lambda", type=int, default=0, help="override (default: 1e8 rays total)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-c3", action="store_true")
     p.add_argument("--engines", default="per_surface,fused_fp64,fused_mixed")
     return p.parse_args()
 
@@ -82,7 +87,7 @@ class Clocks:
         try:
             self.f = tempfile.NamedTemporaryFile("w+", delete=False)
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                          "--format=csv,noheader,nounits", "-lms", "50"], stdout=self.f,
                                          stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -190,6 +195,7 @@ def main():
     cs = S.to_c(S.echelle(), E.spline_init)
     surf = cs.surfaces
     rays_in = E.generate(beams, n)
+    torch.cuda.synchronize()  # generated on the library's stream
     out = E.DeviceRays(n)
     ccd = S.ccd(S.C1_CCD)
     counts = torch.zeros(int(ccd.xdim) * int(ccd.ydim), dtype=torch.int32, device="cuda")
@@ -202,7 +208,10 @@ def main():
     s_arr = (ffi.Surface * len(surf))(*surf)
     b_arr = (ffi.Beam * len(beams))(*beams)
     rin, rout = rays_in.struct(), out.struct()
-    stream = torch.cuda.current_stream()
+    # a stream of its own: a NULL handle (torch's default stream) would send
+    # the library's work to the library's own stream, outside the events
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
 
     def step(o):
         stats = ffi.TraceStats()
@@ -233,54 +242,109 @@ def main():
     engines = {}
     mk = lambda eng, prec: E.opts(engine=eng, precision=prec, fixes=FIXES, state_out=0, ccd=ccd, counts=counts,
                                   n_outside=outside)
-    plan = [("per_surface", ffi.ENGINE_PER_SURFACE, ffi.FP64), ("fused_fp64", ffi.ENGINE_FUSED, ffi.FP64),
-            ("fused_mixed", ffi.ENGINE_FUSED, ffi.MIXED)]
+
+    def traced(st):
+        # beams whose every ray is lost are reported (first one in stats), the
+        # others traced: only a failure of the call itself stops the bench
+        if st not in (ffi.OK, ffi.NO_INTERSECTIONS, ffi.NO_GOOD_RAYS):
+            ffi.check(st, "rtb_plan_run")
+
+    def timed_plan(plan, K, W):
+        for _ in range(W):
+            plan.run(C.c_void_p(stream.cuda_stream))
+        traced(plan.result()[0])
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(K):
+            plan.run(C.c_void_p(stream.cuda_stream))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        if world > 1:
+            t = torch.tensor([ms], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ms = float(t.item())
+        st, stats = plan.result()
+        traced(st)
+        return ms / K, stats
+
     want = set(args.engines.split(","))
     head = None
     clocks = None
-    for name, eng, prec in plan:
-        if name not in want:
-            continue
-        o = mk(eng, prec)
+    plans = {}
+    # the plain FP64 per-surface engine: one kernel per surface (rtb_trace_out)
+    if "per_surface" in want:
+        o = mk(ffi.ENGINE_PER_SURFACE, ffi.FP64)
         try:
             step(o)
+            ms, stats = timed(o, max(2, args.steps // 4), 1)
+            engines["per_surface"] = {"ms_per_step": ms, "value": stats.ray_surfaces * world / (ms * 1e-3),
+                                      "ray_surfaces_per_step": stats.ray_surfaces, "n_good": stats.n_good,
+                                      "launch": "rtb_trace_out, 7 surface kernels + frame kernel"}
+        except RuntimeError as e:
+            engines["per_surface"] = {"error": str(e)}
+    # the fused kernels: a plan each (rays generated in HBM once, one graph
+    # launch per step, launch configuration from the autotuner)
+    for name, prec in (("fused_fp64", ffi.FP64), ("fused_mixed", ffi.MIXED)):
+        if name not in want:
+            continue
+        try:
+            plan = E.Plan(surf, beams, mk(ffi.ENGINE_FUSED, prec))
+            table = plan.autotune(reps=2)
+            block, rpt, _ = plan.config()
+            if name == "fused_mixed" or "fused_mixed" not in want:
+                with Clocks(local) as ck:
+                    ms, stats = timed_plan(plan, args.steps, args.warmup)
+                clocks = ck.summary()
+            else:
+                ms, stats = timed_plan(plan, max(2, args.steps // 4), 1)
         except RuntimeError as e:
             engines[name] = {"error": str(e)}
             continue
-        if name == "fused_mixed" or (head is None and name == "fused_fp64"):
-            with Clocks(local) as ck:
-                ms, stats = timed(o, args.steps, args.warmup)
-            clocks = ck.summary()
-        else:
-            ms, stats = timed(o, max(2, args.steps // 2), 1)
-        rate = stats.ray_surfaces * world / (ms * 1e-3)
-        engines[name] = {"ms_per_step": ms, "value": rate, "ray_surfaces_per_step": stats.ray_surfaces,
-                         "n_good": stats.n_good}
-        if name in ("fused_mixed", "fused_fp64"):
-            head = name if (head is None or name == "fused_mixed") else head
+        plans[name] = plan
+        engines[name] = {"ms_per_step": ms, "value": stats.ray_surfaces * world / (ms * 1e-3),
+                         "ray_surfaces_per_step": stats.ray_surfaces, "n_good": stats.n_good,
+                         "launch": f"rtb_plan_run (CUDA graph), block {block} x {rpt} rays/thread (autotuned)",
+                         "autotune_ms": {f"{b}x{r}": round(t, 4) for b, r, t in table}}
+        head = name if (head is None or name == "fused_mixed") else head
     if head is None and "value" in engines.get("per_surface", {}):
         head = "per_surface"
     if head is None:
         raise SystemExit("no engine ran")
     hv = engines[head]
 
-    # accuracy of the mixed kernel against the FP64 engine on the same rays
+    # accuracy of the mixed kernel against the FP64 kernel on the same rays
+    # (the two plans generate identical rays from the same beam table)
     accuracy = None
-    if "value" in engines.get("fused_mixed", {}) and "value" in engines.get("fused_fp64", {}):
+    if "fused_mixed" in plans and "fused_fp64" in plans:
         from rt_b200 import metrics
-        ref = E.DeviceRays(n)
-        rref = ref.struct()
-        o64 = E.opts(engine=ffi.ENGINE_FUSED, precision=ffi.FP64, fixes=FIXES, state_out=0)
-        omx = E.opts(engine=ffi.ENGINE_FUSED, precision=ffi.MIXED, fixes=FIXES, state_out=0)
-        stats = ffi.TraceStats()
-        ffi.check(L.rtb_trace_out(s_arr, len(surf), b_arr, len(beams), C.byref(o64), C.byref(rin), C.byref(rref),
-                                  C.byref(stats), C.c_void_p(stream.cuda_stream)))
-        ffi.check(L.rtb_trace_out(s_arr, len(surf), b_arr, len(beams), C.byref(omx), C.byref(rin), C.byref(rout),
-                                  C.byref(stats), C.c_void_p(stream.cuda_stream)))
-        torch.cuda.synchronize()
-        accuracy = metrics.ccd_error(out.X, out.Y, out.flag, ref.X, ref.Y, ref.flag, ccd.xsize, ccd.ysize,
+        a = E.device_view(plans["fused_mixed"].rays()[1])
+        b = E.device_view(plans["fused_fp64"].rays()[1])
+        accuracy = metrics.ccd_error(a["X"], a["Y"], a["flag"], b["X"], b["Y"], b["flag"], ccd.xsize, ccd.ysize,
                                      ccd.xpix, ccd.ypix)
-        del ref
+    for p_ in plans.values():
+        p_.destroy()
+    plans.clear()
+
+    # C3: 512 beams of uneven size, wavelength, field angle and order in one
+    # graph launch of the mixed kernel, launch configuration autotuned
+    c3 = None
+    if not args.no_c3 and "fused_mixed" in want:
+        b3 = S.c3_beams()
+        plan = E.Plan(surf, b3, mk(ffi.ENGINE_FUSED, ffi.MIXED))
+        table = plan.autotune(reps=3)
+        block, rpt, n3 = plan.config()
+        ms3, st3 = timed_plan(plan, args.steps, args.warmup)
+        cnt = plan.counts()
+        c3 = {"beams": len(b3), "n_rays": n3, "beams_with_good_rays": int((cnt[:, -1] > 0).sum()), "ray_surfaces_per_run": st3.ray_surfaces, "n_good": st3.n_good,
+              "ms_per_run": ms3, "value": st3.ray_surfaces * world / (ms3 * 1e-3), "unit": UNIT,
+              "config": {"block_size": block, "rays_per_thread": rpt},
+              "autotune_ms": {f"{b}x{r}": round(t, 4) for b, r, t in table},
+              "how": "rtb_plan_run: one CUDA graph (counter clear, fused mixed kernel, counter copy) per run"}
+        plan.destroy()
 
     # roofline of the headline kernel (HBM view): algorithmic bytes per launch
     # = 57 B read (X,Y,Z,cX,cY,cZ,lambda,flag) + 18 B written (X,Y,flag,
@@ -312,8 +376,8 @@ def main():
             times.append(time.perf_counter() - t0)
             ffi.check(st, "rtb_trace_host")
         t = float(np.median(times[2:]))
-        e2e = {"value": stats.ray_surfaces / t, "unit": UNIT, "h2d_bytes_per_step": n * 57,
-               "d2h_bytes_per_step": n * 18, "seconds_per_step": t,
+        e2e = {"value": stats.ray_surfaces / t, "unit": UNIT, "h2d_bytes_per_step": n * (7 * 8 + 1 + 1),
+               "d2h_bytes_per_step": n * (2 * 8 + 1 + 1), "seconds_per_step": t,
                "how": "rtb_trace_host on page-locked host arrays, wall clock, median of steps"}
         h.free()
 
@@ -332,6 +396,7 @@ def main():
                 "speedup_vs_plain_fp64": (hv["value"] / engines["per_surface"]["value"])
                 if "per_surface" in engines and "value" in engines["per_surface"] else None,
                 "accuracy_vs_fp64": accuracy,
+                "c3_batched": c3,
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
                 "gpu_launches": args.steps * 1}
         print(json.dumps(line), flush=True)

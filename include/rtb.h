@@ -314,6 +314,67 @@ RTB_API int rtb_ccd_frame(const rtb_rays* rays, const rtb_ccd* ccd, uint32_t* co
 RTB_API int rtb_reference_order(const rtb_beam* beams, size_t n_beams, size_t n_stages, const rtb_rays* rays,
                         uint32_t* order, void* stream);
 
+/* =========================================================================
+ * 3. Plans: many beams of uneven size, wavelength, field angle and order
+ *    traced by one graph launch, with a launch-configuration autotuner.  No
+ *    counterpart in the reference; Scheme::run's loop over ranges
+ *    (scheme.cpp:983-1055) maps to one plan whose beams are the ranges.
+ *    A plan is used by one host thread at a time.
+ * ========================================================================= */
+typedef struct rtb_plan rtb_plan;
+
+/* One measured launch configuration (rtb_plan_autotune). */
+typedef struct {
+    int32_t block_size;      /* threads per block */
+    int32_t rays_per_thread; /* a warp takes tiles of 32 x rays_per_thread rays */
+    double ms;               /* mean device time of one run */
+} rtb_tune_entry;
+
+/* Prepare a plan on the current device: the scheme and the beam table in
+ * device memory, the rays of all beams generated once (as
+ * rtb_generate_beams), output arrays, the loss counters and page-locked host
+ * copies of them.  opts is copied; opts->engine must be RTB_ENGINE_FUSED.
+ * When opts->ccd and opts->counts are set, every run adds its good rays to
+ * that frame (the plan never clears it).  block_size / rays_per_thread 0
+ * take the configuration an earlier rtb_plan_autotune chose for the same
+ * scheme, precision, frame use and ray count in this process, else the
+ * defaults (256 x 2). */
+RTB_API int rtb_plan_create(const rtb_surface* surfaces, size_t n_surfaces, const rtb_beam* beams, size_t n_beams,
+                            const rtb_trace_opts* opts, rtb_plan** plan);
+/* One trace of the plan's rays as a CUDA graph launched on `stream` (NULL:
+ * the plan's own stream): clear the counters, run the fused kernel, copy the
+ * counters to the host.  The graph is captured on the first run and again
+ * after the launch configuration changes.  Asynchronous.  The generated rays
+ * are read, not modified; results go to the plan's output arrays. */
+RTB_API int rtb_plan_run(rtb_plan* plan, void* stream);
+/* Waits for the last run; its status and statistics as rtb_trace returns them
+ * (RTB_NO_INTERSECTIONS / RTB_NO_GOOD_RAYS name the first beam that lost
+ * every ray; the other beams are traced all the same). */
+RTB_API int rtb_plan_result(rtb_plan* plan, rtb_trace_stats* stats);
+/* Per-(beam, stage) counters of the last run, as rtb_trace_opts.counts
+ * describes them: counts[b * (3 * n_surfaces + 1) + s] rays of beam b lost at
+ * stage s (3 per surface: intersection, aperture, action), then the rays of
+ * beam b that reached the end.  Waits for the last run.  capacity is in
+ * entries; *n_entries (may be NULL) receives the number available. */
+RTB_API int rtb_plan_counts(rtb_plan* plan, uint64_t* counts, size_t capacity, size_t* n_entries);
+/* Device arrays of the plan: `in` the generated rays, `out` the output of the
+ * last run (X, Y, flag, lost_stage; every state array with opts->state_out;
+ * out->lambda is in->lambda).  Either may be NULL. */
+RTB_API int rtb_plan_rays(const rtb_plan* plan, rtb_rays* in, rtb_rays* out);
+/* Time block_size {128, 256, 512 (RTB_MIXED only)} x rays_per_thread
+ * {1, 2, 4, 8}: one untimed run, then `reps` runs, each configuration into a
+ * private frame so the plan's frame is untouched.  The fastest becomes the
+ * plan's configuration and the one later plans of the same key start with.
+ * table (capacity entries, may be NULL) receives the measurements,
+ * *n_entries (may be NULL) their number.  Synchronous. */
+RTB_API int rtb_plan_autotune(rtb_plan* plan, int reps, rtb_tune_entry* table, size_t capacity, size_t* n_entries);
+/* Set the launch configuration explicitly (RTB_BAD_VALUE if unsupported). */
+RTB_API int rtb_plan_set_config(rtb_plan* plan, int32_t block_size, int32_t rays_per_thread);
+/* The plan's launch configuration and ray count. */
+RTB_API int rtb_plan_config(const rtb_plan* plan, int32_t* block_size, int32_t* rays_per_thread, uint64_t* n_rays);
+/* Release everything the plan holds, after its work has finished. */
+RTB_API int rtb_plan_destroy(rtb_plan* plan);
+
 #ifdef __cplusplus
 }
 #endif

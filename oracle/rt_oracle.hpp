@@ -53,7 +53,7 @@ constexpr size_t ITER_MAX = 100000;
 constexpr int RTO_MAX_POLY = 10;   // MAX_POLY_COEFFS, common-lib/surface.h:14
 
 // ---------------------------------------------------------------------------
-// Flags for reference behaviours that are bugs (SURVEY quirk ledger).  The
+// Flags for reference behaviours that are bugs.  The
 // default (0) reproduces the reference; each bit switches one to the
 // mathematically correct form.
 enum QuirkFix : uint32_t {

@@ -25,6 +25,7 @@ SOURCES = {
     "order.cu": [],
     "kernels_mixed.cu": ["--fmad=true"],
     "noalloc.cu": ["--fmad=false"],
+    "plan.cu": ["--fmad=false"],
 }
 
 

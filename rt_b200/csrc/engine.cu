@@ -212,11 +212,6 @@ static void spline_second_derivatives(size_t N, const double* x, const double* y
 
 namespace {
 
-struct Lock {
-    std::lock_guard<std::mutex> g;
-    Lock() : g(engine().mu) {}
-};
-
 // Device copies of up to 8 double arrays and one flag array, from one pool
 // allocation.
 struct Staged {

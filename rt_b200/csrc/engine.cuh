@@ -71,4 +71,59 @@ struct DevBuf {
     }
 };
 
+// ---- trace plumbing shared by the C ABI files (trace.cu) ----
+
+struct Lock {
+    std::lock_guard<std::mutex> g;
+    Lock() : g(engine().mu) {}
+};
+
+// Everything a trace launch reads, in one pool allocation.
+struct TraceArgs {
+    DevBuf buf;
+    DevScheme* sch;
+    double* knots;
+    DevBeam* beams;
+    unsigned long long* counts;
+    unsigned* err;
+    unsigned long long* tiles;  // tile counter of the fused kernels
+    size_t counts_len;
+    int init(const PreparedScheme& ps, const std::vector<DevBeam>& beams_h, cudaStream_t st) {
+        size_t n_beams = beams_h.size();
+        counts_len = n_beams * (size_t)(3 * ps.sch.n_surfaces + 1);
+        size_t off_knots = (sizeof(DevScheme) + 255) / 256 * 256;
+        size_t off_beams = off_knots + (ps.knots.size() * sizeof(double) + 255) / 256 * 256;
+        size_t off_counts = off_beams + (n_beams * sizeof(DevBeam) + 255) / 256 * 256;
+        size_t off_err = off_counts + (counts_len * 8 + 255) / 256 * 256;
+        int s = buf.alloc(off_err + 256, st);
+        if (s != RTB_OK) return s;
+        char* p = buf.as<char>();
+        sch = reinterpret_cast<DevScheme*>(p);
+        knots = reinterpret_cast<double*>(p + off_knots);
+        beams = reinterpret_cast<DevBeam*>(p + off_beams);
+        counts = reinterpret_cast<unsigned long long*>(p + off_counts);
+        err = reinterpret_cast<unsigned*>(p + off_err);
+        tiles = reinterpret_cast<unsigned long long*>(p + off_err + 64);
+        RTB_CUDA_TRY(cudaMemcpyAsync(sch, &ps.sch, sizeof(DevScheme), cudaMemcpyHostToDevice, st));
+        RTB_CUDA_TRY(cudaMemcpyAsync(knots, ps.knots.data(), ps.knots.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+        RTB_CUDA_TRY(cudaMemcpyAsync(beams, beams_h.data(), n_beams * sizeof(DevBeam), cudaMemcpyHostToDevice, st));
+        RTB_CUDA_TRY(cudaMemsetAsync(counts, 0, counts_len * 8, st));
+        RTB_CUDA_TRY(cudaMemsetAsync(err, 0, 256, st));  // err and the tile counter
+        return RTB_OK;
+    }
+};
+
+DevRays dev_rays(const rtb_rays* r);
+// Beam table for the trace kernels; rays of beam b are [first_ray, first_ray + n_rays) < n_rays, in order.
+int check_beams(const rtb_beam* beams, size_t n_beams, size_t n_rays, std::vector<DevBeam>& out);
+// Beam table for the generator; *total is the end of the last beam.
+int gen_beams(const rtb_beam* beams, size_t n_beams, size_t n_rays, std::vector<GenBeam>& out, uint64_t* total);
+FrameArgs frame_args(const rtb_trace_opts* o);
+// Launch the trace kernels of one call (no synchronisation).
+int launch_trace(const PreparedScheme& ps, TraceArgs& a, int n_beams, const rtb_trace_opts& o, const DevRays& in,
+                 const DevRays& out, const FrameArgs& frame, cudaStream_t st);
+// Status and statistics from the per-(beam, stage) counts.
+int trace_result(const PreparedScheme& ps, const unsigned long long* counts, unsigned err, int n_beams,
+                 rtb_trace_stats* stats);
+
 }  // namespace rtb

@@ -8,13 +8,6 @@
 
 namespace rtb {
 
-namespace {
-
-struct Lock {
-    std::lock_guard<std::mutex> g;
-    Lock() : g(engine().mu) {}
-};
-
 DevRays dev_rays(const rtb_rays* r) {
     DevRays d;
     d.X = r->X; d.Y = r->Y; d.Z = r->Z; d.cX = r->cX; d.cY = r->cY; d.cZ = r->cZ;
@@ -44,41 +37,6 @@ int check_beams(const rtb_beam* beams, size_t n_beams, size_t n_rays, std::vecto
     return RTB_OK;
 }
 
-// Everything a trace launch reads, in one pool allocation.
-struct TraceArgs {
-    DevBuf buf;
-    DevScheme* sch;
-    double* knots;
-    DevBeam* beams;
-    unsigned long long* counts;
-    unsigned* err;
-    unsigned long long* tiles;  // tile counter of the fused kernels
-    size_t counts_len;
-    int init(const PreparedScheme& ps, const std::vector<DevBeam>& beams_h, cudaStream_t st) {
-        size_t n_beams = beams_h.size();
-        counts_len = n_beams * (size_t)(3 * ps.sch.n_surfaces + 1);
-        size_t off_knots = (sizeof(DevScheme) + 255) / 256 * 256;
-        size_t off_beams = off_knots + (ps.knots.size() * sizeof(double) + 255) / 256 * 256;
-        size_t off_counts = off_beams + (n_beams * sizeof(DevBeam) + 255) / 256 * 256;
-        size_t off_err = off_counts + (counts_len * 8 + 255) / 256 * 256;
-        int s = buf.alloc(off_err + 256, st);
-        if (s != RTB_OK) return s;
-        char* p = buf.as<char>();
-        sch = reinterpret_cast<DevScheme*>(p);
-        knots = reinterpret_cast<double*>(p + off_knots);
-        beams = reinterpret_cast<DevBeam*>(p + off_beams);
-        counts = reinterpret_cast<unsigned long long*>(p + off_counts);
-        err = reinterpret_cast<unsigned*>(p + off_err);
-        tiles = reinterpret_cast<unsigned long long*>(p + off_err + 64);
-        RTB_CUDA_TRY(cudaMemcpyAsync(sch, &ps.sch, sizeof(DevScheme), cudaMemcpyHostToDevice, st));
-        RTB_CUDA_TRY(cudaMemcpyAsync(knots, ps.knots.data(), ps.knots.size() * sizeof(double), cudaMemcpyHostToDevice, st));
-        RTB_CUDA_TRY(cudaMemcpyAsync(beams, beams_h.data(), n_beams * sizeof(DevBeam), cudaMemcpyHostToDevice, st));
-        RTB_CUDA_TRY(cudaMemsetAsync(counts, 0, counts_len * 8, st));
-        RTB_CUDA_TRY(cudaMemsetAsync(err, 0, 256, st));  // err and the tile counter
-        return RTB_OK;
-    }
-};
-
 FrameArgs frame_args(const rtb_trace_opts* o) {
     FrameArgs f;
     std::memset(&f, 0, sizeof(f));
@@ -95,9 +53,46 @@ FrameArgs frame_args(const rtb_trace_opts* o) {
     return f;
 }
 
-}  // namespace
+int gen_beams(const rtb_beam* beams, size_t n_beams, size_t n_rays, std::vector<GenBeam>& gb, uint64_t* total_out) {
+    if (!beams || n_beams == 0) return RTB_BAD_VALUE;
+    gb.resize(n_beams);
+    uint64_t prev_end = 0, total = 0;
+    for (size_t b = 0; b < n_beams; ++b) {
+        const rtb_beam& in = beams[b];
+        if (in.shape != RTB_CIRCLE || in.n_lambda == 0 || in.first_ray < prev_end || in.first_ray + in.n_rays > n_rays)
+            return RTB_BAD_VALUE;
+        prev_end = in.first_ray + in.n_rays;
+        total = prev_end;
+        GenBeam& g = gb[b];
+        g.first_ray = in.first_ray;
+        g.n_rays = in.n_rays;
+        g.n_lambda = in.n_lambda;
+        g.seed = in.seed;
+        for (int i = 0; i < 3; ++i) {
+            g.disk[i] = in.disk[i];
+            g.center[i] = in.center[i];
+        }
+        g.range[0] = in.range[0];
+        g.range[1] = in.range[1];
+        g.d_lambda = (in.n_lambda > 1) ? (in.range[1] - in.range[0]) / (in.n_lambda - 1) : 0.0;
+        // field direction (tan fx, tan fy, 1) normalised as Beam::Normalize does
+        double cx = std::tan(in.field[0]), cy = std::tan(in.field[1]), cz = 1.0;
+        double acX = std::fabs(cx), acY = std::fabs(cy), acZ = std::fabs(cz), norm;
+        if (acX >= acY) {
+            if (acX >= acZ) norm = acX * std::sqrt(1.0 + acY * acY / acX / acX + acZ * acZ / acX / acX);
+            else norm = acZ * std::sqrt(1.0 + acX * acX / acZ / acZ + acY * acY / acZ / acZ);
+        } else {
+            if (acY >= acZ) norm = acY * std::sqrt(1.0 + acX * acX / acY / acY + acZ * acZ / acY / acY);
+            else norm = acZ * std::sqrt(1.0 + acX * acX / acZ / acZ + acY * acY / acZ / acZ);
+        }
+        g.c0[0] = cx / norm;
+        g.c0[1] = cy / norm;
+        g.c0[2] = cz / norm;
+    }
+    *total_out = total;
+    return RTB_OK;
+}
 
-// Launch the trace kernels of one call (no synchronisation).
 int launch_trace(const PreparedScheme& ps, TraceArgs& a, int n_beams, const rtb_trace_opts& o, const DevRays& in,
                  const DevRays& out, const FrameArgs& frame, cudaStream_t st) {
     if (o.engine == RTB_ENGINE_PER_SURFACE) {
@@ -133,15 +128,14 @@ int launch_trace(const PreparedScheme& ps, TraceArgs& a, int n_beams, const rtb_
     return RTB_OK;
 }
 
-// Status and statistics from the per-(beam, stage) counts.
-int trace_result(const PreparedScheme& ps, const std::vector<unsigned long long>& counts, unsigned err, int n_beams,
+int trace_result(const PreparedScheme& ps, const unsigned long long* counts, unsigned err, int n_beams,
                  rtb_trace_stats* stats) {
     const int ns = 3 * ps.sch.n_surfaces;
     uint64_t ray_surfaces = 0, n_good = 0;
     int failed_beam = -1, failed_stage = -1;
     const int total_nonaux = ps.sch.s[ps.sch.n_surfaces - 1].surfaces_upto;
     for (int b = 0; b < n_beams; ++b) {
-        const unsigned long long* c = counts.data() + (size_t)b * (ns + 1);
+        const unsigned long long* c = counts + (size_t)b * (ns + 1);
         uint64_t alive = c[ns];
         for (int s = 0; s < ns; ++s) alive += c[s];
         for (int s = 0; s < ns; ++s) {
@@ -179,40 +173,9 @@ int rtb_generate_beams(const rtb_beam* beams, size_t n_beams, const rtb_rays* ra
     int st = ensure_init();
     if (st != RTB_OK) return st;
     cudaStream_t s = stream ? (cudaStream_t)stream : engine().stream;
-    std::vector<GenBeam> gb(n_beams);
-    uint64_t prev_end = 0, total = 0;
-    for (size_t b = 0; b < n_beams; ++b) {
-        const rtb_beam& in = beams[b];
-        if (in.shape != RTB_CIRCLE || in.n_lambda == 0 || in.first_ray < prev_end || in.first_ray + in.n_rays > rays->n)
-            return RTB_BAD_VALUE;
-        prev_end = in.first_ray + in.n_rays;
-        total = prev_end;
-        GenBeam& g = gb[b];
-        g.first_ray = in.first_ray;
-        g.n_rays = in.n_rays;
-        g.n_lambda = in.n_lambda;
-        g.seed = in.seed;
-        for (int i = 0; i < 3; ++i) {
-            g.disk[i] = in.disk[i];
-            g.center[i] = in.center[i];
-        }
-        g.range[0] = in.range[0];
-        g.range[1] = in.range[1];
-        g.d_lambda = (in.n_lambda > 1) ? (in.range[1] - in.range[0]) / (in.n_lambda - 1) : 0.0;
-        // field direction (tan fx, tan fy, 1) normalised as Beam::Normalize does
-        double cx = std::tan(in.field[0]), cy = std::tan(in.field[1]), cz = 1.0;
-        double acX = std::fabs(cx), acY = std::fabs(cy), acZ = std::fabs(cz), norm;
-        if (acX >= acY) {
-            if (acX >= acZ) norm = acX * std::sqrt(1.0 + acY * acY / acX / acX + acZ * acZ / acX / acX);
-            else norm = acZ * std::sqrt(1.0 + acX * acX / acZ / acZ + acY * acY / acZ / acZ);
-        } else {
-            if (acY >= acZ) norm = acY * std::sqrt(1.0 + acX * acX / acY / acY + acZ * acZ / acY / acY);
-            else norm = acZ * std::sqrt(1.0 + acX * acX / acZ / acZ + acY * acY / acZ / acZ);
-        }
-        g.c0[0] = cx / norm;
-        g.c0[1] = cy / norm;
-        g.c0[2] = cz / norm;
-    }
+    std::vector<GenBeam> gb;
+    uint64_t total = 0;
+    if ((st = gen_beams(beams, n_beams, rays->n, gb, &total)) != RTB_OK) return st;
     DevBuf gbuf;
     if ((st = gbuf.alloc(n_beams * sizeof(GenBeam), s)) != RTB_OK) return st;
     RTB_CUDA_TRY(cudaMemcpyAsync(gbuf.p, gb.data(), n_beams * sizeof(GenBeam), cudaMemcpyHostToDevice, s));
@@ -243,7 +206,7 @@ int rtb_trace(const rtb_surface* surfaces, size_t n_surfaces, const rtb_beam* be
     RTB_CUDA_TRY(cudaMemcpyAsync(counts.data(), a.counts, a.counts_len * 8, cudaMemcpyDeviceToHost, s));
     RTB_CUDA_TRY(cudaMemcpyAsync(&err, a.err, 4, cudaMemcpyDeviceToHost, s));
     RTB_CUDA_TRY(cudaStreamSynchronize(s));
-    return trace_result(ps, counts, err, (int)n_beams, stats);
+    return trace_result(ps, counts.data(), err, (int)n_beams, stats);
 }
 
 int rtb_trace_out(const rtb_surface* surfaces, size_t n_surfaces, const rtb_beam* beams, size_t n_beams,
@@ -267,7 +230,7 @@ int rtb_trace_out(const rtb_surface* surfaces, size_t n_surfaces, const rtb_beam
     RTB_CUDA_TRY(cudaMemcpyAsync(counts.data(), a.counts, a.counts_len * 8, cudaMemcpyDeviceToHost, s));
     RTB_CUDA_TRY(cudaMemcpyAsync(&err, a.err, 4, cudaMemcpyDeviceToHost, s));
     RTB_CUDA_TRY(cudaStreamSynchronize(s));
-    return trace_result(ps, counts, err, (int)n_beams, stats);
+    return trace_result(ps, counts.data(), err, (int)n_beams, stats);
 }
 
 int rtb_ccd_frame(const rtb_rays* rays, const rtb_ccd* ccd, uint32_t* counts, uint64_t* n_outside, void* stream) {
@@ -352,28 +315,62 @@ int trace_host_impl(const rtb_surface* surfaces, size_t n_surfaces, const rtb_be
     if (chunk == 0) chunk = (size_t)1 << 22;
     if (chunk > n) chunk = n;
     const size_t per_ray = 7 * sizeof(double) + 2;
-    cudaStream_t streams[2];
+    const int ns1 = 3 * ps.sch.n_surfaces + 1;
+    cudaStream_t streams[2] = {nullptr, nullptr};
     for (auto& s : streams) RTB_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    // Per slot: device rays of one chunk, the trace arguments (scheme and
+    // knots uploaded once), and page-locked staging for the chunk's beam
+    // table and its counters.  Page-locked, so that no copy of a chunk blocks
+    // the host and the next chunk's upload is queued while this one runs.
     struct Slot {
         DevBuf buf;
         DevRays r;
-        std::vector<DevBeam> beams;
         TraceArgs args;
-        std::vector<unsigned long long> counts;
+        DevBeam* h_beams = nullptr;
+        unsigned long long* h_counts = nullptr;  // counters, then the error word
+        char* h_flag = nullptr;                  // bounce buffers for pageable flag / lost_stage arrays
+        uint8_t* h_lost = nullptr;
+        uint64_t start = 0, cnt = 0;
         std::vector<int> beam_ids;
-        unsigned err = 0;
     };
     Slot slots[2];
-    for (int i = 0; i < 2; ++i) {
-        if ((st = slots[i].buf.alloc(chunk * per_ray, streams[i])) != RTB_OK) break;
-        char* p = slots[i].buf.as<char>();
-        double** f[7] = {&slots[i].r.X, &slots[i].r.Y, &slots[i].r.Z, &slots[i].r.cX, &slots[i].r.cY, &slots[i].r.cZ,
-                         &slots[i].r.lambda};
+    // The reference allocates Beam::flag with new[] (beam.cpp:328): a copy
+    // between pageable memory and the device blocks the host, so pageable
+    // flag / lost_stage arrays go through page-locked bounce buffers.
+    auto pageable = [](const void* p) {
+        cudaPointerAttributes a;
+        if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+            cudaGetLastError();
+            return true;
+        }
+        return a.type == cudaMemoryTypeUnregistered;
+    };
+    const bool bounce_flag = pageable(h->flag);
+    const bool bounce_lost = h->lost_stage && pageable(h->lost_stage);
+    const size_t stage_bytes = (n_beams * sizeof(DevBeam) + (n_beams * ns1 + 1) * sizeof(unsigned long long) +
+                                (bounce_flag ? chunk : 0) + (bounce_lost ? chunk : 0) + 255) / 256 * 256;
+    unsigned char* h_stage = nullptr;
+    if (cudaMallocHost(&h_stage, 2 * stage_bytes) != cudaSuccess) st = RTB_BAD_ALLOC;
+    for (int i = 0; i < 2 && st == RTB_OK; ++i) {
+        Slot& sl = slots[i];
+        unsigned char* q = h_stage + i * stage_bytes;
+        sl.h_beams = reinterpret_cast<DevBeam*>(q);
+        q += n_beams * sizeof(DevBeam);
+        sl.h_counts = reinterpret_cast<unsigned long long*>(q);
+        q += (n_beams * ns1 + 1) * sizeof(unsigned long long);
+        if (bounce_flag) {
+            sl.h_flag = reinterpret_cast<char*>(q);
+            q += chunk;
+        }
+        if (bounce_lost) sl.h_lost = q;
+        if ((st = sl.buf.alloc(chunk * per_ray, streams[i])) != RTB_OK) break;
+        if ((st = sl.args.init(ps, db, streams[i])) != RTB_OK) break;
+        char* p = sl.buf.as<char>();
+        double** f[7] = {&sl.r.X, &sl.r.Y, &sl.r.Z, &sl.r.cX, &sl.r.cY, &sl.r.cZ, &sl.r.lambda};
         for (int j = 0; j < 7; ++j) *f[j] = reinterpret_cast<double*>(p + (size_t)j * chunk * sizeof(double));
-        slots[i].r.flag = reinterpret_cast<char*>(p + 7 * chunk * sizeof(double));
-        slots[i].r.lost_stage = reinterpret_cast<uint8_t*>(p + 7 * chunk * sizeof(double) + chunk);
+        sl.r.flag = reinterpret_cast<char*>(p + 7 * chunk * sizeof(double));
+        sl.r.lost_stage = reinterpret_cast<uint8_t*>(p + 7 * chunk * sizeof(double) + chunk);
     }
-    const int ns1 = 3 * ps.sch.n_surfaces + 1;
     std::vector<unsigned long long> total((size_t)n_beams * ns1, 0);
     unsigned err_all = 0;
     FrameArgs frame = frame_args(opts);
@@ -382,9 +379,12 @@ int trace_host_impl(const rtb_surface* surfaces, size_t n_surfaces, const rtb_be
     double* hin[7] = {h->X, h->Y, h->Z, h->cX, h->cY, h->cZ, h->lambda};
     auto drain = [&](Slot& sl, cudaStream_t s) -> int {
         RTB_CUDA_TRY(cudaStreamSynchronize(s));
-        for (size_t b = 0; b < sl.beam_ids.size(); ++b)
-            for (int k = 0; k < ns1; ++k) total[(size_t)sl.beam_ids[b] * ns1 + k] += sl.counts[b * ns1 + k];
-        err_all |= sl.err;
+        const size_t nb = sl.beam_ids.size();
+        for (size_t b = 0; b < nb; ++b)
+            for (int k = 0; k < ns1; ++k) total[(size_t)sl.beam_ids[b] * ns1 + k] += sl.h_counts[b * ns1 + k];
+        err_all |= (unsigned)(sl.h_counts[nb * ns1] & 0xffffffffu);
+        if (sl.h_flag) std::memcpy(h->flag + sl.start, sl.h_flag, sl.cnt);
+        if (sl.h_lost) std::memcpy(h->lost_stage + sl.start, sl.h_lost, sl.cnt);
         sl.beam_ids.clear();
         return RTB_OK;
     };
@@ -396,7 +396,7 @@ int trace_host_impl(const rtb_surface* surfaces, size_t n_surfaces, const rtb_be
         if (!sl.beam_ids.empty() && (st = drain(sl, s)) != RTB_OK) break;
         uint64_t cnt = (n - start < chunk) ? n - start : chunk;
         // beams overlapping [start, start+cnt), rebased to the chunk
-        sl.beams.clear();
+        size_t nb = 0;
         for (size_t b = 0; b < n_beams; ++b) {
             uint64_t a0 = db[b].first_ray, a1 = db[b].first_ray + db[b].n_rays;
             uint64_t lo = a0 > start ? a0 : start, hi = a1 < start + cnt ? a1 : start + cnt;
@@ -404,33 +404,48 @@ int trace_host_impl(const rtb_surface* surfaces, size_t n_surfaces, const rtb_be
             DevBeam d = db[b];
             d.first_ray = lo - start;
             d.n_rays = hi - lo;
-            sl.beams.push_back(d);
+            sl.h_beams[nb++] = d;
             sl.beam_ids.push_back((int)b);
         }
-        if (sl.beams.empty()) {  // rays outside every beam are not traced
+        if (nb == 0) {  // rays outside every beam are not traced
             start += cnt;
             ++it;
             continue;
         }
         sl.r.n = cnt;
+        sl.start = start;
+        sl.cnt = cnt;
         for (int j = 0; j < 7; ++j)
             RTB_CUDA_TRY(cudaMemcpyAsync((&sl.r.X)[j], hin[j] + start, cnt * sizeof(double), cudaMemcpyHostToDevice, s));
-        RTB_CUDA_TRY(cudaMemcpyAsync(sl.r.flag, h->flag + start, cnt, cudaMemcpyHostToDevice, s));
-        if (h->lost_stage)
-            RTB_CUDA_TRY(cudaMemcpyAsync(sl.r.lost_stage, h->lost_stage + start, cnt, cudaMemcpyHostToDevice, s));
-        else
+        const char* flag_src = h->flag + start;
+        if (sl.h_flag) {
+            std::memcpy(sl.h_flag, flag_src, cnt);
+            flag_src = sl.h_flag;
+        }
+        RTB_CUDA_TRY(cudaMemcpyAsync(sl.r.flag, flag_src, cnt, cudaMemcpyHostToDevice, s));
+        if (h->lost_stage) {
+            const uint8_t* lost_src = h->lost_stage + start;
+            if (sl.h_lost) {
+                std::memcpy(sl.h_lost, lost_src, cnt);
+                lost_src = sl.h_lost;
+            }
+            RTB_CUDA_TRY(cudaMemcpyAsync(sl.r.lost_stage, lost_src, cnt, cudaMemcpyHostToDevice, s));
+        } else
             RTB_CUDA_TRY(cudaMemsetAsync(sl.r.lost_stage, RTB_NOT_LOST, cnt, s));
-        if ((st = sl.args.init(ps, sl.beams, s)) != RTB_OK) break;
-        if ((st = launch_trace(ps, sl.args, (int)sl.beams.size(), o, sl.r, sl.r, frame, s)) != RTB_OK) break;
+        RTB_CUDA_TRY(cudaMemcpyAsync(sl.args.beams, sl.h_beams, nb * sizeof(DevBeam), cudaMemcpyHostToDevice, s));
+        sl.args.counts_len = nb * ns1;
+        RTB_CUDA_TRY(cudaMemsetAsync(sl.args.counts, 0, sl.args.counts_len * 8, s));
+        RTB_CUDA_TRY(cudaMemsetAsync(sl.args.err, 0, 256, s));  // error word and tile counter
+        if ((st = launch_trace(ps, sl.args, (int)nb, o, sl.r, sl.r, frame, s)) != RTB_OK) break;
         int nout = o.state_out ? 6 : 2;
         for (int j = 0; j < nout; ++j)
             RTB_CUDA_TRY(cudaMemcpyAsync(hin[j] + start, (&sl.r.X)[j], cnt * sizeof(double), cudaMemcpyDeviceToHost, s));
-        RTB_CUDA_TRY(cudaMemcpyAsync(h->flag + start, sl.r.flag, cnt, cudaMemcpyDeviceToHost, s));
+        RTB_CUDA_TRY(cudaMemcpyAsync(sl.h_flag ? sl.h_flag : h->flag + start, sl.r.flag, cnt, cudaMemcpyDeviceToHost, s));
         if (h->lost_stage)
-            RTB_CUDA_TRY(cudaMemcpyAsync(h->lost_stage + start, sl.r.lost_stage, cnt, cudaMemcpyDeviceToHost, s));
-        sl.counts.assign(sl.beams.size() * ns1, 0);
-        RTB_CUDA_TRY(cudaMemcpyAsync(sl.counts.data(), sl.args.counts, sl.counts.size() * 8, cudaMemcpyDeviceToHost, s));
-        RTB_CUDA_TRY(cudaMemcpyAsync(&sl.err, sl.args.err, 4, cudaMemcpyDeviceToHost, s));
+            RTB_CUDA_TRY(cudaMemcpyAsync(sl.h_lost ? sl.h_lost : h->lost_stage + start, sl.r.lost_stage, cnt,
+                                         cudaMemcpyDeviceToHost, s));
+        RTB_CUDA_TRY(cudaMemcpyAsync(sl.h_counts, sl.args.counts, sl.args.counts_len * 8, cudaMemcpyDeviceToHost, s));
+        RTB_CUDA_TRY(cudaMemcpyAsync(sl.h_counts + sl.args.counts_len, sl.args.err, 4, cudaMemcpyDeviceToHost, s));
         start += cnt;
         ++it;
     }
@@ -439,18 +454,20 @@ int trace_host_impl(const rtb_surface* surfaces, size_t n_surfaces, const rtb_be
             int s2 = drain(slots[i], streams[i]);
             if (st == RTB_OK) st = s2;
         }
-        cudaStreamSynchronize(streams[i]);
+        if (streams[i]) cudaStreamSynchronize(streams[i]);
     }
     for (int i = 0; i < 2; ++i) {
         slots[i].args.buf.release();
         slots[i].buf.release();
     }
     for (auto& s : streams) {
+        if (!s) continue;
         cudaStreamSynchronize(s);
         cudaStreamDestroy(s);
     }
+    if (h_stage) cudaFreeHost(h_stage);
     if (st != RTB_OK) return st;
-    return trace_result(ps, total, err_all, (int)n_beams, stats);
+    return trace_result(ps, total.data(), err_all, (int)n_beams, stats);
 }
 
 }  // namespace rtb

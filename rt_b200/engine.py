@@ -34,6 +34,16 @@ def lib() -> C.CDLL:
         L.rtb_alocate_vector.restype = P(C.c_double)
         L.rtb_alocate_vector.argtypes = [C.c_size_t]
         L.rtb_free_vector.argtypes = [P(C.c_double)]
+        L.rtb_plan_create.argtypes = [P(ffi.Surface), C.c_size_t, P(ffi.Beam), C.c_size_t, P(ffi.TraceOpts),
+                                      P(vp)]
+        L.rtb_plan_run.argtypes = [vp, vp]
+        L.rtb_plan_result.argtypes = [vp, P(ffi.TraceStats)]
+        L.rtb_plan_rays.argtypes = [vp, P(ffi.Rays), P(ffi.Rays)]
+        L.rtb_plan_counts.argtypes = [vp, vp, C.c_size_t, P(C.c_size_t)]
+        L.rtb_plan_autotune.argtypes = [vp, C.c_int, P(ffi.TuneEntry), C.c_size_t, P(C.c_size_t)]
+        L.rtb_plan_set_config.argtypes = [vp, C.c_int32, C.c_int32]
+        L.rtb_plan_config.argtypes = [vp, P(C.c_int32), P(C.c_int32), P(C.c_uint64)]
+        L.rtb_plan_destroy.argtypes = [vp]
         _bound = True
     return L
 
@@ -152,8 +162,88 @@ def reference_order(beams, n_stages: int, rays: DeviceRays):
     return order
 
 
+class Plan:
+    """A batched trace (rtb_plan_*): rays generated once on the device, each
+    run one CUDA graph launch of the fused kernel."""
+
+    def __init__(self, surfaces, beams, o: ffi.TraceOpts):
+        self._surf = (ffi.Surface * len(surfaces))(*surfaces)
+        self._beams = _beams(beams)
+        self._opts = o
+        self.n_beams = len(beams)
+        self.h = C.c_void_p()
+        ffi.check(lib().rtb_plan_create(self._surf, len(surfaces), self._beams, len(beams), C.byref(o),
+                                        C.byref(self.h)), "rtb_plan_create")
+
+    def run(self, stream=None):
+        ffi.check(lib().rtb_plan_run(self.h, stream), "rtb_plan_run")
+
+    def result(self):
+        stats = ffi.TraceStats()
+        st = lib().rtb_plan_result(self.h, C.byref(stats))
+        return st, stats
+
+    def counts(self) -> np.ndarray:
+        """Per-(beam, stage) counters of the last run, shape (beams, 3*surfaces+1)."""
+        n = C.c_size_t(0)
+        ffi.check(lib().rtb_plan_counts(self.h, None, 0, C.byref(n)), "rtb_plan_counts")
+        a = np.zeros(n.value, dtype=np.uint64)
+        ffi.check(lib().rtb_plan_counts(self.h, a.ctypes.data, n.value, None), "rtb_plan_counts")
+        return a.reshape(self.n_beams, -1)
+
+    def rays(self):
+        i, o = ffi.Rays(), ffi.Rays()
+        ffi.check(lib().rtb_plan_rays(self.h, C.byref(i), C.byref(o)), "rtb_plan_rays")
+        return i, o
+
+    def autotune(self, reps=3):
+        table = (ffi.TuneEntry * 16)()
+        n = C.c_size_t(0)
+        ffi.check(lib().rtb_plan_autotune(self.h, reps, table, 16, C.byref(n)), "rtb_plan_autotune")
+        return [(t.block_size, t.rays_per_thread, t.ms) for t in table[:n.value]]
+
+    def set_config(self, block, rpt):
+        return lib().rtb_plan_set_config(self.h, block, rpt)
+
+    def config(self):
+        b, r, n = C.c_int32(), C.c_int32(), C.c_uint64()
+        ffi.check(lib().rtb_plan_config(self.h, C.byref(b), C.byref(r), C.byref(n)), "rtb_plan_config")
+        return b.value, r.value, n.value
+
+    def destroy(self):
+        if self.h:
+            lib().rtb_plan_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+class _DevArray:
+    """A device pointer as a __cuda_array_interface__ object (zero copy)."""
+
+    def __init__(self, ptr: int, n: int, typestr: str):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": typestr, "data": (ptr, False), "version": 3}
+
+
+def device_view(r: ffi.Rays) -> dict:
+    """torch views of the non-NULL device arrays of an ffi.Rays."""
+    import torch
+    out = {}
+    for f in FIELDS:
+        p = getattr(r, f)
+        if p:
+            out[f] = torch.as_tensor(_DevArray(p, r.n, "<f8"), device="cuda")
+    out["flag"] = torch.as_tensor(_DevArray(r.flag, r.n, "|i1"), device="cuda")
+    out["lost_stage"] = torch.as_tensor(_DevArray(r.lost_stage, r.n, "|u1"), device="cuda")
+    return out
+
+
 class PinnedRays:
-    """Host ray arrays in page-locked memory (rtb_alocate_vector)."""
+    """Host ray arrays, flags included, in page-locked memory (rtb_alocate_vector)."""
 
     def __init__(self, n: int):
         self.n = n
@@ -164,8 +254,14 @@ class PinnedRays:
                 raise MemoryError("rtb_alocate_vector failed")
             self._ptrs.append(p)
             setattr(self, f, np.ctypeslib.as_array(p, shape=(n,)))
-        self.flag = np.ones(n, dtype=np.int8)
-        self.lost_stage = np.full(n, ffi.NOT_LOST, dtype=np.uint8)
+        for f, dt, v in (("flag", np.int8, 1), ("lost_stage", np.uint8, ffi.NOT_LOST)):
+            p = lib().rtb_alocate_vector((n + 7) // 8)
+            if not p:
+                raise MemoryError("rtb_alocate_vector failed")
+            self._ptrs.append(p)
+            a = np.ctypeslib.as_array(p, shape=((n + 7) // 8,)).view(dt)[:n]
+            a[:] = v
+            setattr(self, f, a)
 
     def struct(self) -> ffi.Rays:
         return ffi.Rays(*(ffi.vptr(getattr(self, f)) for f in FIELDS), ffi.vptr(self.flag),
@@ -175,7 +271,7 @@ class PinnedRays:
         for p in self._ptrs:
             lib().rtb_free_vector(p)
         self._ptrs = []
-        for f in FIELDS:
+        for f in FIELDS + ("flag", "lost_stage"):
             setattr(self, f, None)
 
     def __del__(self):

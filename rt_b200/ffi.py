@@ -82,6 +82,10 @@ class TraceStats(C.Structure):
                 ("failed_stage", C.c_int32)]
 
 
+class TuneEntry(C.Structure):
+    _fields_ = [("block_size", C.c_int32), ("rays_per_thread", C.c_int32), ("ms", C.c_double)]
+
+
 def dptr(a: np.ndarray) -> C.POINTER(C.c_double):
     assert a.dtype == np.float64 and a.flags.c_contiguous
     return a.ctypes.data_as(C.POINTER(C.c_double))

@@ -2,10 +2,9 @@
 
 A scheme is a list of `SurfaceSpec`, the fields of one <surface> element of
 the reference's scheme XML (common-lib/scheme.cpp:416-664); `to_c()` turns it
-into the rtb_surface array of include/rtb.h.  The geometry BASELINE leaves
-open (distances, tilts, apertures, the glass and QE tables) is fixed here,
-seeded, and written out as scheme XML + range/table files by `write_xml` so
-the reference's own ray-tracing program reads the same scheme.
+into the rtb_surface array of include/rtb.h.  The geometry the benchmark
+configurations leave open (distances, tilts, apertures, the glass and QE
+tables) is fixed here and seeded.
 
 Configurations:
   * C0  `littrow_free()`: parabolic collimator R=-800 (k=-1) at z=400, plane
@@ -16,7 +15,10 @@ Configurations:
         turned 90 deg about z, toric fold Rx=-2000 Ry=-2100, even-asphere lens
         R=150/-400 with A4..A10 ~ N(0, 1e-7*10^-3k) and a 61-knot glass n(l),
         plane CCD 4096^2 x 15 um; 64 wavelengths 0.380..0.900 um.
-  * C4  `littrow_free_asphere()`: C0 plus one even-asphere mirror.
+  * C3  `c3_beams()`: 512 beams of log-uniform size (1e3..1e6 rays), each
+        with its own wavelength, field angle and echelle order, through C1.
+  * C4  `littrow_free_asphere()`: C0 extended with an even-asphere field
+        flattener before the CCD; 64 wavelengths 0.400..0.700 um.
 """
 from __future__ import annotations
 
@@ -191,15 +193,68 @@ def littrow_free() -> list[SurfaceSpec]:
     return [par, gr, cam, ccd]
 
 
-def littrow_free_asphere() -> list[SurfaceSpec]:
-    """C4 scheme: C0 with the camera mirror made an even asphere
-    (A4, A6, A8 of small seeded values)."""
+def c0_asphere_camera() -> list[SurfaceSpec]:
+    """C0 with the camera mirror made an even asphere (A4, A6, A8 of small
+    seeded values): a four-surface scheme with an iterative-asphere mirror."""
     s = littrow_free()
     rng = np.random.default_rng(SEED + 4)
     a = [0.0, float(rng.normal(0, 1e-10)), float(rng.normal(0, 1e-13)), float(rng.normal(0, 1e-16))]
     s[2].params = (-1 / 600.0, 0.0, len(a), *a)
     s[2].comment = "camera (even asphere)"
     return s
+
+
+# C4's added surface: an even-asphere field flattener 15 mm in front of C0's
+# CCD plane (same orientation), the CCD immersed in its glass and moved back
+# to the paraxial refocus 15 mm x n(0.55 um).
+C4_FLATTENER = dict(c=1 / 200.0, k=-0.5, A=(1e-6, -1e-9, 1e-12, -1e-15), back=15.0)
+# C4 merit: centroid x target linear in lambda, x_t = X0 + X1 (lambda - 0.55)
+C4_TARGET = (-0.3, -92.0)
+C4_LAMBDA = (0.400, 0.700)
+C4_NLAMBDA = 64
+
+
+def _rot_matrix(ang_deg: Sequence[float]) -> np.ndarray:
+    """R of the reference's transform (v_local = R v): rotations about y, x,
+    z of the pairs (X,Z), (Y,Z), (X,Y) (rt_cuda_engine_beam.cu:320-350)."""
+    K = 3.14159265359 / 180.0
+    R = np.eye(3)
+    for (i, j), a in zip(((0, 2), (1, 2), (0, 1)), ang_deg):
+        c, s_ = math.cos(a * K), math.sin(a * K)
+        M = np.eye(3)
+        M[i, i], M[i, j], M[j, i], M[j, j] = c, -s_, s_, c
+        R = M @ R
+    return R
+
+
+def littrow_free_asphere() -> list[SurfaceSpec]:
+    """C4 scheme: C0 extended with one even-asphere surface, a field
+    flattener (c=1/200, k=-0.5, A4..A10 = 1e-6, -1e-9, 1e-12, -1e-15) that
+    takes the converging beam into glass 15 mm before C0's CCD plane; the CCD
+    sits in the glass at the paraxial refocus."""
+    s = littrow_free()
+    ccd = s[3]
+    f = C4_FLATTENER
+    u = _rot_matrix(ccd.angles).T @ np.array([0.0, 0.0, 1.0])  # CCD axis in the camera frame
+    gx, gy = glass_table()
+    n55 = float(np.interp(0.55, gx, gy))
+    d = [round(float(v), 9) for v in (np.array(ccd.distance) - f["back"] * u)]
+    flat = SurfaceSpec(ffi.CONIC, ffi.LENS, params=(f["c"], f["k"], 5, 0.0, *f["A"]), size=(30.0, 0.0),
+                       distance=d, angles=list(ccd.angles), n1=1.0, n2=(gx, gy),
+                       comment="field flattener (even asphere)")
+    new_ccd = SurfaceSpec(ffi.PLANE, ffi.DETECTOR, shape=ffi.RECTANGLE, size=(30.72, 30.72),
+                          distance=(0.0, 0.0, round(f["back"] * n55, 6)), comment="CCD 2048x2048 15um (in glass)")
+    return s[:3] + [flat, new_ccd]
+
+
+def c4_beams(n_per_lambda: int = 156250, seed: int = SEED + 40) -> list[ffi.Beam]:
+    """C4 beam: 64 wavelengths over 0.40-0.70 um, n_per_lambda rays each
+    (1e7 rays by default), disk r=10 mm."""
+    return [make_beam(0, n_per_lambda, C4_NLAMBDA, C0_RADIUS, C4_LAMBDA, seed)]
+
+
+def c4_target_x(lam):
+    return C4_TARGET[0] + C4_TARGET[1] * (np.asarray(lam) - 0.55)
 
 
 def c0_beams(n_per_lambda: int = 20000, seed: int = SEED, first_ray: int = 0) -> list[ffi.Beam]:
@@ -278,6 +333,51 @@ def c1_beams(n_per_lambda: int | None = None, seed: int = SEED, orders=C1_ORDERS
     for i, m in enumerate(orders):
         beams.append(make_beam(first, n, C1_NLAMBDA, C1_RADIUS, C1_LAMBDA, seed + 1000 + i, orders=(m, 1)))
         first += n * C1_NLAMBDA
+    return beams
+
+
+def philox4x32_10(ctr: Sequence[int], key: int) -> tuple[int, int, int, int]:
+    """Philox4x32-10 (Salmon et al., SC'11) on the host: the generator the
+    device uses for ray positions, here for the per-beam draws of C3."""
+    M0, M1, W0, W1, m = 0xD2511F53, 0xCD9E8D57, 0x9E3779B9, 0xBB67AE85, 0xFFFFFFFF
+    c0, c1, c2, c3 = (int(v) & m for v in ctr)
+    k0, k1 = key & m, (key >> 32) & m
+    for _ in range(10):
+        p0, p1 = M0 * c0, M1 * c2
+        c0, c1, c2, c3 = ((p1 >> 32) ^ c1 ^ k0) & m, p1 & m, ((p0 >> 32) ^ c3 ^ k1) & m, p0 & m
+        k0, k1 = (k0 + W0) & m, (k1 + W1) & m
+    return c0, c1, c2, c3
+
+
+def _u01(hi: int, lo: int) -> float:
+    return float((((hi << 32) | lo) >> 11) + 1) * 2.0 ** -53
+
+
+C3_BEAMS = 512
+C3_COUNTS = (1e3, 1e6)          # log-uniform ray count per beam
+C3_FIELD_DEG = 0.5              # field angle uniform in [-0.5, 0.5] deg in x and in y
+
+
+def c3_beams(n_beams: int = C3_BEAMS, seed: int = SEED + 3, counts=C3_COUNTS, scale: float = 1.0) -> list[ffi.Beam]:
+    """C3: independent beams through the C1 scheme, each with its own ray
+    count (log-uniform in `counts`, times `scale`), wavelength (uniform over
+    0.38-0.90 um), field angle (uniform +-0.5 deg in x and y, direction
+    (tan fx, tan fy, 1) normalised) and echelle order (uniform 30..60).  The
+    draws of beam b come from Philox4x32-10 with counters (b, 0..2, 0, 0) and
+    key `seed`; the rays of beam b use seed + 1 + b."""
+    beams, first = [], 0
+    lo, hi = math.log(counts[0]), math.log(counts[1])
+    for b in range(n_beams):
+        r = philox4x32_10((b, 0, 0, 0), seed)
+        s = philox4x32_10((b, 1, 0, 0), seed)
+        n = max(1, int(round(math.exp(lo + (hi - lo) * _u01(r[0], r[1])) * scale)))
+        lam = C1_LAMBDA[0] + (C1_LAMBDA[1] - C1_LAMBDA[0]) * _u01(r[2], r[3])
+        fx = math.radians(C3_FIELD_DEG * (2.0 * _u01(s[0], s[1]) - 1.0))
+        fy = math.radians(C3_FIELD_DEG * (2.0 * _u01(s[2], s[3]) - 1.0))
+        t = philox4x32_10((b, 2, 0, 0), seed)
+        m = C1_ORDERS[0] + min(len(C1_ORDERS) - 1, int(_u01(t[0], t[1]) * len(C1_ORDERS)))
+        beams.append(make_beam(first, n, 1, C1_RADIUS, (lam, lam), seed + 1 + b, orders=(m, 1), field=(fx, fy)))
+        first += n
     return beams
 
 

@@ -12,7 +12,7 @@ reference's spline_init kernel runs the natural-spline recurrence in parallel
 (rt_cuda_engine_spline.cu:21-37) and returns racy second derivatives, so
 tabulated indices would not be a reproducible fixture.
 
-  python tests/golden/make_golden.py [out_dir]
+  python tests/golden/make_golden.py [out_dir] [--only=case1,case2]
 """
 from __future__ import annotations
 
@@ -63,9 +63,11 @@ def cases():
     c0 = dict(n_lambda=5, radius=10.0, lam_range=(0.4, 0.7))
     c1 = dict(n_lambda=64, radius=25.0, lam_range=(0.38, 0.90))
     small = dict(n_lambda=5, radius=10.0, lam_range=(0.4, 0.8))
+    c4 = dict(n_lambda=64, radius=10.0, lam_range=(0.4, 0.7))
     return {
         "c0": (S.littrow_free(), c0, (), 400),
-        "c4": (S.littrow_free_asphere(), c0, (), 400),
+        "c0_asphere_camera": (S.c0_asphere_camera(), c0, (), 400),
+        "c4": (scalarize(S.littrow_free_asphere()), c4, (), 400),
         "c1_m38": (scalarize(S.echelle()), c1, (38, 1), 40),
         "c1_m52": (scalarize(S.echelle()), c1, (52, 1), 40),
         "c1_sphere_m38": (sphere_fold(scalarize(S.echelle())), c1, (38, 1), 40),
@@ -88,11 +90,13 @@ def spec_arrays(specs):
     return np.array(rows, dtype=np.float64)
 
 
-def main(out_dir=HERE):
+def main(out_dir=HERE, only=None):
     os.makedirs(out_dir, exist_ok=True)
     if H.harness("refgpu") is None:
         raise SystemExit("oracle/_ref/harness_refgpu is not built")
     for name, (specs, kw, orders, n_per) in cases().items():
+        if only and name not in only:
+            continue
         beam = S.make_beam(0, n_per, kw["n_lambda"], kw["radius"], kw["lam_range"], 20141203, orders=orders)
         rays = O.generate([beam], beam.n_rays)
         if name.endswith("_tagged"):
@@ -109,4 +113,6 @@ def main(out_dir=HERE):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else HERE)
+    args = [a for a in sys.argv[1:] if not a.startswith("--only=")]
+    only = [a.split("=", 1)[1] for a in sys.argv[1:] if a.startswith("--only=")]
+    main(args[0] if args else HERE, only=[o for x in only for o in x.split(",")] or None)

@@ -1,0 +1,194 @@
+"""Batched plans (rtb_plan_*): many beams of uneven size, wavelength, field
+angle and order in one graph-launched trace, and the autotuner (GPU tests).
+
+* A plan's FP64 output equals the CPU oracle's trace of the same beams bit
+  for bit; its mixed output equals rtb_trace_out's on the plan's own rays.
+* Every launch configuration the autotuner tries gives the same result.
+* The autotuner leaves the plan's frame untouched and its choice is reused
+  by a later plan of the same scheme and size.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+
+import pyoracle as O
+from rt_b200 import engine as E
+from rt_b200 import ffi, metrics, schemes as S
+
+pytestmark = pytest.mark.gpu
+
+FIXES = ffi.FIX_TORIC_SIGN | ffi.FIX_TORIC_STEP
+TRACED = (ffi.OK, ffi.NO_INTERSECTIONS, ffi.NO_GOOD_RAYS)
+
+
+def small_c3(n_beams=96, scale=0.004):
+    """C3's beam draws with the ray counts scaled down (4..4000 per beam)."""
+    return S.c3_beams(n_beams=n_beams, scale=scale)
+
+
+def frame_opts(precision, ccd, block=0, rpt=0, state_out=0):
+    counts = torch.zeros(int(ccd.xdim) * int(ccd.ydim), dtype=torch.int32, device="cuda")
+    outside = torch.zeros(1, dtype=torch.int64, device="cuda")
+    o = E.opts(engine=ffi.ENGINE_FUSED, precision=precision, fixes=FIXES, state_out=state_out, block=block, rpt=rpt,
+               ccd=ccd, counts=counts, n_outside=outside)
+    return o, counts, outside
+
+
+def plan_output(plan):
+    rin, rout = plan.rays()
+    return E.device_view(rin), E.device_view(rout)
+
+
+def test_plan_fp64_matches_oracle():
+    beams = small_c3()
+    n = S.total_rays(beams)
+    cs_d, cs_o = S.to_c(S.echelle(), E.spline_init), S.to_c(S.echelle(), O.spline_init)
+    plan = E.Plan(cs_d.surfaces, beams, E.opts(engine=ffi.ENGINE_FUSED, precision=ffi.FP64, fixes=FIXES))
+    plan.run()
+    st, stats = plan.result()
+    ora = O.generate(beams, n)
+    st_o, stats_o, _ = O.trace(cs_o.surfaces, beams, ora, fixes=FIXES)
+    assert st == st_o
+    assert (stats.ray_surfaces, stats.n_good) == (stats_o.ray_surfaces, stats_o.n_good)
+    _, out = plan_output(plan)
+    for f in ("X", "Y", "Z", "cX", "cY", "cZ"):
+        a = out[f].cpu().numpy()
+        b = getattr(ora, f)
+        same = (a.view(np.uint64) == b.view(np.uint64)) | (np.isnan(a) & np.isnan(b))
+        assert same.all(), f
+    assert np.array_equal(out["flag"].cpu().numpy(), ora.flag)
+    assert np.array_equal(out["lost_stage"].cpu().numpy(), ora.lost_stage)
+    plan.destroy()
+
+
+@pytest.mark.parametrize("precision", [ffi.MIXED, ffi.FP64])
+def test_plan_equals_trace_out_and_frame(precision):
+    beams = small_c3()
+    ccd = S.ccd(S.C1_CCD)
+    cs = S.to_c(S.echelle(), E.spline_init)
+    o, counts, outside = frame_opts(precision, ccd)
+    plan = E.Plan(cs.surfaces, beams, o)
+    plan.run()
+    st, stats = plan.result()
+    assert st in TRACED  # beams whose every ray is lost are reported, the rest traced
+    rin, rout = plan_output(plan)
+    # the same rays through rtb_trace_out
+    n = S.total_rays(beams)
+    src = E.DeviceRays(n)
+    for f in E.FIELDS:
+        getattr(src, f).copy_(rin[f])
+    src.flag.copy_(rin["flag"])
+    ref = E.DeviceRays(n)
+    o2, counts2, outside2 = frame_opts(precision, ccd)
+    stats2 = ffi.TraceStats()
+    surf = (ffi.Surface * len(cs.surfaces))(*cs.surfaces)
+    L = E.lib()
+    L.rtb_trace_out.argtypes = [C.POINTER(ffi.Surface), C.c_size_t, C.POINTER(ffi.Beam), C.c_size_t,
+                                C.POINTER(ffi.TraceOpts), C.POINTER(ffi.Rays), C.POINTER(ffi.Rays),
+                                C.POINTER(ffi.TraceStats), C.c_void_p]
+    st2 = L.rtb_trace_out(surf, len(surf), E._beams(beams), len(beams), C.byref(o2), C.byref(src.struct()),
+                          C.byref(ref.struct()), C.byref(stats2), None)
+    torch.cuda.synchronize()
+    assert st2 == st
+    assert (stats.ray_surfaces, stats.n_good) == (stats2.ray_surfaces, stats2.n_good)
+    assert torch.equal(rout["X"], ref.X) and torch.equal(rout["Y"], ref.Y)
+    assert torch.equal(rout["flag"], ref.flag) and torch.equal(rout["lost_stage"], ref.lost_stage)
+    assert torch.equal(counts, counts2) and int(outside) == int(outside2)
+    assert int(counts.sum()) + int(outside) == stats.n_good
+    # per-beam counters: every ray of every beam accounted for once
+    cnt = plan.counts()
+    assert [int(r.sum()) for r in cnt] == [b.n_rays for b in beams]
+    assert int(cnt[:, -1].sum()) == stats.n_good
+    # a second run adds to the frame
+    plan.run()
+    assert plan.result()[0] == st
+    assert torch.equal(counts, 2 * counts2)
+    plan.destroy()
+
+
+def test_plan_autotune_sweep_and_reuse():
+    beams = small_c3(n_beams=64)
+    ccd = S.ccd(S.C1_CCD)
+    cs = S.to_c(S.echelle(), E.spline_init)
+    o, counts, outside = frame_opts(ffi.MIXED, ccd)
+    plan = E.Plan(cs.surfaces, beams, o)
+    plan.run()
+    st0, stats0 = plan.result()
+    x0 = plan_output(plan)[1]["X"].clone()
+    counts0 = counts.clone()
+    table = plan.autotune(reps=2)
+    assert len(table) == 12
+    assert {(b, r) for b, r, _ in table} == {(b, r) for b in (128, 256, 512) for r in (1, 2, 4, 8)}
+    assert all(ms > 0 for _, _, ms in table)
+    assert torch.equal(counts, counts0)  # the sweep used its own frame
+    best = min(table, key=lambda t: t[2])
+    block, rpt, n = plan.config()
+    assert (block, rpt) == best[:2] and n == S.total_rays(beams)
+    plan.run()
+    st1, stats1 = plan.result()
+    assert st0 in TRACED and st1 == st0 and stats1.ray_surfaces == stats0.ray_surfaces
+    assert torch.equal(plan_output(plan)[1]["X"], x0)
+    # a second plan of the same scheme, precision, frame use and size starts tuned
+    o2, _, _ = frame_opts(ffi.MIXED, ccd)
+    plan2 = E.Plan(cs.surfaces, beams, o2)
+    assert plan2.config()[:2] == (block, rpt)
+    plan2.destroy()
+    plan.destroy()
+
+
+@pytest.mark.parametrize("block,rpt", [(128, 1), (512, 8), (256, 64)])
+def test_plan_configs_agree(block, rpt):
+    beams = small_c3(n_beams=48)
+    cs = S.to_c(S.echelle(), E.spline_init)
+    plan = E.Plan(cs.surfaces, beams, E.opts(engine=ffi.ENGINE_FUSED, precision=ffi.MIXED, fixes=FIXES,
+                                              state_out=1))
+    plan.run()
+    st0, ref_stats = plan.result()
+    ref = {k: v.clone() for k, v in plan_output(plan)[1].items()}
+    assert plan.set_config(block, rpt) == ffi.OK
+    plan.run()
+    st, stats = plan.result()
+    assert st == st0 and st in TRACED and stats.ray_surfaces == ref_stats.ray_surfaces
+    out = plan_output(plan)[1]
+    for k in ("X", "Y", "Z", "cX", "cY", "cZ", "flag", "lost_stage"):
+        assert torch.equal(out[k], ref[k]), k
+    plan.destroy()
+
+
+def test_plan_rejects_bad_requests():
+    beams = small_c3(n_beams=8)
+    cs = S.to_c(S.echelle(), E.spline_init)
+    surf = (ffi.Surface * len(cs.surfaces))(*cs.surfaces)
+    h = C.c_void_p()
+    o = E.opts(engine=ffi.ENGINE_PER_SURFACE, precision=ffi.FP64)
+    assert E.lib().rtb_plan_create(surf, len(surf), E._beams(beams), len(beams), C.byref(o), C.byref(h)) == \
+        ffi.BAD_VALUE
+    plan = E.Plan(cs.surfaces, beams, E.opts(engine=ffi.ENGINE_FUSED, precision=ffi.FP64))
+    assert plan.set_config(512, 2) == ffi.BAD_VALUE  # 512-thread blocks are for the mixed kernel
+    assert plan.set_config(256, 0) == ffi.BAD_VALUE
+    assert E.lib().rtb_plan_result(plan.h, None) == ffi.BAD_VALUE  # nothing ran yet
+    plan.destroy()
+
+
+def test_plan_mixed_accuracy_on_c3():
+    """C3's mixed-precision run against the FP64 plan on the same beams."""
+    beams = small_c3(n_beams=512, scale=0.02)
+    cs = S.to_c(S.echelle(), E.spline_init)
+    mk = lambda p: E.Plan(cs.surfaces, beams, E.opts(engine=ffi.ENGINE_FUSED, precision=p, fixes=FIXES))  # noqa
+    pm, pr = mk(ffi.MIXED), mk(ffi.FP64)
+    pm.run()
+    pr.run()
+    assert pm.result()[0] == pr.result()[0]
+    assert pm.result()[0] in TRACED
+    a, b = plan_output(pm)[1], plan_output(pr)[1]
+    c = S.C1_CCD
+    m = metrics.ccd_error(a["X"], a["Y"], a["flag"], b["X"], b["Y"], b["flag"], c["xsize"], c["ysize"], c["xpix"],
+                          c["ypix"])
+    print(m)
+    assert m["rays_compared"] > 1000
+    assert m["p99_9_um"] <= 0.05
+    assert m["pixel_mismatch_rate"] < 1e-3
+    pm.destroy()
+    pr.destroy()
