@@ -60,8 +60,11 @@ enum { RTB_FP64 = 0, RTB_MIXED = 1 };
 /* Quirk fixes: 0 reproduces the reference; each bit selects the correct form. */
 enum {
     RTB_FIX_TORIC_SIGN = 1,   /* iter_toric's 1+k1c^2Y^2 becomes 1-k1c^2Y^2 (cuda_engine/rt_cuda_engine_surface.cu:350) */
-    RTB_FIX_TORIC_STEP = 2    /* iter_toric's Steffensen step divides by Fzn-Fxn == 0 once converged and
+    RTB_FIX_TORIC_STEP = 2,   /* iter_toric's Steffensen step divides by Fzn-Fxn == 0 once converged and
                                  sends the ray to inf/NaN (surface.cu:390); the fix stops there instead */
+    RTB_FIX_ASPHERE_ROOT = 4  /* iterative_conic/poly_intersection report the point before the last Newton
+                                 update, up to 1e-7 mm short of the root (surface.cu:288-290); the fix reports
+                                 the updated point */
 };
 
 #define RTB_MAX_POLY 10           /* MAX_POLY_COEFFS, surface.h:14 */
@@ -374,6 +377,71 @@ RTB_API int rtb_plan_set_config(rtb_plan* plan, int32_t block_size, int32_t rays
 RTB_API int rtb_plan_config(const rtb_plan* plan, int32_t* block_size, int32_t* rays_per_thread, uint64_t* n_rays);
 /* Release everything the plan holds, after its work has finished. */
 RTB_API int rtb_plan_destroy(rtb_plan* plan);
+
+/* =========================================================================
+ * 4. Adjoint: gradients of the CCD-plane positions with respect to scheme
+ *    parameters (no counterpart in the reference).  A forward/backward pair
+ *    of the shape a torch.autograd.Function wraps: forward(theta) -> X, Y per
+ *    ray; backward(dL/dX, dL/dY) -> dL/dtheta.  The forward is the plain FP64
+ *    engine (the same bits as rtb_trace's RTB_FP64 fused engine) and keeps
+ *    each ray's state at every surface boundary; the backward recomputes one
+ *    surface at a time from those checkpoints, last to first, and carries the
+ *    adjoint of the ray state back through it.  Root iterations are
+ *    differentiated by the implicit-function theorem at the returned point.
+ *    Lost rays carry no gradient (flags are not differentiable).
+ * ========================================================================= */
+enum {
+    RTB_PARAM_CURVATURE = 0,      /* params[0], c (1/mm) */
+    RTB_PARAM_CONIC = 1,          /* params[1], conic constant k */
+    RTB_PARAM_POLY = 2,           /* params[3 + index], polynomial coefficient a_(index+1) of r^(2 index + 2) */
+    RTB_PARAM_TORIC_CR = 3,       /* the toric's cR, params[3 + N] */
+    RTB_PARAM_DISTANCE = 4,       /* distance[index], mm */
+    RTB_PARAM_ANGLE = 5,          /* angles_deg[index], degrees (about y, x, z) */
+    RTB_PARAM_GROOVE_DENSITY = 6  /* grating lines per mm: gr_const = 1000 / value */
+};
+/* One differentiable scheme parameter: field `kind` (index `index`) of
+ * surface `surface`.  A parameter whose change would switch the surface's
+ * algorithm (the curvature of a conic at c = 0, the conic constant of a
+ * paraboloid, k = -1) is rejected with RTB_BAD_VALUE. */
+typedef struct rtb_param {
+    int32_t surface;
+    int32_t kind;
+    int32_t index;
+    int32_t reserved;
+} rtb_param;
+#define RTB_ADJ_MAX_PARAMS 64
+typedef struct rtb_adjoint rtb_adjoint;
+
+/* Prepare on the current device: copies of the scheme (tables included), the
+ * parameter list, the beam table, and room for n_rays rays' checkpoints
+ * (48 bytes x n_surfaces per ray), wavelengths and outputs. */
+RTB_API int rtb_adjoint_create(const rtb_surface* surfaces, size_t n_surfaces, const rtb_param* params,
+                               size_t n_params, const rtb_beam* beams, size_t n_beams, uint64_t n_rays,
+                               uint32_t fixes, rtb_adjoint** ctx);
+/* The parameters' values in the scheme given to rtb_adjoint_create (host, n_params). */
+RTB_API int rtb_adjoint_theta(const rtb_adjoint* ctx, double* theta);
+/* Trace `rays` (device, n_rays, not modified) through the scheme with the
+ * parameters set to theta (host, n_params; NULL: the create-time values).
+ * X, Y (device, may be NULL) receive the CCD-plane positions and flag
+ * (device, may be NULL) 1 for rays that reach the end.  Synchronous. */
+RTB_API int rtb_adjoint_forward(rtb_adjoint* ctx, const double* theta, const rtb_rays* rays, double* X, double* Y,
+                                char* flag, rtb_trace_stats* stats, void* stream);
+/* grad[j] = sum over rays of gX * dX/dtheta_j + gY * dY/dtheta_j for the last
+ * forward (gX, gY device, n_rays; grad host, n_params).  Deterministic. */
+RTB_API int rtb_adjoint_backward(rtb_adjoint* ctx, const double* gX, const double* gY, double* grad, void* stream);
+/* Forward-mode sensitivities of the last forward along dtheta (host, n_params):
+ * dX, dY (device, n_rays) = sum_j dtheta_j dX/dtheta_j (0 for lost rays). */
+RTB_API int rtb_adjoint_jvp(rtb_adjoint* ctx, const double* dtheta, double* dX, double* dY, void* stream);
+/* The spot merit of the last forward: for every wavelength of every beam
+ * (group g = beam b, wavelength index j; rays first_ray + j + m * n_lambda)
+ * with good rays, RMS spot radius + weight * (centroid x - target_x[g])^2,
+ * summed; *merit (host) receives it and gX, gY (device, n_rays, may be
+ * NULL) its derivatives with respect to each ray's X and Y, ready for
+ * rtb_adjoint_backward.  target_x: host, one value per group, beams in
+ * order.  Deterministic. */
+RTB_API int rtb_adjoint_spot_merit(rtb_adjoint* ctx, const double* target_x, double weight, double* merit,
+                                   double* gX, double* gY, void* stream);
+RTB_API int rtb_adjoint_destroy(rtb_adjoint* ctx);
 
 #ifdef __cplusplus
 }

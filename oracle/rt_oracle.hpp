@@ -60,6 +60,7 @@ enum QuirkFix : uint32_t {
     FIX_NONE = 0,
     FIX_TORIC_SIGN = 1u << 0,      // iter_toric uses 1+k1c^2Y^2 (surface.cu:350)
     FIX_TORIC_STEP = 1u << 1,      // iter_toric divides by Fzn-Fxn == 0 (surface.cu:390)
+    FIX_ASPHERE_ROOT = 1u << 2,    // iterative asphere reports the point before the last Newton update (surface.cu:288-290)
 };
 
 // ---------------------------------------------------------------------------
@@ -164,10 +165,11 @@ inline bool conic_intersection(const SurfConst& s, Ray& r) {
 
 // iterative_conic_intersection (surface.cu:257-333).  Newton on the even
 // asphere sag from the Z=0 plane point; the reported point is the last
-// evaluated one (s1), written even when the ray is lost inside the loop.
+// evaluated one (s1), written even when the ray is lost inside the loop --
+// with `fix_root`, the point of the last update (s2) once converged.
 // The iteration counter is reset per ray (the reference keeps it per thread
 // across its grid-stride loop, which only matters after ~1e5 iterations).
-inline bool iterative_conic_intersection(const SurfConst& s, Ray& r) {
+inline bool iterative_conic_intersection(const SurfConst& s, bool fix_root, Ray& r) {
     double s0 = -r.Z / r.cZ;
     if (!(s0 >= 0)) return false;
     double s1, s2 = 0.0, Xi = 0, Yi = 0, Zi = 0;
@@ -192,6 +194,11 @@ inline bool iterative_conic_intersection(const SurfConst& s, Ray& r) {
         s2 = s1 - F / dF;
         ++Niter;
     } while ((std::fabs(s2 - s1) >= ITER_EPS) && (Niter <= ITER_MAX));
+    if (fix_root && good && Niter <= ITER_MAX) {  // the point of the last update
+        Xi = r.X + (s2 + s0) * r.cX;
+        Yi = r.Y + (s2 + s0) * r.cY;
+        Zi = s2 * r.cZ;
+    }
     r.X = Xi; r.Y = Yi; r.Z = Zi;
     if (Niter > ITER_MAX) good = false;
     return good;
@@ -199,7 +206,7 @@ inline bool iterative_conic_intersection(const SurfConst& s, Ray& r) {
 
 // iterative_poly_intersection (surface.cu:497-561): c == 0 with a polynomial;
 // requires s0 > 0 and uses (-X-Y)*sum in the derivative, as the reference.
-inline bool iterative_poly_intersection(const SurfConst& s, Ray& r) {
+inline bool iterative_poly_intersection(const SurfConst& s, bool fix_root, Ray& r) {
     double s0 = -r.Z / r.cZ;
     if (!(s0 > 0)) return false;
     double s1, s2 = 0.0, Xi = 0, Yi = 0, Zi = 0;
@@ -222,6 +229,11 @@ inline bool iterative_poly_intersection(const SurfConst& s, Ray& r) {
         s2 = s1 - F / dF;
         ++Niter;
     } while ((std::fabs(s2 - s1) >= ITER_EPS) && (Niter <= ITER_MAX));
+    if (fix_root && good && Niter <= ITER_MAX) {  // the point of the last update
+        Xi = r.X + (s2 + s0) * r.cX;
+        Yi = r.Y + (s2 + s0) * r.cY;
+        Zi = s2 * r.cZ;
+    }
     r.X = Xi; r.Y = Yi; r.Z = Zi;
     if (Niter > ITER_MAX) good = false;
     return good;
@@ -290,8 +302,8 @@ inline bool intersect(IsectKind kind, const SurfConst& s, uint32_t fixes, Ray& r
         case IS_PLANE: return plane_intersection(r);
         case IS_PARABOLOID: return paraboloid_intersection(s, r);
         case IS_CONIC: return conic_intersection(s, r);
-        case IS_ITER_POLY: return iterative_poly_intersection(s, r);
-        case IS_ITER_CONIC: return iterative_conic_intersection(s, r);
+        case IS_ITER_POLY: return iterative_poly_intersection(s, (fixes & FIX_ASPHERE_ROOT) != 0, r);
+        case IS_ITER_CONIC: return iterative_conic_intersection(s, (fixes & FIX_ASPHERE_ROOT) != 0, r);
         case IS_TORIC: return iter_toric(s, (fixes & FIX_TORIC_SIGN) != 0, (fixes & FIX_TORIC_STEP) != 0, r);
         default: return true;
     }

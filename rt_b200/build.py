@@ -26,6 +26,7 @@ SOURCES = {
     "kernels_mixed.cu": ["--fmad=true"],
     "noalloc.cu": ["--fmad=false"],
     "plan.cu": ["--fmad=false"],
+    "adjoint.cu": ["--fmad=false"],
 }
 
 

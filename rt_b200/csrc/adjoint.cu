@@ -1,0 +1,687 @@
+// adjoint.cu -- gradients of CCD-plane positions with respect to scheme
+// parameters: forward with checkpoints, reverse sweep over surfaces,
+// forward-mode sensitivities, and the spot merit's per-ray seeds.
+//
+// Forward (k_adj_forward): the fused FP64 engine's per-ray loop (the same
+// bits), storing each ray's state (X Y Z cX cY cZ) at the input of every
+// surface -- 48 bytes x surfaces per ray.
+//
+// Backward (k_adj_backward): per ray, surfaces last to first.  For surface k
+// the local Jacobian of its output state with respect to its input state and
+// to the parameters that live on it is recomputed from checkpoint k in
+// forward mode (dual numbers, W directions per pass); the adjoint of the
+// output state is carried back through it, and the parameter adjoints are
+// accumulated.  Per-thread sums are reduced per block in a fixed order and
+// the block partials summed in block order, so the gradient is reproducible.
+//
+// Translation unit compiled with --fmad=false: the dual numbers' values are
+// the plain engine's.
+#include <cstring>
+#include <vector>
+
+#include "engine.cuh"
+#include "ray_ad.cuh"
+#include "trace_common.cuh"
+
+namespace rtb {
+
+namespace {
+
+constexpr int kAdjW = 4;           // directions per dual pass of the backward sweep
+constexpr int kAdjThreads = 128;
+constexpr int kMeritThreads = 256;
+constexpr int kMeritParts = 32;    // fixed split of each group's rays (deterministic sums)
+
+struct AdjArgs {
+    const DevScheme* sch;
+    const double* knots;
+    const DevBeam* beams;
+    int n_beams;
+    const ad::ParamRef* map;
+    int n_params;
+    const int* surf_params;  // [n_surfaces][RTB_ADJ_MAX_PARAMS]: parameter indices per surface
+    const int* surf_nparams; // [n_surfaces]
+    double* ckpt;            // [(k * 6 + c) * n + i]
+    double* lambda;          // copy of the wavelengths
+    char* flag;              // 1 = reached the end
+    double* X;
+    double* Y;
+    uint64_t n;
+};
+
+__device__ __forceinline__ long long order_of(const DevSurface& s, const DevBeam* beams, int b) {
+    long long order = s.order;
+    if (s.type == RTB_GRATING && beams[b].n_orders > 0) order = beams[b].orders[s.grating_index];
+    return order;
+}
+
+__global__ void __launch_bounds__(256) k_adj_forward(AdjArgs a, DevRays in, unsigned long long* counts,
+                                                     unsigned* err) {
+    const DevScheme* sch = a.sch;
+    const int ns = sch->n_surfaces;
+    const int n_stages = 3 * ns;
+    for (size_t i = gtid(); i < a.n; i += gstride()) {
+        a.lambda[i] = in.lambda[i];
+        if (in.flag[i] != 1) {
+            a.flag[i] = 0;
+            continue;
+        }
+        f64::Ray r{in.X[i], in.Y[i], in.Z[i], in.cX[i], in.cY[i], in.cZ[i]};
+        const double lam = in.lambda[i];
+        const int b = beam_of(a.beams, a.n_beams, i);
+        int stage = -1;
+        for (int k = 0; k < ns; ++k) {
+            double* c = a.ckpt + (size_t)k * 6 * a.n + i;
+            c[0] = r.X;
+            c[a.n] = r.Y;
+            c[2 * a.n] = r.Z;
+            c[3 * a.n] = r.cX;
+            c[4 * a.n] = r.cY;
+            c[5 * a.n] = r.cZ;
+            const DevSurface& s = sch->s[k];
+            f64::transform(s, r);
+            f64::normalize(r.cX, r.cY, r.cZ);
+            if (!s.non_aux) continue;
+            if (!f64::intersect(s, sch->fixes, r)) { stage = 3 * k; break; }
+            if (!f64::aperture_pass(s.type == RTB_SHADE, s.shape, s.size, s.center, r.X, r.Y)) {
+                stage = 3 * k + 1;
+                break;
+            }
+            int act = f64::action(s, a.knots, order_of(s, a.beams, b), lam, r);
+            if (act == f64::ACT_RANGE) { atomicOr(err, DEV_ERR_OUT_OF_RANGE); stage = -2; break; }
+            if (act == f64::ACT_LOST) { stage = 3 * k + 2; break; }
+            f64::normalize(r.cX, r.cY, r.cZ);
+        }
+        a.flag[i] = (stage == -1) ? 1 : 0;
+        a.X[i] = r.X;
+        a.Y[i] = r.Y;
+        if (stage >= 0) atomicAdd(counts + (size_t)b * (n_stages + 1) + stage, 1ull);
+        else if (stage == -1) atomicAdd(counts + (size_t)b * (n_stages + 1) + n_stages, 1ull);
+    }
+}
+
+// Per-thread parameter adjoints live in local memory; the block reduces them
+// in a fixed tree order into partial[blockIdx.x][P].
+__device__ void block_reduce_params(double* g, int P, double* partial) {
+    __shared__ double red[kAdjThreads];
+    for (int p = 0; p < P; ++p) {
+        red[threadIdx.x] = g[p];
+        __syncthreads();
+        for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+            if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) partial[(size_t)blockIdx.x * P + p] = red[0];
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(kAdjThreads) k_adj_backward(AdjArgs a, const double* gX, const double* gY,
+                                                              double* partial) {
+    const DevScheme* sch = a.sch;
+    const int ns = sch->n_surfaces;
+    const int P = a.n_params;
+    double g[RTB_ADJ_MAX_PARAMS];
+    for (int p = 0; p < P; ++p) g[p] = 0.0;
+    for (size_t i = gtid(); i < a.n; i += gstride()) {
+        if (a.flag[i] != 1) continue;
+        double adj[6] = {gX[i], gY[i], 0.0, 0.0, 0.0, 0.0};
+        if (adj[0] == 0.0 && adj[1] == 0.0) continue;
+        const double lam = a.lambda[i];
+        const int b = beam_of(a.beams, a.n_beams, i);
+        for (int k = ns - 1; k >= 0; --k) {
+            const DevSurface& s = sch->s[k];
+            double st[6];
+            for (int c = 0; c < 6; ++c) st[c] = a.ckpt[((size_t)k * 6 + c) * a.n + i];
+            const int npk = a.surf_nparams[k];
+            const int ndir = 6 + npk;
+            double adj_in[6] = {0, 0, 0, 0, 0, 0};
+            for (int d0 = 0; d0 < ndir; d0 += kAdjW) {
+                ad::Seeds<kAdjW> sd;
+                sd.dense = nullptr;
+                for (int l = 0; l < kAdjW; ++l) {
+                    const int d = d0 + l;
+                    sd.state[l] = (d < 6) ? d : -1;
+                    sd.param[l] = (d >= 6 && d < ndir) ? a.surf_params[k * RTB_ADJ_MAX_PARAMS + (d - 6)] : -1;
+                }
+                ad::SurfD<kAdjW> sdv;
+                ad::make_surfd(s, k, a.map, P, sd, sdv);
+                ad::RayD<kAdjW> r;
+                ad::load_state(st, sd, r);
+                ad::surface_step(s, sdv, sch->fixes, a.knots, order_of(s, a.beams, b), lam, r);
+                // the last surface's output is the CCD-plane point: only X, Y carry adjoints
+                const ad::Dual<kAdjW>* out[6] = {&r.X, &r.Y, &r.Z, &r.cX, &r.cY, &r.cZ};
+                for (int l = 0; l < kAdjW; ++l) {
+                    const int d = d0 + l;
+                    if (d >= ndir) break;
+                    double v = 0.0;
+                    for (int c = 0; c < 6; ++c) v += adj[c] * out[c]->d[l];
+                    if (d < 6) adj_in[d] = v;
+                    else g[sd.param[l]] += v;
+                }
+            }
+            for (int c = 0; c < 6; ++c) adj[c] = adj_in[c];
+        }
+    }
+    block_reduce_params(g, P, partial);
+}
+
+__global__ void k_adj_sum_partials(const double* partial, int n_blocks, int P, double* grad) {
+    const int p = threadIdx.x;
+    if (p >= P) return;
+    double s = 0.0;
+    for (int b = 0; b < n_blocks; ++b) s += partial[(size_t)b * P + p];
+    grad[p] = s;
+}
+
+// Forward-mode sensitivities along one parameter direction, through the whole
+// scheme from checkpoint 0 (the input rays).
+__global__ void __launch_bounds__(kAdjThreads) k_adj_jvp(AdjArgs a, const double* dtheta, double* dX, double* dY) {
+    const DevScheme* sch = a.sch;
+    const int ns = sch->n_surfaces;
+    for (size_t i = gtid(); i < a.n; i += gstride()) {
+        if (a.flag[i] != 1) {
+            dX[i] = 0.0;
+            dY[i] = 0.0;
+            continue;
+        }
+        const double lam = a.lambda[i];
+        const int b = beam_of(a.beams, a.n_beams, i);
+        ad::Seeds<1> sd;
+        sd.dense = dtheta;
+        sd.state[0] = -1;
+        sd.param[0] = -1;
+        double st[6];
+        for (int c = 0; c < 6; ++c) st[c] = a.ckpt[(size_t)c * a.n + i];
+        ad::RayD<1> r;
+        ad::load_state(st, sd, r);
+        for (int k = 0; k < ns; ++k) {
+            const DevSurface& s = sch->s[k];
+            ad::SurfD<1> sdv;
+            ad::make_surfd(s, k, a.map, a.n_params, sd, sdv);
+            ad::surface_step(s, sdv, sch->fixes, a.knots, order_of(s, a.beams, b), lam, r);
+        }
+        dX[i] = r.X.d[0];
+        dY[i] = r.Y.d[0];
+    }
+}
+
+// One wavelength group of the spot merit: rays first + m * stride, m < count.
+struct Group {
+    uint64_t first, stride, count;
+};
+
+// pass 0: count, sum X, sum Y; pass 1: sum of squared distances from the
+// centroid.  Block (part, g) sums a fixed slice of group g.
+__global__ void __launch_bounds__(kMeritThreads) k_group_moments(const Group* groups, const char* flag, const double* X,
+                                                                 const double* Y, const double* centroid, int pass,
+                                                                 double* partial) {
+    const int g = blockIdx.y, part = blockIdx.x;
+    const Group G = groups[g];
+    const uint64_t per = (G.count + kMeritParts - 1) / kMeritParts;
+    const uint64_t m0 = (uint64_t)part * per, m1 = (m0 + per < G.count) ? m0 + per : G.count;
+    double v[3] = {0, 0, 0};
+    const double cx = pass ? centroid[2 * g] : 0.0, cy = pass ? centroid[2 * g + 1] : 0.0;
+    for (uint64_t m = m0 + threadIdx.x; m < m1; m += blockDim.x) {
+        const uint64_t i = G.first + m * G.stride;
+        if (flag[i] != 1) continue;
+        if (pass == 0) {
+            v[0] += 1.0;
+            v[1] += X[i];
+            v[2] += Y[i];
+        } else {
+            const double dx = X[i] - cx, dy = Y[i] - cy;
+            v[0] += dx * dx + dy * dy;
+        }
+    }
+    __shared__ double red[3][kMeritThreads];
+    for (int c = 0; c < 3; ++c) red[c][threadIdx.x] = v[c];
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w)
+            for (int c = 0; c < 3; ++c) red[c][threadIdx.x] += red[c][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int c = 0; c < 3; ++c) partial[((size_t)g * kMeritParts + part) * 3 + c] = red[c][0];
+}
+
+// Seeds: gX = a_g (X - xbar) + b_g, gY = a_g (Y - ybar) for good rays.
+__global__ void k_group_seeds(const Group* groups, int n_groups, const double* coef, const char* flag, const double* X,
+                              const double* Y, double* gX, double* gY) {
+    const int g = blockIdx.y;
+    if (g >= n_groups) return;
+    const Group G = groups[g];
+    const double a = coef[4 * g], bx = coef[4 * g + 1], cx = coef[4 * g + 2], cy = coef[4 * g + 3];
+    for (uint64_t m = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; m < G.count; m += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t i = G.first + m * G.stride;
+        if (flag[i] == 1) {
+            gX[i] = a * (X[i] - cx) + bx;
+            gY[i] = a * (Y[i] - cy);
+        } else {
+            gX[i] = 0.0;
+            gY[i] = 0.0;
+        }
+    }
+}
+
+}  // namespace
+
+}  // namespace rtb
+
+using namespace rtb;
+
+struct rtb_adjoint {
+    int device = 0;
+    std::vector<rtb_surface> surf;                 // the scheme, tables repointed to...
+    std::vector<std::vector<double>> tables;       // ...these copies
+    std::vector<rtb_param> params;
+    std::vector<DevBeam> beams_h;
+    std::vector<rtb_beam> beams_in;
+    uint64_t n = 0;
+    uint32_t fixes = 0;
+    PreparedScheme ps;
+    bool have_forward = false;
+    // device
+    void* mem = nullptr;
+    DevScheme* d_sch = nullptr;
+    double* d_knots = nullptr;
+    size_t knots_cap = 0;
+    DevBeam* d_beams = nullptr;
+    ad::ParamRef* d_map = nullptr;
+    int* d_surf_params = nullptr;
+    int* d_surf_nparams = nullptr;
+    double* d_ckpt = nullptr;
+    double* d_lambda = nullptr;
+    char* d_flag = nullptr;
+    double* d_X = nullptr;
+    double* d_Y = nullptr;
+    unsigned long long* d_counts = nullptr;
+    unsigned* d_err = nullptr;
+    double* d_grad = nullptr;
+    double* d_dtheta = nullptr;
+    cudaStream_t stream = nullptr;
+};
+
+namespace {
+
+int check_param(const rtb_surface& s, const rtb_param& p) {
+    const bool conic = s.cls == RTB_CONIC, toric = s.cls == RTB_TORIC;
+    const int N = (s.cls == RTB_PLANE || s.cls == RTB_AUX_CLASS) ? 0 : (int)s.params[2];
+    switch (p.kind) {
+        case RTB_PARAM_CURVATURE:  // c = 0 switches a conic to the plane / polynomial algorithm
+            return ((conic || toric) && s.params[0] != 0.0) ? RTB_OK : RTB_BAD_VALUE;
+        case RTB_PARAM_CONIC:      // k = -1 selects the paraboloid's linear root
+            return ((conic && s.params[1] != -1.0) || toric) ? RTB_OK : RTB_BAD_VALUE;
+        case RTB_PARAM_POLY:
+            return ((conic || toric) && p.index >= 0 && p.index < N) ? RTB_OK : RTB_BAD_VALUE;
+        case RTB_PARAM_TORIC_CR:
+            return toric ? RTB_OK : RTB_BAD_VALUE;
+        case RTB_PARAM_DISTANCE:
+        case RTB_PARAM_ANGLE:
+            return (p.index >= 0 && p.index < 3) ? RTB_OK : RTB_BAD_VALUE;
+        case RTB_PARAM_GROOVE_DENSITY:
+            return (s.type == RTB_GRATING && s.gr_const > 0.0) ? RTB_OK : RTB_BAD_VALUE;
+        default:
+            return RTB_BAD_VALUE;
+    }
+}
+
+double get_param(const rtb_surface& s, const rtb_param& p) {
+    switch (p.kind) {
+        case RTB_PARAM_CURVATURE: return s.params[0];
+        case RTB_PARAM_CONIC: return s.params[1];
+        case RTB_PARAM_POLY: return s.params[3 + p.index];
+        case RTB_PARAM_TORIC_CR: return s.params[3 + (int)s.params[2]];
+        case RTB_PARAM_DISTANCE: return s.distance[p.index];
+        case RTB_PARAM_ANGLE: return s.angles_deg[p.index];
+        case RTB_PARAM_GROOVE_DENSITY: return 1000.0 / s.gr_const;
+        default: return 0.0;
+    }
+}
+
+void set_param(rtb_surface& s, const rtb_param& p, double v) {
+    switch (p.kind) {
+        case RTB_PARAM_CURVATURE: s.params[0] = v; break;
+        case RTB_PARAM_CONIC: s.params[1] = v; break;
+        case RTB_PARAM_POLY: s.params[3 + p.index] = v; break;
+        case RTB_PARAM_TORIC_CR: s.params[3 + (int)s.params[2]] = v; break;
+        case RTB_PARAM_DISTANCE: s.distance[p.index] = v; break;
+        case RTB_PARAM_ANGLE: s.angles_deg[p.index] = v; break;
+        case RTB_PARAM_GROOVE_DENSITY: s.gr_const = 1000.0 / v; break;
+        default: break;
+    }
+}
+
+void copy_table(rtb_table& t, std::vector<std::vector<double>>& store) {
+    if (t.n == 0 || !t.y) return;
+    std::vector<double> v;
+    const size_t n = t.n;
+    if (n == 1) {
+        v.assign(t.y, t.y + 1);
+        store.push_back(v);
+        t.y = store.back().data();
+        t.x = nullptr;
+        t.y2 = nullptr;
+        return;
+    }
+    v.resize(3 * n);
+    std::memcpy(v.data(), t.x, n * sizeof(double));
+    std::memcpy(v.data() + n, t.y, n * sizeof(double));
+    if (t.y2) std::memcpy(v.data() + 2 * n, t.y2, n * sizeof(double));
+    store.push_back(std::move(v));
+    const double* b = store.back().data();
+    t.x = b;
+    t.y = b + n;
+    t.y2 = t.y2 ? b + 2 * n : nullptr;
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+unsigned adj_grid(uint64_t n, int threads) {
+    size_t blocks = (n + threads - 1) / threads;
+    const size_t cap = (size_t)engine().sm_count * 8;
+    if (blocks > cap) blocks = cap;
+    return (unsigned)(blocks ? blocks : 1);
+}
+
+AdjArgs adj_args(const rtb_adjoint* c) {
+    AdjArgs a;
+    a.sch = c->d_sch;
+    a.knots = c->d_knots;
+    a.beams = c->d_beams;
+    a.n_beams = (int)c->beams_h.size();
+    a.map = c->d_map;
+    a.n_params = (int)c->params.size();
+    a.surf_params = c->d_surf_params;
+    a.surf_nparams = c->d_surf_nparams;
+    a.ckpt = c->d_ckpt;
+    a.lambda = c->d_lambda;
+    a.flag = c->d_flag;
+    a.X = c->d_X;
+    a.Y = c->d_Y;
+    a.n = c->n;
+    return a;
+}
+
+}  // namespace
+
+extern "C" {
+
+int rtb_adjoint_create(const rtb_surface* surfaces, size_t n_surfaces, const rtb_param* params, size_t n_params,
+                       const rtb_beam* beams, size_t n_beams, uint64_t n_rays, uint32_t fixes, rtb_adjoint** out) {
+    if (!out || !surfaces || n_surfaces == 0 || n_surfaces > RTB_MAX_SURFACES || !beams || n_beams == 0 ||
+        n_rays == 0 || (n_params && !params) || n_params > RTB_ADJ_MAX_PARAMS)
+        return RTB_BAD_VALUE;
+    *out = nullptr;
+    Lock l;
+    int st = ensure_init();
+    if (st != RTB_OK) return st;
+    rtb_adjoint* c = new rtb_adjoint();
+    cudaGetDevice(&c->device);
+    c->surf.assign(surfaces, surfaces + n_surfaces);
+    c->tables.reserve(2 * n_surfaces);
+    for (auto& s : c->surf) {
+        copy_table(s.n1, c->tables);
+        copy_table(s.n2, c->tables);
+    }
+    c->params.assign(params, params + n_params);
+    for (const auto& p : c->params) {
+        if (p.surface < 0 || p.surface >= (int)n_surfaces || check_param(c->surf[p.surface], p) != RTB_OK) {
+            delete c;
+            return RTB_BAD_VALUE;
+        }
+    }
+    c->n = n_rays;
+    c->fixes = fixes;
+    c->beams_in.assign(beams, beams + n_beams);
+    if ((st = check_beams(beams, n_beams, n_rays, c->beams_h)) != RTB_OK ||
+        (st = prepare_scheme(c->surf.data(), n_surfaces, fixes, 0, c->ps)) != RTB_OK) {
+        delete c;
+        return st;
+    }
+    // parameter lists per surface
+    std::vector<int> sp(n_surfaces * RTB_ADJ_MAX_PARAMS, -1), sn(n_surfaces, 0);
+    std::vector<ad::ParamRef> map(n_params ? n_params : 1);
+    for (size_t j = 0; j < n_params; ++j) {
+        const rtb_param& p = c->params[j];
+        map[j] = ad::ParamRef{p.surface, p.kind, p.index, 0};
+        sp[p.surface * RTB_ADJ_MAX_PARAMS + sn[p.surface]++] = (int)j;
+    }
+    // one allocation: scheme, knots (room for the largest table set), beams,
+    // map, lists, counters, grad; then the per-ray arrays
+    auto al = [](size_t x) { return (x + 255) / 256 * 256; };
+    c->knots_cap = c->ps.knots.size();
+    const size_t ns1 = 3 * n_surfaces + 1;
+    size_t off = 0;
+    const size_t o_sch = off; off += al(sizeof(DevScheme));
+    const size_t o_kn = off; off += al(c->knots_cap * sizeof(double));
+    const size_t o_bm = off; off += al(n_beams * sizeof(DevBeam));
+    const size_t o_map = off; off += al(map.size() * sizeof(ad::ParamRef));
+    const size_t o_sp = off; off += al(sp.size() * sizeof(int));
+    const size_t o_sn = off; off += al(sn.size() * sizeof(int));
+    const size_t o_cnt = off; off += al(n_beams * ns1 * 8);
+    const size_t o_err = off; off += 256;
+    const size_t o_grad = off; off += al(RTB_ADJ_MAX_PARAMS * sizeof(double));
+    const size_t o_dth = off; off += al(RTB_ADJ_MAX_PARAMS * sizeof(double));
+    const size_t o_ck = off; off += al(n_rays * 6 * n_surfaces * sizeof(double));
+    const size_t o_lam = off; off += al(n_rays * sizeof(double));
+    const size_t o_x = off; off += al(n_rays * sizeof(double));
+    const size_t o_y = off; off += al(n_rays * sizeof(double));
+    const size_t o_fl = off; off += al(n_rays);
+    cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&c->mem, off);
+    if (e != cudaSuccess) {
+        if (c->stream) cudaStreamDestroy(c->stream);
+        delete c;
+        return cuda_status(e);
+    }
+    char* b = static_cast<char*>(c->mem);
+    c->d_sch = reinterpret_cast<DevScheme*>(b + o_sch);
+    c->d_knots = reinterpret_cast<double*>(b + o_kn);
+    c->d_beams = reinterpret_cast<DevBeam*>(b + o_bm);
+    c->d_map = reinterpret_cast<ad::ParamRef*>(b + o_map);
+    c->d_surf_params = reinterpret_cast<int*>(b + o_sp);
+    c->d_surf_nparams = reinterpret_cast<int*>(b + o_sn);
+    c->d_counts = reinterpret_cast<unsigned long long*>(b + o_cnt);
+    c->d_err = reinterpret_cast<unsigned*>(b + o_err);
+    c->d_grad = reinterpret_cast<double*>(b + o_grad);
+    c->d_dtheta = reinterpret_cast<double*>(b + o_dth);
+    c->d_ckpt = reinterpret_cast<double*>(b + o_ck);
+    c->d_lambda = reinterpret_cast<double*>(b + o_lam);
+    c->d_X = reinterpret_cast<double*>(b + o_x);
+    c->d_Y = reinterpret_cast<double*>(b + o_y);
+    c->d_flag = b + o_fl;
+    e = cudaMemcpyAsync(c->d_beams, c->beams_h.data(), n_beams * sizeof(DevBeam), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(c->d_map, map.data(), map.size() * sizeof(ad::ParamRef), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(c->d_surf_params, sp.data(), sp.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(c->d_surf_nparams, sn.data(), sn.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) {
+        cudaFree(c->mem);
+        cudaStreamDestroy(c->stream);
+        delete c;
+        return cuda_status(e);
+    }
+    *out = c;
+    return RTB_OK;
+}
+
+int rtb_adjoint_theta(const rtb_adjoint* c, double* theta) {
+    if (!c || (!theta && !c->params.empty())) return RTB_BAD_VALUE;
+    for (size_t j = 0; j < c->params.size(); ++j) theta[j] = get_param(c->surf[c->params[j].surface], c->params[j]);
+    return RTB_OK;
+}
+
+int rtb_adjoint_forward(rtb_adjoint* c, const double* theta, const rtb_rays* rays, double* X, double* Y, char* flag,
+                        rtb_trace_stats* stats, void* stream) {
+    if (!c || !rays || rays->n != c->n || !rays->flag) return RTB_BAD_VALUE;
+    DeviceGuard dg(c->device);
+    Lock l;
+    cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+    std::vector<rtb_surface> sf = c->surf;
+    if (theta)
+        for (size_t j = 0; j < c->params.size(); ++j) {
+            if (c->params[j].kind == RTB_PARAM_GROOVE_DENSITY && !(theta[j] > 0.0)) return RTB_BAD_VALUE;
+            set_param(sf[c->params[j].surface], c->params[j], theta[j]);
+        }
+    PreparedScheme ps;
+    int st = prepare_scheme(sf.data(), sf.size(), c->fixes, 0, ps);
+    if (st != RTB_OK) return st;
+    // a parameter must not switch a surface's algorithm (check_param at create)
+    for (size_t k = 0; k < sf.size(); ++k)
+        if (ps.sch.s[k].kind != c->ps.sch.s[k].kind) return RTB_BAD_VALUE;
+    if (ps.knots.size() > c->knots_cap) return RTB_BAD_VALUE;
+    c->ps = ps;
+    const size_t ns1 = 3 * sf.size() + 1;
+    const size_t nb = c->beams_h.size();
+    RTB_CUDA_TRY(cudaMemcpyAsync(c->d_sch, &ps.sch, sizeof(DevScheme), cudaMemcpyHostToDevice, s));
+    RTB_CUDA_TRY(cudaMemcpyAsync(c->d_knots, ps.knots.data(), ps.knots.size() * sizeof(double), cudaMemcpyHostToDevice,
+                                 s));
+    RTB_CUDA_TRY(cudaMemsetAsync(c->d_counts, 0, nb * ns1 * 8, s));
+    RTB_CUDA_TRY(cudaMemsetAsync(c->d_err, 0, 4, s));
+    AdjArgs a = adj_args(c);
+    k_adj_forward<<<adj_grid(c->n, 256), 256, 0, s>>>(a, dev_rays(rays), c->d_counts, c->d_err);
+    RTB_CUDA_TRY(cudaGetLastError());
+    if (X) RTB_CUDA_TRY(cudaMemcpyAsync(X, c->d_X, c->n * 8, cudaMemcpyDeviceToDevice, s));
+    if (Y) RTB_CUDA_TRY(cudaMemcpyAsync(Y, c->d_Y, c->n * 8, cudaMemcpyDeviceToDevice, s));
+    if (flag) RTB_CUDA_TRY(cudaMemcpyAsync(flag, c->d_flag, c->n, cudaMemcpyDeviceToDevice, s));
+    std::vector<unsigned long long> counts(nb * ns1);
+    unsigned err = 0;
+    RTB_CUDA_TRY(cudaMemcpyAsync(counts.data(), c->d_counts, counts.size() * 8, cudaMemcpyDeviceToHost, s));
+    RTB_CUDA_TRY(cudaMemcpyAsync(&err, c->d_err, 4, cudaMemcpyDeviceToHost, s));
+    RTB_CUDA_TRY(cudaStreamSynchronize(s));
+    c->have_forward = true;
+    return trace_result(ps, counts.data(), err, (int)nb, stats);
+}
+
+int rtb_adjoint_backward(rtb_adjoint* c, const double* gX, const double* gY, double* grad, void* stream) {
+    if (!c || !gX || !gY || (!grad && !c->params.empty()) || !c->have_forward) return RTB_BAD_VALUE;
+    if (c->params.empty()) return RTB_OK;
+    DeviceGuard dg(c->device);
+    Lock l;
+    cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+    const int P = (int)c->params.size();
+    const unsigned grid = adj_grid(c->n, kAdjThreads);
+    DevBuf partial;
+    int st = partial.alloc((size_t)grid * P * sizeof(double), s);
+    if (st != RTB_OK) return st;
+    AdjArgs a = adj_args(c);
+    k_adj_backward<<<grid, kAdjThreads, 0, s>>>(a, gX, gY, partial.as<double>());
+    RTB_CUDA_TRY(cudaGetLastError());
+    k_adj_sum_partials<<<1, RTB_ADJ_MAX_PARAMS, 0, s>>>(partial.as<double>(), (int)grid, P, c->d_grad);
+    RTB_CUDA_TRY(cudaGetLastError());
+    RTB_CUDA_TRY(cudaMemcpyAsync(grad, c->d_grad, P * sizeof(double), cudaMemcpyDeviceToHost, s));
+    RTB_CUDA_TRY(cudaStreamSynchronize(s));
+    return RTB_OK;
+}
+
+int rtb_adjoint_jvp(rtb_adjoint* c, const double* dtheta, double* dX, double* dY, void* stream) {
+    if (!c || !dX || !dY || (!dtheta && !c->params.empty()) || !c->have_forward) return RTB_BAD_VALUE;
+    DeviceGuard dg(c->device);
+    Lock l;
+    cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+    std::vector<double> d(RTB_ADJ_MAX_PARAMS, 0.0);
+    for (size_t j = 0; j < c->params.size(); ++j) d[j] = dtheta[j];
+    RTB_CUDA_TRY(cudaMemcpyAsync(c->d_dtheta, d.data(), d.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+    AdjArgs a = adj_args(c);
+    k_adj_jvp<<<adj_grid(c->n, kAdjThreads), kAdjThreads, 0, s>>>(a, c->d_dtheta, dX, dY);
+    RTB_CUDA_TRY(cudaGetLastError());
+    RTB_CUDA_TRY(cudaStreamSynchronize(s));
+    return RTB_OK;
+}
+
+int rtb_adjoint_spot_merit(rtb_adjoint* c, const double* target_x, double weight, double* merit, double* gX,
+                           double* gY, void* stream) {
+    if (!c || !target_x || !merit || !c->have_forward || ((gX == nullptr) != (gY == nullptr))) return RTB_BAD_VALUE;
+    DeviceGuard dg(c->device);
+    Lock l;
+    cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+    std::vector<Group> groups;
+    for (const auto& b : c->beams_in) {
+        const uint64_t nl = b.n_lambda ? b.n_lambda : 1;
+        for (uint64_t j = 0; j < nl; ++j) {
+            const uint64_t cnt = (b.n_rays > j) ? (b.n_rays - j + nl - 1) / nl : 0;
+            groups.push_back(Group{b.first_ray + j, nl, cnt});
+        }
+    }
+    const int G = (int)groups.size();
+    if (G == 0 || G > 65535) return RTB_BAD_VALUE;
+    DevBuf buf;
+    const size_t part_bytes = (size_t)G * kMeritParts * 3 * sizeof(double);
+    int st = buf.alloc(G * sizeof(Group) + part_bytes + (size_t)G * 4 * sizeof(double) + 256, s);
+    if (st != RTB_OK) return st;
+    char* p = buf.as<char>();
+    Group* d_groups = reinterpret_cast<Group*>(p);
+    double* d_part = reinterpret_cast<double*>(p + (G * sizeof(Group) + 255) / 256 * 256);
+    double* d_coef = d_part + (size_t)G * kMeritParts * 3;
+    RTB_CUDA_TRY(cudaMemcpyAsync(d_groups, groups.data(), G * sizeof(Group), cudaMemcpyHostToDevice, s));
+    std::vector<double> part((size_t)G * kMeritParts * 3);
+    std::vector<double> cen(2 * G, 0.0), nn(G, 0.0), ss(G, 0.0);
+    for (int pass = 0; pass < 2; ++pass) {
+        if (pass == 1) RTB_CUDA_TRY(cudaMemcpyAsync(d_coef, cen.data(), 2 * G * sizeof(double), cudaMemcpyHostToDevice, s));
+        k_group_moments<<<dim3(kMeritParts, G), kMeritThreads, 0, s>>>(d_groups, c->d_flag, c->d_X, c->d_Y, d_coef, pass,
+                                                                      d_part);
+        RTB_CUDA_TRY(cudaGetLastError());
+        RTB_CUDA_TRY(cudaMemcpyAsync(part.data(), d_part, part.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+        RTB_CUDA_TRY(cudaStreamSynchronize(s));
+        for (int g = 0; g < G; ++g) {
+            double v[3] = {0, 0, 0};
+            for (int q = 0; q < kMeritParts; ++q)
+                for (int k = 0; k < 3; ++k) v[k] += part[((size_t)g * kMeritParts + q) * 3 + k];
+            if (pass == 0) {
+                nn[g] = v[0];
+                cen[2 * g] = v[0] > 0 ? v[1] / v[0] : 0.0;
+                cen[2 * g + 1] = v[0] > 0 ? v[2] / v[0] : 0.0;
+            } else {
+                ss[g] = v[0];
+            }
+        }
+    }
+    double M = 0.0;
+    std::vector<double> coef(4 * G, 0.0);
+    for (int g = 0; g < G; ++g) {
+        if (!(nn[g] > 0)) continue;
+        const double rms = std::sqrt(ss[g] / nn[g]);
+        const double dx = cen[2 * g] - target_x[g];
+        M += rms + weight * dx * dx;
+        coef[4 * g] = rms > 0 ? 1.0 / (nn[g] * rms) : 0.0;  // d rms / dX_i = (X_i - xbar) / (N rms)
+        coef[4 * g + 1] = 2.0 * weight * dx / nn[g];        // d w (xbar - t)^2 / dX_i
+        coef[4 * g + 2] = cen[2 * g];
+        coef[4 * g + 3] = cen[2 * g + 1];
+    }
+    *merit = M;
+    if (gX) {
+        RTB_CUDA_TRY(cudaMemsetAsync(gX, 0, c->n * sizeof(double), s));  // rays outside every group
+        RTB_CUDA_TRY(cudaMemsetAsync(gY, 0, c->n * sizeof(double), s));
+        RTB_CUDA_TRY(cudaMemcpyAsync(d_coef, coef.data(), coef.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+        k_group_seeds<<<dim3(64, G), 256, 0, s>>>(d_groups, G, d_coef, c->d_flag, c->d_X, c->d_Y, gX, gY);
+        RTB_CUDA_TRY(cudaGetLastError());
+        RTB_CUDA_TRY(cudaStreamSynchronize(s));
+    }
+    return RTB_OK;
+}
+
+int rtb_adjoint_destroy(rtb_adjoint* c) {
+    if (!c) return RTB_OK;
+    DeviceGuard dg(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->mem) cudaFree(c->mem);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return RTB_OK;
+}
+
+}  // extern "C"

@@ -46,6 +46,7 @@ struct DevSurface {
     double sinA[3], cosA[3];
     double size[2], center[2];
     int32_t n1_off, n1_n, n2_off, n2_n;  // tables: offset/count into the knot buffer (count 1 = single value)
+    double n1_invh, n2_invh;              // 1/knot spacing of a table on a uniform grid, else 0 (mixed engine)
 };
 
 // A prepared scheme in device memory; the fused kernels copy it to shared

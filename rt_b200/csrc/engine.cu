@@ -182,6 +182,46 @@ int prepare_scheme(const rtb_surface* surf, size_t n, uint32_t fixes, int renorm
         for (size_t j = k + 1; j < n; ++j) cnt += 1 + (out.sch.s[j].non_aux ? 1 : 0);
         out.sch.s[k].renorm_after = cnt;
     }
+    // identical tables share one copy (a lens's glass is the index after its
+    // front surface and before its back surface), and a table on a uniform
+    // grid records its inverse spacing for the mixed engine's direct lookup
+    auto same = [&](int32_t o1, int32_t o2, int32_t cnt) {
+        const int32_t len = (cnt == 1) ? 3 : 3 * cnt;
+        for (int32_t i = 0; i < len; ++i)
+            if (out.knots[o1 + i] != out.knots[o2 + i]) return false;
+        return true;
+    };
+    auto inv_spacing = [&](int32_t off, int32_t cnt) {
+        if (cnt < 2) return 0.0;
+        const double* x = out.knots.data() + off;
+        const double h = (x[cnt - 1] - x[0]) / (cnt - 1);
+        if (!(h > 0)) return 0.0;
+        for (int32_t i = 0; i < cnt; ++i)
+            if (std::fabs(x[i] - (x[0] + i * h)) > 1e-9 * h) return 0.0;
+        return 1.0 / h;
+    };
+    for (size_t k = 0; k < n; ++k) {
+        DevSurface& s = out.sch.s[k];
+        int32_t* offs[2] = {&s.n1_off, &s.n2_off};
+        int32_t cnts[2] = {s.n1_n, s.n2_n};
+        for (int t = 0; t < 2; ++t) {
+            for (size_t j = 0; j <= k; ++j) {
+                const DevSurface& e = out.sch.s[j];
+                const int32_t eo[2] = {e.n1_off, e.n2_off}, ec[2] = {e.n1_n, e.n2_n};
+                bool done = false;
+                for (int u = 0; u < 2 && !done; ++u) {
+                    if (j == k && u >= t) break;
+                    if (ec[u] == cnts[t] && eo[u] != *offs[t] && same(eo[u], *offs[t], cnts[t])) {
+                        *offs[t] = eo[u];
+                        done = true;
+                    }
+                }
+                if (done) break;
+            }
+        }
+        s.n1_invh = inv_spacing(s.n1_off, s.n1_n);
+        s.n2_invh = inv_spacing(s.n2_off, s.n2_n);
+    }
     out.sch.n_surfaces = (int32_t)n;
     out.sch.n_knots = (int32_t)out.knots.size();
     out.sch.fixes = fixes;

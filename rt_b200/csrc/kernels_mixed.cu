@@ -49,7 +49,7 @@ __device__ __forceinline__ double rsqrt_n(double x, int steps) {
 // sqrt(x) to FP64 accuracy; NaN for x < 0, 0 for x == 0.
 __device__ __forceinline__ double sqrt_(double x) {
     if (!(x > 0.0)) return (x == 0.0) ? 0.0 : __longlong_as_double(0x7ff8000000000000ll);
-    double y = rsqrt_n(x, 2);
+    double y = rsqrt_n(x, 1);
     double s = x * y;
     return fma(0.5 * y, fma(-s, s, x), s);  // one correction of the product
 }
@@ -177,46 +177,78 @@ __device__ __forceinline__ bool conic_isect(const DevSurface& s, Ray& r) {
 }
 
 // Even asphere (iterative_conic_intersection / iterative_poly_intersection,
-// surface.cu:257-333,497-561): the same surface and the same loss tests
-// (plane point behind the ray, grazing |dF| < 1e-7), with Newton started at
-// the base-conic root and run to |dt| < 1e-12 mm.
+// surface.cu:257-333,497-561): the same surface and loss tests (plane point
+// behind the ray, grazing |dF| < 1e-7), the root found differently.  With
+// w = Z - P(r^2), P the even polynomial, the asphere is the base conic's
+// quadric k1 w^2 + r^2 - 2 w / c = 0 on the branch the conic root selects, so
+// Newton on G(t) = k1 w^2 + r^2 - 2 w / c (a polynomial in the ray parameter:
+// no square root per step) from the base-conic root.  Newton converges
+// quadratically, the next correction being about |G''/2G'| dt^2 (< 1e-2 dt^2
+// for these surfaces), so the loop stops after a step below 1e-6 mm: the root
+// is then good to ~1e-14 mm.  One or two steps from the conic root; at most
+// eight for rays that start far from the surface (far outside the aperture).
 __device__ __forceinline__ bool asphere_isect(const DevSurface& s, Ray& r) {
     double s0 = -r.Z * rcp(r.cZ);
     bool poly_only = s.c == 0.0;
     if (poly_only ? !(s0 > 0) : !(s0 >= 0)) return false;
     double t = s0;
+    double ic = 0.0;
     if (!poly_only) {
         double tc;
         if (conic_root(s.c, s.k1, r, tc)) t = tc;
+        ic = rcp(s.c);
     }
-    for (int it = 0; it < 6; ++it) {
-        double x = fma(t, r.cX, r.X), y = fma(t, r.cY, r.Y), z = fma(t, r.cZ, r.Z);
-        double r2 = fma(x, x, y * y);
-        double sag = 0.0, E = 0.0;
-        if (!poly_only) {
-            double q = fma(-s.k1 * s.c * s.c, r2, 1.0);
-            if (!(q > 0.0)) break;  // outside the conic: keep the current point, as the reference does
-            double sq = sqrt_(q);
-            sag = s.c * r2 * rcp(1.0 + sq);
-            E = s.c * rcp(sq);
+    const int N = s.n_poly;
+    double x = 0, y = 0;
+    for (int it = 0; it < 8; ++it) {
+        x = fma(t, r.cX, r.X);
+        y = fma(t, r.cY, r.Y);
+        const double z = fma(t, r.cZ, r.Z);
+        const double r2 = fma(x, x, y * y);
+        // P(r2) = r2 Q(r2), Q = a_1 + a_2 r2 + ... + a_N r2^(N-1) by Horner
+        // with its derivative Q'; dP/dr2 = Q + r2 Q'
+        double Q = 0.0, dQ = 0.0;
+        for (int i = N; i >= 1; --i) {
+            dQ = fma(dQ, r2, Q);
+            Q = fma(Q, r2, s.poly[i - 1]);
         }
-        double psum = 0.0, dsum = 0.0, rr = 1.0;
-        for (int i = 1; i <= s.n_poly; ++i) {
-            dsum = fma((double)i * s.poly[i - 1], rr, dsum);
-            rr *= r2;
-            psum = fma(s.poly[i - 1], rr, psum);
+        const double P = Q * r2;
+        const double dP = fma(r2, dQ, Q);
+        const double dr2 = 2.0 * fma(x, r.cX, y * r.cY);  // d r2 / dt
+        const double w = z - P;
+        const double dw = fma(-dP, dr2, r.cZ);
+        double G, dG;
+        if (poly_only) {
+            G = w;
+            dG = dw;
+        } else {
+            G = fma(s.k1 * w, w, r2) - 2.0 * w * ic;
+            dG = fma(2.0 * s.k1 * w, dw, dr2) - 2.0 * dw * ic;
         }
-        sag += psum;
-        E = fma(2.0, dsum, E);
-        double F = z - sag;
-        double dF = fma(-E, fma(x, r.cX, y * r.cY), r.cZ);
-        if (fabs(dF) < K_ITER_EPS) return false;
-        double dt = F * rcp(dF);
+        const double dt = G * rcp(dG);
         t -= dt;
-        if (fabs(dt) < 1e-12) break;
+        if (!(fabs(dt) >= 1e-6)) break;
     }
-    r.X = fma(t, r.cX, r.X);
-    r.Y = fma(t, r.cY, r.Y);
+    if (!isfinite(t)) return false;  // no root near the ray (far outside any aperture)
+    x = fma(t, r.cX, r.X);
+    y = fma(t, r.cY, r.Y);
+    // the reference's grazing test on dF = cZ - E (x cX + y cY) at the root
+    {
+        const float xf = (float)x, yf = (float)y, c = (float)s.c;
+        const float r2 = fmaf(xf, xf, yf * yf);
+        float E = 0.0f;
+        if (!poly_only) {
+            const float q = fmaf(-(float)s.k1 * c * c, r2, 1.0f);
+            E = (q > 0.0f) ? c * rsqrtf(q) : 0.0f;
+        }
+        float sum = 0.0f, rr = 1.0f;
+        for (int i = 1; i <= N; ++i, rr *= r2) sum = fmaf((float)i * (float)s.poly[i - 1], rr, sum);
+        E = fmaf(2.0f, sum, E);
+        const float dF = fmaf(-E, fmaf(xf, (float)r.cX, yf * (float)r.cY), (float)r.cZ);
+        if (fabsf(dF) < (float)K_ITER_EPS) return false;
+    }
+    r.X = x;
+    r.Y = y;
     r.Z = fma(t, r.cZ, r.Z);
     return true;
 }
@@ -226,8 +258,9 @@ __device__ __forceinline__ bool asphere_isect(const DevSurface& s, Ray& r) {
 // Newton from the Z=0 plane point with the analytic derivative
 //   dF/dt = cZ - FY' cY - cR (X cX + Z cZ - FY FY' cY),  FY' = c Y / s,
 // s = sqrt(1 -+ k1 c^2 Y^2) (FY = c Y^2 / (1 + s) has this derivative for
-// either sign), to |dt| < 1e-12 mm in at most six steps.  As in the
-// reference, a ray is lost only when the plane point lies behind it.
+// either sign), until a step falls below 1e-6 mm (quadratic convergence: the
+// root is then good to ~1e-14 mm), at most six steps.  As in the reference, a
+// ray is lost only when the plane point lies behind it.
 __device__ __forceinline__ bool toric_isect(const DevSurface& s, uint32_t fixes, Ray& r) {
     const double sgn = (fixes & RTB_FIX_TORIC_SIGN) ? -1.0 : 1.0;
     double t = -r.Z * rcp(r.cZ);
@@ -243,7 +276,7 @@ __device__ __forceinline__ bool toric_isect(const DevSurface& s, uint32_t fixes,
         double dF = r.cZ - dFY * r.cY - s.cR * (fma(X, r.cX, Z * r.cZ) - FY * dFY * r.cY);
         double dt = F * rcp(dF);
         t -= dt;
-        if (!(fabs(dt) >= 1e-12)) break;
+        if (!(fabs(dt) >= 1e-6)) break;  // next correction ~|F''/2F'| dt^2 << 1e-12 mm
     }
     r.X = fma(t, r.cX, r.X);
     r.Y = fma(t, r.cY, r.Y);
@@ -344,8 +377,10 @@ __device__ __forceinline__ bool diffract(const DevSurface& s, double mu, double 
 }
 
 // Tabulated function with the divisions by the knot spacing replaced by a
-// reciprocal; same bisection and exact-knot rule as the plain engine.
-__device__ __forceinline__ bool table_eval(const double* tab, int n, double xval, double& out) {
+// reciprocal.  A table on a uniform grid (invh = 1/spacing > 0) finds its
+// interval directly, a non-uniform one by bisection; at a knot the spline
+// formula returns y there to rounding, so no exact-knot branch is needed.
+__device__ __forceinline__ bool table_eval(const double* tab, int n, double invh, double xval, double& out) {
     if (n == 1) {
         out = tab[1];
         return true;
@@ -354,14 +389,24 @@ __device__ __forceinline__ bool table_eval(const double* tab, int n, double xval
     const double* y = tab + n;
     const double* y2 = tab + 2 * n;
     if ((xval < x[0]) || (xval > x[n - 1])) return false;
-    int il = 0, ir = n;
-    while ((ir - il) > 1) {
-        int i = (il + ir) >> 1;
-        if (x[i] == xval) {
-            out = y[i];
-            return true;
+    int il, ir;
+    if (invh > 0.0) {
+        il = (int)((xval - x[0]) * invh);
+        il = il < 0 ? 0 : (il > n - 2 ? n - 2 : il);
+        if (x[il] > xval && il > 0) --il;
+        else if (x[il + 1] < xval && il < n - 2) ++il;
+        ir = il + 1;
+    } else {
+        il = 0;
+        ir = n;
+        while ((ir - il) > 1) {
+            int i = (il + ir) >> 1;
+            if (x[i] > xval) ir = i; else il = i;
         }
-        if (x[i] > xval) ir = i; else il = i;
+        if (ir == n) {  // xval == x[n-1]
+            il = n - 2;
+            ir = n - 1;
+        }
     }
     double h = x[ir] - x[il];
     double ih = rcp(h);
@@ -372,25 +417,49 @@ __device__ __forceinline__ bool table_eval(const double* tab, int n, double xval
     return true;
 }
 
+// The last table value a ray evaluated (a lens's glass is looked up by its
+// front and its back surface at the same wavelength).
+struct TableMemo {
+    int off = -1;
+    double v = 0.0;
+};
+
+__device__ __forceinline__ bool table_at(const double* knots, int off, int n, double invh, double lambda,
+                                         TableMemo& m, double& out) {
+    if (n == 1) {
+        out = knots[off + 1];
+        return true;
+    }
+    if (off == m.off) {
+        out = m.v;
+        return true;
+    }
+    if (!table_eval(knots + off, n, invh, lambda, out)) return false;
+    m.off = off;
+    m.v = out;
+    return true;
+}
+
 __device__ __forceinline__ int action(const DevSurface& s, const double* knots, long long order, double lambda,
-                                      Ray& r) {
+                                      TableMemo& memo, Ray& r) {
     if (s.type == RTB_MIRROR) {
         reflect(s, r);
         return 0;
     }
     if (s.type == RTB_LENS) {
         double a, b;
-        if (!table_eval(knots + s.n1_off, s.n1_n, lambda, a) || !table_eval(knots + s.n2_off, s.n2_n, lambda, b))
+        if (!table_at(knots, s.n1_off, s.n1_n, s.n1_invh, lambda, memo, a) ||
+            !table_at(knots, s.n2_off, s.n2_n, s.n2_invh, lambda, memo, b))
             return 2;
         return refract(s, a * rcp(b), r) ? 0 : 1;
     }
     if (s.type == RTB_GRATING) {
         double n2v, mu = 0.0;
-        if (!table_eval(knots + s.n2_off, s.n2_n, lambda, n2v)) return 2;
+        if (!table_at(knots, s.n2_off, s.n2_n, s.n2_invh, lambda, memo, n2v)) return 2;
         double in2 = rcp(n2v);
         if (s.gr_type == RTB_TRANSPARENT) {
             double n1v;
-            if (!table_eval(knots + s.n1_off, s.n1_n, lambda, n1v)) return 2;
+            if (!table_at(knots, s.n1_off, s.n1_n, s.n1_invh, lambda, memo, n1v)) return 2;
             mu = n1v * in2;
         }
         double L = (double)order * lambda * in2 * rcp(s.gr_const);
@@ -407,14 +476,14 @@ __device__ __forceinline__ int action(const DevSurface& s, const double* knots, 
 // rotations and the reflection, refraction and grating formulas preserve a
 // unit vector, so here the cosines are normalised once, when a ray is loaded.
 __device__ __forceinline__ int mx_surface(const DevSurface& s, int k, uint32_t fixes, const double* knots,
-                                          const DevBeam* beams, int b, double lam, mx::Ray& r) {
+                                          const DevBeam* beams, int b, double lam, mx::TableMemo& memo, mx::Ray& r) {
     mx::transform(s, r);
     if (!s.non_aux) return -1;
     if (!mx::intersect(s, fixes, r)) return 3 * k;
     if (!f64::aperture_pass(s.type == RTB_SHADE, s.shape, s.size, s.center, r.X, r.Y)) return 3 * k + 1;
     long long order = s.order;
     if (s.type == RTB_GRATING && beams[b].n_orders > 0) order = beams[b].orders[s.grating_index];
-    int a = mx::action(s, knots, order, lam, r);
+    int a = mx::action(s, knots, order, lam, memo, r);
     if (a == 2) return -2;
     if (a == 1) return 3 * k + 2;
     return -1;
@@ -435,6 +504,7 @@ __global__ void __maxnreg__(80) k_fused_mixed(const DevScheme* __restrict__ g_sc
     const uint64_t tile_rays = 32ull * (uint64_t)ts.rpt;
     const uint64_t n_tiles = (in.n + tile_rays - 1) / tile_rays;
     uint64_t tile;
+    int b = 0;
     while (next_tile(ts, n_tiles, tile)) {
         for (int j = 0; j < ts.rpt; ++j) {
             const size_t i = tile * tile_rays + (size_t)j * 32 + (threadIdx.x & 31);
@@ -445,9 +515,14 @@ __global__ void __maxnreg__(80) k_fused_mixed(const DevScheme* __restrict__ g_sc
                 mx::Ray r{in.X[i], in.Y[i], in.Z[i], in.cX[i], in.cY[i], in.cZ[i]};
                 mx::normalize(r);
                 const double lam = in.lambda[i];
-                const int b = beam_of(beams, n_beams, i);
+                // rays come in increasing order per thread: the previous
+                // ray's beam is usually this one's
+                if (!(b + 1 >= n_beams || i < beams[b + 1].first_ray) || i < beams[b].first_ray)
+                    b = beam_of(beams, n_beams, i);
+                mx::TableMemo memo;
                 int stage = -1;
-                for (int k = 0; k < ns && stage == -1; ++k) stage = mx_surface(sch->s[k], k, sch->fixes, s_knots, beams, b, lam, r);
+                for (int k = 0; k < ns && stage == -1; ++k)
+                    stage = mx_surface(sch->s[k], k, sch->fixes, s_knots, beams, b, lam, memo, r);
                 if (stage == -2) atomicOr(err, DEV_ERR_OUT_OF_RANGE);
                 if (stage >= 0) {
                     ev = true;

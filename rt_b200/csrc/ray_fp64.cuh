@@ -131,7 +131,7 @@ __device__ __forceinline__ bool conic_isect(const DevSurface& s, Ray& r) {
 
 // iterative_conic_intersection (rt_cuda_engine_surface.cu:257-333); the
 // iteration count is per ray and bounded by K_ITER_MAX.
-__device__ __forceinline__ bool iter_conic_isect(const DevSurface& s, Ray& r) {
+__device__ __forceinline__ bool iter_conic_isect(const DevSurface& s, bool fix_root, Ray& r) {
     double s0 = -r.Z / r.cZ;
     if (!(s0 >= 0)) return false;
     double s1, s2 = 0.0, Xi = 0, Yi = 0, Zi = 0;
@@ -159,6 +159,11 @@ __device__ __forceinline__ bool iter_conic_isect(const DevSurface& s, Ray& r) {
         ++niter;
         cyc.step(s2, 0.0, niter);
     } while ((fabs(s2 - s1) >= K_ITER_EPS) && (niter <= K_ITER_MAX));
+    if (fix_root && good && niter <= K_ITER_MAX) {  // RTB_FIX_ASPHERE_ROOT: the point of the last update
+        Xi = r.X + (s2 + s0) * r.cX;
+        Yi = r.Y + (s2 + s0) * r.cY;
+        Zi = s2 * r.cZ;
+    }
     r.X = Xi;
     r.Y = Yi;
     r.Z = Zi;
@@ -167,7 +172,7 @@ __device__ __forceinline__ bool iter_conic_isect(const DevSurface& s, Ray& r) {
 }
 
 // iterative_poly_intersection (rt_cuda_engine_surface.cu:497-561)
-__device__ __forceinline__ bool iter_poly_isect(const DevSurface& s, Ray& r) {
+__device__ __forceinline__ bool iter_poly_isect(const DevSurface& s, bool fix_root, Ray& r) {
     double s0 = -r.Z / r.cZ;
     if (!(s0 > 0)) return false;
     double s1, s2 = 0.0, Xi = 0, Yi = 0, Zi = 0;
@@ -192,6 +197,11 @@ __device__ __forceinline__ bool iter_poly_isect(const DevSurface& s, Ray& r) {
         ++niter;
         cyc.step(s2, 0.0, niter);
     } while ((fabs(s2 - s1) >= K_ITER_EPS) && (niter <= K_ITER_MAX));
+    if (fix_root && good && niter <= K_ITER_MAX) {  // RTB_FIX_ASPHERE_ROOT: the point of the last update
+        Xi = r.X + (s2 + s0) * r.cX;
+        Yi = r.Y + (s2 + s0) * r.cY;
+        Zi = s2 * r.cZ;
+    }
     r.X = Xi;
     r.Y = Yi;
     r.Z = Zi;
@@ -242,8 +252,8 @@ __device__ __forceinline__ bool intersect(const DevSurface& s, uint32_t fixes, R
         case IS_PLANE: return plane_isect(r);
         case IS_PARABOLOID: return paraboloid_isect(s, r);
         case IS_CONIC: return conic_isect(s, r);
-        case IS_ITER_POLY: return iter_poly_isect(s, r);
-        case IS_ITER_CONIC: return iter_conic_isect(s, r);
+        case IS_ITER_POLY: return iter_poly_isect(s, (fixes & RTB_FIX_ASPHERE_ROOT) != 0, r);
+        case IS_ITER_CONIC: return iter_conic_isect(s, (fixes & RTB_FIX_ASPHERE_ROOT) != 0, r);
         case IS_TORIC: return toric_isect(s, fixes, r);
         default: return true;
     }

@@ -44,6 +44,14 @@ def lib() -> C.CDLL:
         L.rtb_plan_set_config.argtypes = [vp, C.c_int32, C.c_int32]
         L.rtb_plan_config.argtypes = [vp, P(C.c_int32), P(C.c_int32), P(C.c_uint64)]
         L.rtb_plan_destroy.argtypes = [vp]
+        L.rtb_adjoint_create.argtypes = [P(ffi.Surface), C.c_size_t, P(ffi.Param), C.c_size_t, P(ffi.Beam),
+                                         C.c_size_t, C.c_uint64, C.c_uint32, P(vp)]
+        L.rtb_adjoint_theta.argtypes = [vp, vp]
+        L.rtb_adjoint_forward.argtypes = [vp, vp, P(ffi.Rays), vp, vp, vp, P(ffi.TraceStats), vp]
+        L.rtb_adjoint_backward.argtypes = [vp, vp, vp, vp, vp]
+        L.rtb_adjoint_jvp.argtypes = [vp, vp, vp, vp, vp]
+        L.rtb_adjoint_spot_merit.argtypes = [vp, vp, C.c_double, P(C.c_double), vp, vp, vp]
+        L.rtb_adjoint_destroy.argtypes = [vp]
         _bound = True
     return L
 
@@ -213,6 +221,85 @@ class Plan:
     def destroy(self):
         if self.h:
             lib().rtb_plan_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+class Adjoint:
+    """Gradients of CCD-plane positions with respect to scheme parameters
+    (rtb_adjoint_*): forward(theta) -> X, Y, flag (torch device tensors),
+    backward(gX, gY) -> dL/dtheta, jvp(dtheta) -> dX, dY, spot_merit()."""
+
+    def __init__(self, surfaces, params, beams, n_rays: int, fixes: int = 0):
+        import torch
+        self._surf = (ffi.Surface * len(surfaces))(*surfaces)
+        self._surfaces = surfaces
+        self.params = list(params)
+        self._params = (ffi.Param * max(1, len(self.params)))(*[ffi.Param(*p, 0) for p in self.params])
+        self._beams = _beams(beams)
+        self.n = n_rays
+        self.h = C.c_void_p()
+        ffi.check(lib().rtb_adjoint_create(self._surf, len(surfaces), self._params, len(self.params), self._beams,
+                                           len(beams), n_rays, fixes, C.byref(self.h)), "rtb_adjoint_create")
+        self.X = torch.empty(n_rays, dtype=torch.float64, device="cuda")
+        self.Y = torch.empty(n_rays, dtype=torch.float64, device="cuda")
+        self.flag = torch.empty(n_rays, dtype=torch.int8, device="cuda")
+
+    def theta(self) -> np.ndarray:
+        t = np.zeros(len(self.params))
+        ffi.check(lib().rtb_adjoint_theta(self.h, t.ctypes.data), "rtb_adjoint_theta")
+        return t
+
+    @staticmethod
+    def _sync():
+        # inputs made by torch on its stream must be complete before the
+        # library's stream reads them (the library's calls return synchronised)
+        import torch
+        torch.cuda.current_stream().synchronize()
+
+    def forward(self, theta, rays: "DeviceRays"):
+        self._sync()
+        th = None if theta is None else np.ascontiguousarray(theta, dtype=np.float64)
+        stats = ffi.TraceStats()
+        st = lib().rtb_adjoint_forward(self.h, None if th is None else th.ctypes.data, C.byref(rays.struct()),
+                                       ffi.vptr(self.X), ffi.vptr(self.Y), ffi.vptr(self.flag), C.byref(stats), None)
+        return st, stats
+
+    def backward(self, gX, gY) -> np.ndarray:
+        self._sync()
+        g = np.zeros(len(self.params))
+        ffi.check(lib().rtb_adjoint_backward(self.h, ffi.vptr(gX), ffi.vptr(gY), g.ctypes.data, None),
+                  "rtb_adjoint_backward")
+        return g
+
+    def jvp(self, dtheta):
+        import torch
+        d = np.ascontiguousarray(dtheta, dtype=np.float64)
+        self._sync()
+        dX = torch.empty(self.n, dtype=torch.float64, device="cuda")
+        dY = torch.empty(self.n, dtype=torch.float64, device="cuda")
+        ffi.check(lib().rtb_adjoint_jvp(self.h, d.ctypes.data, ffi.vptr(dX), ffi.vptr(dY), None), "rtb_adjoint_jvp")
+        return dX, dY
+
+    def spot_merit(self, target_x, weight: float):
+        import torch
+        t = np.ascontiguousarray(target_x, dtype=np.float64)
+        m = C.c_double(0.0)
+        gX = torch.empty(self.n, dtype=torch.float64, device="cuda")
+        gY = torch.empty(self.n, dtype=torch.float64, device="cuda")
+        self._sync()
+        ffi.check(lib().rtb_adjoint_spot_merit(self.h, t.ctypes.data, weight, C.byref(m), ffi.vptr(gX), ffi.vptr(gY),
+                                               None), "rtb_adjoint_spot_merit")
+        return m.value, gX, gY
+
+    def destroy(self):
+        if self.h:
+            lib().rtb_adjoint_destroy(self.h)
             self.h = C.c_void_p()
 
     def __del__(self):

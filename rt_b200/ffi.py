@@ -31,6 +31,7 @@ ENGINE_PER_SURFACE, ENGINE_FUSED = range(2)
 FP64, MIXED = range(2)
 FIX_TORIC_SIGN = 1
 FIX_TORIC_STEP = 2
+FIX_ASPHERE_ROOT = 4
 
 MAX_POLY = 10
 MAX_PARAMS = 16
@@ -80,6 +81,14 @@ class TraceOpts(C.Structure):
 class TraceStats(C.Structure):
     _fields_ = [("ray_surfaces", C.c_uint64), ("n_good", C.c_uint64), ("failed_beam", C.c_int32),
                 ("failed_stage", C.c_int32)]
+
+
+class Param(C.Structure):
+    _fields_ = [("surface", C.c_int32), ("kind", C.c_int32), ("index", C.c_int32), ("reserved", C.c_int32)]
+
+
+PARAM_CURVATURE, PARAM_CONIC, PARAM_POLY, PARAM_TORIC_CR, PARAM_DISTANCE, PARAM_ANGLE, PARAM_GROOVE_DENSITY = range(7)
+ADJ_MAX_PARAMS = 64
 
 
 class TuneEntry(C.Structure):

@@ -257,6 +257,28 @@ def c4_target_x(lam):
     return C4_TARGET[0] + C4_TARGET[1] * (np.asarray(lam) - 0.55)
 
 
+def c4_params() -> list[tuple[int, int, int]]:
+    """C4's 24 differentiable parameters as (surface, kind, index):
+    curvatures (collimator, camera, flattener), conic constants (camera,
+    flattener; the collimator's k = -1 selects the paraboloid algorithm and is
+    held), the flattener's A4..A10, the grating's groove density, the
+    collimator's decenter in y (its axial spacing does not act on a collimated
+    beam), the axial spacings of the other four surfaces, and tilts about x
+    and y of the grating, camera, flattener and CCD plus the collimator's tilt
+    about x."""
+    P = ffi
+    p = [(0, P.PARAM_CURVATURE, 0), (2, P.PARAM_CURVATURE, 0), (3, P.PARAM_CURVATURE, 0),
+         (2, P.PARAM_CONIC, 0), (3, P.PARAM_CONIC, 0)]
+    p += [(3, P.PARAM_POLY, i) for i in (1, 2, 3, 4)]          # A4, A6, A8, A10 (a2..a5)
+    p += [(1, P.PARAM_GROOVE_DENSITY, 0)]
+    p += [(0, P.PARAM_DISTANCE, 1)]                            # collimator decenter in y
+    p += [(k, P.PARAM_DISTANCE, 2) for k in range(1, 5)]       # axial spacings
+    p += [(k, P.PARAM_ANGLE, i) for k in (1, 2, 3, 4) for i in (1, 0)]
+    p += [(0, P.PARAM_ANGLE, 1)]
+    assert len(p) == 24
+    return p
+
+
 def c0_beams(n_per_lambda: int = 20000, seed: int = SEED, first_ray: int = 0) -> list[ffi.Beam]:
     return [make_beam(first_ray, n_per_lambda, C0_NLAMBDA, C0_RADIUS, C0_LAMBDA, seed)]
 

@@ -1,0 +1,236 @@
+"""Adjoint gradients (rtb_adjoint_*) on C4: C0's spectrograph extended with
+an even-asphere field flattener, 64 wavelengths over 0.40-0.70 um, 24
+parameters (GPU tests).
+
+* The forward is the plain FP64 engine: the same bits as rtb_trace's fused
+  FP64 trace, also with the parameters moved.
+* The backward (reverse sweep over surfaces from checkpoints) equals the
+  contraction of the forward-mode sensitivities with the same seeds.
+* Forward-mode sensitivities match central finite differences ray by ray.
+* The merit sum_lambda RMS + 10 (xbar - x_t(lambda))^2, differentiated
+  through a torch.autograd.Function around forward/backward, matches central
+  finite differences of the FP64 forward (relative step 1e-6) to 1e-6.
+"""
+import numpy as np
+import pytest
+import torch
+
+from rt_b200 import engine as E
+from rt_b200 import ffi, schemes as S
+
+pytestmark = pytest.mark.gpu
+
+WEIGHT = 10.0
+REL_STEP = 1e-6
+# the reference's asphere iteration reports the point before its last Newton
+# update (up to 1e-7 mm short of the root), which makes the forward jump when a
+# parameter moves the stopping decision; the gradient is of the converged model
+FIXES = ffi.FIX_ASPHERE_ROOT
+
+
+def setup(n_per_lambda=1600):
+    specs = S.littrow_free_asphere()
+    cs = S.to_c(specs, E.spline_init)
+    beams = S.c4_beams(n_per_lambda=n_per_lambda)
+    n = S.total_rays(beams)
+    rays = E.generate(beams, n)
+    torch.cuda.synchronize()
+    adj = E.Adjoint(cs.surfaces, S.c4_params(), beams, n, fixes=FIXES)
+    return specs, cs, beams, n, rays, adj
+
+
+def steps(theta):
+    return np.where(theta != 0.0, REL_STEP * np.abs(theta), REL_STEP)
+
+
+def group_ids(n, n_lambda=S.C4_NLAMBDA):
+    return torch.arange(n, device="cuda") % n_lambda
+
+
+def merit_difference(Xp, Yp, Xm, Ym, mask, G, target):
+    """M(+) - M(-) for two forwards on the same rays, summed from per-ray
+    differences (Xp - Xm is exact for nearby doubles), so that the finite
+    difference keeps its digits where M itself is ~1e5 times larger.
+    Rays are grouped by wavelength index i mod G (n = G * rays per group)."""
+    Xp, Yp, Xm, Ym = (torch.where(mask, a, torch.zeros_like(a)) for a in (Xp, Yp, Xm, Ym))
+    w = mask.double().view(-1, G)
+    N = w.sum(0)
+    mean = lambda a: (a.view(-1, G) * w).sum(0) / N  # noqa: E731
+    Dx, Dy = mean(Xp - Xm), mean(Yp - Ym)              # xbar+ - xbar-
+    Sx, Sy = mean(Xp + Xm), mean(Yp + Ym)              # xbar+ + xbar-
+    up, um = Xp.view(-1, G) - (Sx + Dx) / 2, Xm.view(-1, G) - (Sx - Dx) / 2
+    vp, vm = Yp.view(-1, G) - (Sy + Dy) / 2, Ym.view(-1, G) - (Sy - Dy) / 2
+    d_du = (Xp - Xm).view(-1, G) - Dx                  # u+ - u-, accurate
+    d_dv = (Yp - Ym).view(-1, G) - Dy
+    drms2 = ((d_du * (up + um) + d_dv * (vp + vm)) * w).sum(0) / N
+    rms_p = torch.sqrt(((up * up + vp * vp) * w).sum(0) / N)
+    rms_m = torch.sqrt(((um * um + vm * vm) * w).sum(0) / N)
+    return float((drms2 / (rms_p + rms_m)).sum() + WEIGHT * (Dx * (Sx - 2 * target)).sum())
+
+
+def merit_torch(X, Y, mask, gid, target, G):
+    X, Y = torch.where(mask, X, torch.zeros_like(X)), torch.where(mask, Y, torch.zeros_like(Y))
+    w = mask.double()
+    N = torch.zeros(G, dtype=torch.float64, device="cuda").index_add_(0, gid, w)
+    xbar = torch.zeros(G, dtype=torch.float64, device="cuda").index_add_(0, gid, X * w) / N
+    ybar = torch.zeros(G, dtype=torch.float64, device="cuda").index_add_(0, gid, Y * w) / N
+    d2 = ((X - xbar[gid]) ** 2 + (Y - ybar[gid]) ** 2) * w
+    rms = torch.sqrt(torch.zeros(G, dtype=torch.float64, device="cuda").index_add_(0, gid, d2) / N)
+    return (rms + WEIGHT * (xbar - target) ** 2).sum()
+
+
+class TraceFn(torch.autograd.Function):
+    """The shape rtb_adjoint_forward / rtb_adjoint_backward are made for."""
+
+    @staticmethod
+    def forward(ctx, theta, adj, rays):
+        st, _ = adj.forward(theta.detach().cpu().numpy(), rays)
+        assert st == ffi.OK
+        ctx.adj = adj
+        return adj.X.clone(), adj.Y.clone()
+
+    @staticmethod
+    def backward(ctx, gX, gY):
+        g = ctx.adj.backward(gX.contiguous(), gY.contiguous())
+        return torch.as_tensor(g, dtype=torch.float64), None, None
+
+
+def test_forward_equals_plain_fp64_engine():
+    specs, cs, beams, n, rays, adj = setup()
+    st, stats = adj.forward(None, rays)
+    ref = rays.copy()
+    st2, stats2 = E.trace(cs.surfaces, beams, ref, E.opts(engine=ffi.ENGINE_FUSED, precision=ffi.FP64, fixes=FIXES))
+    assert st == st2 == ffi.OK and stats.n_good == stats2.n_good and stats.ray_surfaces == stats2.ray_surfaces
+    assert torch.equal(adj.flag, ref.flag)
+    g = ref.flag == 1
+    assert torch.equal(adj.X[g].view(torch.int64), ref.X[g].view(torch.int64))
+    assert torch.equal(adj.Y[g].view(torch.int64), ref.Y[g].view(torch.int64))
+    # with every parameter moved: the plain engine on the moved scheme
+    theta = adj.theta()
+    moved = theta + steps(theta) * 1e3 * np.where(np.arange(len(theta)) % 2 == 0, 1.0, -1.0)
+    st, _ = adj.forward(moved, rays)
+    specs2 = [S.SurfaceSpec(**s.__dict__) for s in specs]
+    for (k, kind, idx), v in zip(S.c4_params(), moved):
+        sp = specs2[k]
+        if kind == ffi.PARAM_CURVATURE:
+            sp.params = (v, *sp.params[1:])
+        elif kind == ffi.PARAM_CONIC:
+            sp.params = (sp.params[0], v, *sp.params[2:])
+        elif kind == ffi.PARAM_POLY:
+            p = list(sp.params)
+            p[3 + idx] = v
+            sp.params = tuple(p)
+        elif kind == ffi.PARAM_DISTANCE:
+            d = list(sp.distance)
+            d[idx] = v
+            sp.distance = d
+        elif kind == ffi.PARAM_ANGLE:
+            a = list(sp.angles)
+            a[idx] = v
+            sp.angles = a
+        elif kind == ffi.PARAM_GROOVE_DENSITY:
+            sp.gr_const = 1000.0 / v
+    cs2 = S.to_c(specs2, E.spline_init)
+    ref = rays.copy()
+    st2, _ = E.trace(cs2.surfaces, beams, ref, E.opts(engine=ffi.ENGINE_FUSED, precision=ffi.FP64, fixes=FIXES))
+    assert st == st2 == ffi.OK
+    assert torch.equal(adj.flag, ref.flag)
+    g = ref.flag == 1
+    assert torch.equal(adj.X[g], ref.X[g]) and torch.equal(adj.Y[g], ref.Y[g])
+    adj.destroy()
+
+
+def test_backward_equals_forward_mode_contraction():
+    _, _, _, n, rays, adj = setup()
+    adj.forward(None, rays)
+    gen = torch.Generator(device="cuda").manual_seed(5)
+    gX = torch.randn(n, dtype=torch.float64, device="cuda", generator=gen)
+    gY = torch.randn(n, dtype=torch.float64, device="cuda", generator=gen)
+    grad = adj.backward(gX, gY)
+    P = len(grad)
+    for j in range(P):
+        e = np.zeros(P)
+        e[j] = 1.0
+        dX, dY = adj.jvp(e)
+        dot = float((gX * dX + gY * dY).sum())
+        assert abs(grad[j] - dot) <= 1e-10 * max(abs(dot), 1e-300) + 1e-300, (j, grad[j], dot)
+    # reproducible
+    assert np.array_equal(grad, adj.backward(gX, gY))
+    adj.destroy()
+
+
+def test_forward_mode_matches_central_differences_per_ray():
+    _, _, _, n, rays, adj = setup(n_per_lambda=400)
+    adj.forward(None, rays)
+    theta = adj.theta()
+    base_flag = adj.flag.clone()
+    h = steps(theta)
+    worst = []
+    for j in range(len(theta)):
+        e = np.zeros(len(theta))
+        e[j] = 1.0
+        dX, dY = adj.jvp(e)
+        out = []
+        for sgn in (1.0, -1.0):
+            adj.forward(theta + sgn * h[j] * e, rays)
+            out.append((adj.X.clone(), adj.Y.clone(), adj.flag.clone()))
+        adj.forward(None, rays)
+        m = (base_flag == 1) & (out[0][2] == 1) & (out[1][2] == 1)
+        fx = (out[0][0] - out[1][0]) / (2 * h[j])
+        fy = (out[0][1] - out[1][1]) / (2 * h[j])
+        # a central difference of a forward rounded to ~1e-13 of |X| carries
+        # an error of about 1e-13 |X| / h: allow that on top of 1e-6 relative
+        floor = 1e-13 * (adj.X.abs() + adj.Y.abs() + 1.0) / h[j]
+        err = torch.hypot(fx - dX, fy - dY)
+        tol = 1e-6 * torch.hypot(dX, dY) + floor
+        bad = int(((err > tol) & m).sum())
+        worst.append((j, bad, int(m.sum()), float((err / tol)[m].max())))
+    print(worst)
+    for j, bad, nm, ratio in worst:
+        assert bad <= 1e-3 * nm, (j, bad, nm, ratio)
+    adj.destroy()
+
+
+@pytest.mark.parametrize("n_per_lambda", [1600, 156250])
+def test_merit_gradient_matches_central_differences(n_per_lambda):
+    """C4 at 1e5 rays and at its full 1e7 rays."""
+    _, _, beams, n, rays, adj = setup(n_per_lambda)
+    theta0 = adj.theta()
+    P = len(theta0)
+    h = steps(theta0)
+    gid = group_ids(n)
+    lam = np.linspace(S.C4_LAMBDA[0], S.C4_LAMBDA[1], S.C4_NLAMBDA)
+    target = torch.as_tensor(S.c4_target_x(lam), dtype=torch.float64, device="cuda")
+    # the rays good at theta0 and at every finite-difference point
+    adj.forward(None, rays)
+    mask = adj.flag == 1
+    pts = []
+    for j in range(P):
+        for sgn in (1.0, -1.0):
+            t = theta0.copy()
+            t[j] += sgn * h[j]
+            st, _ = adj.forward(t, rays)
+            assert st == ffi.OK
+            mask &= adj.flag == 1
+            pts.append((adj.X.clone(), adj.Y.clone()))
+    fd = np.array([merit_difference(*pts[2 * j], *pts[2 * j + 1], mask, S.C4_NLAMBDA, target) / (2 * h[j])
+                   for j in range(P)])
+    del pts
+    # adjoint: merit in torch on the same rays, gradient through TraceFn
+    theta = torch.tensor(theta0, dtype=torch.float64, requires_grad=True)
+    X, Y = TraceFn.apply(theta, adj, rays)
+    M = merit_torch(X, Y, mask, gid, target, S.C4_NLAMBDA)
+    M.backward()
+    g = theta.grad.numpy()
+    rel = np.abs(g - fd) / np.abs(fd)
+    print("merit", float(M), "rel err", rel.max(), list(zip(range(P), g, fd, rel)))
+    assert np.all(np.abs(fd) > 0)
+    assert rel.max() <= 1e-6, (int(np.argmax(rel)), rel.max())
+    # the library's own merit and seeds agree with torch's on the forward's good rays
+    adj.forward(None, rays)
+    if bool(torch.equal(mask, adj.flag == 1)):
+        m_lib, gX, gY = adj.spot_merit(S.c4_target_x(lam), WEIGHT)
+        assert abs(m_lib - float(M)) <= 1e-12 * abs(float(M))
+        g_lib = adj.backward(gX, gY)
+        assert np.allclose(g_lib, g, rtol=1e-9, atol=0)
+    adj.destroy()

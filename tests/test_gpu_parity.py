@@ -26,7 +26,7 @@ SCHEMES = {
     "lenses": (lambda: S.coverage_schemes()["lenses"], dict(n_lambda=5, radius=10.0, lam_range=(0.4, 0.8)), ()),
     "gratings": (lambda: S.coverage_schemes()["gratings"], dict(n_lambda=5, radius=10.0, lam_range=(0.4, 0.8)), ()),
 }
-FIXES = [0, ffi.FIX_TORIC_SIGN | ffi.FIX_TORIC_STEP]
+FIXES = [0, ffi.FIX_TORIC_SIGN | ffi.FIX_TORIC_STEP, ffi.FIX_TORIC_SIGN | ffi.FIX_TORIC_STEP | ffi.FIX_ASPHERE_ROOT]
 
 
 def same_bits(a, b):

@@ -62,7 +62,7 @@ def test_literal_equals_reference_host_classes(case):
 
 
 @pytest.mark.parametrize("case", list(CASES))
-@pytest.mark.parametrize("fixes", [0, ffi.FIX_TORIC_SIGN | ffi.FIX_TORIC_STEP])
+@pytest.mark.parametrize("fixes", [0, ffi.FIX_TORIC_SIGN | ffi.FIX_TORIC_STEP, 7])
 def test_per_ray_equals_literal(case, fixes):
     specs, beam = _beam(case, n_per=80, seed=7)
     cs = S.to_c(specs, O.spline_init)
