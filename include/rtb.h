@@ -379,6 +379,67 @@ RTB_API int rtb_plan_config(const rtb_plan* plan, int32_t* block_size, int32_t* 
 RTB_API int rtb_plan_destroy(rtb_plan* plan);
 
 /* =========================================================================
+ * 5. Scheme files: the reference's scheme XML (Scheme::load_from_file,
+ *    common-lib/scheme.cpp:272-857) read without Mini-XML.  Values are element
+ *    texts; n1/n2 and the beam range may name files (two-column tables of at
+ *    least 4 rows; range rows "w1 w2 order_1 .. order_G"), looked up relative
+ *    to the working directory as the reference does, then to the scheme
+ *    file's directory.  Surfaces are taken in document order.
+ * ========================================================================= */
+enum { RTB_BEAM_PARALLEL = 0, RTB_BEAM_CONIC = 1, RTB_BEAM_GAUSS = 2 };          /* beam.h:31 */
+enum { RTB_PROFILE_RANDOM = 0, RTB_PROFILE_CONCENTRIC = 1 };                      /* beam.h:33 */
+enum { RTB_RANGE_RANDOM = 0, RTB_RANGE_UNIFORM = 1, RTB_RANGE_MONOCHROMATIC = 2 }; /* beam.h:34 */
+enum { RTB_SCHEME_NAME = 0, RTB_SCHEME_RESULT_FILE = 1, RTB_SCHEME_LOG_FILE = 2, RTB_SCHEME_COMMENT = 3 };
+typedef struct rtb_scheme rtb_scheme;
+/* The <beam> element (scheme.cpp:684-850). */
+typedef struct rtb_scheme_beam {
+    int32_t type;          /* RTB_BEAM_* */
+    int32_t shape;         /* RTB_CIRCLE / RTB_RECTANGLE */
+    int32_t profile;       /* RTB_PROFILE_* */
+    int32_t range_distr;   /* RTB_RANGE_* */
+    double params[6];      /* N, R_in, R_out [, ratio] [, angle or fwhm] */
+    int32_t n_params;
+    int32_t reserved;
+    double center[3];
+    uint64_t n_lambda;     /* 0: not a composite beam */
+} rtb_scheme_beam;
+/* Load a scheme file.  On failure returns RTB_BAD_VALUE (RTB_BAD_ALLOC) and,
+ * when scheme_error is not NULL, the Scheme::SchemeError the reference throws
+ * (scheme.h:25-27: 0 FileOpenFailure, 1 ParseFailure, 3 BadAttrValue, ...). */
+RTB_API int rtb_scheme_load(const char* path, rtb_scheme** scheme, int* scheme_error);
+/* The surfaces as rtb_surface (valid until rtb_scheme_free; tables included). */
+RTB_API int rtb_scheme_surfaces(const rtb_scheme* scheme, const rtb_surface** surfaces, size_t* n);
+/* RTB_SCHEME_NAME, _RESULT_FILE, _LOG_FILE, or RTB_SCHEME_COMMENT + k for
+ * surface k's comment; NULL if out of range. */
+RTB_API const char* rtb_scheme_text(const rtb_scheme* scheme, int which);
+RTB_API int rtb_scheme_get_beam(const rtb_scheme* scheme, rtb_scheme_beam* beam);
+/* Wavelength ranges, n_rows rows of row_len numbers: w1 w2 and, for a range
+ * file, one order per grating in scheme order (scheme.cpp:1026-1032). */
+RTB_API int rtb_scheme_ranges(const rtb_scheme* scheme, const double** rows, size_t* n_rows, size_t* row_len);
+RTB_API void rtb_scheme_free(rtb_scheme* scheme);
+
+/* ---- result files ---------------------------------------------------------- */
+/* Write beam [first, first+n) of the device arrays `rays` as a .dat file
+ * (Beam::Save, common-lib/beam.cpp:636-715): size_t n, n_good, n_lambda, then
+ * X Y Z cX cY cZ lambda of the good rays, then of the lost rays, in the
+ * reference's order: order (device) as rtb_reference_order fills it
+ * (order[first + k] is the beam-local index of the ray at position k;
+ * positions [0, n_good) are the good rays).  Synchronous. */
+RTB_API int rtb_save_dat(const char* path, const rtb_rays* rays, const uint32_t* order, uint64_t first, uint64_t n,
+                         uint64_t n_good, uint64_t n_lambda, void* stream);
+/* Header of a .dat file. */
+RTB_API int rtb_read_dat_header(const char* path, uint64_t* n, uint64_t* n_good, uint64_t* n_lambda);
+/* Read a .dat file into host arrays of host_rays->n rays (flag, if given,
+ * becomes 1 for the first n_good rays and 0 after). */
+RTB_API int rtb_read_dat(const char* path, const rtb_rays* host_rays);
+/* Write an image (host, xdim x ydim doubles, row-major, x fastest) as a FITS
+ * file with BITPIX -64, as ccd_frame writes its image (ccd/ccd_frame.cpp:
+ * 263-314), plus n_keys string keywords (RT_LIST, QE_FILE, SPECFILE, CCDINFO in
+ * the reference). */
+RTB_API int rtb_write_fits(const char* path, const double* image, uint64_t xdim, uint64_t ydim,
+                           const char* const* keys, const char* const* values, size_t n_keys);
+
+/* =========================================================================
  * 4. Adjoint: gradients of the CCD-plane positions with respect to scheme
  *    parameters (no counterpart in the reference).  A forward/backward pair
  *    of the shape a torch.autograd.Function wraps: forward(theta) -> X, Y per

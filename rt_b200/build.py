@@ -27,6 +27,8 @@ SOURCES = {
     "noalloc.cu": ["--fmad=false"],
     "plan.cu": ["--fmad=false"],
     "adjoint.cu": ["--fmad=false"],
+    "scheme_xml.cpp": [],
+    "io.cu": [],
 }
 
 
@@ -51,7 +53,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
     objs = []
     for src, flags in SOURCES.items():
         s = os.path.join(CSRC, src)
-        o = os.path.join(BUILD, src.replace(".cu", ".o"))
+        o = os.path.join(BUILD, os.path.splitext(src)[0] + ".o")
         objs.append(o)
         if force or _stale(o, s):
             cmd = [nvcc()] + ARCH + COMMON + flags + ["-c", s, "-o", o]
@@ -63,7 +65,29 @@ def build(verbose: bool = False, force: bool = False) -> str:
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
+    build_programs(verbose, force)
     return LIB
+
+
+# Host programs over the C ABI (rt_b200/host/*.cpp -> rt_b200/bin/), linked
+# against librtb200.so with a run path relative to the program.
+PROGRAMS = ["rt_trace"]
+BIN = os.path.join(HERE, "bin")
+
+
+def build_programs(verbose: bool = False, force: bool = False) -> None:
+    os.makedirs(BIN, exist_ok=True)
+    for name in PROGRAMS:
+        src = os.path.join(HERE, "host", name + ".cpp")
+        out = os.path.join(BIN, name)
+        if not force and os.path.exists(out) and os.path.getmtime(out) >= max(
+                os.path.getmtime(src), os.path.getmtime(LIB)):
+            continue
+        cmd = [nvcc(), "-O2", "-std=c++17", "-Wno-deprecated-gpu-targets", src, "-I" + os.path.join(HERE, "..", "include"), "-L" + HERE,
+               "-lrtb200", "-lcudart", "-Xlinker", "-rpath,$ORIGIN/..", "-o", out]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
 
 
 if __name__ == "__main__":

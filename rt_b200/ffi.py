@@ -91,6 +91,12 @@ PARAM_CURVATURE, PARAM_CONIC, PARAM_POLY, PARAM_TORIC_CR, PARAM_DISTANCE, PARAM_
 ADJ_MAX_PARAMS = 64
 
 
+class SchemeBeam(C.Structure):
+    _fields_ = [("type", C.c_int32), ("shape", C.c_int32), ("profile", C.c_int32), ("range_distr", C.c_int32),
+                ("params", C.c_double * 6), ("n_params", C.c_int32), ("reserved", C.c_int32),
+                ("center", C.c_double * 3), ("n_lambda", C.c_uint64)]
+
+
 class TuneEntry(C.Structure):
     _fields_ = [("block_size", C.c_int32), ("rays_per_thread", C.c_int32), ("ms", C.c_double)]
 

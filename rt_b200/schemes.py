@@ -481,3 +481,154 @@ def coverage_schemes() -> dict[str, list[SurfaceSpec]]:
                     distance=(-20.850663, 0.0, -21.569651), angles=(-135.971022, 0.0, 0.0), comment="detector"),
     ]
     return {"mirrors": mirrors, "lenses": lenses, "gratings": gratings}
+
+
+# ---------------------------------------------------------------------------
+# scheme files in the reference's format (common-lib/scheme.cpp:272-857)
+
+_CLASS = {ffi.PLANE: "PLANE", ffi.CONIC: "CONIC", ffi.TORIC: "TORIC", ffi.AUX_CLASS: "AUX"}
+_TYPE = {ffi.MIRROR: "MIRROR", ffi.LENS: "LENS", ffi.GRATING: "GRATING", ffi.STOP: "STOP", ffi.SHADE: "SHADE",
+         ffi.DETECTOR: "DETECTOR", ffi.AUX_TYPE: "AUX"}
+
+
+def _num(v) -> str:
+    return " ".join(repr(float(x)) for x in (v if isinstance(v, (list, tuple, np.ndarray)) else [v]))
+
+
+def write_table(path: str, x, y) -> None:
+    """Two-column table file (TabulatedFunction::Load), newline-terminated."""
+    with open(path, "w") as f:
+        f.write("# lambda(um) value\n")
+        for a, b in zip(x, y):
+            f.write(f"{float(a)!r} {float(b)!r}\n")
+
+
+def write_xml(path: str, specs: Sequence[SurfaceSpec], name: str, result_file: str, n_per_lambda: int,
+              radius: float, ranges: Sequence[Sequence[float]], n_lambda: int = 0) -> None:
+    """Write a scheme file the reference's ray-tracing program reads: values
+    as element texts on one line, tables and (for more than one range) the
+    range rows "w1 w2 order_1 .. order_G" in files beside it."""
+    import os
+    d = os.path.dirname(os.path.abspath(path))
+    base = os.path.splitext(os.path.basename(path))[0]
+    tables = {}
+
+    def table_ref(t):
+        if isinstance(t, (int, float)):
+            return _num(t)
+        key = (tuple(np.asarray(t[0]).tolist()), tuple(np.asarray(t[1]).tolist()))
+        if key not in tables:
+            fn = f"{base}_table{len(tables)}.txt"
+            write_table(os.path.join(d, fn), t[0], t[1])
+            tables[key] = fn
+        return tables[key]
+
+    L = ['<?xml version="1.0"?>', "<scheme>", "  <general>", f"    <name>{name}</name>",
+         f"    <result_file>{result_file}</result_file>", "  </general>"]
+    for s in specs:
+        L.append("  <surface>")
+        L.append(f"    <class>{_CLASS[s.cls]}</class>")
+        if s.cls != ffi.AUX_CLASS:
+            L.append(f"    <type>{_TYPE[s.type]}</type>")
+            L.append(f"    <shape>{'CIRC' if s.shape == ffi.CIRCLE else 'RECT'}</shape>")
+            L.append(f"    <params>{_num(list(s.params))}</params>")
+            L.append(f"    <size>{_num(list(s.size) if s.shape == ffi.RECTANGLE else [s.size[0]])}</size>")
+            L.append(f"    <center>{_num(list(s.center))}</center>")
+        L.append(f"    <distance>{_num(list(s.distance))}</distance>")
+        L.append(f"    <angles>{_num(list(s.angles))}</angles>")
+        if s.comment:
+            L.append(f"    <comment>{s.comment}</comment>")
+        if s.type == ffi.GRATING:
+            L.append(f"    <grating_type>{'TRANSPARENT' if s.grating_type == ffi.TRANSPARENT else 'REFLECTIVE'}"
+                     "</grating_type>")
+            L.append(f"    <order>{int(s.order)}</order>")
+            L.append(f"    <const>{_num(s.gr_const)}</const>")
+        if s.type in (ffi.GRATING, ffi.LENS):
+            L.append(f"    <n1>{table_ref(s.n1)}</n1>")
+            L.append(f"    <n2>{table_ref(s.n2)}</n2>")
+        L.append("  </surface>")
+    if len(ranges) == 1 and len(ranges[0]) == 2:
+        rng = _num(list(ranges[0]))
+    else:
+        rng = f"{base}_ranges.txt"
+        with open(os.path.join(d, rng), "w") as f:
+            f.write("# w1 w2 orders of the gratings in scheme order\n")
+            for r in ranges:
+                f.write(" ".join([repr(float(r[0])), repr(float(r[1]))] + [str(int(o)) for o in r[2:]]) + "\n")
+    L += ["  <beam>", "    <type>PARALLEL</type>", "    <shape>CIRC</shape>", "    <profile>RANDOM</profile>",
+          "    <range_distr>UNIFORM</range_distr>", f"    <params>{n_per_lambda} 0 {_num(radius)}</params>",
+          "    <center>0 0 0</center>", f"    <range>{rng}</range>"]
+    if n_lambda:
+        L.append(f"    <nlambda>{int(n_lambda)}</nlambda>")
+    L += ["  </beam>", "</scheme>", ""]
+    with open(path, "w") as f:
+        f.write("\n".join(L))
+
+
+class LoadedScheme:
+    """A scheme file read by the library (rtb_scheme_load): `surfaces` are
+    rtb_surface structs (valid while this object lives), `beam` the <beam>
+    element, `ranges` an (n, row_len) array, plus name / result_file /
+    log_file / comments."""
+
+    def __init__(self, path: str):
+        L = ffi.load()
+        L.rtb_scheme_load.argtypes = [C.c_char_p, C.POINTER(C.c_void_p), C.POINTER(C.c_int)]
+        L.rtb_scheme_surfaces.argtypes = [C.c_void_p, C.POINTER(C.POINTER(ffi.Surface)), C.POINTER(C.c_size_t)]
+        L.rtb_scheme_text.argtypes = [C.c_void_p, C.c_int]
+        L.rtb_scheme_text.restype = C.c_char_p
+        L.rtb_scheme_get_beam.argtypes = [C.c_void_p, C.POINTER(ffi.SchemeBeam)]
+        L.rtb_scheme_ranges.argtypes = [C.c_void_p, C.POINTER(C.POINTER(C.c_double)), C.POINTER(C.c_size_t),
+                                        C.POINTER(C.c_size_t)]
+        L.rtb_scheme_free.argtypes = [C.c_void_p]
+        self._L = L
+        self.h = C.c_void_p()
+        err = C.c_int(-1)
+        self.status = L.rtb_scheme_load(path.encode(), C.byref(self.h), C.byref(err))
+        self.scheme_error = err.value
+        if self.status != ffi.OK:
+            self.h = C.c_void_p()
+            return
+        p = C.POINTER(ffi.Surface)()
+        n = C.c_size_t()
+        ffi.check(L.rtb_scheme_surfaces(self.h, C.byref(p), C.byref(n)), "rtb_scheme_surfaces")
+        self.surfaces = [p[i] for i in range(n.value)]
+        for s in self.surfaces:
+            s._owner = self
+        self.beam = ffi.SchemeBeam()
+        ffi.check(L.rtb_scheme_get_beam(self.h, C.byref(self.beam)), "rtb_scheme_get_beam")
+        rp = C.POINTER(C.c_double)()
+        nr, rl = C.c_size_t(), C.c_size_t()
+        ffi.check(L.rtb_scheme_ranges(self.h, C.byref(rp), C.byref(nr), C.byref(rl)), "rtb_scheme_ranges")
+        self.ranges = np.array([rp[i] for i in range(nr.value * rl.value)]).reshape(nr.value, rl.value)
+        txt = lambda k: (L.rtb_scheme_text(self.h, k) or b"").decode()  # noqa: E731
+        self.name, self.result_file, self.log_file = txt(0), txt(1), txt(2)
+        self.comments = [txt(3 + k) for k in range(n.value)]
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self._L.rtb_scheme_free(self.h)
+            self.h = C.c_void_p()
+
+
+def benchmark_scheme_files(out_dir: str) -> list[str]:
+    """Write C0, C1 and C4 as scheme files (with their tables and C1's range
+    file of one row per echelle order)."""
+    import os
+    os.makedirs(out_dir, exist_ok=True)
+    c0 = os.path.join(out_dir, "c0_littrow_free.xml")
+    write_xml(c0, littrow_free(), "C0 Littrow-free spectrograph", "c0", 20000, C0_RADIUS,
+              [list(C0_LAMBDA)], n_lambda=C0_NLAMBDA)
+    c1 = os.path.join(out_dir, "c1_echelle.xml")
+    write_xml(c1, echelle(), "C1 cross-dispersed echelle", "c1", c1_rays_per_lambda(), C1_RADIUS,
+              [[C1_LAMBDA[0], C1_LAMBDA[1], m, 1] for m in C1_ORDERS], n_lambda=C1_NLAMBDA)
+    c4 = os.path.join(out_dir, "c4_littrow_free_flattener.xml")
+    write_xml(c4, littrow_free_asphere(), "C4 Littrow-free spectrograph with an aspheric field flattener", "c4",
+              156250, C0_RADIUS, [list(C4_LAMBDA)], n_lambda=C4_NLAMBDA)
+    return [c0, c1, c4]
+
+
+if __name__ == "__main__":
+    import sys
+    for p in benchmark_scheme_files(sys.argv[1] if len(sys.argv) > 1 else "."):
+        print(p)

@@ -67,7 +67,7 @@ def cases():
     return {
         "c0": (S.littrow_free(), c0, (), 400),
         "c0_asphere_camera": (S.c0_asphere_camera(), c0, (), 400),
-        "c4": (scalarize(S.littrow_free_asphere()), c4, (), 400),
+        "c4": (scalarize(S.littrow_free_asphere()), c4, (), 100),
         "c1_m38": (scalarize(S.echelle()), c1, (38, 1), 40),
         "c1_m52": (scalarize(S.echelle()), c1, (52, 1), 40),
         "c1_sphere_m38": (sphere_fold(scalarize(S.echelle())), c1, (38, 1), 40),
