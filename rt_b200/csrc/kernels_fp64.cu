@@ -199,9 +199,12 @@ __global__ void k_generate(const GenBeam* beams, int n_beams, uint64_t total, De
 // Normalize of surface k, and written back; a ray lost here gets
 // lost_stage, flag 0 and the Normalize calls the reference would still
 // apply to it.  After the last surface the survivors are counted.
-__global__ void __launch_bounds__(256) k_surface_step(const DevScheme* __restrict__ sch, int k, const double* knots,
-                                                      const DevBeam* beams, int n_beams, DevRays in, DevRays out,
-                                                      unsigned long long* counts, unsigned* err) {
+// 64 registers: four 256-thread blocks per SM; the FP64 division and
+// square-root chains need the warps more than the registers (measured on C1:
+// 48 ms per pass at 64 registers, 67 ms at 98).
+__global__ void __maxnreg__(64) k_surface_step(const DevScheme* __restrict__ sch, int k, const double* knots,
+                                               const DevBeam* beams, int n_beams, DevRays in, DevRays out,
+                                               unsigned long long* counts, unsigned* err) {
     const DevSurface& s = sch->s[k];
     const int n_stages = 3 * sch->n_surfaces;
     const bool last = k == sch->n_surfaces - 1;
@@ -274,10 +277,10 @@ __global__ void k_ccd_frame(DevRays rays, FrameArgs f) {
 // scheme and knot tables in shared memory, a persistent grid whose warps take
 // tiles of rays (next_tile).  Bit-identical to k_surface_step.  With a frame, good rays add
 // their pixel with warp-aggregated atomics.
-__global__ void __launch_bounds__(256) k_fused_fp64(const DevScheme* __restrict__ g_sch, const double* knots,
-                                                    const DevBeam* beams, int n_beams, DevRays in, DevRays out,
-                                                    unsigned long long* counts, unsigned* err, int state_out,
-                                                    FrameArgs frame, TileSched ts) {
+__global__ void __maxnreg__(64) k_fused_fp64(const DevScheme* __restrict__ g_sch, const double* knots,
+                                             const DevBeam* beams, int n_beams, DevRays in, DevRays out,
+                                             unsigned long long* counts, unsigned* err, int state_out,
+                                             FrameArgs frame, TileSched ts) {
     const double* s_knots;
     const DevScheme* sch = stage_scheme(g_sch, knots, s_knots);
     const int ns = sch->n_surfaces;

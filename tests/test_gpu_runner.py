@@ -99,3 +99,48 @@ def test_mixed_precision_runner(tmp_path):
     b = np.sort(np.round(ora.X[:ng], 6))
     k = min(len(a), len(b))
     assert np.abs(a[:k] - b[:k]).max() < 1e-4
+
+
+RT_CCD = os.path.join(ROOT, "rt_b200", "bin", "rt_ccd_frame")
+
+
+def test_ccd_frame_program(tmp_path):
+    """rt_trace then rt_ccd_frame on C0: the FITS image equals the image the
+    CPU oracle's ccd_coordinates / compute_ccd_image make from the same .dat
+    file, QE block and spectrum (FP64 sums in a different order: 1e-12)."""
+    xml = os.path.join(ROOT, "rt_b200", "data", "c0_littrow_free.xml")
+    files = run(tmp_path, xml)
+    (tmp_path / "rt_list.txt").write_text("".join(f + "\n" for f in files))
+    qx, qy = S.qe_table()
+    with open(tmp_path / "qe.bin", "wb") as f:
+        f.write(np.array([len(qx)], dtype=np.uint64).tobytes() + qx.tobytes() + qy.tobytes())
+    sx = np.linspace(0.3, 0.9, 13)
+    S.write_table(str(tmp_path / "spec.txt"), sx, 1.0 + 0.5 * sx)
+    c = S.C0_CCD
+    (tmp_path / "ccd.txt").write_text(f"# CCD\n{c['xsize']} {c['ysize']}\n{c['xdim']} {c['ydim']}\n"
+                                      f"{c['xpix']} {c['ypix']}\n")
+    out = subprocess.run([RT_CCD, "rt_list.txt", "qe.bin", "spec.txt", "ccd.txt", "frame.fits"], cwd=str(tmp_path),
+                         capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr + out.stdout
+    raw = open(tmp_path / "frame.fits", "rb").read()
+    img = np.frombuffer(raw[2880:2880 + 8 * c["xdim"] * c["ydim"]], dtype=">f8").reshape(c["ydim"], c["xdim"])
+    # the oracle on the same rays
+    r, ng, _ = read_dat(str(tmp_path / files[0]))
+    Lo = O.load()
+    cx, cy = np.zeros(ng, dtype=np.uint32), np.zeros(ng, dtype=np.uint32)
+    Lo.oracle_ccd_coordinates(C.c_size_t(ng), ffi.dptr(r.X), ffi.dptr(r.Y), C.c_double(c["xsize"]),
+                              C.c_double(c["ysize"]), C.c_double(c["xpix"]), C.c_double(c["ypix"]),
+                              ffi.vptr(cx), ffi.vptr(cy))
+    qt = ffi.TableHolder(x=qx, y=qy)
+    qt.y2[:] = O.spline_init(qt.x, qt.y)
+    st = ffi.TableHolder(x=sx, y=1.0 + 0.5 * sx)
+    st.y2[:] = O.spline_init(st.x, st.y)
+    ref = np.zeros(c["xdim"] * c["ydim"])
+    nout = C.c_uint64(0)
+    assert Lo.oracle_compute_ccd_image(C.c_size_t(ng), ffi.vptr(cx), ffi.vptr(cy), ffi.dptr(r.lambda_),
+                                       C.byref(qt.table), C.byref(st.table), C.c_size_t(c["xdim"]),
+                                       C.c_size_t(c["ydim"]), C.c_double(c["xpix"]), C.c_double(c["ypix"]),
+                                       ffi.dptr(ref), C.byref(nout)) == ffi.OK
+    ref = ref.reshape(c["ydim"], c["xdim"])
+    assert ref.sum() > 0
+    assert np.allclose(img, ref, rtol=1e-12, atol=0)
