@@ -24,6 +24,7 @@
 #include "tabulated_function.h"
 #include "rt_engine_func.h"
 
+#include <chrono>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -168,6 +169,7 @@ static int run_trace(const char* spec_path, const char* beam_path, const char* o
     for (size_t i = 0; i < n; ++i) flag[i] = 1;
 
     int rc = 0;
+    const auto t0 = std::chrono::steady_clock::now();
     try {
         size_t i_grating = 0;
         for (Surface* s : scheme) {       // scheme.cpp:983-1055
@@ -184,6 +186,10 @@ static int run_trace(const char* spec_path, const char* beam_path, const char* o
                 beam.Normalize();
             }
         }
+        // wall time of the surface loop: the engine calls with their host
+        // copies and the host loops of Beam and Surface, as Scheme::run runs them
+        const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        std::fprintf(stderr, "trace_seconds=%.6f good=%zu\n", sec, (size_t)beam.GetNumberOfGoodRays());
         beam.Save(out_path);
     } catch (Surface::bad_surface& e) {
         Surface::SurfaceError err = e.surface_error();
