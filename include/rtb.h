@@ -418,6 +418,43 @@ RTB_API int rtb_scheme_get_beam(const rtb_scheme* scheme, rtb_scheme_beam* beam)
 RTB_API int rtb_scheme_ranges(const rtb_scheme* scheme, const double** rows, size_t* n_rows, size_t* row_len);
 RTB_API void rtb_scheme_free(rtb_scheme* scheme);
 
+/* ---- throughput curves (Scheme::ComputeQE, scheme.cpp:1123-1338) ---------- */
+/* One surface of ComputeQE's list: a non-AUX surface of type MIRROR, LENS,
+ * GRATING or DETECTOR, in document order, with its qe_curve (a number, or a
+ * two-column table file).  ComputeQE builds every such surface but a grating
+ * as a plain mirror (scheme.cpp:1187-1189), so a DETECTOR's curve counts. */
+typedef struct rtb_qe_surface {
+    int32_t type;          /* RTB_MIRROR, RTB_LENS, RTB_GRATING or RTB_DETECTOR */
+    int32_t reserved;
+    rtb_table qe;          /* qe_curve; n == 1 for a single value */
+    int64_t order;         /* gratings: the order attribute (used with one range) */
+    double gr_const;       /* the const attribute */
+    double alpha_deg, gamma_deg, blaze_deg;  /* alpha, gamma, blaze_angle, degrees */
+    double rule_start, rule_stop;            /* rule_params: default 0 1; one value v: 0 v */
+} rtb_qe_surface;
+/* The QE surfaces of a loaded scheme (valid until rtb_scheme_free).  Returns
+ * RTB_BAD_VALUE with the SchemeError where ComputeQE fails on them: a missing
+ * type, qe_curve or grating attribute (1 ParseFailure), a qe_curve value <= 0,
+ * an unreadable table or rule_params whose start >= stop after clamping to
+ * [0, 1] (3 BadAttrValue), no QE surface (8 NoSurfaceDesc). */
+RTB_API int rtb_scheme_qe_surfaces(const rtb_scheme* scheme, const rtb_qe_surface** surfaces, size_t* n,
+                                   int* scheme_error);
+/* ComputeQE's curves (scheme.cpp:1249-1316) for n_rows wavelength ranges
+ * (rows of row_len numbers, as rtb_scheme_ranges gives them) of n_lambda >= 2
+ * wavelengths each, in one launch: lambda[r*n_lambda + i] = w1 +
+ * (w2 - w1)/(n_lambda - 1)*i, and qe[r*n_lambda + i] the product, surface after
+ * surface, of QE(lambda) (surface_QE) and, for a grating, of its energy in
+ * |order| (grating_energy_distr; angles converted as Grating::SetRuleParams
+ * does, surface.cpp:595-611).  With more than one range, grating g takes its
+ * order from column 2 + g.  Host arrays of n_rows*n_lambda doubles;
+ * synchronous.  RTB_OUT_OF_RANGE: a wavelength outside a QE table. */
+RTB_API int rtb_qe_curves(const rtb_qe_surface* surfaces, size_t n_surfaces, const double* rows, size_t n_rows,
+                          size_t row_len, size_t n_lambda, double* lambda, double* qe);
+/* Write curves as ComputeQE writes its QE file (scheme.cpp:1318-1334): one
+ * block per range, {size_t n_lambda; double lambda[n_lambda]; double
+ * qe[n_lambda]}.  ccd_frame reads one block per ray-tracing file. */
+RTB_API int rtb_save_qe(const char* path, size_t n_rows, size_t n_lambda, const double* lambda, const double* qe);
+
 /* ---- result files ---------------------------------------------------------- */
 /* Write beam [first, first+n) of the device arrays `rays` as a .dat file
  * (Beam::Save, common-lib/beam.cpp:636-715): size_t n, n_good, n_lambda, then

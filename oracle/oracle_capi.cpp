@@ -399,6 +399,57 @@ int oracle_surface_QE(size_t n, const double* lambda, double* spec, const rtb_ta
     return OK;
 }
 
+// grating_energy_distr (rt_engine_func.h:75-78; rt_cuda_engine_surface.cu:
+// 2098-2153,2190-2290): energy_distr[i] *= the blaze efficiency in `order`;
+// angles in radians.
+int oracle_grating_energy_distr(size_t n, const double* lambda, long order, double blaze_angle, double alpha,
+                                double gamma, double gr_const, double rule_start, double rule_stop,
+                                double* energy_distr) {
+    const double rule_size = rule_stop - rule_start;
+    for (size_t i = 0; i < n; ++i)
+        energy_distr[i] *= grating_energy(lambda[i], order, blaze_angle, alpha, gamma, gr_const, rule_size);
+    return OK;
+}
+
+// Scheme::ComputeQE's curves (scheme.cpp:1249-1316) for explicit QE
+// surfaces: per range, lambda_i = w1 + (w2-w1)/(N-1)*i and QE = 1, then per
+// surface Surface::ApplyQE (surface.cpp:331-340: QE *= qe_curve(lambda)) and
+// for a grating Grating::ApplyQE (surface.cpp:614-635: also *= its blaze
+// efficiency in |order|, with SetRuleParams's conversions, surface.cpp:595-611).
+// With more than one range, grating g takes its order from column 2 + g.
+int oracle_qe_curves(const rtb_qe_surface* s, size_t n_s, const double* rows, size_t n_rows, size_t row_len,
+                     size_t n_lambda, double* lambda, double* qe) {
+    if (n_lambda < 2) return BAD_VALUE;
+    for (size_t r = 0; r < n_rows; ++r) {
+        const double* val = rows + r * row_len;
+        double* lam = lambda + r * n_lambda;
+        double* q = qe + r * n_lambda;
+        double d_lambda = (val[1] - val[0]) / (n_lambda - 1);
+        for (size_t i = 0; i < n_lambda; ++i) {
+            lam[i] = val[0] + d_lambda * i;
+            q[i] = 1.0;
+        }
+        size_t i_grating = 0;
+        for (size_t k = 0; k < n_s; ++k) {
+            int st = oracle_surface_QE(n_lambda, lam, q, &s[k].qe);
+            if (st != OK) return st;
+            if (s[k].type != RTB_GRATING) continue;
+            long order = (long)s[k].order;
+            if (n_rows > 1) order = static_cast<long>(val[i_grating + 2]);
+            ++i_grating;
+            double a = s[k].rule_start, b = s[k].rule_stop;
+            a = a < 0.0 ? 0.0 : (a > 1.0 ? 1.0 : a);
+            b = b < 0.0 ? 0.0 : (b > 1.0 ? 1.0 : b);
+            if (a >= b) return BAD_VALUE;
+            // `x*deg2rad` is x*RT_PI/180.0, evaluated left to right
+            oracle_grating_energy_distr(n_lambda, lam, std::labs(order), s[k].blaze_deg * RTO_PI / 180.0,
+                                        s[k].alpha_deg * RTO_PI / 180.0, s[k].gamma_deg * RTO_PI / 180.0,
+                                        s[k].gr_const, a, b, q);
+        }
+    }
+    return OK;
+}
+
 // ---- the trace ------------------------------------------------------------
 
 // Per-ray formulation of Scheme::run over a batch of beams (host arrays,

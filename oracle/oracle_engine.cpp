@@ -143,9 +143,13 @@ RT_engine_error surface_QE(size_t N, real_t* lambda, real_t* spec, TabulatedFunc
     return ENGINE_ERROR_OK;
 }
 
-RT_engine_error grating_energy_distr(size_t, real_t*, long, real_t, real_t, real_t, real_t, real_t, real_t,
-                                     real_t*) {
-    return ENGINE_ERROR_FAILED;
+RT_engine_error grating_energy_distr(size_t N, real_t* lambda, long order, real_t blaze_angle, real_t alpha,
+                                     real_t gamma, real_t gr_const, real_t rule_start, real_t rule_stop,
+                                     real_t* energy_distr) {
+    const real_t rule_size = rule_stop - rule_start;
+    for (size_t i = 0; i < N; ++i)
+        energy_distr[i] *= rto::grating_energy(lambda[i], order, blaze_angle, alpha, gamma, gr_const, rule_size);
+    return ENGINE_ERROR_OK;
 }
 
 void rt_engine_free_vector(real_t* data) { free(data); }

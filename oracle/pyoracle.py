@@ -134,3 +134,28 @@ def spline_init(x: np.ndarray, y: np.ndarray) -> np.ndarray:
     y2 = np.zeros_like(x)
     ffi.check(load().oracle_spline_init(len(x), ffi.vptr(x), ffi.vptr(y), ffi.vptr(y2)), "oracle_spline_init")
     return y2
+
+
+def qe_curves(cqe, rows, n_lambda: int) -> tuple[np.ndarray, np.ndarray]:
+    """Scheme::ComputeQE's curves (oracle_qe_curves) for the QE surfaces of
+    `cqe` (rt_b200.schemes.CQe): (lambda, qe), each n_rows x n_lambda."""
+    rows = np.ascontiguousarray(np.atleast_2d(rows), dtype=np.float64)
+    lam = np.zeros((rows.shape[0], n_lambda))
+    qe = np.zeros_like(lam)
+    L = load()
+    L.oracle_qe_curves.argtypes = [C.POINTER(ffi.QeSurface), C.c_size_t, C.c_void_p, C.c_size_t, C.c_size_t,
+                                   C.c_size_t, C.c_void_p, C.c_void_p]
+    ffi.check(L.oracle_qe_curves(cqe.array, len(cqe), ffi.vptr(rows), rows.shape[0], rows.shape[1], n_lambda,
+                                 ffi.vptr(lam), ffi.vptr(qe)), "oracle_qe_curves")
+    return lam, qe
+
+
+def grating_energy_distr(lam, order, blaze, alpha, gamma, gr_const, rule_start=0.0, rule_stop=1.0, energy=None):
+    """grating_energy_distr (oracle_grating_energy_distr); angles in radians."""
+    lam = np.ascontiguousarray(lam, dtype=np.float64)
+    e = np.ones_like(lam) if energy is None else np.array(energy, dtype=np.float64)
+    L = load()
+    L.oracle_grating_energy_distr.argtypes = [C.c_size_t, C.c_void_p, C.c_long] + [C.c_double] * 6 + [C.c_void_p]
+    ffi.check(L.oracle_grating_energy_distr(len(lam), ffi.vptr(lam), order, blaze, alpha, gamma, gr_const,
+                                            rule_start, rule_stop, ffi.vptr(e)), "oracle_grating_energy_distr")
+    return e

@@ -17,8 +17,9 @@
 //   harness trace <spec.txt> <beam.bin> <out.dat>
 //   harness tabfunc <table.txt> <xs.bin> <out.bin>
 //   harness ccd <xy.bin> <xsize> <ysize> <xpix> <ypix> <out.bin>
+//   harness qe <qe_spec.txt> <out.bin>
 // Exit codes: 0 ok, 5 NoIntersections, 6 NoGoodRays, 7 table out of range,
-// 3 other engine failure, 2 usage / IO.
+// 4 BadRuleParams, 3 other engine failure, 2 usage / IO.
 #include "beam.h"
 #include "surface.h"
 #include "tabulated_function.h"
@@ -249,6 +250,98 @@ static int run_ccd(int argc, char** argv) {
     return 0;
 }
 
+// Scheme::ComputeQE after its XML pass (scheme.cpp:1164-1201 for the
+// surfaces, 1249-1334 for the curves and the QE file), on surfaces read from
+// a text spec:
+//   n_lambda n_rows row_len   then n_rows rows of row_len numbers
+//   n_surfaces                then per surface:
+//   type qe_token             (type 0 MIRROR, 1 LENS, 2 GRATING, 5 DETECTOR;
+//                              qe_token v:<number> or f:<table file>)
+//   and for a grating:  order const alpha gamma blaze_angle n_rule rule_1 .. rule_n
+// The surfaces are built as ComputeQE builds them: a grating as
+// Grating(Plane, Rectangle, Reflective, {order}, const, 1, 1) with
+// SetRuleParams, every other type as Surface(Plane, Mirror, Circle).
+static int run_qe(const char* spec_path, const char* out_path) {
+    std::ifstream spec(spec_path);
+    if (!spec) return 2;
+    size_t n_lambda, n_rows, row_len, n_s;
+    spec >> n_lambda >> n_rows >> row_len;
+    std::vector<std::vector<real_t>> ranges(n_rows, std::vector<real_t>(row_len));
+    for (auto& r : ranges)
+        for (auto& v : r) spec >> v;
+    spec >> n_s;
+    if (!spec) return 2;
+    std::vector<Surface*> scheme;
+    int rc = 0;
+    try {
+        for (size_t k = 0; k < n_s; ++k) {
+            int type;
+            std::string tok;
+            spec >> type >> tok;
+            Surface* surface;
+            if (type == Surface::Grating) {
+                long order;
+                real_t gr_const, alpha, gamma, blaze;
+                size_t n_rule;
+                spec >> order >> gr_const >> alpha >> gamma >> blaze >> n_rule;
+                std::vector<real_t> val(n_rule);
+                for (auto& v : val) spec >> v;
+                if (val.size() == 1) val.insert(val.begin(), 0.0);
+                if (val.empty()) val = {0.0, 1.0};
+                surface = new Grating(Surface::Plane, Surface::Rectangle, Grating::Reflective,
+                                      std::vector<long>(1, order), gr_const, 1.0, 1.0);
+                scheme.push_back(surface);
+                static_cast<Grating*>(surface)->SetRuleParams(blaze, alpha, gamma, val[0], val[1]);
+            } else {
+                surface = new Surface(Surface::Plane, Surface::Mirror, Surface::Circle);
+                scheme.push_back(surface);
+            }
+            IndexSpec q = parse_index(tok);
+            if (q.is_file) surface->SetQE(q.file.c_str());
+            else surface->SetQE(q.value);
+        }
+        if (!spec) { rc = 2; throw 0; }
+        FILE* file = std::fopen(out_path, "wb");
+        if (!file) { rc = 2; throw 0; }
+        std::vector<real_t> lambda(n_lambda, 0.0), qe_val;
+        for (const auto& val : ranges) {        // scheme.cpp:1272-1334
+            real_t d_lambda = (val[1] - val[0]) / (n_lambda - 1);
+            for (size_t i = 0; i < n_lambda; ++i) lambda[i] = val[0] + d_lambda * i;
+            qe_val = std::vector<real_t>(n_lambda, 1.0);
+            size_t i_grating = 0;
+            for (Surface* s : scheme) {
+                switch (s->GetType()) {
+                    case Surface::Grating:
+                        if (ranges.size() > 1) {
+                            static_cast<Grating*>(s)->SetOrder(static_cast<long>(val[i_grating + 2]));
+                            ++i_grating;
+                        }
+                        static_cast<Grating*>(s)->ApplyQE(lambda, qe_val);
+                        break;
+                    case Surface::Mirror:
+                    case Surface::Lens:
+                        s->ApplyQE(lambda, qe_val);
+                        break;
+                    default:;
+                }
+            }
+            std::fwrite(&n_lambda, sizeof(size_t), 1, file);
+            std::fwrite(lambda.data(), sizeof(real_t), n_lambda, file);
+            std::fwrite(qe_val.data(), sizeof(real_t), n_lambda, file);
+        }
+        std::fclose(file);
+    } catch (Grating::bad_grating&) {
+        rc = 4;
+    } catch (Surface::bad_surface&) {
+        rc = 3;
+    } catch (TabulatedFunction::bad_tab_func& e) {
+        rc = (e.bad_tab_func_error() == TabulatedFunction::OutOfRange) ? 7 : 3;
+    } catch (int) {
+    }
+    for (Surface* s : scheme) delete s;
+    return rc;
+}
+
 int main(int argc, char** argv) {
     if (argc < 2) return usage();
     rt_engine_init();
@@ -256,5 +349,6 @@ int main(int argc, char** argv) {
     if (mode == "trace" && argc == 5) return run_trace(argv[2], argv[3], argv[4]);
     if (mode == "tabfunc" && argc == 5) return run_tabfunc(argv[2], argv[3], argv[4]);
     if (mode == "ccd") return run_ccd(argc, argv);
+    if (mode == "qe" && argc == 4) return run_qe(argv[2], argv[3]);
     return usage();
 }

@@ -800,4 +800,50 @@ inline double uniform_lambda(const double range[2], size_t n_lambda, size_t j) {
     return range[0] + j * d_l;
 }
 
+// ===========================================================================
+// Grating blaze efficiency (the throughput curves of Scheme::ComputeQE)
+// ===========================================================================
+
+// __double2ll_rz for the finite, in-range values the order bounds take:
+// truncation toward zero.
+inline long long double2ll_rz(double v) { return (long long)v; }
+
+// I1_func_Tarasov (rt_cuda_engine_surface.cu:1988-2019) in double: blaze
+// angle c, incidence k1 (alpha), grating constant eps, relative rule length
+// rule_size; the small-argument branch is the reference's series for
+// sin(u)/u.
+inline double i1_tarasov(double c, double k1, double eps, double rule_size, double lambda, double beta) {
+    double I1 = RTO_PI * eps * rule_size / lambda * std::cos(beta) / std::cos(c - beta) *
+                (std::sin(c - k1) + std::sin(c - beta));
+    double term = std::cos(beta) * std::cos(c - k1) / std::cos(c - beta);
+    if (std::fabs(I1) < RTO_PI / 2.0) {
+        I1 *= I1;
+        I1 = (0.00761 * I1 - 0.16605) * I1 + 1;
+    } else {
+        I1 = std::sin(I1) / (I1);
+    }
+    I1 *= term;
+    I1 *= I1;
+    return I1;
+}
+
+// grating_energy_distr_kernel (rt_cuda_engine_surface.cu:2098-2153) for one
+// wavelength: I1 in `order` over the sum of I1 over every order from
+// trunc(eps/lambda*(sin(alpha)-1)*cos(gamma)) to trunc(eps/lambda*(sin(alpha)+1)*cos(gamma)).
+inline double grating_energy(double l, long order, double blaze, double alpha, double gamma, double eps,
+                             double rule_size) {
+    double sin_alpha = std::sin(alpha);
+    double cos_gamma = std::cos(gamma);
+    long order_min = (long)double2ll_rz(eps / l * (sin_alpha - 1) * cos_gamma);
+    long order_max = (long)double2ll_rz(eps / l * (sin_alpha + 1) * cos_gamma);
+    double norm = 0.0;
+    for (long m = order_min; m <= order_max; ++m) {
+        double beta = std::asin(m * l / eps / cos_gamma - sin_alpha);
+        norm += i1_tarasov(blaze, alpha, eps, rule_size, l, beta);
+    }
+    double beta = std::asin(order * l / (eps * cos_gamma) - sin_alpha);
+    double I1 = i1_tarasov(blaze, alpha, eps, rule_size, l, beta);
+    return I1 / norm;
+}
+
 }  // namespace rto

@@ -71,7 +71,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
 
 # Host programs over the C ABI (rt_b200/host/*.cpp -> rt_b200/bin/), linked
 # against librtb200.so with a run path relative to the program.
-PROGRAMS = ["rt_trace", "rt_ccd_frame"]
+PROGRAMS = ["rt_trace", "rt_ccd_frame", "rt_qe_comp"]
 BIN = os.path.join(HERE, "bin")
 
 

@@ -715,3 +715,68 @@ extern "C" int rtb_grating_energy_distr(size_t n, const double* lambda, long ord
     if ((st = d2h(energy_distr, g.d[1], n * sizeof(double), s)) != RTB_OK) return st;
     return finish(s, nullptr, nullptr, nullptr);
 }
+
+extern "C" int rtb_qe_curves(const rtb_qe_surface* surfaces, size_t n_surfaces, const double* rows, size_t n_rows,
+                             size_t row_len, size_t n_lambda, double* lambda, double* qe) {
+    if (n_rows == 0) return RTB_OK;
+    if (!rows || !lambda || !qe || (n_surfaces && !surfaces) || n_lambda < 2 || row_len < 2) return RTB_BAD_VALUE;
+    if (n_surfaces > (size_t)RTB_MAX_SURFACES || n_lambda > ((size_t)1 << 40) / n_rows) return RTB_BAD_VALUE;
+    std::vector<QeSurface> qs(n_surfaces);
+    std::vector<double> knots;
+    size_t n_gratings = 0;
+    for (size_t k = 0; k < n_surfaces; ++k) {
+        const rtb_qe_surface& in = surfaces[k];
+        QeSurface& o = qs[k];
+        std::memset(&o, 0, sizeof(o));
+        int st = add_table(&in.qe, knots, o.off, o.cnt);
+        if (st != RTB_OK) return st;
+        if (in.type == RTB_GRATING) {
+            // Grating::SetRuleParams (surface.cpp:595-611): `x*deg2rad` expands
+            // to x*RT_PI/180.0, evaluated left to right
+            o.grating = 1;
+            o.order = in.order;
+            o.gr_const = in.gr_const;
+            o.blaze = in.blaze_deg * K_RT_PI / 180.0;
+            o.alpha = in.alpha_deg * K_RT_PI / 180.0;
+            o.gamma = in.gamma_deg * K_RT_PI / 180.0;
+            double a = in.rule_start, b = in.rule_stop;
+            if (a < 0.0) a = 0.0;
+            if (a > 1.0) a = 1.0;
+            if (b < 0.0) b = 0.0;
+            if (b > 1.0) b = 1.0;
+            if (a >= b) return RTB_BAD_VALUE;
+            o.rule_size = b - a;
+            ++n_gratings;
+        } else if (in.type != RTB_MIRROR && in.type != RTB_LENS && in.type != RTB_DETECTOR) {
+            return RTB_BAD_VALUE;
+        }
+    }
+    const int from_rows = n_rows > 1;
+    if (from_rows && row_len < 2 + n_gratings) return RTB_BAD_VALUE;
+    const size_t total = n_rows * n_lambda;
+    Lock l;
+    int st = ensure_init();
+    if (st != RTB_OK) return st;
+    cudaStream_t s = engine().stream;
+    auto up = [](size_t b) { return (b + 255) / 256 * 256; };
+    const size_t b_rows = up(n_rows * row_len * sizeof(double)), b_s = up(qs.size() * sizeof(QeSurface) + 16),
+                 b_k = up(knots.size() * sizeof(double) + 16), b_out = total * sizeof(double);
+    DevBuf buf;
+    if ((st = buf.alloc(256 + b_rows + b_s + b_k + 2 * up(b_out), s)) != RTB_OK) return st;
+    char* p = buf.as<char>();
+    unsigned* err = reinterpret_cast<unsigned*>(p);
+    double* d_rows = reinterpret_cast<double*>(p + 256);
+    QeSurface* d_s = reinterpret_cast<QeSurface*>(p + 256 + b_rows);
+    double* d_k = reinterpret_cast<double*>(p + 256 + b_rows + b_s);
+    double* d_l = reinterpret_cast<double*>(p + 256 + b_rows + b_s + b_k);
+    double* d_q = reinterpret_cast<double*>(p + 256 + b_rows + b_s + b_k + up(b_out));
+    RTB_CUDA_TRY(cudaMemsetAsync(err, 0, 256, s));
+    if ((st = h2d(d_rows, rows, n_rows * row_len * sizeof(double), s)) != RTB_OK) return st;
+    if ((st = h2d(d_s, qs.data(), qs.size() * sizeof(QeSurface), s)) != RTB_OK) return st;
+    if ((st = h2d(d_k, knots.data(), knots.size() * sizeof(double), s)) != RTB_OK) return st;
+    k_qe_curves<<<grid_for(total, 128, 16), 128, 0, s>>>(n_lambda, n_rows, d_rows, row_len, d_s, (int)qs.size(), d_k,
+                                                          from_rows, d_l, d_q, err);
+    if ((st = d2h(lambda, d_l, b_out, s)) != RTB_OK) return st;
+    if ((st = d2h(qe, d_q, b_out, s)) != RTB_OK) return st;
+    return finish(s, err, nullptr, nullptr);
+}

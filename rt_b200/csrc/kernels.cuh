@@ -37,6 +37,16 @@ struct TileSched {
 };
 constexpr int kDefaultRpt = 2;
 
+// One surface of a throughput curve (k_qe_curves): its QE table in the knot
+// array, and for a grating the order and rule parameters, angles in radians.
+struct QeSurface {
+    int32_t off, cnt;
+    int32_t grating;
+    int32_t pad;
+    long long order;
+    double gr_const, alpha, gamma, blaze, rule_size;
+};
+
 // ---- drop-in kernels (kernels_fp64.cu) ----
 __global__ void k_transform(size_t n, DevSurface s, double* X, double* Y, double* Z, double* cX, double* cY,
                             double* cZ);
@@ -58,6 +68,9 @@ __global__ void k_ccd_image(size_t n, const unsigned* ix, const unsigned* iy, co
                             double pix_area, double* image, unsigned long long* n_outside, unsigned* err);
 __global__ void k_surface_qe(size_t n, const double* lambda, double* spec, const double* knots, int off, int cnt,
                              unsigned* err);
+__global__ void k_qe_curves(size_t n_lambda, size_t n_rows, const double* rows, size_t row_len, const QeSurface* s,
+                            int n_s, const double* knots, int orders_from_rows, double* lambda, double* qe,
+                            unsigned* err);
 __global__ void k_beam_random(size_t n, double p1, double p2, double cx, double cy, double cz, uint64_t seed,
                               uint64_t first, double* X, double* Y, double* Z);
 __global__ void k_uniform_range(size_t n, double l0, double d_l, double* lambda);

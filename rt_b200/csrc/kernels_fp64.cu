@@ -374,25 +374,65 @@ __device__ __forceinline__ double i1_tarasov(double c, double k1, double eps, do
     return I1;
 }
 
-// grating_energy_distr_kernel (rt_cuda_engine_surface.cu:2098-2153): the
-// energy in `order`, normalised over all propagating orders.
+// grating_energy_distr_kernel (rt_cuda_engine_surface.cu:2098-2153) for one
+// wavelength: the energy in `order`, normalised over all propagating orders.
+__device__ __forceinline__ double grating_energy(double l, long long order, double blaze, double alpha, double gamma,
+                                                 double gr_const, double rule_size) {
+    double sin_alpha = sin(alpha);
+    double cos_gamma = cos(gamma);
+    long long order_min = __double2ll_rz(gr_const / l * (sin_alpha - 1) * cos_gamma);
+    long long order_max = __double2ll_rz(gr_const / l * (sin_alpha + 1) * cos_gamma);
+    double norm = 0.0;
+    for (long long m = order_min; m <= order_max; ++m) {
+        double beta = asin(m * l / gr_const / cos_gamma - sin_alpha);
+        norm += i1_tarasov(blaze, alpha, gr_const, rule_size, l, beta);
+    }
+    double beta = asin(order * l / (gr_const * cos_gamma) - sin_alpha);
+    double I1 = i1_tarasov(blaze, alpha, gr_const, rule_size, l, beta);
+    return I1 / norm;
+}
+
 __global__ void k_grating_energy(size_t n, const double* lambda, long long order, double blaze, double alpha,
                                  double gamma, double gr_const, double rule_start, double rule_stop, double* energy) {
     const double rule_size = rule_stop - rule_start;
-    for (size_t i = gtid(); i < n; i += gstride()) {
-        double l = lambda[i];
-        double sin_alpha = sin(alpha);
-        double cos_gamma = cos(gamma);
-        long long order_min = __double2ll_rz(gr_const / l * (sin_alpha - 1) * cos_gamma);
-        long long order_max = __double2ll_rz(gr_const / l * (sin_alpha + 1) * cos_gamma);
-        double norm = 0.0;
-        for (long long m = order_min; m <= order_max; ++m) {
-            double beta = asin(m * l / gr_const / cos_gamma - sin_alpha);
-            norm += i1_tarasov(blaze, alpha, gr_const, rule_size, l, beta);
+    for (size_t i = gtid(); i < n; i += gstride())
+        energy[i] *= grating_energy(lambda[i], order, blaze, alpha, gamma, gr_const, rule_size);
+}
+
+// Scheme::ComputeQE's curves (scheme.cpp:1249-1316), every range in one
+// launch: element e = r * n_lambda + i is wavelength i of range r,
+// lambda = w1 + (w2 - w1) / (n_lambda - 1) * i, and its throughput is 1
+// multiplied, surface after surface, by QE(lambda) (surface_QE) and, for a
+// grating, by its energy in |order| (grating_energy_distr): the products in
+// the order the reference's per-surface calls make them.  With more than one
+// range, grating g takes its order from column 2 + g of the range row.
+__global__ void k_qe_curves(size_t n_lambda, size_t n_rows, const double* rows, size_t row_len, const QeSurface* s,
+                            int n_s, const double* knots, int orders_from_rows, double* lambda, double* qe,
+                            unsigned* err) {
+    const size_t total = n_lambda * n_rows;
+    for (size_t e = gtid(); e < total; e += gstride()) {
+        const size_t r = e / n_lambda, i = e - r * n_lambda;
+        const double* row = rows + r * row_len;
+        const double d_lambda = (row[1] - row[0]) / (double)(n_lambda - 1);
+        const double l = row[0] + d_lambda * (double)i;
+        double q = 1.0;
+        int g = 0;
+        for (int k = 0; k < n_s; ++k) {
+            double v;
+            if (!f64::table_eval(knots + s[k].off, s[k].cnt, l, v)) {
+                atomicOr(err, DEV_ERR_OUT_OF_RANGE);
+                break;
+            }
+            q *= v;
+            if (s[k].grating) {
+                long long order = orders_from_rows ? (long long)(long)row[2 + g] : s[k].order;
+                ++g;
+                if (order < 0) order = -order;
+                q *= grating_energy(l, order, s[k].blaze, s[k].alpha, s[k].gamma, s[k].gr_const, s[k].rule_size);
+            }
         }
-        double beta = asin(order * l / (gr_const * cos_gamma) - sin_alpha);
-        double I1 = i1_tarasov(blaze, alpha, gr_const, rule_size, l, beta);
-        energy[i] *= I1 / norm;
+        lambda[e] = l;
+        qe[e] = q;
     }
 }
 

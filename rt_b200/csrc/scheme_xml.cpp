@@ -18,6 +18,7 @@
 // (mxmlIndexNew/mxmlIndexFind, scheme.cpp:399-402) is what the reference
 // iterates, and whether it yields document order is a property of that
 // library this code cannot check.
+#include <algorithm>
 #include <cctype>
 #include <cerrno>
 #include <cmath>
@@ -247,6 +248,8 @@ struct rtb_scheme {
     rtb_scheme_beam beam{};
     std::vector<double> ranges;  // rows of row_len numbers
     size_t row_len = 0;
+    std::vector<rtb_qe_surface> qe;  // ComputeQE's surfaces
+    int qe_error = -1;               // SchemeError ComputeQE meets on them, -1 none
 };
 
 namespace {
@@ -286,6 +289,50 @@ void index_table(rtb_scheme& sc, const Node* at, const char* name, const std::st
     t.y2 = b + 2 * n;
 }
 
+// The surfaces of Scheme::ComputeQE (scheme.cpp:1140-1209): non-AUX surfaces
+// of type MIRROR, LENS, GRATING or DETECTOR with their qe_curve, gratings with
+// alpha, gamma, blaze_angle, const, order and rule_params, read in that order.
+// qe_curve is a number, or else a table file (a missing attribute is an
+// error, scheme.cpp:1194-1201); a number must be > 0 (TabulatedFunction::Set,
+// tabulated_function.cpp:121-137).  rule_params: none gives 0 1, one value v
+// gives 0 v, both clamped to [0, 1] and start < stop required
+// (Grating::SetRuleParams, surface.cpp:595-611).
+void load_qe(const std::vector<const Node*>& surf, const std::string& dir, rtb_scheme& sc) {
+    for (const Node* s : surf) {
+        if (value(s, "class") == "AUX") continue;
+        const std::string type = value(s, "type");
+        rtb_qe_surface q;
+        std::memset(&q, 0, sizeof(q));
+        if (type == "MIRROR") q.type = RTB_MIRROR;
+        else if (type == "LENS") q.type = RTB_LENS;
+        else if (type == "GRATING") q.type = RTB_GRATING;
+        else if (type == "DETECTOR") q.type = RTB_DETECTOR;
+        else continue;
+        if (q.type == RTB_GRATING) {
+            q.alpha_deg = numbers(s, "alpha")[0];
+            q.gamma_deg = numbers(s, "gamma")[0];
+            q.blaze_deg = numbers(s, "blaze_angle")[0];
+            q.gr_const = numbers(s, "const")[0];
+            q.order = (int64_t)(long)numbers(s, "order")[0];
+            std::vector<double> rp;
+            try {
+                rp = numbers(s, "rule_params", true);
+                if (rp.size() == 1) rp.insert(rp.begin(), 0.0);
+            } catch (Fail&) {
+                rp = {0.0, 1.0};
+            }
+            q.rule_start = rp[0];
+            q.rule_stop = rp[1];
+            const double a = std::min(std::max(rp[0], 0.0), 1.0), b = std::min(std::max(rp[1], 0.0), 1.0);
+            if (a >= b) throw Fail{BadAttrValue};
+        }
+        index_table(sc, s, "qe_curve", dir, q.qe);
+        if (q.qe.n == 1 && !(q.qe.y[0] > 0.0)) throw Fail{BadAttrValue};
+        sc.qe.push_back(q);
+    }
+    if (sc.qe.empty()) throw Fail{NoSurfaceDesc};
+}
+
 void load(const std::string& path, rtb_scheme& sc) {
     std::ifstream f(path, std::ios::binary);
     if (!f) throw Fail{FileOpenFailure};
@@ -318,7 +365,7 @@ void load(const std::string& path, rtb_scheme& sc) {
     find_all(root.get(), "surface", surf);
     if (surf.empty()) throw Fail{NoSurfaceDesc};
     if (surf.size() > RTB_MAX_SURFACES) throw Fail{BadAttrValue};
-    sc.tables.reserve(2 * surf.size() + 1);  // pointers into it stay valid
+    sc.tables.reserve(3 * surf.size() + 1);  // pointers into it stay valid
     int n_gratings = 0;
     for (const Node* s : surf) {
         rtb_surface o;
@@ -443,6 +490,13 @@ void load(const std::string& path, rtb_scheme& sc) {
             b.n_lambda = 0;
         }
     }
+    // ComputeQE's own attributes: a scheme that traces may lack them
+    try {
+        load_qe(surf, dir, sc);
+    } catch (Fail& e) {
+        sc.qe.clear();
+        sc.qe_error = e.code;
+    }
 }
 
 }  // namespace
@@ -502,5 +556,34 @@ RTB_API int rtb_scheme_ranges(const rtb_scheme* sc, const double** rows, size_t*
 }
 
 RTB_API void rtb_scheme_free(rtb_scheme* sc) { delete sc; }
+
+RTB_API int rtb_scheme_qe_surfaces(const rtb_scheme* sc, const rtb_qe_surface** surfaces, size_t* n,
+                                   int* scheme_error) {
+    if (scheme_error) *scheme_error = -1;
+    if (!sc || !surfaces || !n) return RTB_BAD_VALUE;
+    *surfaces = nullptr;
+    *n = 0;
+    if (sc->qe_error >= 0) {
+        if (scheme_error) *scheme_error = sc->qe_error;
+        return RTB_BAD_VALUE;
+    }
+    *surfaces = sc->qe.data();
+    *n = sc->qe.size();
+    return RTB_OK;
+}
+
+RTB_API int rtb_save_qe(const char* path, size_t n_rows, size_t n_lambda, const double* lambda, const double* qe) {
+    if (!path || (n_rows && n_lambda && (!lambda || !qe))) return RTB_BAD_VALUE;
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return RTB_BAD_VALUE;
+    bool ok = true;
+    for (size_t r = 0; r < n_rows && ok; ++r) {
+        ok = std::fwrite(&n_lambda, sizeof(size_t), 1, f) == 1 &&
+             std::fwrite(lambda + r * n_lambda, sizeof(double), n_lambda, f) == n_lambda &&
+             std::fwrite(qe + r * n_lambda, sizeof(double), n_lambda, f) == n_lambda;
+    }
+    ok = (std::fclose(f) == 0) && ok;
+    return ok ? RTB_OK : RTB_BAD_VALUE;
+}
 
 }  // extern "C"

@@ -52,6 +52,9 @@ def lib() -> C.CDLL:
         L.rtb_adjoint_jvp.argtypes = [vp, vp, vp, vp, vp]
         L.rtb_adjoint_spot_merit.argtypes = [vp, vp, C.c_double, P(C.c_double), vp, vp, vp]
         L.rtb_adjoint_destroy.argtypes = [vp]
+        L.rtb_qe_curves.argtypes = [P(ffi.QeSurface), C.c_size_t, vp, C.c_size_t, C.c_size_t, C.c_size_t, vp, vp]
+        L.rtb_grating_energy_distr.argtypes = [C.c_size_t, vp, C.c_long] + [C.c_double] * 6 + [vp]
+        L.rtb_surface_QE.argtypes = [C.c_size_t, vp, vp, P(ffi.Table)]
         _bound = True
     return L
 
@@ -63,6 +66,18 @@ def spline_init(x: np.ndarray, y: np.ndarray) -> np.ndarray:
     y2 = np.zeros_like(x)
     ffi.check(lib().rtb_spline_init(len(x), ffi.vptr(x), ffi.vptr(y), ffi.vptr(y2)), "rtb_spline_init")
     return y2
+
+
+def qe_curves(cqe, rows, n_lambda: int) -> tuple[np.ndarray, np.ndarray]:
+    """Scheme::ComputeQE's curves on the GPU (rtb_qe_curves, one launch) for
+    the QE surfaces of `cqe` (schemes.CQe) over the wavelength-range rows:
+    (lambda, qe), each n_rows x n_lambda."""
+    rows = np.ascontiguousarray(np.atleast_2d(rows), dtype=np.float64)
+    lam = np.zeros((rows.shape[0], n_lambda))
+    qe = np.zeros_like(lam)
+    ffi.check(lib().rtb_qe_curves(cqe.array, len(cqe), ffi.vptr(rows), rows.shape[0], rows.shape[1], n_lambda,
+                                  ffi.vptr(lam), ffi.vptr(qe)), "rtb_qe_curves")
+    return lam, qe
 
 
 def info() -> str:

@@ -97,6 +97,12 @@ class SchemeBeam(C.Structure):
                 ("center", C.c_double * 3), ("n_lambda", C.c_uint64)]
 
 
+class QeSurface(C.Structure):
+    _fields_ = [("type", C.c_int32), ("reserved", C.c_int32), ("qe", Table), ("order", C.c_int64),
+                ("gr_const", C.c_double), ("alpha_deg", C.c_double), ("gamma_deg", C.c_double),
+                ("blaze_deg", C.c_double), ("rule_start", C.c_double), ("rule_stop", C.c_double)]
+
+
 class TuneEntry(C.Structure):
     _fields_ = [("block_size", C.c_int32), ("rays_per_thread", C.c_int32), ("ms", C.c_double)]
 

@@ -44,6 +44,14 @@ def qe_table(seed: int = SEED) -> tuple[np.ndarray, np.ndarray]:
     return x, rng.uniform(0.6, 0.95, size=41)
 
 
+def qe_table_wide(seed: int = SEED + 5) -> tuple[np.ndarray, np.ndarray]:
+    """CCD QE for the echelle: 61 knots over 0.35..0.95 um, a broad hump
+    0.9 - 1.2 (l - 0.6)^2 with a seeded ripple of +-0.02."""
+    rng = np.random.default_rng(seed)
+    x = np.linspace(0.35, 0.95, 61)
+    return x, 0.9 - 1.2 * (x - 0.6) ** 2 + rng.uniform(-0.02, 0.02, size=61)
+
+
 def glass_table() -> tuple[np.ndarray, np.ndarray]:
     """Camera-lens glass n(lambda): 61 knots over 0.35..0.95 um, a Cauchy law
     n = 1.5046 + 0.00420/l^2 (a borosilicate crown)."""
@@ -70,6 +78,14 @@ class SurfaceSpec:
     n1: object = 1.0                               # float or (x, y) table
     n2: object = 1.0
     comment: str = ""
+    # throughput (Scheme::ComputeQE): qe_curve as a float or (x, y) table,
+    # None for none; grating blaze parameters in degrees, rule_params as
+    # () for none, (v,) or (start, stop)
+    qe: object = None
+    alpha: float = 0.0
+    gamma: float = 0.0
+    blaze: float = 0.0
+    rule_params: Sequence[float] = ()
 
 
 def frame_towards(p: Sequence[float], v: Sequence[float]) -> tuple[list, list]:
@@ -142,6 +158,39 @@ def to_c(specs: Sequence[SurfaceSpec], spline: SplineFn) -> CScheme:
     return CScheme(specs, spline)
 
 
+QE_TYPES = (ffi.MIRROR, ffi.LENS, ffi.GRATING, ffi.DETECTOR)
+
+
+class CQe:
+    """rtb_qe_surface array of the surfaces Scheme::ComputeQE takes
+    (scheme.cpp:1140-1209: non-AUX MIRROR, LENS, GRATING and DETECTOR
+    surfaces, each with a qe_curve); owns the table arrays."""
+
+    def __init__(self, specs: Sequence[SurfaceSpec], spline: SplineFn):
+        self.specs = [s for s in specs if s.cls != ffi.AUX_CLASS and s.type in QE_TYPES]
+        self.holders = []
+        self.array = (ffi.QeSurface * max(1, len(self.specs)))()
+        for k, s in enumerate(self.specs):
+            if s.qe is None:
+                raise ValueError(f"surface {k} has no qe_curve")
+            c = self.array[k]
+            c.type = s.type
+            c.qe = CScheme._table(self, s.qe, spline)
+            if s.type == ffi.GRATING:
+                c.order, c.gr_const = int(s.order), float(s.gr_const)
+                c.alpha_deg, c.gamma_deg, c.blaze_deg = float(s.alpha), float(s.gamma), float(s.blaze)
+                rp = list(s.rule_params)
+                rp = [0.0, 1.0] if not rp else ([0.0, rp[0]] if len(rp) == 1 else rp[:2])
+                c.rule_start, c.rule_stop = float(rp[0]), float(rp[1])
+
+    def __len__(self) -> int:
+        return len(self.specs)
+
+
+def qe_surfaces(specs: Sequence[SurfaceSpec], spline: SplineFn) -> CQe:
+    return CQe(specs, spline)
+
+
 # ---------------------------------------------------------------------------
 # beams
 
@@ -180,16 +229,16 @@ def littrow_free() -> list[SurfaceSpec]:
     the camera mirror 600 mm further on and the CCD in the camera's image of
     the focus.  Distances along the chief ray of 0.55 um."""
     par = SurfaceSpec(ffi.CONIC, ffi.MIRROR, params=(-1 / 800.0, -1.0, 0), size=(40.0, 0.0),
-                      distance=(0.0, 0.0, 400.0), comment="collimator")
+                      distance=(0.0, 0.0, 400.0), comment="collimator", qe=0.92)
     gr = SurfaceSpec(ffi.PLANE, ffi.GRATING, shape=ffi.RECTANGLE, size=(80.0, 80.0),
                      distance=(0.0, 0.0, -700.0), angles=(180.0, 10.0, 0.0), order=1,
-                     gr_const=1.0 / 0.6, comment="grating 600 l/mm")
+                     gr_const=1.0 / 0.6, comment="grating 600 l/mm", qe=0.9, alpha=10.0, gamma=0.0, blaze=9.5)
     cam_d, cam_a = C0_FRAMES["camera"]
     cam = SurfaceSpec(ffi.CONIC, ffi.MIRROR, params=(-1 / 600.0, 0.0, 0), size=(80.0, 0.0),
-                      distance=cam_d, angles=cam_a, comment="camera")
+                      distance=cam_d, angles=cam_a, comment="camera", qe=0.92)
     ccd_d, ccd_a = C0_FRAMES["ccd"]
     ccd = SurfaceSpec(ffi.PLANE, ffi.DETECTOR, shape=ffi.RECTANGLE, size=(30.72, 30.72),
-                      distance=ccd_d, angles=ccd_a, comment="CCD 2048x2048 15um")
+                      distance=ccd_d, angles=ccd_a, comment="CCD 2048x2048 15um", qe=qe_table())
     return [par, gr, cam, ccd]
 
 
@@ -241,9 +290,10 @@ def littrow_free_asphere() -> list[SurfaceSpec]:
     d = [round(float(v), 9) for v in (np.array(ccd.distance) - f["back"] * u)]
     flat = SurfaceSpec(ffi.CONIC, ffi.LENS, params=(f["c"], f["k"], 5, 0.0, *f["A"]), size=(30.0, 0.0),
                        distance=d, angles=list(ccd.angles), n1=1.0, n2=(gx, gy),
-                       comment="field flattener (even asphere)")
+                       comment="field flattener (even asphere)", qe=0.98)
     new_ccd = SurfaceSpec(ffi.PLANE, ffi.DETECTOR, shape=ffi.RECTANGLE, size=(30.72, 30.72),
-                          distance=(0.0, 0.0, round(f["back"] * n55, 6)), comment="CCD 2048x2048 15um (in glass)")
+                          distance=(0.0, 0.0, round(f["back"] * n55, 6)), comment="CCD 2048x2048 15um (in glass)",
+                          qe=qe_table())
     return s[:3] + [flat, new_ccd]
 
 
@@ -325,21 +375,23 @@ def echelle(glass=None) -> list[SurfaceSpec]:
     f = C1_FRAMES
     return [
         SurfaceSpec(ffi.CONIC, ffi.MIRROR, params=(-1 / 1600.0, -1.0, 0), size=(140.0, 0.0),
-                    distance=f["oap"][0], angles=f["oap"][1], comment="off-axis parabola"),
+                    distance=f["oap"][0], angles=f["oap"][1], comment="off-axis parabola", qe=0.92),
         SurfaceSpec(ffi.PLANE, ffi.GRATING, shape=ffi.RECTANGLE, size=(260.0, 120.0),
                     distance=f["echelle"][0], angles=f["echelle"][1], order=45, gr_const=1000.0 / 31.6,
-                    comment="echelle 31.6 l/mm, blaze 63.5 deg"),
+                    comment="echelle 31.6 l/mm, blaze 63.5 deg", qe=0.85, alpha=64.5, gamma=4.0, blaze=63.5),
         SurfaceSpec(ffi.PLANE, ffi.GRATING, shape=ffi.RECTANGLE, size=(160.0, 160.0),
                     distance=f["xdisp"][0], angles=f["xdisp"][1], order=1, gr_const=1000.0 / 300.0,
-                    comment="cross-disperser 300 l/mm"),
+                    comment="cross-disperser 300 l/mm", qe=0.9, alpha=10.0, gamma=0.0, blaze=4.3),
         SurfaceSpec(ffi.TORIC, ffi.MIRROR, params=(-1 / 2100.0, 0.0, 0, -1 / 2000.0), size=(110.0, 0.0),
-                    distance=f["fold"][0], angles=f["fold"][1], comment="toric fold"),
+                    distance=f["fold"][0], angles=f["fold"][1], comment="toric fold", qe=0.92),
         SurfaceSpec(ffi.CONIC, ffi.LENS, params=(1 / 150.0, 0.0, 5, 0.0, *a1), size=(75.0, 0.0),
-                    distance=f["lens1"][0], angles=f["lens1"][1], n1=1.0, n2=g, comment="camera lens front"),
+                    distance=f["lens1"][0], angles=f["lens1"][1], n1=1.0, n2=g, comment="camera lens front",
+                    qe=0.98),
         SurfaceSpec(ffi.CONIC, ffi.LENS, params=(-1 / 400.0, 0.0, 5, 0.0, *a2), size=(75.0, 0.0),
-                    distance=f["lens2"][0], angles=f["lens2"][1], n1=g, n2=1.0, comment="camera lens back"),
+                    distance=f["lens2"][0], angles=f["lens2"][1], n1=g, n2=1.0, comment="camera lens back",
+                    qe=0.98),
         SurfaceSpec(ffi.PLANE, ffi.DETECTOR, shape=ffi.RECTANGLE, size=(61.44, 61.44),
-                    distance=f["ccd"][0], angles=f["ccd"][1], comment="CCD 4096x4096 15um"),
+                    distance=f["ccd"][0], angles=f["ccd"][1], comment="CCD 4096x4096 15um", qe=qe_table_wide()),
     ]
 
 
@@ -546,6 +598,14 @@ def write_xml(path: str, specs: Sequence[SurfaceSpec], name: str, result_file: s
         if s.type in (ffi.GRATING, ffi.LENS):
             L.append(f"    <n1>{table_ref(s.n1)}</n1>")
             L.append(f"    <n2>{table_ref(s.n2)}</n2>")
+        if s.qe is not None:
+            L.append(f"    <qe_curve>{table_ref(s.qe)}</qe_curve>")
+            if s.type == ffi.GRATING:
+                L.append(f"    <alpha>{_num(s.alpha)}</alpha>")
+                L.append(f"    <gamma>{_num(s.gamma)}</gamma>")
+                L.append(f"    <blaze_angle>{_num(s.blaze)}</blaze_angle>")
+                if len(s.rule_params):
+                    L.append(f"    <rule_params>{_num(list(s.rule_params))}</rule_params>")
         L.append("  </surface>")
     if len(ranges) == 1 and len(ranges[0]) == 2:
         rng = _num(list(ranges[0]))
@@ -604,6 +664,16 @@ class LoadedScheme:
         txt = lambda k: (L.rtb_scheme_text(self.h, k) or b"").decode()  # noqa: E731
         self.name, self.result_file, self.log_file = txt(0), txt(1), txt(2)
         self.comments = [txt(3 + k) for k in range(n.value)]
+        L.rtb_scheme_qe_surfaces.argtypes = [C.c_void_p, C.POINTER(C.POINTER(ffi.QeSurface)),
+                                             C.POINTER(C.c_size_t), C.POINTER(C.c_int)]
+        qp = C.POINTER(ffi.QeSurface)()
+        nq, qerr = C.c_size_t(), C.c_int(-1)
+        self.qe_status = L.rtb_scheme_qe_surfaces(self.h, C.byref(qp), C.byref(nq), C.byref(qerr))
+        self.qe_error = qerr.value
+        self.qe_array = (ffi.QeSurface * max(1, nq.value))()
+        for i in range(nq.value):
+            self.qe_array[i] = qp[i]          # tables still point into the scheme (kept alive by self)
+        self.n_qe = nq.value
 
     def __del__(self):
         if getattr(self, "h", None):

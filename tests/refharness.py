@@ -84,3 +84,46 @@ def run_trace(kind: str, specs, orders, rays, sl=slice(None), timeout=600):
         if p.returncode != 0 or not os.path.exists(out):
             return p.returncode, None
         return 0, read_dat(out)
+
+
+def read_qe(path: str):
+    """QE file (Scheme::ComputeQE, scheme.cpp:1318-1334) -> [(lambda, qe)]."""
+    blocks = []
+    with open(path, "rb") as f:
+        while True:
+            h = f.read(8)
+            if len(h) < 8:
+                break
+            (n,) = struct.unpack("<Q", h)
+            lam = np.frombuffer(f.read(8 * n), dtype=np.float64)
+            qe = np.frombuffer(f.read(8 * n), dtype=np.float64)
+            blocks.append((lam, qe))
+    return blocks
+
+
+def run_qe(kind: str, specs, rows, n_lambda: int, timeout=600):
+    """ComputeQE's curves through the harness (the reference's Surface /
+    Grating ApplyQE over one engine): specs are SurfaceSpec of the QE
+    surfaces in scheme order.  Returns (exit code, blocks or None)."""
+    exe = harness(kind)
+    if exe is None:
+        raise FileNotFoundError(f"harness_{kind} not built")
+    rows = np.atleast_2d(np.asarray(rows, dtype=np.float64))
+    with tempfile.TemporaryDirectory() as d:
+        lines = [f"{n_lambda} {rows.shape[0]} {rows.shape[1]}"]
+        lines += [" ".join(repr(float(v)) for v in r) for r in rows]
+        lines.append(str(len(specs)))
+        for k, s in enumerate(specs):
+            row = [str(int(s.type)), _index_token(s.qe, d, f"qe_{k}.txt")]
+            if s.type == ffi.GRATING:
+                row += [str(int(s.order))] + [repr(float(v)) for v in (s.gr_const, s.alpha, s.gamma, s.blaze)]
+                row += [str(len(s.rule_params))] + [repr(float(v)) for v in s.rule_params]
+            lines.append(" ".join(row))
+        spec = os.path.join(d, "qe_spec.txt")
+        with open(spec, "w") as f:
+            f.write("\n".join(lines) + "\n")
+        out = os.path.join(d, "qe.bin")
+        p = subprocess.run([exe, "qe", spec, out], capture_output=True, timeout=timeout)
+        if p.returncode != 0 or not os.path.exists(out):
+            return p.returncode, None
+        return 0, read_qe(out)

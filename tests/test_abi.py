@@ -37,7 +37,9 @@ def test_library_loads_and_exports_every_declared_symbol():
 
 def test_struct_layouts_match_ctypes():
     structs = {"rtb_table": ffi.Table, "rtb_surface": ffi.Surface, "rtb_beam": ffi.Beam, "rtb_rays": ffi.Rays,
-               "rtb_trace_opts": ffi.TraceOpts, "rtb_trace_stats": ffi.TraceStats, "rtb_ccd": ffi.CCD}
+               "rtb_trace_opts": ffi.TraceOpts, "rtb_trace_stats": ffi.TraceStats, "rtb_ccd": ffi.CCD,
+               "rtb_qe_surface": ffi.QeSurface, "rtb_scheme_beam": ffi.SchemeBeam, "rtb_param": ffi.Param,
+               "rtb_tune_entry": ffi.TuneEntry}
     src = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void) {"]
     for cname, py in structs.items():
         src.append(f'printf("{cname} __sizeof__ %zu\\n", sizeof({cname}));')
