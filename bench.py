@@ -294,7 +294,11 @@ def main():
         if name not in want:
             continue
         try:
+            torch.cuda.synchronize()
+            t_create = time.perf_counter()
             plan = E.Plan(surf, beams, mk(ffi.ENGINE_FUSED, prec))
+            torch.cuda.synchronize()
+            t_create = time.perf_counter() - t_create
             table = [] if args.no_autotune else plan.autotune(reps=2)
             block, rpt, _ = plan.config()
             if name == "fused_mixed" or "fused_mixed" not in want:
@@ -303,6 +307,13 @@ def main():
                 clocks = ck.summary()
             else:
                 ms, stats = timed_plan(plan, max(2, args.steps // 4), 1)
+            # the same plan in index order: what the coherent tracing order gains
+            o_idx = mk(ffi.ENGINE_FUSED, prec)
+            o_idx.ray_order = ffi.ORDER_INDEX
+            p_idx = E.Plan(surf, beams, o_idx)
+            ffi.check(p_idx.set_config(block, rpt), "rtb_plan_set_config")
+            ms_idx, _ = timed_plan(p_idx, max(2, args.steps // 4), 1)
+            p_idx.destroy()
         except RuntimeError as e:
             engines[name] = {"error": str(e)}
             continue
@@ -311,6 +322,11 @@ def main():
                          "ray_surfaces_per_step": stats.ray_surfaces, "n_good": stats.n_good,
                          "launch": f"rtb_plan_run (CUDA graph), block {block} x {rpt} rays/thread"
                                    + ("" if args.no_autotune else " (autotuned)"),
+                         "ray_order": "coherent (beam, wavelength, Morton code of the entrance position), "
+                                      "sorted once when the plan is made",
+                         "plan_create_s": t_create,
+                         "index_order": {"ms_per_step": ms_idx,
+                                         "value": stats.ray_surfaces * world / (ms_idx * 1e-3)},
                          "autotune_ms": {f"{b}x{r}": round(t, 4) for b, r, t in table}}
         head = name if (head is None or name == "fused_mixed") else head
     if head is None and "value" in engines.get("per_surface", {}):

@@ -134,6 +134,15 @@ typedef struct rtb_ccd {
     double xpix, ypix;
 } rtb_ccd;
 
+/* The order in which a plan's fused kernel takes its rays (results do not
+ * depend on it).  RTB_ORDER_COHERENT sorts the rays once, when the plan is
+ * made, by beam, wavelength and Morton code of their entrance position, so
+ * that a warp traces neighbouring rays of one wavelength, and keeps a copy of
+ * the generated rays in that order, which the runs read (writes to the input
+ * arrays rtb_plan_rays returns do not reach them; 62 bytes more per ray);
+ * RTB_ORDER_INDEX takes the rays in index order from those arrays. */
+enum { RTB_ORDER_COHERENT = 0, RTB_ORDER_INDEX = 1 };
+
 typedef struct rtb_trace_opts {
     int32_t engine;                 /* RTB_ENGINE_PER_SURFACE / RTB_ENGINE_FUSED */
     int32_t precision;              /* RTB_FP64 / RTB_MIXED */
@@ -142,7 +151,7 @@ typedef struct rtb_trace_opts {
     int32_t block_size;             /* 0: tuned default */
     int32_t rays_per_thread;        /* 0: tuned default */
     int32_t state_out;              /* fused: 1 writes X..cZ back, 0 writes only the CCD-plane X,Y */
-    int32_t reserved;
+    int32_t ray_order;              /* plans: RTB_ORDER_COHERENT (0) or RTB_ORDER_INDEX; other traces run in index order */
     const rtb_ccd* ccd;             /* optional: add good rays to frame counts (see rtb_ccd_frame) */
     uint32_t* counts;               /* device, ccd->xdim*ccd->ydim pixels; not cleared */
     uint64_t* n_outside;            /* device, may be NULL */

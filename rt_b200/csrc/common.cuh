@@ -47,6 +47,11 @@ struct DevSurface {
     double size[2], center[2];
     int32_t n1_off, n1_n, n2_off, n2_n;  // tables: offset/count into the knot buffer (count 1 = single value)
     double n1_invh, n2_invh;              // 1/knot spacing of a table on a uniform grid, else 0 (mixed engine)
+    // Even asphere with a circular pass aperture (mixed engine): every point of
+    // the surface inside the aperture has sag_lo <= Z <= sag_hi.
+    double sag_lo, sag_hi;
+    int32_t sag_cull;                     // 1: sag_lo / sag_hi are set
+    int32_t sag_pad;
 };
 
 // A prepared scheme in device memory; the fused kernels copy it to shared

@@ -6,6 +6,7 @@
 // the kernel are ordered on the library stream, the temporaries come from the
 // stream-ordered pool (no cudaMalloc/cudaFree per call as in
 // rt_cuda_engine_common.cu:72-155).
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -124,6 +125,45 @@ int add_table(const rtb_table* t, std::vector<double>& knots, int32_t& off, int3
     return RTB_OK;
 }
 
+// The sag range of an even asphere over its circular pass aperture, for the
+// mixed engine's test that a ray cannot meet the surface inside the aperture
+// (mx::asphere_isect).  Points of the aperture (radius R about the centre c)
+// lie at radii [max(0, |c| - R), |c| + R] from the axis; the sag
+// c r^2 / (1 + sqrt(1 - k1 c^2 r^2)) + sum a_i r^(2i) is sampled there at 4097
+// radii and the range widened by 1 % of its width plus 1 um, far more than
+// the sag moves between samples.  No bounds where the base conic has no
+// surface inside that radius.
+void asphere_sag_bounds(DevSurface& s) {
+    s.sag_cull = 0;
+    s.sag_lo = s.sag_hi = 0.0;
+    if (s.kind != IS_ITER_CONIC && s.kind != IS_ITER_POLY) return;
+    if (s.shape != RTB_CIRCLE || s.type == RTB_SHADE || !(s.size[0] > 0)) return;
+    const double rc = std::hypot(s.center[0], s.center[1]);
+    const double r_lo = std::max(0.0, rc - s.size[0]), r_hi = rc + s.size[0];
+    double lo = 1e300, hi = -1e300;
+    const int n = 4097;
+    for (int i = 0; i < n; ++i) {
+        const double r = r_lo + (r_hi - r_lo) * i / (n - 1);
+        const double r2 = r * r;
+        double z = 0.0;
+        if (s.kind == IS_ITER_CONIC) {
+            const double q = 1.0 - s.k1 * s.c * s.c * r2;
+            if (!(q >= 0.0)) return;
+            z = s.c * r2 / (1.0 + std::sqrt(q));
+        }
+        double p = 0.0;
+        for (int k = s.n_poly; k >= 1; --k) p = (p + s.poly[k - 1]) * r2;
+        z += p;
+        if (!std::isfinite(z)) return;
+        lo = std::min(lo, z);
+        hi = std::max(hi, z);
+    }
+    const double m = 0.01 * (hi - lo) + 1e-3;
+    s.sag_lo = lo - m;
+    s.sag_hi = hi + m;
+    s.sag_cull = 1;
+}
+
 int prepare_surface(const rtb_surface& in, DevSurface& s, std::vector<double>& knots) {
     bool non_aux = in.type != RTB_AUX_TYPE;
     int st = surface_from_params(non_aux ? in.cls : RTB_AUX_CLASS, in.params, s);
@@ -147,6 +187,7 @@ int prepare_surface(const rtb_surface& in, DevSurface& s, std::vector<double>& k
         s.size[i] = in.size[i];
         s.center[i] = in.center[i];
     }
+    asphere_sag_bounds(s);
     s.n1_off = s.n2_off = 0;
     s.n1_n = s.n2_n = 1;
     if (in.type == RTB_LENS || in.type == RTB_GRATING) {

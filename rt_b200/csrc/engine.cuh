@@ -31,6 +31,8 @@ int prepare_surface(const rtb_surface& in, DevSurface& out, std::vector<double>&
 int prepare_scheme(const rtb_surface* s, size_t n, uint32_t fixes, int renorm_lost, PreparedScheme& out);
 int surface_from_params(int cls, const double* params, DevSurface& s);
 int add_table(const rtb_table* t, std::vector<double>& knots, int32_t& off, int32_t& cnt);
+// Sag range of an even asphere over its circular aperture (DevSurface::sag_*).
+void asphere_sag_bounds(DevSurface& s);
 void transform_constants(const double angles_rad[3], const double dist[3], DevSurface& s);
 double scheme_angle_rad(double deg);
 
@@ -120,8 +122,16 @@ int check_beams(const rtb_beam* beams, size_t n_beams, size_t n_rays, std::vecto
 int gen_beams(const rtb_beam* beams, size_t n_beams, size_t n_rays, std::vector<GenBeam>& out, uint64_t* total);
 FrameArgs frame_args(const rtb_trace_opts* o);
 // Launch the trace kernels of one call (no synchronisation).
+// `order` (fused kernels; may be NULL): the order in which the rays are
+// traced; in_by_slot: `in` holds the rays in that order.
 int launch_trace(const PreparedScheme& ps, TraceArgs& a, int n_beams, const rtb_trace_opts& o, const DevRays& in,
-                 const DevRays& out, const FrameArgs& frame, cudaStream_t st);
+                 const DevRays& out, const FrameArgs& frame, cudaStream_t st, const uint32_t* order = nullptr,
+                 bool in_by_slot = false);
+// The coherent tracing order (beam, chunk, wavelength, Morton code of the
+// entrance position) of n <= 2^32 generated rays, as a permutation in
+// `order` (device, n).
+int coherent_order(const GenBeam* d_beams, int n_beams, uint64_t n, const DevRays& rays, uint32_t* order,
+                   int chunk_shift, cudaStream_t st);
 // Status and statistics from the per-(beam, stage) counts.
 int trace_result(const PreparedScheme& ps, const unsigned long long* counts, unsigned err, int n_beams,
                  rtb_trace_stats* stats);

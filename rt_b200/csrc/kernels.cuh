@@ -30,10 +30,16 @@ inline size_t fused_smem_bytes(int n_knots) {
 }
 
 // Scheduling of the persistent fused kernels: `next` is a counter of
-// 32*rpt-ray tiles handed out to warps (zeroed before each launch).
+// 32*rpt-ray tiles handed out to warps (zeroed before each launch).  Slot s
+// of the tiles traces ray order[s] (a permutation of the rays), or ray s when
+// order is NULL; its input is read at s when in_by_slot (the input arrays
+// hold the rays in tracing order), else at the ray's index.  Outputs go to
+// the ray's index.
 struct TileSched {
     unsigned long long* next;
     int rpt;
+    const uint32_t* order;
+    int in_by_slot;
 };
 constexpr int kDefaultRpt = 2;
 
@@ -76,6 +82,11 @@ __global__ void k_beam_random(size_t n, double p1, double p2, double cx, double 
 __global__ void k_uniform_range(size_t n, double l0, double d_l, double* lambda);
 __global__ void k_random_range(size_t n, double l0, double l1, uint64_t seed, double* lambda);
 __global__ void k_generate(const GenBeam* beams, int n_beams, uint64_t total, DevRays rays);
+// order.cu: sort keys of the coherent tracing order of generated rays
+__global__ void k_order_keys(const GenBeam* beams, int n_beams, uint64_t total, DevRays rays,
+                             unsigned long long* keys, uint32_t* idx, int chunk_shift);
+// dst[s] = src[order[s]] for X..lambda and flag
+__global__ void k_gather_rays(const uint32_t* order, uint64_t n, DevRays src, DevRays dst);
 __global__ void k_ccd_frame(DevRays rays, FrameArgs f);
 
 // ---- trace kernels ----

@@ -288,16 +288,22 @@ __global__ void __maxnreg__(64) k_fused_fp64(const DevScheme* __restrict__ g_sch
     const uint64_t tile_rays = 32ull * (uint64_t)ts.rpt;
     const uint64_t n_tiles = (in.n + tile_rays - 1) / tile_rays;
     uint64_t tile;
+    int b = 0;
     while (next_tile(ts, n_tiles, tile)) {
         for (int j = 0; j < ts.rpt; ++j) {
-            const size_t i = tile * tile_rays + (size_t)j * 32 + (threadIdx.x & 31);
+            const size_t slot = tile * tile_rays + (size_t)j * 32 + (threadIdx.x & 31);
+            const size_t i = (ts.order && slot < in.n) ? (size_t)ts.order[slot] : slot;  // the ray (outputs)
+            const size_t ri = ts.in_by_slot ? slot : i;                                  // its input
             bool ev = false, good = false;
             int key = 0;
             double outX = 0, outY = 0;
-            if (i < in.n && in.flag[i] == 1) {
-                Ray r{in.X[i], in.Y[i], in.Z[i], in.cX[i], in.cY[i], in.cZ[i]};
-                const double lam = in.lambda[i];
-                const int b = beam_of(beams, n_beams, i);
+            if (slot < in.n && in.flag[ri] == 1) {
+                Ray r{in.X[ri], in.Y[ri], in.Z[ri], in.cX[ri], in.cY[ri], in.cZ[ri]};
+                const double lam = in.lambda[ri];
+                // rays come in increasing order per thread: the previous
+                // ray's beam is usually this one's
+                if (!(b + 1 >= n_beams || i < beams[b + 1].first_ray) || i < beams[b].first_ray)
+                    b = beam_of(beams, n_beams, i);
                 int stage = -1;
                 for (int k = 0; k < ns; ++k) {
                     const DevSurface& s = sch->s[k];
@@ -343,8 +349,8 @@ __global__ void __maxnreg__(64) k_fused_fp64(const DevScheme* __restrict__ g_sch
                 outX = r.X;
                 outY = r.Y;
             }
-            else if (i < in.n && in.flag != out.flag) {
-                out.flag[i] = in.flag[i];
+            else if (slot < in.n && in.flag != out.flag) {
+                out.flag[i] = in.flag[ri];
             }
             count_event(ev, key, counts);
             if (frame.counts) frame_add(good, outX, outY, frame);

@@ -187,10 +187,35 @@ __device__ __forceinline__ bool conic_isect(const DevSurface& s, Ray& r) {
 // for these surfaces), so the loop stops after a step below 1e-6 mm: the root
 // is then good to ~1e-14 mm.  One or two steps from the conic root; at most
 // eight for rays that start far from the surface (far outside the aperture).
-__device__ __forceinline__ bool asphere_isect(const DevSurface& s, Ray& r) {
+//
+// Rays far outside the aperture take most of those steps, and their lanes
+// hold the warp: a ray that within the slab sag_lo <= Z <= sag_hi (every
+// surface point inside a circular aperture lies in it) stays outside the
+// aperture's cylinder cannot meet the surface inside the aperture, so it is
+// lost at the aperture without a root.  Returns 0 for a hit, 1 for a loss at
+// the intersection, 2 for a loss at the aperture.
+__device__ __forceinline__ bool misses_aperture(const DevSurface& s, const Ray& r) {
+    if (r.cZ == 0.0) return false;
+    const double iz = rcp(r.cZ);
+    double ta = (s.sag_lo - r.Z) * iz, tb = (s.sag_hi - r.Z) * iz;
+    if (ta > tb) {
+        const double u = ta;
+        ta = tb;
+        tb = u;
+    }
+    const double px = r.X - s.center[0], py = r.Y - s.center[1];
+    const double dd = fma(r.cX, r.cX, r.cY * r.cY);
+    double t = (dd > 0.0) ? -fma(px, r.cX, py * r.cY) * rcp(dd) : ta;
+    t = fmin(fmax(t, ta), tb);
+    const double x = fma(t, r.cX, px), y = fma(t, r.cY, py);
+    return fma(x, x, y * y) > s.size[0] * s.size[0] * (1.0 + 1e-9);
+}
+
+__device__ __forceinline__ int asphere_isect(const DevSurface& s, Ray& r) {
     double s0 = -r.Z * rcp(r.cZ);
     bool poly_only = s.c == 0.0;
-    if (poly_only ? !(s0 > 0) : !(s0 >= 0)) return false;
+    if (poly_only ? !(s0 > 0) : !(s0 >= 0)) return 1;
+    if (s.sag_cull && misses_aperture(s, r)) return 2;
     double t = s0;
     double ic = 0.0;
     if (!poly_only) {
@@ -229,7 +254,7 @@ __device__ __forceinline__ bool asphere_isect(const DevSurface& s, Ray& r) {
         t -= dt;
         if (!(fabs(dt) >= 1e-6)) break;
     }
-    if (!isfinite(t)) return false;  // no root near the ray (far outside any aperture)
+    if (!isfinite(t)) return 1;  // no root near the ray (far outside any aperture)
     x = fma(t, r.cX, r.X);
     y = fma(t, r.cY, r.Y);
     // the reference's grazing test on dF = cZ - E (x cX + y cY) at the root
@@ -245,12 +270,12 @@ __device__ __forceinline__ bool asphere_isect(const DevSurface& s, Ray& r) {
         for (int i = 1; i <= N; ++i, rr *= r2) sum = fmaf((float)i * (float)s.poly[i - 1], rr, sum);
         E = fmaf(2.0f, sum, E);
         const float dF = fmaf(-E, fmaf(xf, (float)r.cX, yf * (float)r.cY), (float)r.cZ);
-        if (fabsf(dF) < (float)K_ITER_EPS) return false;
+        if (fabsf(dF) < (float)K_ITER_EPS) return 1;
     }
     r.X = x;
     r.Y = y;
     r.Z = fma(t, r.cZ, r.Z);
-    return true;
+    return 0;
 }
 
 // Toric surface (iter_toric, surface.cu:359-410): the same function F of the
@@ -284,36 +309,31 @@ __device__ __forceinline__ bool toric_isect(const DevSurface& s, uint32_t fixes,
     return true;
 }
 
-__device__ __forceinline__ bool intersect(const DevSurface& s, uint32_t fixes, Ray& r) {
+// 0: hit, 1: lost at the intersection, 2: lost at the aperture (known before the root).
+__device__ __forceinline__ int intersect(const DevSurface& s, uint32_t fixes, Ray& r) {
     switch (s.kind) {
-        case IS_PLANE: return plane_isect(r);
-        case IS_PARABOLOID: return paraboloid_isect(s, r);
-        case IS_CONIC: return conic_isect(s, r);
+        case IS_PLANE: return plane_isect(r) ? 0 : 1;
+        case IS_PARABOLOID: return paraboloid_isect(s, r) ? 0 : 1;
+        case IS_CONIC: return conic_isect(s, r) ? 0 : 1;
         case IS_ITER_POLY:
         case IS_ITER_CONIC: return asphere_isect(s, r);
-        case IS_TORIC: return toric_isect(s, fixes, r);
-        default: return true;
+        case IS_TORIC: return toric_isect(s, fixes, r) ? 0 : 1;
+        default: return 0;
     }
 }
 
 // ---- actions -------------------------------------------------------------------
 
-__device__ __forceinline__ void reflect(const DevSurface& s, Ray& r) {
-    if (s.cls == RTB_PLANE) {
-        r.cZ = -r.cZ;
-        return;
-    }
-    double nx, ny, nz;
-    normal(s, r, nx, ny, nz);
+// The actions take the surface normal (nx, ny, nz) at the ray's point,
+// computed once per surface by action(); (0, 0, 1) on a plane.
+__device__ __forceinline__ void reflect(double nx, double ny, double nz, Ray& r) {
     double a2 = 2.0 * fma(r.cX, nx, fma(r.cY, ny, r.cZ * nz)) * rcp(fma(nx, nx, fma(ny, ny, nz * nz)));
     r.cX = fma(-a2, nx, r.cX);
     r.cY = fma(-a2, ny, r.cY);
     r.cZ = fma(-a2, nz, r.cZ);
 }
 
-__device__ __forceinline__ bool refract(const DevSurface& s, double mu, Ray& r) {
-    double nx = 0.0, ny = 0.0, nz = 1.0;
-    if (s.cls != RTB_PLANE) normal(s, r, nx, ny, nz);
+__device__ __forceinline__ bool refract(double mu, double nx, double ny, double nz, Ray& r) {
     double iG = rcp(fma(nx, nx, fma(ny, ny, nz * nz)));
     double a = mu * fma(r.cX, nx, fma(r.cY, ny, r.cZ * nz)) * iG;
     double b = fma(mu, mu, -1.0) * iG;
@@ -327,7 +347,8 @@ __device__ __forceinline__ bool refract(const DevSurface& s, double mu, Ray& r) 
 }
 
 // Grating equation (surface.cu:1247-1520) in FP64.
-__device__ __forceinline__ bool diffract(const DevSurface& s, double mu, double L, Ray& r) {
+__device__ __forceinline__ bool diffract(const DevSurface& s, double mu, double L, double nx, double ny, double nz,
+                                         Ray& r) {
     const bool trans = s.gr_type == RTB_TRANSPARENT;
     if (s.cls == RTB_PLANE) {
         double a = trans ? mu * r.cZ : r.cZ;
@@ -345,8 +366,6 @@ __device__ __forceinline__ bool diffract(const DevSurface& s, double mu, double 
         }
         return true;
     }
-    double nx, ny, nz;
-    normal(s, r, nx, ny, nz);
     // rule direction p = (u, v, w), as the reference builds it (including its
     // L^2+M+M for the toric, surface.cu:1438,1487)
     double den = (s.cls == RTB_TORIC) ? fma(ny, ny, nz + nz) : fma(ny, ny, 1.0);
@@ -440,30 +459,39 @@ __device__ __forceinline__ bool table_at(const double* knots, int off, int n, do
     return true;
 }
 
+// One site for each of the table lookups and the normal keeps the kernel's
+// code small: it is bound by instruction fetch as much as by FP64 issue.
 __device__ __forceinline__ int action(const DevSurface& s, const double* knots, long long order, double lambda,
                                       TableMemo& memo, Ray& r) {
-    if (s.type == RTB_MIRROR) {
-        reflect(s, r);
+    if (s.type == RTB_MIRROR && s.cls == RTB_PLANE) {
+        r.cZ = -r.cZ;
         return 0;
     }
-    if (s.type == RTB_LENS) {
-        double a, b;
-        if (!table_at(knots, s.n1_off, s.n1_n, s.n1_invh, lambda, memo, a) ||
-            !table_at(knots, s.n2_off, s.n2_n, s.n2_invh, lambda, memo, b))
-            return 2;
-        return refract(s, a * rcp(b), r) ? 0 : 1;
-    }
-    if (s.type == RTB_GRATING) {
-        double n2v, mu = 0.0;
-        if (!table_at(knots, s.n2_off, s.n2_n, s.n2_invh, lambda, memo, n2v)) return 2;
-        double in2 = rcp(n2v);
-        if (s.gr_type == RTB_TRANSPARENT) {
-            double n1v;
-            if (!table_at(knots, s.n1_off, s.n1_n, s.n1_invh, lambda, memo, n1v)) return 2;
-            mu = n1v * in2;
+    double n1v = 1.0, n2v = 1.0;
+    if (s.type == RTB_LENS || s.type == RTB_GRATING) {
+        const int first = (s.type == RTB_LENS || s.gr_type == RTB_TRANSPARENT) ? 0 : 1;
+#pragma unroll 1
+        for (int t = first; t < 2; ++t) {
+            double v;
+            if (!table_at(knots, t ? s.n2_off : s.n1_off, t ? s.n2_n : s.n1_n, t ? s.n2_invh : s.n1_invh, lambda,
+                          memo, v))
+                return 2;
+            if (t) n2v = v;
+            else n1v = v;
         }
-        double L = (double)order * lambda * in2 * rcp(s.gr_const);
-        return diffract(s, mu, L, r) ? 0 : 1;
+    }
+    double nx = 0.0, ny = 0.0, nz = 1.0;
+    if (s.cls != RTB_PLANE) normal(s, r, nx, ny, nz);
+    if (s.type == RTB_MIRROR) {
+        reflect(nx, ny, nz, r);
+        return 0;
+    }
+    const double in2 = rcp(n2v);
+    if (s.type == RTB_LENS) return refract(n1v * in2, nx, ny, nz, r) ? 0 : 1;
+    if (s.type == RTB_GRATING) {
+        const double mu = (s.gr_type == RTB_TRANSPARENT) ? n1v * in2 : 0.0;
+        const double L = (double)order * lambda * in2 * rcp(s.gr_const);
+        return diffract(s, mu, L, nx, ny, nz, r) ? 0 : 1;
     }
     return 0;
 }
@@ -479,7 +507,9 @@ __device__ __forceinline__ int mx_surface(const DevSurface& s, int k, uint32_t f
                                           const DevBeam* beams, int b, double lam, mx::TableMemo& memo, mx::Ray& r) {
     mx::transform(s, r);
     if (!s.non_aux) return -1;
-    if (!mx::intersect(s, fixes, r)) return 3 * k;
+    const int hit = mx::intersect(s, fixes, r);
+    if (hit == 1) return 3 * k;
+    if (hit == 2) return 3 * k + 1;
     if (!f64::aperture_pass(s.type == RTB_SHADE, s.shape, s.size, s.center, r.X, r.Y)) return 3 * k + 1;
     long long order = s.order;
     if (s.type == RTB_GRATING && beams[b].n_orders > 0) order = beams[b].orders[s.grating_index];
@@ -509,14 +539,16 @@ __global__ void __maxnreg__(64) k_fused_mixed(const DevScheme* __restrict__ g_sc
     int b = 0;
     while (next_tile(ts, n_tiles, tile)) {
         for (int j = 0; j < ts.rpt; ++j) {
-            const size_t i = tile * tile_rays + (size_t)j * 32 + (threadIdx.x & 31);
+            const size_t slot = tile * tile_rays + (size_t)j * 32 + (threadIdx.x & 31);
+            const size_t i = (ts.order && slot < in.n) ? (size_t)ts.order[slot] : slot;  // the ray (outputs)
+            const size_t ri = ts.in_by_slot ? slot : i;                                  // its input
             bool ev = false, good = false;
             int key = 0;
             double outX = 0, outY = 0;
-            if (i < in.n && in.flag[i] == 1) {
-                mx::Ray r{in.X[i], in.Y[i], in.Z[i], in.cX[i], in.cY[i], in.cZ[i]};
+            if (slot < in.n && in.flag[ri] == 1) {
+                mx::Ray r{in.X[ri], in.Y[ri], in.Z[ri], in.cX[ri], in.cY[ri], in.cZ[ri]};
                 mx::normalize(r);
-                const double lam = in.lambda[i];
+                const double lam = in.lambda[ri];
                 // rays come in increasing order per thread: the previous
                 // ray's beam is usually this one's
                 if (!(b + 1 >= n_beams || i < beams[b + 1].first_ray) || i < beams[b].first_ray)
@@ -551,8 +583,8 @@ __global__ void __maxnreg__(64) k_fused_mixed(const DevScheme* __restrict__ g_sc
                 }
                 outX = r.X;
                 outY = r.Y;
-            } else if (i < in.n && in.flag != out.flag) {
-                out.flag[i] = in.flag[i];
+            } else if (slot < in.n && in.flag != out.flag) {
+                out.flag[i] = in.flag[ri];
             }
             count_event(ev, key, counts);
             if (frame.counts) frame_add(good, outX, outY, frame);

@@ -215,4 +215,86 @@ int rearrange_device(size_t ng, double* arrays[7], char* flag, size_t* ng_out, c
     return RTB_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Coherent tracing order of generated rays.  A composite beam interleaves its
+// wavelengths (ray j has wavelength j mod n_lambda) and draws positions
+// independently, so the 32 rays of a warp go to 32 wavelengths and 32 points
+// of the pupil, and which surface loses each of them is close to random: the
+// lanes of rays lost early idle while the others finish the scheme.  Sorted
+// by (beam, chunk of 2^chunk_shift consecutive rays, wavelength, Morton code
+// of the entrance position), a warp traces neighbouring rays of one
+// wavelength, which mostly share their fate.  The key only orders the work:
+// any key gives a permutation.
+
+__device__ __forceinline__ uint32_t spread12(uint32_t v) {
+    v &= 0xfffu;
+    v = (v | (v << 8)) & 0x00ff00ffu;
+    v = (v | (v << 4)) & 0x0f0f0f0fu;
+    v = (v | (v << 2)) & 0x33333333u;
+    v = (v | (v << 1)) & 0x55555555u;
+    return v;
+}
+
+__global__ void k_order_keys(const GenBeam* beams, int n_beams, uint64_t total, DevRays rays,
+                             unsigned long long* keys, uint32_t* idx, int chunk_shift) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
+         i += (uint64_t)blockDim.x * gridDim.x) {
+        int lo = 0, hi = n_beams - 1;
+        while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if (beams[mid].first_ray <= i) lo = mid; else hi = mid - 1;
+        }
+        const GenBeam& b = beams[lo];
+        const uint64_t j = i - b.first_ray;
+        const uint64_t lam = (j < b.n_rays && b.n_lambda > 0) ? j % b.n_lambda : 0;
+        const double R = b.disk[2] > 0 ? b.disk[2] : 1.0;
+        auto q = [R](double v, double c) {
+            double u = (v - c) / (2.0 * R) + 0.5;
+            u = u < 0.0 ? 0.0 : (u > 1.0 ? 1.0 : u);
+            return (uint32_t)(u * 4095.0);
+        };
+        const uint32_t m = spread12(q(rays.X[i], b.center[0])) | (spread12(q(rays.Y[i], b.center[1])) << 1);
+        const uint64_t chunk = j >> chunk_shift;
+        keys[i] = ((unsigned long long)(lo & 0xffff) << 48) | ((unsigned long long)(chunk & 0xfffu) << 36) |
+                  ((unsigned long long)(lam & 0xfffu) << 24) | m;
+        idx[i] = (uint32_t)i;
+    }
+}
+
+int coherent_order(const GenBeam* d_beams, int n_beams, uint64_t n, const DevRays& rays, uint32_t* order,
+                   int chunk_shift, cudaStream_t st) {
+    if (n == 0) return RTB_OK;
+    if (n > 0xffffffffull) return RTB_BAD_VALUE;
+    DevBuf buf;
+    const size_t kb = (n * 8 + 255) / 256 * 256, ib = (n * 4 + 255) / 256 * 256;
+    size_t tmp = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tmp, (unsigned long long*)nullptr, (unsigned long long*)nullptr,
+                                    (uint32_t*)nullptr, (uint32_t*)nullptr, (int64_t)n, 0, 64, st);
+    int s = buf.alloc(2 * kb + ib + tmp + 256, st);
+    if (s != RTB_OK) return s;
+    char* p = buf.as<char>();
+    auto* k_in = reinterpret_cast<unsigned long long*>(p);
+    auto* k_out = reinterpret_cast<unsigned long long*>(p + kb);
+    auto* i_in = reinterpret_cast<uint32_t*>(p + 2 * kb);
+    void* t = p + 2 * kb + ib;
+    k_order_keys<<<grid_for(n, 256, 8), 256, 0, st>>>(d_beams, n_beams, n, rays, k_in, i_in, chunk_shift);
+    RTB_CUDA_TRY(cudaGetLastError());
+    RTB_CUDA_TRY(cub::DeviceRadixSort::SortPairs(t, tmp, k_in, k_out, i_in, order, (int64_t)n, 0, 64, st));
+    return RTB_OK;
+}
+
+__global__ void k_gather_rays(const uint32_t* order, uint64_t n, DevRays src, DevRays dst) {
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < n; t += (uint64_t)blockDim.x * gridDim.x) {
+        const uint64_t i = order[t];
+        dst.X[t] = src.X[i];
+        dst.Y[t] = src.Y[i];
+        dst.Z[t] = src.Z[i];
+        dst.cX[t] = src.cX[i];
+        dst.cY[t] = src.cY[i];
+        dst.cZ[t] = src.cZ[i];
+        dst.lambda[t] = src.lambda[i];
+        dst.flag[t] = src.flag[i];
+    }
+}
+
 }  // namespace rtb

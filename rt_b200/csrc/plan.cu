@@ -29,6 +29,9 @@ struct rtb_plan {
     TraceArgs args;                  // scheme, knots, beams, counters (device)
     void* in_mem = nullptr;          // generated rays
     void* out_mem = nullptr;         // output arrays
+    uint32_t* order = nullptr;       // coherent tracing order (device), or NULL for index order
+    void* slot_mem = nullptr;        // the input rays in tracing order (with `order`)
+    DevRays in_slot{};
     DevRays in{}, out{};
     unsigned long long* h_counts = nullptr;  // page-locked: counters, then the error word
     cudaStream_t stream = nullptr;
@@ -43,7 +46,7 @@ struct rtb_plan {
 namespace {
 
 // Configurations the autotuner chose, by plan key (scheme, precision, frame
-// use, ray count), for the life of the process.
+// use, ray order, ray count), for the life of the process.
 std::mutex g_tuned_mu;
 std::map<uint64_t, std::pair<int32_t, int32_t>> g_tuned;
 
@@ -58,7 +61,7 @@ uint64_t plan_key(const rtb_plan& p) {
     h = fnv1a(h, &p.ps.sch, sizeof(DevScheme));
     h = fnv1a(h, p.ps.knots.data(), p.ps.knots.size() * sizeof(double));
     h = fnv1a(h, &p.n_rays, sizeof(p.n_rays));
-    int32_t tags[2] = {p.opts.precision, p.has_frame ? 1 : 0};
+    int32_t tags[3] = {p.opts.precision, p.has_frame ? 1 : 0, p.opts.ray_order};
     return fnv1a(h, tags, sizeof(tags));
 }
 
@@ -103,7 +106,8 @@ int enqueue_run(rtb_plan* p, const FrameArgs& frame, cudaStream_t s) {
     rtb_trace_opts o = p->opts;
     o.block_size = p->block;
     o.rays_per_thread = p->rpt;
-    int st = launch_trace(p->ps, p->args, (int)p->n_beams, o, p->in, p->out, frame, s);
+    int st = p->order ? launch_trace(p->ps, p->args, (int)p->n_beams, o, p->in_slot, p->out, frame, s, p->order, true)
+                      : launch_trace(p->ps, p->args, (int)p->n_beams, o, p->in, p->out, frame, s);
     if (st != RTB_OK) return st;
     RTB_CUDA_TRY(cudaMemcpyAsync(p->h_counts, p->args.counts, p->args.counts_len * 8, cudaMemcpyDeviceToHost, s));
     RTB_CUDA_TRY(cudaMemcpyAsync(p->h_counts + p->args.counts_len, p->args.err, 4, cudaMemcpyDeviceToHost, s));
@@ -153,6 +157,8 @@ void release(rtb_plan* p) {
     if (p->stream) cudaStreamSynchronize(p->stream);
     if (p->in_mem) cudaFree(p->in_mem);
     if (p->out_mem) cudaFree(p->out_mem);
+    if (p->order) cudaFree(p->order);
+    if (p->slot_mem) cudaFree(p->slot_mem);
     if (p->h_counts) cudaFreeHost(p->h_counts);
     if (p->done) cudaEventDestroy(p->done);
     if (p->stream) cudaStreamDestroy(p->stream);
@@ -255,6 +261,32 @@ int rtb_plan_create(const rtb_surface* surfaces, size_t n_surfaces, const rtb_be
     if (e == cudaSuccess) {
         k_generate<<<grid_for(total, 256, 8), 256, 0, p->stream>>>(gbuf.as<GenBeam>(), (int)n_beams, total, p->in);
         e = cudaGetLastError();
+    }
+    // the coherent tracing order and a copy of the rays in that order, once
+    // (index order for plans beyond 2^32 rays).  Wavelength groups span up to
+    // 2^30 rays of a beam: on C1 both kernels were faster with whole-beam
+    // groups than with chunks of 2^18 rays (the stores scatter either way).
+    if (e == cudaSuccess && opts->ray_order == RTB_ORDER_COHERENT && p->n_rays <= 0xffffffffull) {
+        e = cudaMalloc(&p->order, p->n_rays * sizeof(uint32_t));
+        if (e == cudaSuccess) e = cudaMalloc(&p->slot_mem, rays_bytes(p->n_rays, true));
+        if (e == cudaSuccess) {
+            p->in_slot = carve(p->slot_mem, p->n_rays, true);
+            st = coherent_order(gbuf.as<GenBeam>(), (int)n_beams, p->n_rays, p->in, p->order, 30, p->stream);
+            if (st == RTB_OK) {
+                k_gather_rays<<<grid_for(p->n_rays, 256, 8), 256, 0, p->stream>>>(p->order, p->n_rays, p->in,
+                                                                                  p->in_slot);
+                e = cudaGetLastError();
+            }
+            if (st != RTB_OK) {
+                gbuf.release();
+                release(p);
+                return st;
+            }
+        }
+    } else if (e == cudaSuccess && opts->ray_order != RTB_ORDER_COHERENT && opts->ray_order != RTB_ORDER_INDEX) {
+        gbuf.release();
+        release(p);
+        return RTB_BAD_VALUE;
     }
     gbuf.release();
     if (e == cudaSuccess) e = cudaStreamSynchronize(p->stream);

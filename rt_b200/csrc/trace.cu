@@ -94,7 +94,8 @@ int gen_beams(const rtb_beam* beams, size_t n_beams, size_t n_rays, std::vector<
 }
 
 int launch_trace(const PreparedScheme& ps, TraceArgs& a, int n_beams, const rtb_trace_opts& o, const DevRays& in,
-                 const DevRays& out, const FrameArgs& frame, cudaStream_t st) {
+                 const DevRays& out, const FrameArgs& frame, cudaStream_t st, const uint32_t* order,
+                 bool in_by_slot) {
     if (o.engine == RTB_ENGINE_PER_SURFACE) {
         if (o.precision != RTB_FP64) return RTB_BAD_VALUE;
         unsigned grid = grid_for(in.n, 256, 8);
@@ -120,7 +121,7 @@ int launch_trace(const PreparedScheme& ps, TraceArgs& a, int n_beams, const rtb_
         if (per_sm < 1) per_sm = 1;
         unsigned grid = grid_for(in.n, threads * rpt, per_sm);
         kern<<<grid, threads, smem, st>>>(a.sch, a.knots, a.beams, n_beams, in, out, a.counts, a.err,
-                                          o.state_out ? 1 : 0, frame, TileSched{a.tiles, rpt});
+                                          o.state_out ? 1 : 0, frame, TileSched{a.tiles, rpt, order, in_by_slot ? 1 : 0});
     } else {
         return RTB_BAD_VALUE;
     }

@@ -32,6 +32,7 @@ FP64, MIXED = range(2)
 FIX_TORIC_SIGN = 1
 FIX_TORIC_STEP = 2
 FIX_ASPHERE_ROOT = 4
+ORDER_COHERENT, ORDER_INDEX = 0, 1
 
 MAX_POLY = 10
 MAX_PARAMS = 16
@@ -74,7 +75,7 @@ class CCD(C.Structure):
 class TraceOpts(C.Structure):
     _fields_ = [("engine", C.c_int32), ("precision", C.c_int32), ("fixes", C.c_uint32),
                 ("renormalize_lost", C.c_int32), ("block_size", C.c_int32), ("rays_per_thread", C.c_int32),
-                ("state_out", C.c_int32), ("reserved", C.c_int32), ("ccd", C.POINTER(CCD)),
+                ("state_out", C.c_int32), ("ray_order", C.c_int32), ("ccd", C.POINTER(CCD)),
                 ("counts", C.c_void_p), ("n_outside", C.c_void_p)]
 
 

@@ -6,6 +6,8 @@ angle and order in one graph-launched trace, and the autotuner (GPU tests).
 * Every launch configuration the autotuner tries gives the same result.
 * The autotuner leaves the plan's frame untouched and its choice is reused
   by a later plan of the same scheme and size.
+* The coherent tracing order (the default) and index order give the same
+  rays, counters and frame.
 """
 import ctypes as C
 
@@ -192,3 +194,41 @@ def test_plan_mixed_accuracy_on_c3():
     assert m["pixel_mismatch_rate"] < 1e-3
     pm.destroy()
     pr.destroy()
+
+
+@pytest.mark.parametrize("precision", [ffi.MIXED, ffi.FP64])
+@pytest.mark.parametrize("workload", ["c1", "c3"])
+def test_plan_ray_order_does_not_change_results(precision, workload):
+    """Plans trace their rays sorted by beam, wavelength and entrance
+    position (RTB_ORDER_COHERENT) unless asked for index order; every output
+    is the same either way."""
+    beams = S.c1_beams(n_per_lambda=300) if workload == "c1" else small_c3()
+    ccd = S.ccd(S.C1_CCD)
+    cs = S.to_c(S.echelle(), E.spline_init)
+    res = []
+    for order in (ffi.ORDER_COHERENT, ffi.ORDER_INDEX):
+        o, counts, outside = frame_opts(precision, ccd, state_out=1)
+        o.ray_order = order
+        plan = E.Plan(cs.surfaces, beams, o)
+        plan.run()
+        st, stats = plan.result()
+        _, out = plan_output(plan)
+        res.append((st, stats.ray_surfaces, stats.n_good, {k: v.clone() for k, v in out.items()}, counts.clone(),
+                    int(outside), plan.counts()))
+        plan.destroy()
+    a, b = res
+    assert a[:3] == b[:3] and a[0] in TRACED
+    for f in ("X", "Y", "Z", "cX", "cY", "cZ"):
+        x, y = a[3][f].view(torch.int64), b[3][f].view(torch.int64)
+        assert torch.equal(x, y), f
+    assert torch.equal(a[3]["flag"], b[3]["flag"]) and torch.equal(a[3]["lost_stage"], b[3]["lost_stage"])
+    assert torch.equal(a[4], b[4]) and a[5] == b[5]
+    assert np.array_equal(a[6], b[6])
+
+
+def test_plan_rejects_unknown_ray_order():
+    cs = S.to_c(S.echelle(), E.spline_init)
+    o = E.opts(engine=ffi.ENGINE_FUSED, precision=ffi.MIXED, fixes=FIXES)
+    o.ray_order = 7
+    with pytest.raises(RuntimeError, match="BAD_VALUE"):
+        E.Plan(cs.surfaces, small_c3(n_beams=4), o)
