@@ -29,8 +29,9 @@ inline size_t fused_smem_bytes(int n_knots) {
     return ((sizeof(DevScheme) + 15) / 16) * 16 + sizeof(double) * (size_t)n_knots;
 }
 
-// Scheduling of the persistent fused kernels: `next` is a counter of
-// 32*rpt-ray tiles handed out to warps (zeroed before each launch).  Slot s
+// Scheduling of the persistent fused kernels: `next` is a counter of tiles
+// (zeroed before each launch) handed out to warps, 32*rpt rays each
+// (k_fused_mixed), or to blocks, blockDim*rpt rays each (k_fused_fp64).  Slot s
 // of the tiles traces ray order[s] (a permutation of the rays), or ray s when
 // order is NULL; its input is read at s when in_by_slot (the input arrays
 // hold the rays in tracing order), else at the ray's index.  Outputs go to
