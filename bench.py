@@ -42,7 +42,7 @@ WORKLOAD = ("C1 cross-dispersed echelle: 1.0e8 rays (31 echelle orders 30..60 x 
             "x 50404 rays, disk r=25 mm), OAP + echelle + cross-disperser + toric fold + 2 even-asphere lens "
             "surfaces + CCD 4096^2, frame counts accumulated")
 FIXES = 3  # RTB_FIX_TORIC_SIGN | RTB_FIX_TORIC_STEP: the toric fold's Steffensen step divides 0/0 otherwise
-TRAFFIC_PER_RAY_MIXED = (134.097152e6 + 24.593920e6) / 1_984_000  # ncu dram__bytes_read+write per ray
+TRAFFIC_PER_RAY_MIXED = (143.314176e6 + 25.566464e6) / 1_984_000  # ncu dram__bytes_read+write per ray
 
 
 def parse():
@@ -377,15 +377,17 @@ def main():
     peak = peaks.get("hbm_gbs", 6650.0)
     achieved = alg_bytes / (hv["ms_per_step"] * 1e-3) / 1e9
     # DRAM traffic of k_fused_mixed from an ncu capture of the same workload
-    # at 1,984,000 rays (134.1 MB read + 24.6 MB written), scaled by rays
+    # at 1,984,000 rays (143.3 MB read + 25.6 MB written, the tracing-order
+    # index and the plan's ordered copy of the rays included), scaled by rays
     traffic = TRAFFIC_PER_RAY_MIXED * n if head == "fused_mixed" else None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "traffic_per_ray_bytes": TRAFFIC_PER_RAY_MIXED if traffic else None,
                 "alg_bytes": alg_bytes,
                 "kernel": "k_fused_mixed" if head == "fused_mixed" else "k_fused_fp64",
                 "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "fallback",
-                "note": "HBM view of a kernel that is FP64-issue bound: ncu shows FP64 pipe 47% active, "
-                        "DRAM 6% of peak, 17.4/32 threads active per instruction"}
+                "note": "HBM view of a kernel bound by instruction issue and FP64 latency: ncu shows issue "
+                        "slots 65% busy, FP64 pipe 35% active, 29.6/32 threads active per instruction, "
+                        "DRAM 10% of peak"}
 
     e2e = None
     if not args.no_e2e and rank == 0:
