@@ -11,8 +11,12 @@
 // to the parameters that live on it is recomputed from checkpoint k in
 // forward mode (dual numbers, W directions per pass); the adjoint of the
 // output state is carried back through it, and the parameter adjoints are
-// accumulated.  Per-thread sums are reduced per block in a fixed order and
-// the block partials summed in block order, so the gradient is reproducible.
+// accumulated.  The surface's dual-number constants of every pass (which do
+// not depend on the ray) are built once per call into a table
+// (k_build_surfd) that all threads read.  Each warp sums a parameter's
+// contributions over its 32 lanes with a shuffle tree and adds them to its
+// row in shared memory; the block adds its warps' rows in order and the block
+// partials are summed in block order, so the gradient is reproducible.
 //
 // Translation unit compiled with --fmad=false: the dual numbers' values are
 // the plain engine's.
@@ -27,7 +31,7 @@ namespace rtb {
 
 namespace {
 
-constexpr int kAdjW = 4;           // directions per dual pass of the backward sweep
+constexpr int kAdjW = 2;           // directions per dual pass of the backward sweep (2 ran faster than 4)
 constexpr int kAdjThreads = 128;
 constexpr int kMeritThreads = 256;
 constexpr int kMeritParts = 32;    // fixed split of each group's rays (deterministic sums)
@@ -100,70 +104,103 @@ __global__ void __launch_bounds__(256) k_adj_forward(AdjArgs a, DevRays in, unsi
     }
 }
 
-// Per-thread parameter adjoints live in local memory; the block reduces them
-// in a fixed tree order into partial[blockIdx.x][P].
-__device__ void block_reduce_params(double* g, int P, double* partial) {
-    __shared__ double red[kAdjThreads];
-    for (int p = 0; p < P; ++p) {
-        red[threadIdx.x] = g[p];
-        __syncthreads();
-        for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-            if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
-            __syncthreads();
-        }
-        if (threadIdx.x == 0) partial[(size_t)blockIdx.x * P + p] = red[0];
-        __syncthreads();
+// The dual-number surface constants of pass (k, d0) of the backward sweep:
+// lane l differentiates state component d0 + l (< 6) or the surface's
+// parameter d0 + l - 6.
+__device__ __forceinline__ void backward_seeds(const AdjArgs& a, int k, int d0, ad::Seeds<kAdjW>& sd) {
+    const int ndir = 6 + a.surf_nparams[k];
+    sd.dense = nullptr;
+    for (int l = 0; l < kAdjW; ++l) {
+        const int d = d0 + l;
+        sd.state[l] = (d < 6) ? d : -1;
+        sd.param[l] = (d >= 6 && d < ndir) ? a.surf_params[k * RTB_ADJ_MAX_PARAMS + (d - 6)] : -1;
     }
 }
 
-__global__ void __launch_bounds__(kAdjThreads) k_adj_backward(AdjArgs a, const double* gX, const double* gY,
-                                                              double* partial) {
+// One thread per table entry (k, d0).
+__global__ void k_build_surfd(AdjArgs a, const int2* entries, int n_entries, ad::SurfD<kAdjW>* table) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n_entries) return;
+    const int k = entries[e].x;
+    ad::Seeds<kAdjW> sd;
+    backward_seeds(a, k, entries[e].y, sd);
+    ad::make_surfd(a.sch->s[k], k, a.map, a.n_params, sd, table[e]);
+}
+
+// The forward-mode constants of surface k along the direction dtheta.
+__global__ void k_build_surfd_dense(AdjArgs a, const double* dtheta, ad::SurfD<1>* table) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= a.sch->n_surfaces) return;
+    ad::Seeds<1> sd;
+    sd.dense = dtheta;
+    sd.state[0] = -1;
+    sd.param[0] = -1;
+    ad::make_surfd(a.sch->s[k], k, a.map, a.n_params, sd, table[k]);
+}
+
+constexpr int kAdjWarps = kAdjThreads / 32;
+
+// Rays are taken 32 at a time per warp, every lane of a warp the same number
+// of steps, so the warp can sum each parameter's contributions with shuffles.
+// first_entry[k]: the table entry of surface k's first pass.
+__global__ void __launch_bounds__(kAdjThreads) k_adj_backward(AdjArgs a, const ad::SurfD<kAdjW>* table,
+                                                              const int* first_entry, const double* gX,
+                                                              const double* gY, double* partial) {
+    __shared__ double acc[kAdjWarps][RTB_ADJ_MAX_PARAMS];
     const DevScheme* sch = a.sch;
     const int ns = sch->n_surfaces;
     const int P = a.n_params;
-    double g[RTB_ADJ_MAX_PARAMS];
-    for (int p = 0; p < P; ++p) g[p] = 0.0;
-    for (size_t i = gtid(); i < a.n; i += gstride()) {
-        if (a.flag[i] != 1) continue;
-        double adj[6] = {gX[i], gY[i], 0.0, 0.0, 0.0, 0.0};
-        if (adj[0] == 0.0 && adj[1] == 0.0) continue;
-        const double lam = a.lambda[i];
-        const int b = beam_of(a.beams, a.n_beams, i);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int p = lane; p < P; p += 32) acc[warp][p] = 0.0;
+    __syncwarp();
+    for (size_t i0 = (size_t)blockIdx.x * blockDim.x + (size_t)warp * 32; i0 < a.n; i0 += gstride()) {
+        const size_t i = i0 + lane;
+        bool act = i < a.n && a.flag[i] == 1;
+        double adj[6] = {act ? gX[i] : 0.0, act ? gY[i] : 0.0, 0.0, 0.0, 0.0, 0.0};
+        act = act && !(adj[0] == 0.0 && adj[1] == 0.0);
+        if (!__any_sync(0xffffffffu, act)) continue;
+        const double lam = act ? a.lambda[i] : 0.0;
+        const int b = act ? beam_of(a.beams, a.n_beams, i) : 0;
         for (int k = ns - 1; k >= 0; --k) {
             const DevSurface& s = sch->s[k];
             double st[6];
-            for (int c = 0; c < 6; ++c) st[c] = a.ckpt[((size_t)k * 6 + c) * a.n + i];
-            const int npk = a.surf_nparams[k];
-            const int ndir = 6 + npk;
+            if (act)
+                for (int c = 0; c < 6; ++c) st[c] = a.ckpt[((size_t)k * 6 + c) * a.n + i];
+            const int ndir = 6 + a.surf_nparams[k];
             double adj_in[6] = {0, 0, 0, 0, 0, 0};
-            for (int d0 = 0; d0 < ndir; d0 += kAdjW) {
+            for (int d0 = 0, e = first_entry[k]; d0 < ndir; d0 += kAdjW, ++e) {
                 ad::Seeds<kAdjW> sd;
-                sd.dense = nullptr;
-                for (int l = 0; l < kAdjW; ++l) {
-                    const int d = d0 + l;
-                    sd.state[l] = (d < 6) ? d : -1;
-                    sd.param[l] = (d >= 6 && d < ndir) ? a.surf_params[k * RTB_ADJ_MAX_PARAMS + (d - 6)] : -1;
-                }
-                ad::SurfD<kAdjW> sdv;
-                ad::make_surfd(s, k, a.map, P, sd, sdv);
+                backward_seeds(a, k, d0, sd);
                 ad::RayD<kAdjW> r;
-                ad::load_state(st, sd, r);
-                ad::surface_step(s, sdv, sch->fixes, a.knots, order_of(s, a.beams, b), lam, r);
+                if (act) {
+                    ad::load_state(st, sd, r);
+                    ad::surface_step(s, table[e], sch->fixes, a.knots, order_of(s, a.beams, b), lam, r);
+                }
                 // the last surface's output is the CCD-plane point: only X, Y carry adjoints
                 const ad::Dual<kAdjW>* out[6] = {&r.X, &r.Y, &r.Z, &r.cX, &r.cY, &r.cZ};
                 for (int l = 0; l < kAdjW; ++l) {
                     const int d = d0 + l;
                     if (d >= ndir) break;
                     double v = 0.0;
-                    for (int c = 0; c < 6; ++c) v += adj[c] * out[c]->d[l];
-                    if (d < 6) adj_in[d] = v;
-                    else g[sd.param[l]] += v;
+                    if (act)
+                        for (int c = 0; c < 6; ++c) v += adj[c] * out[c]->d[l];
+                    if (d < 6) {
+                        adj_in[d] = v;
+                    } else {
+                        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                        if (lane == 0) acc[warp][sd.param[l]] += v;
+                    }
                 }
             }
             for (int c = 0; c < 6; ++c) adj[c] = adj_in[c];
         }
     }
-    block_reduce_params(g, P, partial);
+    __syncthreads();
+    for (int p = threadIdx.x; p < P; p += blockDim.x) {
+        double sum = 0.0;
+        for (int w = 0; w < kAdjWarps; ++w) sum += acc[w][p];
+        partial[(size_t)blockIdx.x * P + p] = sum;
+    }
 }
 
 __global__ void k_adj_sum_partials(const double* partial, int n_blocks, int P, double* grad) {
@@ -175,8 +212,10 @@ __global__ void k_adj_sum_partials(const double* partial, int n_blocks, int P, d
 }
 
 // Forward-mode sensitivities along one parameter direction, through the whole
-// scheme from checkpoint 0 (the input rays).
-__global__ void __launch_bounds__(kAdjThreads) k_adj_jvp(AdjArgs a, const double* dtheta, double* dX, double* dY) {
+// scheme from checkpoint 0 (the input rays); table[k]: surface k's constants
+// along that direction.
+__global__ void __launch_bounds__(kAdjThreads) k_adj_jvp(AdjArgs a, const ad::SurfD<1>* table, double* dX,
+                                                         double* dY) {
     const DevScheme* sch = a.sch;
     const int ns = sch->n_surfaces;
     for (size_t i = gtid(); i < a.n; i += gstride()) {
@@ -188,7 +227,7 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_jvp(AdjArgs a, const double
         const double lam = a.lambda[i];
         const int b = beam_of(a.beams, a.n_beams, i);
         ad::Seeds<1> sd;
-        sd.dense = dtheta;
+        sd.dense = nullptr;
         sd.state[0] = -1;
         sd.param[0] = -1;
         double st[6];
@@ -197,9 +236,7 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_jvp(AdjArgs a, const double
         ad::load_state(st, sd, r);
         for (int k = 0; k < ns; ++k) {
             const DevSurface& s = sch->s[k];
-            ad::SurfD<1> sdv;
-            ad::make_surfd(s, k, a.map, a.n_params, sd, sdv);
-            ad::surface_step(s, sdv, sch->fixes, a.knots, order_of(s, a.beams, b), lam, r);
+            ad::surface_step(s, table[k], sch->fixes, a.knots, order_of(s, a.beams, b), lam, r);
         }
         dX[i] = r.X.d[0];
         dY[i] = r.Y.d[0];
@@ -276,6 +313,7 @@ struct rtb_adjoint {
     std::vector<rtb_surface> surf;                 // the scheme, tables repointed to...
     std::vector<std::vector<double>> tables;       // ...these copies
     std::vector<rtb_param> params;
+    std::vector<int> surf_nparams;                 // parameters per surface
     std::vector<DevBeam> beams_h;
     std::vector<rtb_beam> beams_in;
     uint64_t n = 0;
@@ -457,6 +495,7 @@ int rtb_adjoint_create(const rtb_surface* surfaces, size_t n_surfaces, const rtb
         map[j] = ad::ParamRef{p.surface, p.kind, p.index, 0};
         sp[p.surface * RTB_ADJ_MAX_PARAMS + sn[p.surface]++] = (int)j;
     }
+    c->surf_nparams = sn;
     // one allocation: scheme, knots (room for the largest table set), beams,
     // map, lists, counters, grad; then the per-ray arrays
     auto al = [](size_t x) { return (x + 255) / 256 * 256; };
@@ -575,13 +614,33 @@ int rtb_adjoint_backward(rtb_adjoint* c, const double* gX, const double* gY, dou
     cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
     const int P = (int)c->params.size();
     const unsigned grid = adj_grid(c->n, kAdjThreads);
-    DevBuf partial;
-    int st = partial.alloc((size_t)grid * P * sizeof(double), s);
+    // the passes of every surface: (k, first direction)
+    std::vector<int2> entries;
+    std::vector<int> first(c->surf_nparams.size());
+    for (size_t k = 0; k < c->surf_nparams.size(); ++k) {
+        first[k] = (int)entries.size();
+        for (int d0 = 0; d0 < 6 + c->surf_nparams[k]; d0 += kAdjW) entries.push_back(make_int2((int)k, d0));
+    }
+    const size_t ne = entries.size();
+    auto al = [](size_t x) { return (x + 255) / 256 * 256; };
+    const size_t o_ent = al(ne * sizeof(ad::SurfD<kAdjW>)), o_first = o_ent + al(ne * sizeof(int2)),
+                 o_part = o_first + al(first.size() * sizeof(int));
+    DevBuf buf;
+    int st = buf.alloc(o_part + (size_t)grid * P * sizeof(double), s);
     if (st != RTB_OK) return st;
+    char* p = buf.as<char>();
+    auto* table = reinterpret_cast<ad::SurfD<kAdjW>*>(p);
+    auto* d_ent = reinterpret_cast<int2*>(p + o_ent);
+    auto* d_first = reinterpret_cast<int*>(p + o_first);
+    double* partial = reinterpret_cast<double*>(p + o_part);
+    RTB_CUDA_TRY(cudaMemcpyAsync(d_ent, entries.data(), ne * sizeof(int2), cudaMemcpyHostToDevice, s));
+    RTB_CUDA_TRY(cudaMemcpyAsync(d_first, first.data(), first.size() * sizeof(int), cudaMemcpyHostToDevice, s));
     AdjArgs a = adj_args(c);
-    k_adj_backward<<<grid, kAdjThreads, 0, s>>>(a, gX, gY, partial.as<double>());
+    k_build_surfd<<<(unsigned)((ne + 63) / 64), 64, 0, s>>>(a, d_ent, (int)ne, table);
     RTB_CUDA_TRY(cudaGetLastError());
-    k_adj_sum_partials<<<1, RTB_ADJ_MAX_PARAMS, 0, s>>>(partial.as<double>(), (int)grid, P, c->d_grad);
+    k_adj_backward<<<grid, kAdjThreads, 0, s>>>(a, table, d_first, gX, gY, partial);
+    RTB_CUDA_TRY(cudaGetLastError());
+    k_adj_sum_partials<<<1, RTB_ADJ_MAX_PARAMS, 0, s>>>(partial, (int)grid, P, c->d_grad);
     RTB_CUDA_TRY(cudaGetLastError());
     RTB_CUDA_TRY(cudaMemcpyAsync(grad, c->d_grad, P * sizeof(double), cudaMemcpyDeviceToHost, s));
     RTB_CUDA_TRY(cudaStreamSynchronize(s));
@@ -597,7 +656,13 @@ int rtb_adjoint_jvp(rtb_adjoint* c, const double* dtheta, double* dX, double* dY
     for (size_t j = 0; j < c->params.size(); ++j) d[j] = dtheta[j];
     RTB_CUDA_TRY(cudaMemcpyAsync(c->d_dtheta, d.data(), d.size() * sizeof(double), cudaMemcpyHostToDevice, s));
     AdjArgs a = adj_args(c);
-    k_adj_jvp<<<adj_grid(c->n, kAdjThreads), kAdjThreads, 0, s>>>(a, c->d_dtheta, dX, dY);
+    const int ns = (int)c->surf_nparams.size();
+    DevBuf table;
+    int st = table.alloc((size_t)ns * sizeof(ad::SurfD<1>), s);
+    if (st != RTB_OK) return st;
+    k_build_surfd_dense<<<(unsigned)((ns + 31) / 32), 32, 0, s>>>(a, c->d_dtheta, table.as<ad::SurfD<1>>());
+    RTB_CUDA_TRY(cudaGetLastError());
+    k_adj_jvp<<<adj_grid(c->n, kAdjThreads), kAdjThreads, 0, s>>>(a, table.as<ad::SurfD<1>>(), dX, dY);
     RTB_CUDA_TRY(cudaGetLastError());
     RTB_CUDA_TRY(cudaStreamSynchronize(s));
     return RTB_OK;
