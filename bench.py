@@ -61,16 +61,8 @@ def parse():
 
 
 def dist_init(args):
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
-        import torch
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    return world, rank, local
+    from rt_b200 import replicas
+    return replicas.init("nccl")
 
 
 class Clocks:
@@ -165,7 +157,9 @@ def cpu_baseline(specs_fn, beams_all, budget_s=6.0):
 
 
 def reference_arm(args):
-    world, rank, _ = dist_init(args)
+    # rank 0 alone runs (on the host cores) and prints; the other ranks exit
+    from rt_b200 import replicas
+    world, rank, _ = replicas.env()
     if rank != 0:
         return
     from rt_b200 import schemes as S
@@ -192,7 +186,8 @@ def main():
     from rt_b200 import ffi, schemes as S
 
     npl = args.rays_per_lambda or S.c1_rays_per_lambda()
-    beams = S.c1_beams(n_per_lambda=npl, seed=S.SEED + 7919 * rank)
+    from rt_b200 import replicas
+    beams = S.c1_beams(n_per_lambda=npl, seed=replicas.seed(S.SEED, rank))
     n = S.total_rays(beams)
     cs = S.to_c(S.echelle(), E.spline_init)
     surf = cs.surfaces
@@ -222,11 +217,12 @@ def main():
         ffi.check(st, "rtb_trace_out")
         return stats
 
+    # device time of K steps, the maximum over ranks; `rs` the ray-surfaces of
+    # one step summed over ranks (each replica traces its own rays)
     def timed(o, K, W):
         for _ in range(W):
             stats = step(o)
-        if world > 1:
-            torch.distributed.barrier()
+        replicas.barrier()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -234,11 +230,8 @@ def main():
             stats = step(o)
         e1.record(stream)
         torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1)
-        if world > 1:
-            t = torch.tensor([ms], device="cuda")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = replicas.max_over_ranks(e0.elapsed_time(e1))
+        stats.rs = replicas.sum_over_ranks(stats.ray_surfaces)
         return ms / K, stats
 
     engines = {}
@@ -255,8 +248,7 @@ def main():
         for _ in range(W):
             plan.run(C.c_void_p(stream.cuda_stream))
         traced(plan.result()[0])
-        if world > 1:
-            torch.distributed.barrier()
+        replicas.barrier()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -264,13 +256,10 @@ def main():
             plan.run(C.c_void_p(stream.cuda_stream))
         e1.record(stream)
         torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1)
-        if world > 1:
-            t = torch.tensor([ms], device="cuda")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = replicas.max_over_ranks(e0.elapsed_time(e1))
         st, stats = plan.result()
         traced(st)
+        stats.rs = replicas.sum_over_ranks(stats.ray_surfaces)
         return ms / K, stats
 
     want = set(args.engines.split(","))
@@ -283,7 +272,7 @@ def main():
         try:
             step(o)
             ms, stats = timed(o, max(2, args.steps // 4), 1)
-            engines["per_surface"] = {"ms_per_step": ms, "value": stats.ray_surfaces * world / (ms * 1e-3),
+            engines["per_surface"] = {"ms_per_step": ms, "value": stats.rs / (ms * 1e-3),
                                       "ray_surfaces_per_step": stats.ray_surfaces, "n_good": stats.n_good,
                                       "launch": "rtb_trace_out, 7 surface kernels + frame kernel"}
         except RuntimeError as e:
@@ -318,7 +307,7 @@ def main():
             engines[name] = {"error": str(e)}
             continue
         plans[name] = plan
-        engines[name] = {"ms_per_step": ms, "value": stats.ray_surfaces * world / (ms * 1e-3),
+        engines[name] = {"ms_per_step": ms, "value": stats.rs / (ms * 1e-3),
                          "ray_surfaces_per_step": stats.ray_surfaces, "n_good": stats.n_good,
                          "launch": f"rtb_plan_run (CUDA graph), block {block} x {rpt} rays/thread"
                                    + ("" if args.no_autotune else " (autotuned)"),
@@ -326,7 +315,7 @@ def main():
                                       "sorted once when the plan is made",
                          "plan_create_s": t_create,
                          "index_order": {"ms_per_step": ms_idx,
-                                         "value": stats.ray_surfaces * world / (ms_idx * 1e-3)},
+                                         "value": stats.rs / (ms_idx * 1e-3)},
                          "autotune_ms": {f"{b}x{r}": round(t, 4) for b, r, t in table}}
         head = name if (head is None or name == "fused_mixed") else head
     if head is None and "value" in engines.get("per_surface", {}):
@@ -359,7 +348,7 @@ def main():
         ms3, st3 = timed_plan(plan, args.steps, args.warmup)
         cnt = plan.counts()
         c3 = {"beams": len(b3), "n_rays": n3, "beams_with_good_rays": int((cnt[:, -1] > 0).sum()), "ray_surfaces_per_run": st3.ray_surfaces, "n_good": st3.n_good,
-              "ms_per_run": ms3, "value": st3.ray_surfaces * world / (ms3 * 1e-3), "unit": UNIT,
+              "ms_per_run": ms3, "value": st3.rs / (ms3 * 1e-3), "unit": UNIT,
               "config": {"block_size": block, "rays_per_thread": rpt},
               "autotune_ms": {f"{b}x{r}": round(t, 4) for b, r, t in table},
               "how": "rtb_plan_run: one CUDA graph (counter clear, fused mixed kernel, counter copy) per run"}
@@ -389,8 +378,10 @@ def main():
                         "slots 65% busy, FP64 pipe 35% active, 29.6/32 threads active per instruction, "
                         "DRAM 10% of peak"}
 
+    # end to end through the C ABI on host arrays: every rank its own rays,
+    # each step started together, the slowest rank's wall time
     e2e = None
-    if not args.no_e2e and rank == 0:
+    if not args.no_e2e:
         h = E.PinnedRays(n)
         src_cpu = {f: getattr(rays_in, f).cpu().numpy() for f in E.FIELDS}
         o = mk(ffi.ENGINE_FUSED, ffi.MIXED if head == "fused_mixed" else ffi.FP64)
@@ -399,14 +390,17 @@ def main():
             for f in E.FIELDS:
                 np.copyto(getattr(h, f), src_cpu[f])
             h.flag[:] = 1
+            replicas.barrier()
             t0 = time.perf_counter()
             st, stats = E.trace_host(surf, beams, h, o)
-            times.append(time.perf_counter() - t0)
+            times.append(replicas.max_over_ranks(time.perf_counter() - t0))
             ffi.check(st, "rtb_trace_host")
         t = float(np.median(times[2:]))
-        e2e = {"value": stats.ray_surfaces / t, "unit": UNIT, "h2d_bytes_per_step": n * (7 * 8 + 1 + 1),
-               "d2h_bytes_per_step": n * (2 * 8 + 1 + 1), "seconds_per_step": t,
-               "how": "rtb_trace_host on page-locked host arrays, wall clock, median of steps"}
+        rs = replicas.sum_over_ranks(stats.ray_surfaces)
+        n_all = replicas.sum_over_ranks(n)
+        e2e = {"value": rs / t, "unit": UNIT, "h2d_bytes_per_step": int(n_all) * (7 * 8 + 1 + 1),
+               "d2h_bytes_per_step": int(n_all) * (2 * 8 + 1 + 1), "seconds_per_step": t,
+               "how": "rtb_trace_host on page-locked host arrays, wall clock (slowest rank), median of steps"}
         h.free()
 
     cpu = None
@@ -428,8 +422,7 @@ def main():
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
                 "gpu_launches": args.steps * 1}
         print(json.dumps(line), flush=True)
-    if world > 1:
-        torch.distributed.destroy_process_group()
+    replicas.finish()
 
 
 if __name__ == "__main__":
