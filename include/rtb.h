@@ -464,6 +464,23 @@ RTB_API int rtb_qe_curves(const rtb_qe_surface* surfaces, size_t n_surfaces, con
  * qe[n_lambda]}.  ccd_frame reads one block per ray-tracing file. */
 RTB_API int rtb_save_qe(const char* path, size_t n_rows, size_t n_lambda, const double* lambda, const double* qe);
 
+/* ---- reductions of a trace's wavelengths (efficiency/losses_comp.cpp, tools/print_lambda.cpp) ---- */
+/* losses_comp's per-wavelength transmission of one result (losses_comp.cpp:
+ * 60-90) from the device array lambda of n rays, good rays first (the .dat
+ * order): with nl = n / n_lambda, ll[i] is the (i*nl)-th smallest of all n
+ * wavelengths and ratio[i] the number of good rays equal to ll[i] among the
+ * next nl of the sorted good wavelengths (from where the previous count
+ * ended), divided by nl.  The reference reads past the good rays when that
+ * window runs over their end; here it stops there.  ll and ratio: host arrays
+ * of n_lambda.  Synchronous. */
+RTB_API int rtb_loss_ratios(const double* lambda, uint64_t n, uint64_t n_good, uint64_t n_lambda, double* ll,
+                            double* ratio, void* stream);
+/* print_lambda's list (print_lambda.cpp:36-71): the distinct wavelengths of the
+ * good rays lambda[0, n_good) (device) in order of first occurrence, at most
+ * max_out of them, into out (host); *n_out their number.  Synchronous. */
+RTB_API int rtb_unique_lambdas(const double* lambda, uint64_t n_good, uint64_t max_out, double* out,
+                               uint64_t* n_out, void* stream);
+
 /* ---- result files ---------------------------------------------------------- */
 /* Write beam [first, first+n) of the device arrays `rays` as a .dat file
  * (Beam::Save, common-lib/beam.cpp:636-715): size_t n, n_good, n_lambda, then
@@ -476,7 +493,7 @@ RTB_API int rtb_save_dat(const char* path, const rtb_rays* rays, const uint32_t*
 /* Header of a .dat file. */
 RTB_API int rtb_read_dat_header(const char* path, uint64_t* n, uint64_t* n_good, uint64_t* n_lambda);
 /* Read a .dat file into host arrays of host_rays->n rays (flag, if given,
- * becomes 1 for the first n_good rays and 0 after). */
+ * becomes 1 for the first n_good rays and 0 after); a NULL array is skipped. */
 RTB_API int rtb_read_dat(const char* path, const rtb_rays* host_rays);
 /* Write an image (host, xdim x ydim doubles, row-major, x fastest) as a FITS
  * file with BITPIX -64, as ccd_frame writes its image (ccd/ccd_frame.cpp:

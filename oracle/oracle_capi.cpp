@@ -411,6 +411,52 @@ int oracle_grating_energy_distr(size_t n, const double* lambda, long order, doub
     return OK;
 }
 
+// losses_comp's per-file computation (efficiency/losses_comp.cpp:60-90) on
+// host arrays: lambda of all n rays (good first); ll[i] = i*nl-th of the
+// sorted wavelengths, ratio[i] = count of ll[i] in the next nl sorted good
+// wavelengths / nl.  The window is clipped to the good rays (the reference
+// reads past their end when it runs over).
+int oracle_loss_ratios(const double* lambda, uint64_t n, uint64_t n_good, uint64_t n_lambda, double* ll,
+                       double* ratio) {
+    if (n_lambda == 0 || n_good > n) return BAD_VALUE;
+    std::vector<double> all(lambda, lambda + n), good(lambda, lambda + n_good);
+    std::sort(all.begin(), all.end());
+    std::sort(good.begin(), good.end());
+    const size_t nl = n / n_lambda;
+    for (size_t i = 0; i < n_lambda; ++i) ll[i] = all[i * nl];
+    size_t cur = 0;
+    for (size_t i = 0; i < n_lambda; ++i) {
+        const size_t e = std::min(cur + nl, (size_t)n_good);
+        const size_t cnt = (size_t)std::count(good.begin() + cur, good.begin() + e, ll[i]);
+        ratio[i] = 1.0 * cnt / nl;
+        cur += cnt;
+        if (cur > n_good) break;
+    }
+    return OK;
+}
+
+// print_lambda's scan (tools/print_lambda.cpp:52-71): the distinct values of
+// lambda[0, n_good) in order of first occurrence, the first one always, then
+// stopping when their count equals n_lambda at the end of a step; at most
+// cap values are written, *n_out is the count.
+int oracle_unique_lambdas(const double* lambda, uint64_t n_good, uint64_t n_lambda, double* out, uint64_t cap,
+                          uint64_t* n_out) {
+    *n_out = 0;
+    if (n_good == 0) return OK;
+    std::vector<double> uniq{lambda[0]};
+    for (size_t i = 1; i < n_good; ++i) {
+        size_t j = 0;
+        for (; j < uniq.size(); ++j)
+            if (lambda[i] == uniq[j]) break;
+        if (j == uniq.size()) uniq.push_back(lambda[i]);
+        if (uniq.size() == n_lambda) break;
+    }
+    const size_t m = std::min((size_t)cap, uniq.size());
+    std::copy(uniq.begin(), uniq.begin() + m, out);
+    *n_out = m;
+    return OK;
+}
+
 // Scheme::ComputeQE's curves (scheme.cpp:1249-1316) for explicit QE
 // surfaces: per range, lambda_i = w1 + (w2-w1)/(N-1)*i and QE = 1, then per
 // surface Surface::ApplyQE (surface.cpp:331-340: QE *= qe_curve(lambda)) and

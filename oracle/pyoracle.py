@@ -159,3 +159,27 @@ def grating_energy_distr(lam, order, blaze, alpha, gamma, gr_const, rule_start=0
     ffi.check(L.oracle_grating_energy_distr(len(lam), ffi.vptr(lam), order, blaze, alpha, gamma, gr_const,
                                             rule_start, rule_stop, ffi.vptr(e)), "oracle_grating_energy_distr")
     return e
+
+
+def loss_ratios(lam, n_good: int, n_lambda: int):
+    """losses_comp's (ll, ratio) for one result's wavelengths (good first)."""
+    lam = np.ascontiguousarray(lam, dtype=np.float64)
+    ll, ratio = np.zeros(n_lambda), np.zeros(n_lambda)
+    L = load()
+    L.oracle_loss_ratios.argtypes = [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint64, C.c_void_p, C.c_void_p]
+    ffi.check(L.oracle_loss_ratios(ffi.vptr(lam), len(lam), n_good, n_lambda, ffi.vptr(ll), ffi.vptr(ratio)),
+              "oracle_loss_ratios")
+    return ll, ratio
+
+
+def unique_lambdas(lam, n_good: int, n_lambda: int):
+    """print_lambda's list of distinct good wavelengths."""
+    lam = np.ascontiguousarray(lam, dtype=np.float64)
+    out = np.zeros(max(1, n_good))
+    n = C.c_uint64(0)
+    L = load()
+    L.oracle_unique_lambdas.argtypes = [C.c_void_p, C.c_uint64, C.c_uint64, C.c_void_p, C.c_uint64,
+                                        C.POINTER(C.c_uint64)]
+    ffi.check(L.oracle_unique_lambdas(ffi.vptr(lam), n_good, n_lambda, ffi.vptr(out), len(out), C.byref(n)),
+              "oracle_unique_lambdas")
+    return out[:n.value].copy()

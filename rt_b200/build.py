@@ -28,6 +28,7 @@ SOURCES = {
     "plan.cu": ["--fmad=false"],
     "adjoint.cu": ["--fmad=false"],
     "scheme_xml.cpp": [],
+    "reduce.cu": [],
     "io.cu": [],
 }
 
@@ -71,7 +72,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
 
 # Host programs over the C ABI (rt_b200/host/*.cpp -> rt_b200/bin/), linked
 # against librtb200.so with a run path relative to the program.
-PROGRAMS = ["rt_trace", "rt_ccd_frame", "rt_qe_comp"]
+PROGRAMS = ["rt_trace", "rt_ccd_frame", "rt_qe_comp", "rt_loss_comp", "rt_print_lambda"]
 BIN = os.path.join(HERE, "bin")
 
 

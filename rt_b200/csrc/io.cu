@@ -125,7 +125,11 @@ int rtb_read_dat(const char* path, const rtb_rays* host_rays) {
                       host_rays->lambda};
     for (int part = 0; part < 2 && ok; ++part) {
         const size_t k0 = part ? hdr[1] : 0, cnt = part ? hdr[0] - hdr[1] : hdr[1];
-        for (int c = 0; c < 7 && ok; ++c) ok = !cnt || (dst[c] && std::fread(dst[c] + k0, sizeof(double), cnt, f) == cnt);
+        for (int c = 0; c < 7 && ok; ++c) {
+            if (!cnt) continue;
+            ok = dst[c] ? std::fread(dst[c] + k0, sizeof(double), cnt, f) == cnt
+                        : std::fseek(f, (long)(cnt * sizeof(double)), SEEK_CUR) == 0;
+        }
     }
     std::fclose(f);
     if (!ok) return RTB_BAD_VALUE;

@@ -55,6 +55,8 @@ def lib() -> C.CDLL:
         L.rtb_qe_curves.argtypes = [P(ffi.QeSurface), C.c_size_t, vp, C.c_size_t, C.c_size_t, C.c_size_t, vp, vp]
         L.rtb_grating_energy_distr.argtypes = [C.c_size_t, vp, C.c_long] + [C.c_double] * 6 + [vp]
         L.rtb_surface_QE.argtypes = [C.c_size_t, vp, vp, P(ffi.Table)]
+        L.rtb_loss_ratios.argtypes = [vp, C.c_uint64, C.c_uint64, C.c_uint64, vp, vp, vp]
+        L.rtb_unique_lambdas.argtypes = [vp, C.c_uint64, C.c_uint64, vp, P(C.c_uint64), vp]
         _bound = True
     return L
 
@@ -78,6 +80,25 @@ def qe_curves(cqe, rows, n_lambda: int) -> tuple[np.ndarray, np.ndarray]:
     ffi.check(lib().rtb_qe_curves(cqe.array, len(cqe), ffi.vptr(rows), rows.shape[0], rows.shape[1], n_lambda,
                                   ffi.vptr(lam), ffi.vptr(qe)), "rtb_qe_curves")
     return lam, qe
+
+
+def loss_ratios(lam, n_good: int, n_lambda: int):
+    """losses_comp's (ll, ratio) from a device tensor of wavelengths (good
+    rays first), on the GPU (rtb_loss_ratios)."""
+    ll, ratio = np.zeros(n_lambda), np.zeros(n_lambda)
+    ffi.check(lib().rtb_loss_ratios(ffi.vptr(lam), lam.numel(), n_good, n_lambda, ffi.vptr(ll), ffi.vptr(ratio),
+                                    None), "rtb_loss_ratios")
+    return ll, ratio
+
+
+def unique_lambdas(lam, n_good: int, max_out: int):
+    """print_lambda's distinct wavelengths of lam[:n_good] (device tensor) in
+    order of first occurrence, at most max_out (rtb_unique_lambdas)."""
+    out = np.zeros(max(1, max_out))
+    n = C.c_uint64(0)
+    ffi.check(lib().rtb_unique_lambdas(ffi.vptr(lam), n_good, max_out, ffi.vptr(out), C.byref(n), None),
+              "rtb_unique_lambdas")
+    return out[:n.value].copy()
 
 
 def info() -> str:
