@@ -43,6 +43,14 @@ WORKLOAD = ("C1 cross-dispersed echelle: 1.0e8 rays (31 echelle orders 30..60 x 
             "surfaces + CCD 4096^2, frame counts accumulated")
 FIXES = 3  # RTB_FIX_TORIC_SIGN | RTB_FIX_TORIC_STEP: the toric fold's Steffensen step divides 0/0 otherwise
 TRAFFIC_PER_RAY_MIXED = (143.314176e6 + 25.566464e6) / 1_984_000  # ncu dram__bytes_read+write per ray
+# FP64 / FP32 floating-point operations k_fused_mixed executes per ray on C1
+# (ncu sm__sass_thread_inst_executed_op_{dfma x2, dadd, dmul} and the f32
+# ones, same capture workload): the compute side of its roofline
+F64_FLOPS_PER_RAY_MIXED = 1.621e9 / 1_984_000
+F32_FLOPS_PER_RAY_MIXED = 0.167e9 / 1_984_000
+# bytes per ray-surface of a minimal per-surface FP64 pass: read X..cZ, lambda,
+# flag (57 B), write X..cZ, flag (49 B)
+ALG_BYTES_PER_RAY_SURFACE = 106
 
 
 def parse():
@@ -154,6 +162,28 @@ def cpu_baseline(specs_fn, beams_all, budget_s=6.0):
     return {"value": rs / dt, "unit": UNIT, "cores": threads, "kind": "port",
             "sample": f"first {m} rays of each of the {len(beams_all)} order beams ({n} rays, {rs} ray-surfaces), "
                       f"CPU oracle (C++, OpenMP, FP64), {dt:.2f} s"}
+
+
+def dgemm_tflops(n=4096, reps=5):
+    """cuBLAS FP64 GEMM throughput on this GPU (TFLOP/s, best of reps)."""
+    import torch
+    try:
+        a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+        b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+        torch.matmul(a, b)
+        torch.cuda.synchronize()
+        best = 1e30
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch.matmul(a, b)
+            e1.record()
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        del a, b
+        return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+    except RuntimeError:
+        return None
 
 
 def reference_arm(args):
@@ -380,6 +410,22 @@ def main():
 
     # end to end through the C ABI on host arrays: every rank its own rays,
     # each step started together, the slowest rank's wall time
+    # compute roofline of the headline kernel: executed FP64 flops per second
+    # against cuBLAS DGEMM measured here
+    fp64_peak = dgemm_tflops()
+    f64_achieved = F64_FLOPS_PER_RAY_MIXED * n / (hv["ms_per_step"] * 1e-3) / 1e12 if head == "fused_mixed" else None
+    roofline_fp64 = {"bound": "fp64", "achieved": f64_achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                     "frac": (f64_achieved / fp64_peak) if (f64_achieved and fp64_peak) else None,
+                     "flops_per_ray": F64_FLOPS_PER_RAY_MIXED, "f32_flops_per_ray": F32_FLOPS_PER_RAY_MIXED,
+                     "peak_source": "cuBLAS DGEMM 4096^3 measured in this run (best of 5)",
+                     "note": "executed FP64 operations (FMA = 2) from ncu op counters, Newton refinements of "
+                             "reciprocals and square roots included"}
+    if "per_surface" in engines and "value" in engines["per_surface"]:
+        ps = engines["per_surface"]
+        gbs = ALG_BYTES_PER_RAY_SURFACE * ps["value"] / 1e9
+        ps["hbm_roofline"] = {"achieved_gbs": gbs, "peak_gbs": peak, "frac": gbs / peak,
+                              "bytes_per_ray_surface": ALG_BYTES_PER_RAY_SURFACE}
+
     e2e = None
     if not args.no_e2e:
         h = E.PinnedRays(n)
@@ -419,7 +465,8 @@ def main():
                 if "per_surface" in engines and "value" in engines["per_surface"] else None,
                 "accuracy_vs_fp64": accuracy,
                 "c3_batched": c3,
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+                "roofline": roofline, "roofline_fp64": roofline_fp64, "cpu_baseline": cpu, "e2e": e2e,
+                "clocks": clocks,
                 "gpu_launches": args.steps * 1}
         print(json.dumps(line), flush=True)
     replicas.finish()
