@@ -350,7 +350,13 @@ typedef struct {
  * that frame (the plan never clears it).  block_size / rays_per_thread 0
  * take the configuration an earlier rtb_plan_autotune chose for the same
  * scheme, precision, frame use and ray count in this process, else the
- * defaults (256 x 2). */
+ * defaults (256 x 2).  An RTB_MIXED plan launches a copy of the fused mixed
+ * kernel compiled for its scheme's structure with NVRTC when the plan is
+ * made (the same arithmetic, without the per-surface branching on surface
+ * kind, type and shape; cached per structure for the process), unless
+ * RTB_SPECIALIZE=0 is set in the environment or NVRTC is unavailable; see
+ * rtb_plan_specialized.  No counterpart in the reference, which has no
+ * fused kernel. */
 RTB_API int rtb_plan_create(const rtb_surface* surfaces, size_t n_surfaces, const rtb_beam* beams, size_t n_beams,
                             const rtb_trace_opts* opts, rtb_plan** plan);
 /* One trace of the plan's rays as a CUDA graph launched on `stream` (NULL:
@@ -384,6 +390,16 @@ RTB_API int rtb_plan_autotune(rtb_plan* plan, int reps, rtb_tune_entry* table, s
 RTB_API int rtb_plan_set_config(rtb_plan* plan, int32_t block_size, int32_t rays_per_thread);
 /* The plan's launch configuration and ray count. */
 RTB_API int rtb_plan_config(const rtb_plan* plan, int32_t* block_size, int32_t* rays_per_thread, uint64_t* n_rays);
+/* *specialized = 1 when the plan launches a kernel compiled for its scheme,
+ * else 0; note (may be NULL, note_len bytes) receives why not ("" when
+ * specialised). */
+RTB_API int rtb_plan_specialized(const rtb_plan* plan, int32_t* specialized, char* note, size_t note_len);
+/* Compile the fused mixed kernel specialised to this scheme's structure
+ * ahead of rtb_plan_create (which compiles it otherwise, once per structure
+ * and process); needs no device.  RTB_OK when compiled; RTB_FAILED with the
+ * reason in note (may be NULL) when NVRTC is unavailable or fails. */
+RTB_API int rtb_specialize(const rtb_surface* surfaces, size_t n_surfaces, uint32_t fixes, char* note,
+                           size_t note_len);
 /* Release everything the plan holds, after its work has finished. */
 RTB_API int rtb_plan_destroy(rtb_plan* plan);
 

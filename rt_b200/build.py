@@ -30,7 +30,35 @@ SOURCES = {
     "scheme_xml.cpp": [],
     "reduce.cu": [],
     "io.cu": [],
+    "jit.cpp": ["-I" + BUILD],
 }
+
+# Device sources compiled again at run time for scheme-specialised kernels
+# (jit.cpp), by the names they are included under.
+JIT_HEADERS = {
+    "common.cuh": os.path.join(CSRC, "common.cuh"),
+    "kernels.cuh": os.path.join(CSRC, "kernels.cuh"),
+    "trace_common.cuh": os.path.join(CSRC, "trace_common.cuh"),
+    "ray_fp64.cuh": os.path.join(CSRC, "ray_fp64.cuh"),
+    "mixed.cuh": os.path.join(CSRC, "mixed.cuh"),
+    "../../include/rtb.h": os.path.join(HERE, "..", "include", "rtb.h"),
+}
+
+
+def write_jit_headers() -> None:
+    """_build/jit_headers.inc: the JIT_HEADERS as C++ raw string literals
+    (rewritten only when they change)."""
+    out = ["// generated by rt_b200/build.py from the device sources\n", "const JitHeader kJitHeaders[] = {\n"]
+    for name, path in JIT_HEADERS.items():
+        text = open(path).read()
+        assert ')rtbjit"' not in text
+        out.append(f'    {{"{name}", R"rtbjit({text})rtbjit"}},\n')
+    out.append("};\n")
+    body = "".join(out)
+    path = os.path.join(BUILD, "jit_headers.inc")
+    if not os.path.exists(path) or open(path).read() != body:
+        with open(path, "w") as f:
+            f.write(body)
 
 
 def nvcc() -> str:
@@ -51,6 +79,7 @@ def _stale(obj: str, src: str) -> bool:
 
 def build(verbose: bool = False, force: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
+    write_jit_headers()
     objs = []
     for src, flags in SOURCES.items():
         s = os.path.join(CSRC, src)
@@ -62,7 +91,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
                 print(" ".join(cmd), flush=True)
             subprocess.run(cmd, check=True)
     if force or not os.path.exists(LIB) or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
-        cmd = [nvcc()] + ARCH + ["-shared", "-Xcompiler", "-fPIC", "-o", LIB] + objs + ["-lcudart"]
+        cmd = [nvcc()] + ARCH + ["-shared", "-Xcompiler", "-fPIC", "-o", LIB] + objs + ["-lcudart", "-ldl"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

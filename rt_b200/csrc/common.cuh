@@ -84,6 +84,7 @@ struct DevRays {
 
 }  // namespace rtb
 
+#ifndef __CUDACC_RTC__  // host code (not in run-time compiled kernels)
 #define RTB_CUDA_TRY(expr)                              \
     do {                                                \
         cudaError_t _e = (expr);                        \
@@ -95,3 +96,4 @@ inline int cuda_status(cudaError_t e) {
     return (e == cudaErrorMemoryAllocation) ? RTB_BAD_ALLOC : RTB_FAILED;
 }
 }  // namespace rtb
+#endif

@@ -25,6 +25,9 @@ int ensure_init();
 struct PreparedScheme {
     DevScheme sch;
     std::vector<double> knots;
+    // fused mixed traces launch this kernel (a copy of k_fused_mixed
+    // specialised to the scheme, jit.cpp) instead of k_fused_mixed when set
+    const void* mixed_kernel = nullptr;
 };
 
 int prepare_surface(const rtb_surface& in, DevSurface& out, std::vector<double>& knots);

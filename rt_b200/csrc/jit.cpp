@@ -1,0 +1,232 @@
+// jit.cpp -- scheme-specialised copies of the fused mixed-precision kernel,
+// compiled at run time with NVRTC for plans.
+//
+// The generic kernel (k_fused_mixed) reads each surface's structure -- its
+// intersection algorithm, type, class, aperture shape, which rotations apply,
+// the number of polynomial terms -- from the scheme in shared memory and
+// branches on it, surface by surface, in a loop.  A plan traces one scheme
+// many times, so when it is made the same device code (mixed.cuh) is
+// compiled once more with the scheme's structure fixed: one mx_surface call
+// per surface with that surface's FixedShape, the untaken branches and
+// polynomial loop bounds folded away.  The surfaces' numbers (curvatures,
+// distances, angles, tables) are still read from the scheme at run time, so
+// one compiled kernel serves every scheme of the same structure; kernels are
+// cached by their source for the life of the process.
+//
+// The device sources are built into the library (jit_headers.inc, generated
+// from rt_b200/csrc and include/ at build time).  libnvrtc is opened at run
+// time; without it, or with RTB_SPECIALIZE=0 in the environment, plans launch
+// the generic kernel.  The arithmetic is the same code in both kernels.
+#include <dlfcn.h>
+#include <nvrtc.h>
+
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "engine.cuh"
+#include "jit.h"
+
+namespace rtb {
+namespace {
+
+struct JitHeader {
+    const char* name;
+    const char* text;
+};
+
+#include "jit_headers.inc"  // kJitHeaders[]: the device sources, by the names they are included as
+
+// <cstdint>, <stdint.h>, <stddef.h> and <cuda_runtime.h> as the device code
+// needs them (NVRTC has no system headers): the LP64 types of the host.
+const char* const kTypes =
+    "#pragma once\n"
+    "typedef signed char int8_t; typedef short int16_t; typedef int int32_t; typedef long int64_t;\n"
+    "typedef unsigned char uint8_t; typedef unsigned short uint16_t; typedef unsigned int uint32_t;\n"
+    "typedef unsigned long uint64_t; typedef unsigned long size_t; typedef long ptrdiff_t;\n";
+
+const char* const kKernelName = "rtb_fused_mixed_scheme";
+
+struct Nvrtc {
+    bool ok = false;
+    std::string why;
+    decltype(&nvrtcCreateProgram) create = nullptr;
+    decltype(&nvrtcCompileProgram) compile = nullptr;
+    decltype(&nvrtcGetProgramLogSize) log_size = nullptr;
+    decltype(&nvrtcGetProgramLog) log = nullptr;
+    decltype(&nvrtcGetCUBINSize) cubin_size = nullptr;
+    decltype(&nvrtcGetCUBIN) cubin = nullptr;
+    decltype(&nvrtcDestroyProgram) destroy = nullptr;
+};
+
+Nvrtc load_nvrtc() {
+    Nvrtc n;
+    void* h = nullptr;
+    for (const char* name : {"libnvrtc.so.12", "libnvrtc.so", "/usr/local/cuda/lib64/libnvrtc.so.12"}) {
+        h = dlopen(name, RTLD_NOW | RTLD_LOCAL);
+        if (h) break;
+    }
+    if (!h) {
+        n.why = "libnvrtc not found";
+        return n;
+    }
+    n.create = reinterpret_cast<decltype(n.create)>(dlsym(h, "nvrtcCreateProgram"));
+    n.compile = reinterpret_cast<decltype(n.compile)>(dlsym(h, "nvrtcCompileProgram"));
+    n.log_size = reinterpret_cast<decltype(n.log_size)>(dlsym(h, "nvrtcGetProgramLogSize"));
+    n.log = reinterpret_cast<decltype(n.log)>(dlsym(h, "nvrtcGetProgramLog"));
+    n.cubin_size = reinterpret_cast<decltype(n.cubin_size)>(dlsym(h, "nvrtcGetCUBINSize"));
+    n.cubin = reinterpret_cast<decltype(n.cubin)>(dlsym(h, "nvrtcGetCUBIN"));
+    n.destroy = reinterpret_cast<decltype(n.destroy)>(dlsym(h, "nvrtcDestroyProgram"));
+    n.ok = n.create && n.compile && n.log_size && n.log && n.cubin_size && n.cubin && n.destroy;
+    if (!n.ok) n.why = "libnvrtc lacks a function";
+    return n;
+}
+
+const Nvrtc& nvrtc() {
+    static const Nvrtc n = load_nvrtc();
+    return n;
+}
+
+std::mutex g_mu;
+std::map<std::string, std::vector<char>> g_cubins;  // compiled kernels, by source
+std::map<std::string, cudaKernel_t> g_kernels;      // loaded kernels, by source
+
+int compile_to_cubin(const std::string& src, std::vector<char>& cubin, std::string& log) {
+    const Nvrtc& n = nvrtc();
+    std::vector<const char*> names, texts;
+    for (const char* t : {"cstdint", "stdint.h", "stddef.h"}) {
+        names.push_back(t);
+        texts.push_back(kTypes);
+    }
+    names.push_back("cuda_runtime.h");
+    texts.push_back("#pragma once\n");
+    for (const JitHeader& h : kJitHeaders) {
+        names.push_back(h.name);
+        texts.push_back(h.text);
+    }
+    nvrtcProgram prog = nullptr;
+    if (n.create(&prog, src.c_str(), "rtb_fused_mixed_scheme.cu", (int)names.size(), texts.data(), names.data()) !=
+        NVRTC_SUCCESS)
+        return RTB_FAILED;
+    // the options of kernels_mixed.cu; -default-device: the host function
+    // declarations of the headers are compiled as (unused) device functions
+    const char* opts[] = {"--gpu-architecture=sm_100a", "-std=c++17", "--fmad=true", "-lineinfo",
+                          "-default-device"};
+    nvrtcResult r = n.compile(prog, (int)(sizeof(opts) / sizeof(opts[0])), opts);
+    size_t ls = 0;
+    if (n.log_size(prog, &ls) == NVRTC_SUCCESS && ls > 1) {
+        log.resize(ls);
+        n.log(prog, &log[0]);
+    }
+    size_t cs = 0;
+    if (r == NVRTC_SUCCESS && n.cubin_size(prog, &cs) == NVRTC_SUCCESS && cs > 0) {
+        cubin.resize(cs);
+        if (n.cubin(prog, cubin.data()) != NVRTC_SUCCESS) cubin.clear();
+    }
+    n.destroy(&prog);
+    return cubin.empty() ? RTB_FAILED : RTB_OK;
+}
+
+}  // namespace
+
+std::string mixed_scheme_source(const DevScheme& sch) {
+    std::string calls;
+    char line[320];
+    for (int k = 0; k < sch.n_surfaces; ++k) {
+        const DevSurface& s = sch.s[k];
+        std::snprintf(line, sizeof(line),
+                      "        if (stage == -1) stage = mx_surface<mx::FixedShape<%d, %d, %d, %d, %d, %d, %d, %d, %d, "
+                      "%d, %d>>(sch->s[%d], %d, sch->fixes, knots, beams, b, lam, memo, r);\n",
+                      (int)s.kind, (int)s.type, (int)s.cls, (int)s.shape, (int)s.gr_type, s.translate != 0 ? 1 : 0,
+                      (int)s.rot_mask, (int)s.n_poly, s.non_aux != 0 ? 1 : 0, s.sag_cull != 0 ? 1 : 0,
+                      s.c == 0.0 ? 1 : 0, k, k);
+        calls += line;
+    }
+    return std::string("#include \"mixed.cuh\"\n"
+                       "namespace rtb {\n"
+                       "struct SchemeSurfaces {\n"
+                       "    __device__ __forceinline__ static void run(const DevScheme* sch, const double* knots,\n"
+                       "        const DevBeam* beams, int b, double lam, mx::TableMemo& memo, mx::Ray& r, int& stage) {\n") +
+           calls +
+           "    }\n"
+           "};\n"
+           "}  // namespace rtb\n"
+           "extern \"C\" __global__ void __maxnreg__(64) rtb_fused_mixed_scheme(\n"
+           "        const rtb::DevScheme* __restrict__ g_sch, const double* knots, const rtb::DevBeam* beams,\n"
+           "        int n_beams, rtb::DevRays in, rtb::DevRays out, unsigned long long* counts, unsigned* err,\n"
+           "        int state_out, rtb::FrameArgs frame, rtb::TileSched ts) {\n"
+           "    rtb::fused_mixed<rtb::SchemeSurfaces>(g_sch, knots, beams, n_beams, in, out, counts, err,\n"
+           "                                        state_out, frame, ts);\n"
+           "}\n";
+}
+
+bool specialize_enabled() {
+    const char* e = std::getenv("RTB_SPECIALIZE");
+    return !(e && std::strcmp(e, "0") == 0);
+}
+
+// The compiled kernel for `src` (g_mu held), compiled on first use.
+static const std::vector<char>* cubin_for(const std::string& src, std::string* why) {
+    auto it = g_cubins.find(src);
+    if (it != g_cubins.end()) return &it->second;
+    const Nvrtc& n = nvrtc();
+    if (!n.ok) {
+        if (why) *why = n.why;
+        return nullptr;
+    }
+    std::vector<char> cubin;
+    std::string log;
+    if (compile_to_cubin(src, cubin, log) != RTB_OK) {
+        if (why) *why = "NVRTC failed: " + log.substr(0, 2000);
+        return nullptr;
+    }
+    return &g_cubins.emplace(src, std::move(cubin)).first->second;
+}
+
+int compile_mixed_scheme(const DevScheme& sch, std::string* why) {
+    std::lock_guard<std::mutex> g(g_mu);
+    return cubin_for(mixed_scheme_source(sch), why) ? RTB_OK : RTB_FAILED;
+}
+
+int mixed_scheme_kernel(const DevScheme& sch, const void** kernel, std::string* why) {
+    *kernel = nullptr;
+    const std::string src = mixed_scheme_source(sch);
+    std::lock_guard<std::mutex> g(g_mu);
+    auto it = g_kernels.find(src);
+    if (it != g_kernels.end()) {
+        *kernel = reinterpret_cast<const void*>(it->second);
+        return RTB_OK;
+    }
+    const std::vector<char>* cubin = cubin_for(src, why);
+    if (!cubin) return RTB_OK;
+    cudaLibrary_t lib = nullptr;
+    cudaKernel_t k = nullptr;
+    cudaError_t e = cudaLibraryLoadData(&lib, cubin->data(), nullptr, nullptr, 0, nullptr, nullptr, 0);
+    if (e == cudaSuccess) e = cudaLibraryGetKernel(&k, lib, kKernelName);
+    if (e != cudaSuccess) {
+        if (lib) cudaLibraryUnload(lib);
+        return cuda_status(e);
+    }
+    g_kernels.emplace(src, k);
+    *kernel = reinterpret_cast<const void*>(k);
+    return RTB_OK;
+}
+
+}  // namespace rtb
+
+using namespace rtb;
+
+int rtb_specialize(const rtb_surface* surfaces, size_t n_surfaces, uint32_t fixes, char* note, size_t note_len) {
+    if (note && note_len > 0) note[0] = 0;
+    PreparedScheme ps;
+    int st = prepare_scheme(surfaces, n_surfaces, fixes, 0, ps);
+    if (st != RTB_OK) return st;
+    std::string why;
+    st = compile_mixed_scheme(ps.sch, &why);
+    if (note && note_len > 0) std::snprintf(note, note_len, "%s", why.c_str());
+    return st;
+}

@@ -1,0 +1,27 @@
+// jit.h -- scheme-specialised fused mixed-precision kernels (jit.cpp).
+#pragma once
+
+#include <string>
+
+#include "common.cuh"
+
+namespace rtb {
+
+// The CUDA source of the fused mixed kernel specialised to the structure of
+// `sch` (one FixedShape per surface).
+std::string mixed_scheme_source(const DevScheme& sch);
+
+// False when RTB_SPECIALIZE=0 is set in the environment.
+bool specialize_enabled();
+
+// Compile (without loading) the specialised kernel for `sch`: RTB_OK, or
+// RTB_FAILED with `why`.  Needs no device.
+int compile_mixed_scheme(const DevScheme& sch, std::string* why);
+
+// The specialised kernel for `sch` (compiled on first use, then cached), as
+// a function handle for cudaLaunchKernel; *kernel is NULL, and `why` says
+// why, when NVRTC is unavailable or fails.  Error status only for CUDA errors
+// of loading a compiled kernel.
+int mixed_scheme_kernel(const DevScheme& sch, const void** kernel, std::string* why);
+
+}  // namespace rtb

@@ -24,10 +24,12 @@ struct FrameArgs {
     unsigned long long* n_outside;  // device; may be NULL
 };
 
+#ifndef __CUDACC_RTC__
 // Size of the dynamic shared memory the fused kernels use.
 inline size_t fused_smem_bytes(int n_knots) {
     return ((sizeof(DevScheme) + 15) / 16) * 16 + sizeof(double) * (size_t)n_knots;
 }
+#endif
 
 // Scheduling of the persistent fused kernels: `next` is a counter of tiles
 // (zeroed before each launch) handed out to warps, 32*rpt rays each
@@ -105,9 +107,12 @@ __global__ void k_fused_mixed(const DevScheme* sch, const double* knots, const D
                               DevRays in, DevRays out, unsigned long long* counts, unsigned* err, int state_out,
                               FrameArgs frame, TileSched ts);
 
+#ifndef __CUDACC_RTC__
 // ---- ordering (order.cu) ----
 int reference_order(const DevBeam* h_beams, int n_beams, int n_stages, const DevRays& rays, uint32_t* order,
                     cudaStream_t stream);
 int rearrange_device(size_t n_good, double* arrays[7], char* flag, size_t* n_good_out, cudaStream_t stream);
+
+#endif
 
 }  // namespace rtb

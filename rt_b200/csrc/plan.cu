@@ -8,12 +8,15 @@
 // captured once into a CUDA graph and then replayed with one
 // cudaGraphLaunch.  Beams of any size, wavelength, field angle and grating
 // order share the launch: the kernel finds a ray's beam from the beam table.
+#include <cstdio>
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <string>
 #include <vector>
 
 #include "engine.cuh"
+#include "jit.h"
 
 using namespace rtb;
 
@@ -41,6 +44,7 @@ struct rtb_plan {
     bool ran = false;
     int32_t block = 256, rpt = kDefaultRpt;
     uint64_t key = 0;
+    std::string jit_note;            // why the generic mixed kernel is launched ("" if specialised)
 };
 
 namespace {
@@ -61,7 +65,7 @@ uint64_t plan_key(const rtb_plan& p) {
     h = fnv1a(h, &p.ps.sch, sizeof(DevScheme));
     h = fnv1a(h, p.ps.knots.data(), p.ps.knots.size() * sizeof(double));
     h = fnv1a(h, &p.n_rays, sizeof(p.n_rays));
-    int32_t tags[3] = {p.opts.precision, p.has_frame ? 1 : 0, p.opts.ray_order};
+    int32_t tags[4] = {p.opts.precision, p.has_frame ? 1 : 0, p.opts.ray_order, p.ps.mixed_kernel ? 1 : 0};
     return fnv1a(h, tags, sizeof(tags));
 }
 
@@ -214,6 +218,16 @@ int rtb_plan_create(const rtb_surface* surfaces, size_t n_surfaces, const rtb_be
         (st = gen_beams(beams, n_beams, p->n_rays, gb, &total)) != RTB_OK) {
         delete p;
         return st;
+    }
+    if (opts->precision == RTB_MIXED) {
+        if (!specialize_enabled()) {
+            p->jit_note = "RTB_SPECIALIZE=0";
+        } else if ((st = mixed_scheme_kernel(p->ps.sch, &p->ps.mixed_kernel, &p->jit_note)) != RTB_OK) {
+            delete p;
+            return st;
+        }
+    } else {
+        p->jit_note = "FP64 plan";
     }
     if (opts->block_size > 0 || opts->rays_per_thread > 0) {
         p->block = opts->block_size > 0 ? opts->block_size : 256;
@@ -418,6 +432,13 @@ int rtb_plan_autotune(rtb_plan* p, int reps, rtb_tune_entry* table, size_t capac
         g_tuned[p->key] = {best_b, best_r};
     }
     return st;
+}
+
+int rtb_plan_specialized(const rtb_plan* p, int32_t* specialized, char* note, size_t note_len) {
+    if (!p || !specialized) return RTB_BAD_VALUE;
+    *specialized = p->ps.mixed_kernel ? 1 : 0;
+    if (note && note_len > 0) std::snprintf(note, note_len, "%s", p->jit_note.c_str());
+    return RTB_OK;
 }
 
 int rtb_plan_destroy(rtb_plan* p) {

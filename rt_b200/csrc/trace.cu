@@ -114,14 +114,27 @@ int launch_trace(const PreparedScheme& ps, TraceArgs& a, int n_beams, const rtb_
         if (rpt < 1 || rpt > 64) return RTB_BAD_VALUE;
         const size_t smem = fused_smem_bytes(ps.sch.n_knots);
         if (smem > (size_t)engine().max_smem_optin) return RTB_BAD_VALUE;
-        auto kern = mixed ? k_fused_mixed : k_fused_fp64;
+        const void* kern = !mixed ? reinterpret_cast<const void*>(k_fused_fp64)
+                           : ps.mixed_kernel ? ps.mixed_kernel
+                                             : reinterpret_cast<const void*>(k_fused_mixed);
         RTB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int per_sm = 0;
         RTB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
         if (per_sm < 1) per_sm = 1;
         unsigned grid = grid_for(in.n, threads * rpt, per_sm);
-        kern<<<grid, threads, smem, st>>>(a.sch, a.knots, a.beams, n_beams, in, out, a.counts, a.err,
-                                          o.state_out ? 1 : 0, frame, TileSched{a.tiles, rpt, order, in_by_slot ? 1 : 0});
+        // the fused kernels' parameters, in order
+        const DevScheme* sch = a.sch;
+        const double* knots = a.knots;
+        const DevBeam* beams = a.beams;
+        int nb = n_beams;
+        DevRays rin = in, rout = out;
+        unsigned long long* counts = a.counts;
+        unsigned* err = a.err;
+        int state_out = o.state_out ? 1 : 0;
+        FrameArgs fr = frame;
+        TileSched ts{a.tiles, rpt, order, in_by_slot ? 1 : 0};
+        void* params[] = {&sch, &knots, &beams, &nb, &rin, &rout, &counts, &err, &state_out, &fr, &ts};
+        RTB_CUDA_TRY(cudaLaunchKernel(kern, dim3(grid), dim3(threads), params, smem, st));
     } else {
         return RTB_BAD_VALUE;
     }

@@ -44,6 +44,8 @@ def lib() -> C.CDLL:
         L.rtb_plan_set_config.argtypes = [vp, C.c_int32, C.c_int32]
         L.rtb_plan_config.argtypes = [vp, P(C.c_int32), P(C.c_int32), P(C.c_uint64)]
         L.rtb_plan_destroy.argtypes = [vp]
+        L.rtb_plan_specialized.argtypes = [vp, P(C.c_int32), C.c_char_p, C.c_size_t]
+        L.rtb_specialize.argtypes = [P(ffi.Surface), C.c_size_t, C.c_uint32, C.c_char_p, C.c_size_t]
         L.rtb_adjoint_create.argtypes = [P(ffi.Surface), C.c_size_t, P(ffi.Param), C.c_size_t, P(ffi.Beam),
                                          C.c_size_t, C.c_uint64, C.c_uint32, P(vp)]
         L.rtb_adjoint_theta.argtypes = [vp, vp]
@@ -206,6 +208,15 @@ def reference_order(beams, n_stages: int, rays: DeviceRays):
     return order
 
 
+def specialize(surfaces, fixes=0):
+    """Compile the mixed kernel specialised to this scheme's structure
+    (rtb_specialize; no device needed): (status, note)."""
+    arr = (ffi.Surface * len(surfaces))(*surfaces)
+    note = C.create_string_buffer(4096)
+    st = lib().rtb_specialize(arr, len(surfaces), fixes, note, len(note))
+    return st, note.value.decode()
+
+
 class Plan:
     """A batched trace (rtb_plan_*): rays generated once on the device, each
     run one CUDA graph launch of the fused kernel."""
@@ -253,6 +264,13 @@ class Plan:
         b, r, n = C.c_int32(), C.c_int32(), C.c_uint64()
         ffi.check(lib().rtb_plan_config(self.h, C.byref(b), C.byref(r), C.byref(n)), "rtb_plan_config")
         return b.value, r.value, n.value
+
+    def specialized(self):
+        """(True when the plan launches a kernel compiled for its scheme, why not)."""
+        on = C.c_int32()
+        note = C.create_string_buffer(2048)
+        ffi.check(lib().rtb_plan_specialized(self.h, C.byref(on), note, len(note)), "rtb_plan_specialized")
+        return bool(on.value), note.value.decode()
 
     def destroy(self):
         if self.h:

@@ -8,6 +8,8 @@ angle and order in one graph-launched trace, and the autotuner (GPU tests).
   by a later plan of the same scheme and size.
 * The coherent tracing order (the default) and index order give the same
   rays, counters and frame.
+* A mixed plan's kernel compiled for its scheme's structure gives the
+  generic kernel's result bit for bit.
 """
 import ctypes as C
 
@@ -232,3 +234,64 @@ def test_plan_rejects_unknown_ray_order():
     o.ray_order = 7
     with pytest.raises(RuntimeError, match="BAD_VALUE"):
         E.Plan(cs.surfaces, small_c3(n_beams=4), o)
+
+
+SPEC_SCHEMES = {
+    "c0": (S.littrow_free, dict(n_lambda=5, radius=10.0, lam_range=(0.4, 0.7)), ()),
+    "c0_asphere": (S.c0_asphere_camera, dict(n_lambda=5, radius=10.0, lam_range=(0.4, 0.7)), ()),
+    "c4": (S.littrow_free_asphere, dict(n_lambda=5, radius=10.0, lam_range=(0.4, 0.7)), ()),
+    "c1": (S.echelle, dict(n_lambda=64, radius=25.0, lam_range=(0.38, 0.90)), (41, 1)),
+    "mirrors": (lambda: S.coverage_schemes()["mirrors"], dict(n_lambda=5, radius=10.0, lam_range=(0.4, 0.8)), ()),
+    "lenses": (lambda: S.coverage_schemes()["lenses"], dict(n_lambda=5, radius=10.0, lam_range=(0.4, 0.8)), ()),
+    "gratings": (lambda: S.coverage_schemes()["gratings"], dict(n_lambda=5, radius=10.0, lam_range=(0.4, 0.8)), ()),
+}
+
+
+@pytest.mark.parametrize("name", sorted(SPEC_SCHEMES))
+def test_specialised_plan_equals_generic_kernel(name, monkeypatch):
+    """A mixed plan launches the kernel compiled for its scheme's structure;
+    it computes what the generic kernel (RTB_SPECIALIZE=0) computes: the same
+    lost flags, stages, counters and frame, and positions and cosines equal
+    to 1e-9 (mm, or of a unit vector) -- bit for bit on most schemes, a few
+    ulps apart where folding the scheme's branches lets the compiler
+    contract a product and a sum into an FMA that the generic kernel keeps
+    apart (the gratings scheme).  Both are far inside the mixed engine's
+    0.05 um budget against the FP64 oracle."""
+    make, kw, orders = SPEC_SCHEMES[name]
+    beams = [S.make_beam(0, 3000, kw["n_lambda"], kw["radius"], kw["lam_range"], 11, orders=orders)]
+    ccd = S.ccd(S.C1_CCD)
+    cs = S.to_c(make(), E.spline_init)
+    res = []
+    for spec in ("1", "0"):
+        monkeypatch.setenv("RTB_SPECIALIZE", spec)
+        o, counts, outside = frame_opts(ffi.MIXED, ccd, state_out=1)
+        plan = E.Plan(cs.surfaces, beams, o)
+        on, note = plan.specialized()
+        assert on == (spec == "1"), note
+        plan.run()
+        st, stats = plan.result()
+        _, out = plan_output(plan)
+        res.append((st, stats.ray_surfaces, stats.n_good, {k: v.clone() for k, v in out.items()}, counts.clone(),
+                    int(outside), plan.counts()))
+        plan.destroy()
+    a, b = res
+    assert a[:3] == b[:3] and a[0] in TRACED + (ffi.OUT_OF_RANGE,)
+    assert a[2] > 0
+    same = 0
+    for f in ("X", "Y", "Z", "cX", "cY", "cZ"):
+        x, y = a[3][f], b[3][f]
+        fin = torch.isfinite(x)
+        assert torch.equal(fin, torch.isfinite(y)), f
+        assert float((x[fin] - y[fin]).abs().max()) <= 1e-9, f
+        same += int((x.view(torch.int64) == y.view(torch.int64)).sum())
+    print(name, "bit-identical values:", same / (6 * x.numel()))
+    assert torch.equal(a[3]["flag"], b[3]["flag"]) and torch.equal(a[3]["lost_stage"], b[3]["lost_stage"])
+    assert torch.equal(a[4], b[4]) and a[5] == b[5]
+    assert np.array_equal(a[6], b[6])
+
+
+def test_fp64_plan_is_not_specialised():
+    cs = S.to_c(S.echelle(), E.spline_init)
+    plan = E.Plan(cs.surfaces, small_c3(n_beams=4), E.opts(engine=ffi.ENGINE_FUSED, precision=ffi.FP64, fixes=FIXES))
+    assert plan.specialized() == (False, "FP64 plan")
+    plan.destroy()
