@@ -56,7 +56,7 @@ ALG_BYTES_PER_RAY_SURFACE = 106
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--steps", type=int, default=100)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--rays-per-lambda", type=int, default=0, help="override (default: 1e8 rays total)")
@@ -93,6 +93,13 @@ class Clocks:
                                          stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return self
+        # nvidia-smi takes a moment to start: begin the region at its first sample
+        t0 = time.time()
+        while time.time() - t0 < 5.0 and self.proc.poll() is None:
+            if os.path.getsize(self.f.name) > 0:
+                break
+            time.sleep(0.01)
         return self
 
     def __exit__(self, *a):
@@ -194,7 +201,7 @@ def reference_arm(args):
         return
     from rt_b200 import schemes as S
     beams = S.c1_beams()
-    res = cpu_baseline(S.echelle, beams, budget_s=max(2.0, 0.5 * args.steps))
+    res = cpu_baseline(S.echelle, beams, budget_s=min(30.0, max(2.0, 0.3 * args.steps)))
     line = {"impl": "reference", "metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -337,7 +344,12 @@ def main():
             engines[name] = {"error": str(e)}
             continue
         plans[name] = plan
+        spec_on, spec_note = plan.specialized()
         engines[name] = {"ms_per_step": ms, "value": stats.rs / (ms * 1e-3),
+                         "kernel": ("rtb_fused_mixed_scheme (k_fused_mixed compiled for the scheme's structure "
+                                    "with NVRTC when the plan is made)") if spec_on else
+                                   ("k_fused_mixed" if prec == ffi.MIXED else "k_fused_fp64"),
+                         "specialised": spec_on, "specialise_note": spec_note,
                          "ray_surfaces_per_step": stats.ray_surfaces, "n_good": stats.n_good,
                          "launch": f"rtb_plan_run (CUDA graph), block {block} x {rpt} rays/thread"
                                    + ("" if args.no_autotune else " (autotuned)"),
@@ -431,6 +443,12 @@ def main():
         h = E.PinnedRays(n)
         src_cpu = {f: getattr(rays_in, f).cpu().numpy() for f in E.FIELDS}
         o = mk(ffi.ENGINE_FUSED, ffi.MIXED if head == "fused_mixed" else ffi.FP64)
+        spec = None
+        if head == "fused_mixed":
+            # the kernel compiled for the scheme (cached from the plan above;
+            # rtb_specialize is the call a user makes ahead of one-shot traces)
+            st_s, note = E.specialize(surf, FIXES)
+            spec = "rtb_fused_mixed_scheme" if st_s == ffi.OK else f"k_fused_mixed ({note})"
         times = []
         for it in range(2 + max(1, args.steps // 3)):
             for f in E.FIELDS:
@@ -446,7 +464,8 @@ def main():
         n_all = replicas.sum_over_ranks(n)
         e2e = {"value": rs / t, "unit": UNIT, "h2d_bytes_per_step": int(n_all) * (7 * 8 + 1 + 1),
                "d2h_bytes_per_step": int(n_all) * (2 * 8 + 1 + 1), "seconds_per_step": t,
-               "how": "rtb_trace_host on page-locked host arrays, wall clock (slowest rank), median of steps"}
+               "how": "rtb_trace_host on page-locked host arrays, wall clock (slowest rank), median of steps",
+               "kernel": spec}
         h.free()
 
     cpu = None

@@ -396,8 +396,11 @@ RTB_API int rtb_plan_config(const rtb_plan* plan, int32_t* block_size, int32_t* 
 RTB_API int rtb_plan_specialized(const rtb_plan* plan, int32_t* specialized, char* note, size_t note_len);
 /* Compile the fused mixed kernel specialised to this scheme's structure
  * ahead of rtb_plan_create (which compiles it otherwise, once per structure
- * and process); needs no device.  RTB_OK when compiled; RTB_FAILED with the
- * reason in note (may be NULL) when NVRTC is unavailable or fails. */
+ * and process); needs no device.  Once compiled, one-shot fused mixed traces
+ * of a scheme of that structure (rtb_trace, rtb_trace_out, rtb_trace_host)
+ * launch it too; they never compile it themselves.  RTB_OK when compiled;
+ * RTB_FAILED with the reason in note (may be NULL) when NVRTC is unavailable
+ * or fails.  No counterpart in the reference. */
 RTB_API int rtb_specialize(const rtb_surface* surfaces, size_t n_surfaces, uint32_t fixes, char* note,
                            size_t note_len);
 /* Release everything the plan holds, after its work has finished. */

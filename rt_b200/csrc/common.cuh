@@ -52,6 +52,14 @@ struct DevSurface {
     double sag_lo, sag_hi;
     int32_t sag_cull;                     // 1: sag_lo / sag_hi are set
     int32_t sag_pad;
+    // 1/c and 1/gr_const (0 where c or gr_const is 0): the mixed engine
+    // multiplies by them where the plain engine divides
+    double inv_c, inv_gr;
+    // FP32 copies for the mixed engine's normals and Newton derivatives:
+    // c, k1, cR, 1/c, the polynomial coefficients a_i and i * a_i
+    float f_c, f_k1, f_cR, f_inv_c;
+    float f_poly[RTB_MAX_POLY], f_ipoly[RTB_MAX_POLY];
+    float f_sag_lo, f_sag_hi, f_size0, f_pad;  // sag range and aperture radius
 };
 
 // A prepared scheme in device memory; the fused kernels copy it to shared

@@ -164,6 +164,24 @@ void asphere_sag_bounds(DevSurface& s) {
     s.sag_cull = 1;
 }
 
+void mixed_constants(DevSurface& s) {
+    asphere_sag_bounds(s);
+    s.inv_c = (s.c != 0.0) ? 1.0 / s.c : 0.0;
+    s.inv_gr = (s.gr_const != 0.0) ? 1.0 / s.gr_const : 0.0;
+    s.f_c = (float)s.c;
+    s.f_k1 = (float)s.k1;
+    s.f_cR = (float)s.cR;
+    s.f_inv_c = (float)s.inv_c;
+    s.f_sag_lo = (float)s.sag_lo;
+    s.f_sag_hi = (float)s.sag_hi;
+    s.f_size0 = (float)s.size[0];
+    s.f_pad = 0.0f;
+    for (int i = 0; i < RTB_MAX_POLY; ++i) {
+        s.f_poly[i] = (float)s.poly[i];
+        s.f_ipoly[i] = (float)(i + 1) * (float)s.poly[i];
+    }
+}
+
 int prepare_surface(const rtb_surface& in, DevSurface& s, std::vector<double>& knots) {
     bool non_aux = in.type != RTB_AUX_TYPE;
     int st = surface_from_params(non_aux ? in.cls : RTB_AUX_CLASS, in.params, s);
@@ -187,7 +205,7 @@ int prepare_surface(const rtb_surface& in, DevSurface& s, std::vector<double>& k
         s.size[i] = in.size[i];
         s.center[i] = in.center[i];
     }
-    asphere_sag_bounds(s);
+    mixed_constants(s);
     s.n1_off = s.n2_off = 0;
     s.n1_n = s.n2_n = 1;
     if (in.type == RTB_LENS || in.type == RTB_GRATING) {

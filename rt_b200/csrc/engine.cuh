@@ -36,6 +36,8 @@ int surface_from_params(int cls, const double* params, DevSurface& s);
 int add_table(const rtb_table* t, std::vector<double>& knots, int32_t& off, int32_t& cnt);
 // Sag range of an even asphere over its circular aperture (DevSurface::sag_*).
 void asphere_sag_bounds(DevSurface& s);
+// The mixed engine's per-surface constants: the sag range and inv_c, inv_gr.
+void mixed_constants(DevSurface& s);
 void transform_constants(const double angles_rad[3], const double dist[3], DevSurface& s);
 double scheme_angle_rad(double deg);
 

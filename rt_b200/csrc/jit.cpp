@@ -169,10 +169,15 @@ bool specialize_enabled() {
     return !(e && std::strcmp(e, "0") == 0);
 }
 
-// The compiled kernel for `src` (g_mu held), compiled on first use.
-static const std::vector<char>* cubin_for(const std::string& src, std::string* why) {
+// The compiled kernel for `src` (g_mu held), compiled on first use when
+// `compile`, else only when compiled before.
+static const std::vector<char>* cubin_for(const std::string& src, std::string* why, bool compile = true) {
     auto it = g_cubins.find(src);
     if (it != g_cubins.end()) return &it->second;
+    if (!compile) {
+        if (why) *why = "not compiled yet";
+        return nullptr;
+    }
     const Nvrtc& n = nvrtc();
     if (!n.ok) {
         if (why) *why = n.why;
@@ -192,7 +197,7 @@ int compile_mixed_scheme(const DevScheme& sch, std::string* why) {
     return cubin_for(mixed_scheme_source(sch), why) ? RTB_OK : RTB_FAILED;
 }
 
-int mixed_scheme_kernel(const DevScheme& sch, const void** kernel, std::string* why) {
+int mixed_scheme_kernel(const DevScheme& sch, const void** kernel, std::string* why, bool compile) {
     *kernel = nullptr;
     const std::string src = mixed_scheme_source(sch);
     std::lock_guard<std::mutex> g(g_mu);
@@ -201,7 +206,7 @@ int mixed_scheme_kernel(const DevScheme& sch, const void** kernel, std::string* 
         *kernel = reinterpret_cast<const void*>(it->second);
         return RTB_OK;
     }
-    const std::vector<char>* cubin = cubin_for(src, why);
+    const std::vector<char>* cubin = cubin_for(src, why, compile);
     if (!cubin) return RTB_OK;
     cudaLibrary_t lib = nullptr;
     cudaKernel_t k = nullptr;

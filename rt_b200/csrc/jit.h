@@ -18,10 +18,11 @@ bool specialize_enabled();
 // RTB_FAILED with `why`.  Needs no device.
 int compile_mixed_scheme(const DevScheme& sch, std::string* why);
 
-// The specialised kernel for `sch` (compiled on first use, then cached), as
-// a function handle for cudaLaunchKernel; *kernel is NULL, and `why` says
-// why, when NVRTC is unavailable or fails.  Error status only for CUDA errors
-// of loading a compiled kernel.
-int mixed_scheme_kernel(const DevScheme& sch, const void** kernel, std::string* why);
+// The specialised kernel for `sch` (compiled on first use when `compile`,
+// then cached), as a function handle for cudaLaunchKernel; *kernel is NULL,
+// and `why` says why, when NVRTC is unavailable or fails, or when the kernel
+// was not compiled before and `compile` is false.  Error status only for CUDA
+// errors of loading a compiled kernel.
+int mixed_scheme_kernel(const DevScheme& sch, const void** kernel, std::string* why, bool compile = true);
 
 }  // namespace rtb

@@ -74,6 +74,14 @@ __device__ __forceinline__ double rcp(double x) {
     return fma(r, e, r);
 }
 
+// 1/x to about 2^-22 (the seed alone): the inverse of a Newton derivative,
+// whose error slows the convergence by that factor but does not move the root.
+__device__ __forceinline__ double rcp_seed(double x) {
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+    return r;
+}
+
 // 1/sqrt(x): rsqrt.approx.f64 seed and `steps` Newton steps.
 __device__ __forceinline__ double rsqrt_n(double x, int steps) {
     double y;
@@ -124,11 +132,11 @@ template <class Sh>
 __device__ __forceinline__ void conic_normal(const DevSurface& s, double X, double Y, double& nx, double& ny) {
     float x = (float)X, y = (float)Y;
     float r2 = fmaf(x, x, y * y);
-    float c = (float)s.c, k1 = (float)s.k1;
+    float c = s.f_c, k1 = s.f_k1;
     float E = c * rsqrtf(fmaf(-k1 * c * c, r2, 1.0f));
     float sum = 0.0f, rr = 1.0f;
     const int N = Sh::n_poly(s);
-    for (int i = 1; i <= N; ++i, rr *= r2) sum = fmaf((float)i * (float)s.poly[i - 1], rr, sum);
+    for (int i = 1; i <= N; ++i, rr *= r2) sum = fmaf(s.f_ipoly[i - 1], rr, sum);
     E = fmaf(2.0f, sum, E);
     nx = (double)(-E * x);
     ny = (double)(-E * y);
@@ -140,18 +148,18 @@ __device__ __forceinline__ void toric_normal(const DevSurface& s, double X, doub
                                              double& nz) {
     float y = (float)Y;
     float Y2 = y * y;
-    float c = (float)s.c, k1 = (float)s.k1, cR = (float)s.cR;
+    float c = s.f_c, k1 = s.f_k1, cR = s.f_cR;
     float q = fmaf(-k1 * c * c, Y2, 1.0f);
     float rq = rsqrtf(q);
     float Fy = c * Y2 / (1.0f + q * rq);
     float sum = 0.0f, rr = Y2;
     const int N = Sh::n_poly(s);
-    for (int i = 0; i < N; ++i, rr *= Y2) sum = fmaf((float)s.poly[i], rr, sum);
+    for (int i = 0; i < N; ++i, rr *= Y2) sum = fmaf(s.f_poly[i], rr, sum);
     Fy += sum;
     float dFy = c * y * rq;
     sum = 0.0f;
     rr = 1.0f;
-    for (int i = 1; i <= N; ++i, rr *= Y2) sum = fmaf((float)i * (float)s.poly[i - 1], rr, sum);
+    for (int i = 1; i <= N; ++i, rr *= Y2) sum = fmaf(s.f_ipoly[i - 1], rr, sum);
     dFy = fmaf(2.0f, sum, dFy);
     nx = (double)(-cR * (float)X);
     ny = (double)((cR * Fy - 1.0f) * dFy);
@@ -181,7 +189,7 @@ __device__ __forceinline__ bool plane_isect(Ray& r) {
 
 // Paraboloid with the reference's linear root (surface.cu:183-213).
 __device__ __forceinline__ bool paraboloid_isect(const DevSurface& s, Ray& r) {
-    double ic = rcp(s.c);
+    double ic = s.inv_c;
     double B = 2.0 * (fma(s.k1 * r.Z, r.cZ, fma(r.X, r.cX, r.Y * r.cY)) - r.cZ * ic);
     double C = fma(s.k1 * r.Z, r.Z, fma(r.X, r.X, r.Y * r.Y)) - 2.0 * r.Z * ic;
     double t = -C * rcp(B);
@@ -194,8 +202,7 @@ __device__ __forceinline__ bool paraboloid_isect(const DevSurface& s, Ray& r) {
 
 // Root of the base conic (c, k1) chosen as conic_intersection chooses it
 // (surface.cu:240-244), evaluated without cancellation.  False if D < 0.
-__device__ __forceinline__ bool conic_root(double c, double k1, const Ray& r, double& t) {
-    double ic = rcp(c);
+__device__ __forceinline__ bool conic_root(double c, double k1, double ic, const Ray& r, double& t) {
     double A = fma(k1 * r.cZ, r.cZ, fma(r.cX, r.cX, r.cY * r.cY));
     double B = 2.0 * (fma(k1 * r.Z, r.cZ, fma(r.X, r.cX, r.Y * r.cY)) - r.cZ * ic);
     double C = fma(k1 * r.Z, r.Z, fma(r.X, r.X, r.Y * r.Y)) - 2.0 * r.Z * ic;
@@ -213,7 +220,7 @@ __device__ __forceinline__ bool conic_root(double c, double k1, const Ray& r, do
 
 __device__ __forceinline__ bool conic_isect(const DevSurface& s, Ray& r) {
     double t;
-    if (!conic_root(s.c, s.k1, r, t)) return false;
+    if (!conic_root(s.c, s.k1, s.inv_c, r, t)) return false;
     r.X = fma(t, r.cX, r.X);
     r.Y = fma(t, r.cY, r.Y);
     r.Z = fma(t, r.cZ, r.Z);
@@ -226,7 +233,8 @@ __device__ __forceinline__ bool conic_isect(const DevSurface& s, Ray& r) {
 // w = Z - P(r^2), P the even polynomial, the asphere is the base conic's
 // quadric k1 w^2 + r^2 - 2 w / c = 0 on the branch the conic root selects, so
 // Newton on G(t) = k1 w^2 + r^2 - 2 w / c (a polynomial in the ray parameter:
-// no square root per step) from the base-conic root.  Newton converges
+// no square root per step) from the base-conic root, the derivative's inverse
+// taken from the reciprocal seed (rcp_seed).  Newton converges
 // quadratically, the next correction being about |G''/2G'| dt^2 (< 1e-2 dt^2
 // for these surfaces), so the loop stops after a step below 1e-6 mm: the root
 // is then good to ~1e-14 mm.  One or two steps from the conic root; at most
@@ -265,8 +273,8 @@ __device__ __forceinline__ int asphere_isect(const DevSurface& s, Ray& r) {
     double ic = 0.0;
     if (!poly_only) {
         double tc;
-        if (conic_root(s.c, s.k1, r, tc)) t = tc;
-        ic = rcp(s.c);
+        if (conic_root(s.c, s.k1, s.inv_c, r, tc)) t = tc;
+        ic = s.inv_c;
     }
     const int N = Sh::n_poly(s);
     double x = 0, y = 0;
@@ -295,7 +303,7 @@ __device__ __forceinline__ int asphere_isect(const DevSurface& s, Ray& r) {
             G = fma(s.k1 * w, w, r2) - 2.0 * w * ic;
             dG = fma(2.0 * s.k1 * w, dw, dr2) - 2.0 * dw * ic;
         }
-        const double dt = G * rcp(dG);
+        const double dt = G * rcp_seed(dG);
         t -= dt;
         if (!(fabs(dt) >= 1e-6)) break;
     }
@@ -304,15 +312,15 @@ __device__ __forceinline__ int asphere_isect(const DevSurface& s, Ray& r) {
     y = fma(t, r.cY, r.Y);
     // the reference's grazing test on dF = cZ - E (x cX + y cY) at the root
     {
-        const float xf = (float)x, yf = (float)y, c = (float)s.c;
+        const float xf = (float)x, yf = (float)y, c = s.f_c;
         const float r2 = fmaf(xf, xf, yf * yf);
         float E = 0.0f;
         if (!poly_only) {
-            const float q = fmaf(-(float)s.k1 * c * c, r2, 1.0f);
+            const float q = fmaf(-s.f_k1 * c * c, r2, 1.0f);
             E = (q > 0.0f) ? c * rsqrtf(q) : 0.0f;
         }
         float sum = 0.0f, rr = 1.0f;
-        for (int i = 1; i <= N; ++i, rr *= r2) sum = fmaf((float)i * (float)s.poly[i - 1], rr, sum);
+        for (int i = 1; i <= N; ++i, rr *= r2) sum = fmaf(s.f_ipoly[i - 1], rr, sum);
         E = fmaf(2.0f, sum, E);
         const float dF = fmaf(-E, fmaf(xf, (float)r.cX, yf * (float)r.cY), (float)r.cZ);
         if (fabsf(dF) < (float)K_ITER_EPS) return 1;
@@ -325,7 +333,8 @@ __device__ __forceinline__ int asphere_isect(const DevSurface& s, Ray& r) {
 
 // Toric surface (iter_toric, surface.cu:359-410): the same function F of the
 // reference (with its 1+k1c^2Y^2 unless RTB_FIX_TORIC_SIGN), solved by
-// Newton from the Z=0 plane point with the analytic derivative
+// Newton from the Z=0 plane point with the analytic derivative (its FY' and
+// its inverse from the reciprocal seed, rcp_seed)
 //   dF/dt = cZ - FY' cY - cR (X cX + Z cZ - FY FY' cY),  FY' = c Y / s,
 // s = sqrt(1 -+ k1 c^2 Y^2) (FY = c Y^2 / (1 + s) has this derivative for
 // either sign), until a step falls below 1e-6 mm (quadratic convergence: the
@@ -341,10 +350,10 @@ __device__ __forceinline__ bool toric_isect(const DevSurface& s, uint32_t fixes,
         double Y2 = Y * Y;
         double sq = sqrt_(fma(kc2, Y2, 1.0));
         double FY = s.c * Y2 * rcp(1.0 + sq);
-        double dFY = s.c * Y * rcp(sq);
+        double dFY = s.c * Y * rcp_seed(sq);
         double F = Z - FY - 0.5 * s.cR * (fma(X, X, Z * Z) - FY * FY);
         double dF = r.cZ - dFY * r.cY - s.cR * (fma(X, r.cX, Z * r.cZ) - FY * dFY * r.cY);
-        double dt = F * rcp(dF);
+        double dt = F * rcp_seed(dF);
         t -= dt;
         if (!(fabs(dt) >= 1e-6)) break;  // next correction ~|F''/2F'| dt^2 << 1e-12 mm
     }
@@ -540,7 +549,7 @@ __device__ __forceinline__ int action(const DevSurface& s, const double* knots, 
     if (type == RTB_LENS) return refract(n1v * in2, nx, ny, nz, r) ? 0 : 1;
     if (type == RTB_GRATING) {
         const double mu = (gr_type == RTB_TRANSPARENT) ? n1v * in2 : 0.0;
-        const double L = (double)order * lambda * in2 * rcp(s.gr_const);
+        const double L = (double)order * lambda * in2 * s.inv_gr;
         return diffract<Sh>(s, mu, L, nx, ny, nz, r) ? 0 : 1;
     }
     return 0;

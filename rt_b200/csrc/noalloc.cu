@@ -128,7 +128,7 @@ int prepare_fixed(const rtb_surface* surf, size_t n, uint32_t fixes, int renorm_
             s.size[i] = in.size[i];
             s.center[i] = in.center[i];
         }
-        asphere_sag_bounds(s);
+        mixed_constants(s);
         s.n1_off = s.n2_off = 0;
         s.n1_n = s.n2_n = 1;
         if (in.type == RTB_LENS || in.type == RTB_GRATING) {

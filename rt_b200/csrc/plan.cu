@@ -277,15 +277,23 @@ int rtb_plan_create(const rtb_surface* surfaces, size_t n_surfaces, const rtb_be
         e = cudaGetLastError();
     }
     // the coherent tracing order and a copy of the rays in that order, once
-    // (index order for plans beyond 2^32 rays).  Wavelength groups span up to
-    // 2^30 rays of a beam: on C1 both kernels were faster with whole-beam
-    // groups than with chunks of 2^18 rays (the stores scatter either way).
+    // (index order for plans beyond 2^32 rays).  The rays of a beam are
+    // grouped by wavelength within chunks of 2^20 consecutive rays for the
+    // mixed kernel and of the whole beam (up to 2^30) for the FP64 kernel:
+    // the best of 2^11..2^30 for each on C1 (mixed: 5.24 ms at 2^20, 5.36
+    // whole beams, 5.65 at 2^11; FP64: 24.7 ms whole beams, 25.1 at 2^20).
+    // Outputs are stored at the rays' indices, 8 bytes apart per lane, which
+    // costs the mixed kernel 0.8 ms of its 5.3 on C1 against coalesced stores;
+    // chunks small enough to stage a block's stores in shared memory lose
+    // more in coherence than that.
     if (e == cudaSuccess && opts->ray_order == RTB_ORDER_COHERENT && p->n_rays <= 0xffffffffull) {
         e = cudaMalloc(&p->order, p->n_rays * sizeof(uint32_t));
         if (e == cudaSuccess) e = cudaMalloc(&p->slot_mem, rays_bytes(p->n_rays, true));
         if (e == cudaSuccess) {
             p->in_slot = carve(p->slot_mem, p->n_rays, true);
-            st = coherent_order(gbuf.as<GenBeam>(), (int)n_beams, p->n_rays, p->in, p->order, 30, p->stream);
+            const int chunk_shift = opts->precision == RTB_MIXED ? 20 : 30;
+            st = coherent_order(gbuf.as<GenBeam>(), (int)n_beams, p->n_rays, p->in, p->order, chunk_shift,
+                                p->stream);
             if (st == RTB_OK) {
                 k_gather_rays<<<grid_for(p->n_rays, 256, 8), 256, 0, p->stream>>>(p->order, p->n_rays, p->in,
                                                                                   p->in_slot);

@@ -5,6 +5,7 @@
 #include <vector>
 
 #include "engine.cuh"
+#include "jit.h"
 
 namespace rtb {
 
@@ -16,6 +17,14 @@ DevRays dev_rays(const rtb_rays* r) {
     d.lost_stage = r->lost_stage;
     d.n = r->n;
     return d;
+}
+
+// One-shot fused mixed traces launch the kernel specialised to the scheme's
+// structure when one was compiled already in this process (by a plan or
+// rtb_specialize); they never compile one themselves.
+int attach_compiled(PreparedScheme& ps, const rtb_trace_opts& o) {
+    if (o.engine != RTB_ENGINE_FUSED || o.precision != RTB_MIXED || !specialize_enabled()) return RTB_OK;
+    return mixed_scheme_kernel(ps.sch, &ps.mixed_kernel, nullptr, false);
 }
 
 int check_beams(const rtb_beam* beams, size_t n_beams, size_t n_rays, std::vector<DevBeam>& out) {
@@ -207,7 +216,9 @@ int rtb_trace(const rtb_surface* surfaces, size_t n_surfaces, const rtb_beam* be
     if (st != RTB_OK) return st;
     cudaStream_t s = stream ? (cudaStream_t)stream : engine().stream;
     PreparedScheme ps;
-    if ((st = prepare_scheme(surfaces, n_surfaces, opts->fixes, opts->renormalize_lost, ps)) != RTB_OK) return st;
+    if ((st = prepare_scheme(surfaces, n_surfaces, opts->fixes, opts->renormalize_lost, ps)) != RTB_OK ||
+        (st = attach_compiled(ps, *opts)) != RTB_OK)
+        return st;
     std::vector<DevBeam> db;
     if ((st = check_beams(beams, n_beams, rays->n, db)) != RTB_OK) return st;
     TraceArgs a;
@@ -232,7 +243,9 @@ int rtb_trace_out(const rtb_surface* surfaces, size_t n_surfaces, const rtb_beam
     if (st != RTB_OK) return st;
     cudaStream_t s = stream ? (cudaStream_t)stream : engine().stream;
     PreparedScheme ps;
-    if ((st = prepare_scheme(surfaces, n_surfaces, opts->fixes, opts->renormalize_lost, ps)) != RTB_OK) return st;
+    if ((st = prepare_scheme(surfaces, n_surfaces, opts->fixes, opts->renormalize_lost, ps)) != RTB_OK ||
+        (st = attach_compiled(ps, *opts)) != RTB_OK)
+        return st;
     std::vector<DevBeam> db;
     if ((st = check_beams(beams, n_beams, in->n, db)) != RTB_OK) return st;
     TraceArgs a;
@@ -321,6 +334,7 @@ int trace_host_impl(const rtb_surface* surfaces, size_t n_surfaces, const rtb_be
                     const rtb_trace_opts* opts, const rtb_rays* h, rtb_trace_stats* stats, size_t chunk) {
     PreparedScheme ps;
     int st = prepare_scheme(surfaces, n_surfaces, opts->fixes, opts->renormalize_lost, ps);
+    if (st == RTB_OK) st = attach_compiled(ps, *opts);
     if (st != RTB_OK) return st;
     std::vector<DevBeam> db;
     if ((st = check_beams(beams, n_beams, h->n, db)) != RTB_OK) return st;

@@ -295,3 +295,42 @@ def test_fp64_plan_is_not_specialised():
     plan = E.Plan(cs.surfaces, small_c3(n_beams=4), E.opts(engine=ffi.ENGINE_FUSED, precision=ffi.FP64, fixes=FIXES))
     assert plan.specialized() == (False, "FP64 plan")
     plan.destroy()
+
+
+def test_one_shot_trace_uses_a_compiled_specialisation(monkeypatch):
+    """Once the kernel for a scheme's structure is compiled (rtb_specialize
+    or a plan), rtb_trace_out launches it: on the gratings scheme, where the
+    two kernels differ in the last bits, its output then equals the
+    specialised plan's bit for bit."""
+    monkeypatch.setenv("RTB_SPECIALIZE", "1")
+    specs = S.coverage_schemes()["gratings"]
+    beams = [S.make_beam(0, 3000, 5, 10.0, (0.4, 0.8), 11)]
+    cs = S.to_c(specs, E.spline_init)
+    st, note = E.specialize(list(cs.surfaces), FIXES)
+    assert st == ffi.OK, note
+    plan = E.Plan(cs.surfaces, beams, E.opts(engine=ffi.ENGINE_FUSED, precision=ffi.MIXED, fixes=FIXES,
+                                              state_out=1))
+    assert plan.specialized()[0]
+    plan.run()
+    st_p, stats_p = plan.result()
+    rin, rout = plan_output(plan)
+    n = S.total_rays(beams)
+    src = E.DeviceRays(n)
+    for f in E.FIELDS:
+        getattr(src, f).copy_(rin[f])
+    src.flag.copy_(rin["flag"])
+    ref = E.DeviceRays(n)
+    o2 = E.opts(engine=ffi.ENGINE_FUSED, precision=ffi.MIXED, fixes=FIXES, state_out=1)
+    stats2 = ffi.TraceStats()
+    surf = (ffi.Surface * len(cs.surfaces))(*cs.surfaces)
+    L = E.lib()
+    L.rtb_trace_out.argtypes = [C.POINTER(ffi.Surface), C.c_size_t, C.POINTER(ffi.Beam), C.c_size_t,
+                                C.POINTER(ffi.TraceOpts), C.POINTER(ffi.Rays), C.POINTER(ffi.Rays),
+                                C.POINTER(ffi.TraceStats), C.c_void_p]
+    st2 = L.rtb_trace_out(surf, len(surf), E._beams(beams), len(beams), C.byref(o2), C.byref(src.struct()),
+                          C.byref(ref.struct()), C.byref(stats2), None)
+    torch.cuda.synchronize()
+    assert st2 == st_p and stats2.n_good == stats_p.n_good > 0
+    for f in ("X", "Y", "Z", "cX", "cY", "cZ"):
+        assert torch.equal(rout[f].view(torch.int64), getattr(ref, f).view(torch.int64)), f
+    plan.destroy()
