@@ -42,12 +42,15 @@ WORKLOAD = ("C1 cross-dispersed echelle: 1.0e8 rays (31 echelle orders 30..60 x 
             "x 50404 rays, disk r=25 mm), OAP + echelle + cross-disperser + toric fold + 2 even-asphere lens "
             "surfaces + CCD 4096^2, frame counts accumulated")
 FIXES = 3  # RTB_FIX_TORIC_SIGN | RTB_FIX_TORIC_STEP: the toric fold's Steffensen step divides 0/0 otherwise
-TRAFFIC_PER_RAY_MIXED = (143.314176e6 + 25.566464e6) / 1_984_000  # ncu dram__bytes_read+write per ray
-# FP64 / FP32 floating-point operations k_fused_mixed executes per ray on C1
-# (ncu sm__sass_thread_inst_executed_op_{dfma x2, dadd, dmul} and the f32
-# ones, same capture workload): the compute side of its roofline
-F64_FLOPS_PER_RAY_MIXED = 1.621e9 / 1_984_000
-F32_FLOPS_PER_RAY_MIXED = 0.167e9 / 1_984_000
+# DRAM bytes per ray of the headline kernel (rtb_fused_mixed_scheme, the
+# mixed kernel compiled for C1's structure): ncu dram__bytes_read + write of
+# one launch on C1 at 1,984,000 rays
+TRAFFIC_PER_RAY_MIXED = (143.441920e6 + 27.038208e6) / 1_984_000
+# FP64 / FP32 floating-point operations it executes per ray on C1 (ncu
+# sm__sass_thread_inst_executed_op_{dfma x2, dadd, dmul} and the f32 ones,
+# same capture workload): the compute side of its roofline
+F64_FLOPS_PER_RAY_MIXED = 707.08
+F32_FLOPS_PER_RAY_MIXED = 56.66
 # bytes per ray-surface of a minimal per-surface FP64 pass: read X..cZ, lambda,
 # flag (57 B), write X..cZ, flag (49 B)
 ALG_BYTES_PER_RAY_SURFACE = 106
@@ -60,6 +63,8 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--rays-per-lambda", type=int, default=0, help="override (default: 1e8 rays total)")
+    p.add_argument("--surfaces", type=int, default=0,
+                   help="profiling: trace only the scheme's first K surfaces (per-surface cost by difference)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-c3", action="store_true")
@@ -226,7 +231,10 @@ def main():
     from rt_b200 import replicas
     beams = S.c1_beams(n_per_lambda=npl, seed=replicas.seed(S.SEED, rank))
     n = S.total_rays(beams)
-    cs = S.to_c(S.echelle(), E.spline_init)
+    specs = S.echelle()
+    if args.surfaces > 0:
+        specs = specs[:args.surfaces]
+    cs = S.to_c(specs, E.spline_init)
     surf = cs.surfaces
     rays_in = E.generate(beams, n)
     torch.cuda.synchronize()  # generated on the library's stream
@@ -407,18 +415,18 @@ def main():
         pass
     peak = peaks.get("hbm_gbs", 6650.0)
     achieved = alg_bytes / (hv["ms_per_step"] * 1e-3) / 1e9
-    # DRAM traffic of k_fused_mixed from an ncu capture of the same workload
-    # at 1,984,000 rays (143.3 MB read + 25.6 MB written, the tracing-order
-    # index and the plan's ordered copy of the rays included), scaled by rays
+    # DRAM traffic of the headline kernel from an ncu capture of the same
+    # workload at 1,984,000 rays (143.4 MB read + 27.0 MB written, the
+    # tracing-order index included), scaled by rays
     traffic = TRAFFIC_PER_RAY_MIXED * n if head == "fused_mixed" else None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "traffic_per_ray_bytes": TRAFFIC_PER_RAY_MIXED if traffic else None,
                 "alg_bytes": alg_bytes,
-                "kernel": "k_fused_mixed" if head == "fused_mixed" else "k_fused_fp64",
+                "kernel": (hv.get("kernel", "k_fused_mixed").split(" ")[0]) if head == "fused_mixed" else "k_fused_fp64",
                 "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "fallback",
                 "note": "HBM view of a kernel bound by instruction issue and FP64 latency: ncu shows issue "
-                        "slots 65% busy, FP64 pipe 35% active, 29.6/32 threads active per instruction, "
-                        "DRAM 10% of peak"}
+                        "slots 57% busy, FP64 pipe 45% active, 29.2/32 threads active per instruction, "
+                        "DRAM 14% of peak"}
 
     # end to end through the C ABI on host arrays: every rank its own rays,
     # each step started together, the slowest rank's wall time

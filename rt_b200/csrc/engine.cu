@@ -13,6 +13,7 @@
 #include <string>
 
 #include "engine.cuh"
+#include "jit.h"
 
 namespace rtb {
 
@@ -386,6 +387,7 @@ int rtb_info(char* buf, size_t buflen) {
     s += "Computing ability: " + std::to_string(prop.major) + "." + std::to_string(prop.minor) + "\n";
     s += "Global memory: " + std::to_string(prop.totalGlobalMem) + "\n";
     s += "Number of multiprocessors: " + std::to_string(prop.multiProcessorCount) + "\n";
+    s += "NVRTC (scheme-specialised kernels): " + nvrtc_info() + "\n";
     if (!buf || buflen == 0) return RTB_BAD_VALUE;
     std::snprintf(buf, buflen, "%s", s.c_str());
     return RTB_OK;

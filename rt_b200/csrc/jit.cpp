@@ -61,6 +61,7 @@ struct Nvrtc {
     decltype(&nvrtcGetCUBINSize) cubin_size = nullptr;
     decltype(&nvrtcGetCUBIN) cubin = nullptr;
     decltype(&nvrtcDestroyProgram) destroy = nullptr;
+    int major = 0, minor = 0;
 };
 
 Nvrtc load_nvrtc() {
@@ -81,6 +82,8 @@ Nvrtc load_nvrtc() {
     n.cubin_size = reinterpret_cast<decltype(n.cubin_size)>(dlsym(h, "nvrtcGetCUBINSize"));
     n.cubin = reinterpret_cast<decltype(n.cubin)>(dlsym(h, "nvrtcGetCUBIN"));
     n.destroy = reinterpret_cast<decltype(n.destroy)>(dlsym(h, "nvrtcDestroyProgram"));
+    auto version = reinterpret_cast<decltype(&nvrtcVersion)>(dlsym(h, "nvrtcVersion"));
+    if (version) version(&n.major, &n.minor);
     n.ok = n.create && n.compile && n.log_size && n.log && n.cubin_size && n.cubin && n.destroy;
     if (!n.ok) n.why = "libnvrtc lacks a function";
     return n;
@@ -162,6 +165,13 @@ std::string mixed_scheme_source(const DevScheme& sch) {
            "    rtb::fused_mixed<rtb::SchemeSurfaces>(g_sch, knots, beams, n_beams, in, out, counts, err,\n"
            "                                        state_out, frame, ts);\n"
            "}\n";
+}
+
+std::string nvrtc_info() {
+    const Nvrtc& n = nvrtc();
+    if (!n.ok) return "unavailable (" + n.why + ")";
+    return std::to_string(n.major) + "." + std::to_string(n.minor) +
+           (specialize_enabled() ? "" : " (RTB_SPECIALIZE=0)");
 }
 
 bool specialize_enabled() {

@@ -11,6 +11,9 @@ namespace rtb {
 // `sch` (one FixedShape per surface).
 std::string mixed_scheme_source(const DevScheme& sch);
 
+// NVRTC's version, or why it is unavailable (rtb_info).
+std::string nvrtc_info();
+
 // False when RTB_SPECIALIZE=0 is set in the environment.
 bool specialize_enabled();
 
