@@ -49,8 +49,8 @@ TRAFFIC_PER_RAY_MIXED = (143.441920e6 + 27.038208e6) / 1_984_000
 # FP64 / FP32 floating-point operations it executes per ray on C1 (ncu
 # sm__sass_thread_inst_executed_op_{dfma x2, dadd, dmul} and the f32 ones,
 # same capture workload): the compute side of its roofline
-F64_FLOPS_PER_RAY_MIXED = 707.08
-F32_FLOPS_PER_RAY_MIXED = 56.66
+F64_FLOPS_PER_RAY_MIXED = 717.75
+F32_FLOPS_PER_RAY_MIXED = 57.91
 # bytes per ray-surface of a minimal per-surface FP64 pass: read X..cZ, lambda,
 # flag (57 B), write X..cZ, flag (49 B)
 ALG_BYTES_PER_RAY_SURFACE = 106
