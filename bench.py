@@ -354,9 +354,10 @@ def main():
         plans[name] = plan
         spec_on, spec_note = plan.specialized()
         engines[name] = {"ms_per_step": ms, "value": stats.rs / (ms * 1e-3),
-                         "kernel": ("rtb_fused_mixed_scheme (k_fused_mixed compiled for the scheme's structure "
-                                    "with NVRTC when the plan is made)") if spec_on else
-                                   ("k_fused_mixed" if prec == ffi.MIXED else "k_fused_fp64"),
+                         "kernel": ((("rtb_fused_mixed_scheme (k_fused_mixed" if prec == ffi.MIXED else
+                                     "rtb_fused_fp64_scheme (k_fused_fp64") +
+                                    " compiled for the scheme's structure with NVRTC when the plan is made)")
+                                   if spec_on else ("k_fused_mixed" if prec == ffi.MIXED else "k_fused_fp64")),
                          "specialised": spec_on, "specialise_note": spec_note,
                          "ray_surfaces_per_step": stats.ray_surfaces, "n_good": stats.n_good,
                          "launch": f"rtb_plan_run (CUDA graph), block {block} x {rpt} rays/thread"
@@ -451,12 +452,12 @@ def main():
         h = E.PinnedRays(n)
         src_cpu = {f: getattr(rays_in, f).cpu().numpy() for f in E.FIELDS}
         o = mk(ffi.ENGINE_FUSED, ffi.MIXED if head == "fused_mixed" else ffi.FP64)
-        spec = None
-        if head == "fused_mixed":
-            # the kernel compiled for the scheme (cached from the plan above;
-            # rtb_specialize is the call a user makes ahead of one-shot traces)
-            st_s, note = E.specialize(surf, FIXES)
-            spec = "rtb_fused_mixed_scheme" if st_s == ffi.OK else f"k_fused_mixed ({note})"
+        # the kernel compiled for the scheme (cached from the plan above;
+        # rtb_specialize is the call a user makes ahead of one-shot traces)
+        st_s, note = E.specialize(surf, FIXES, o.precision)
+        mixed = head == "fused_mixed"
+        spec = (("rtb_fused_mixed_scheme" if mixed else "rtb_fused_fp64_scheme") if st_s == ffi.OK else
+                ("k_fused_mixed" if mixed else "k_fused_fp64") + f" ({note})")
         times = []
         for it in range(2 + max(1, args.steps // 3)):
             for f in E.FIELDS:

@@ -350,13 +350,13 @@ typedef struct {
  * that frame (the plan never clears it).  block_size / rays_per_thread 0
  * take the configuration an earlier rtb_plan_autotune chose for the same
  * scheme, precision, frame use and ray count in this process, else the
- * defaults (256 x 2).  An RTB_MIXED plan launches a copy of the fused mixed
- * kernel compiled for its scheme's structure with NVRTC when the plan is
- * made (the same arithmetic, without the per-surface branching on surface
- * kind, type and shape; cached per structure for the process), unless
- * RTB_SPECIALIZE=0 is set in the environment or NVRTC is unavailable; see
- * rtb_plan_specialized.  No counterpart in the reference, which has no
- * fused kernel. */
+ * defaults (256 x 2).  A plan launches a copy of the fused kernel of its
+ * precision compiled for its scheme's structure with NVRTC when the plan is
+ * made (the same arithmetic -- for RTB_FP64 the same IEEE operations, bit
+ * for bit -- without the per-surface branching on surface kind, type and
+ * shape; cached per structure for the process), unless RTB_SPECIALIZE=0 is
+ * set in the environment or NVRTC is unavailable; see rtb_plan_specialized.
+ * No counterpart in the reference, which has no fused kernel. */
 RTB_API int rtb_plan_create(const rtb_surface* surfaces, size_t n_surfaces, const rtb_beam* beams, size_t n_beams,
                             const rtb_trace_opts* opts, rtb_plan** plan);
 /* One trace of the plan's rays as a CUDA graph launched on `stream` (NULL:
@@ -394,15 +394,16 @@ RTB_API int rtb_plan_config(const rtb_plan* plan, int32_t* block_size, int32_t* 
  * else 0; note (may be NULL, note_len bytes) receives why not ("" when
  * specialised). */
 RTB_API int rtb_plan_specialized(const rtb_plan* plan, int32_t* specialized, char* note, size_t note_len);
-/* Compile the fused mixed kernel specialised to this scheme's structure
- * ahead of rtb_plan_create (which compiles it otherwise, once per structure
- * and process); needs no device.  Once compiled, one-shot fused mixed traces
- * of a scheme of that structure (rtb_trace, rtb_trace_out, rtb_trace_host)
- * launch it too; they never compile it themselves.  RTB_OK when compiled;
- * RTB_FAILED with the reason in note (may be NULL) when NVRTC is unavailable
- * or fails.  No counterpart in the reference. */
-RTB_API int rtb_specialize(const rtb_surface* surfaces, size_t n_surfaces, uint32_t fixes, char* note,
-                           size_t note_len);
+/* Compile the fused kernel of `precision` (RTB_FP64 / RTB_MIXED) specialised
+ * to this scheme's structure ahead of rtb_plan_create (which compiles it
+ * otherwise, once per structure and process); needs no device.  Once
+ * compiled, one-shot fused traces of that precision and a scheme of that
+ * structure (rtb_trace, rtb_trace_out, rtb_trace_host) launch it too; they
+ * never compile it themselves.  RTB_OK when compiled; RTB_FAILED with the
+ * reason in note (may be NULL) when NVRTC is unavailable or fails.  No
+ * counterpart in the reference. */
+RTB_API int rtb_specialize(const rtb_surface* surfaces, size_t n_surfaces, uint32_t fixes, int32_t precision,
+                           char* note, size_t note_len);
 /* Release everything the plan holds, after its work has finished. */
 RTB_API int rtb_plan_destroy(rtb_plan* plan);
 

@@ -25,9 +25,10 @@ int ensure_init();
 struct PreparedScheme {
     DevScheme sch;
     std::vector<double> knots;
-    // fused mixed traces launch this kernel (a copy of k_fused_mixed
-    // specialised to the scheme, jit.cpp) instead of k_fused_mixed when set
-    const void* mixed_kernel = nullptr;
+    // fused traces launch this kernel (a copy of k_fused_mixed or
+    // k_fused_fp64, of the trace's precision, specialised to the scheme;
+    // jit.cpp) instead of the generic one when set
+    const void* scheme_kernel = nullptr;
 };
 
 int prepare_surface(const rtb_surface& in, DevSurface& out, std::vector<double>& knots);

@@ -1,22 +1,24 @@
-// jit.cpp -- scheme-specialised copies of the fused mixed-precision kernel,
-// compiled at run time with NVRTC for plans.
+// jit.cpp -- copies of the fused trace kernels specialised to one scheme's
+// structure, compiled at run time with NVRTC for plans.
 //
-// The generic kernel (k_fused_mixed) reads each surface's structure -- its
-// intersection algorithm, type, class, aperture shape, which rotations apply,
-// the number of polynomial terms -- from the scheme in shared memory and
-// branches on it, surface by surface, in a loop.  A plan traces one scheme
-// many times, so when it is made the same device code (mixed.cuh) is
-// compiled once more with the scheme's structure fixed: one mx_surface call
-// per surface with that surface's FixedShape, the untaken branches and
-// polynomial loop bounds folded away.  The surfaces' numbers (curvatures,
-// distances, angles, tables) are still read from the scheme at run time, so
-// one compiled kernel serves every scheme of the same structure; kernels are
-// cached by their source for the life of the process.
+// The generic fused kernels (k_fused_mixed, k_fused_fp64) read each surface's
+// structure -- its intersection algorithm, type, class, aperture shape, which
+// rotations apply, the number of polynomial terms -- from the scheme in
+// shared memory and branch on it, surface by surface, in a loop.  A plan
+// traces one scheme many times, so when it is made the same device code
+// (mixed.cuh, fused_fp64.cuh) is compiled once more with the scheme's
+// structure fixed: one call per surface with that surface's FixedShape, the
+// untaken branches and polynomial loop bounds folded away.  The surfaces'
+// numbers (curvatures, distances, angles, tables) are still read from the
+// scheme at run time, so one compiled kernel serves every scheme of the same
+// structure; kernels are cached by their source for the life of the process.
+// The FP64 copy is compiled with --fmad=false like k_fused_fp64 and executes
+// the same IEEE operations in the same order: its results are bit-identical.
 //
 // The device sources are built into the library (jit_headers.inc, generated
 // from rt_b200/csrc and include/ at build time).  libnvrtc is opened at run
 // time; without it, or with RTB_SPECIALIZE=0 in the environment, plans launch
-// the generic kernel.  The arithmetic is the same code in both kernels.
+// the generic kernels.
 #include <dlfcn.h>
 #include <nvrtc.h>
 
@@ -49,7 +51,8 @@ const char* const kTypes =
     "typedef unsigned char uint8_t; typedef unsigned short uint16_t; typedef unsigned int uint32_t;\n"
     "typedef unsigned long uint64_t; typedef unsigned long size_t; typedef long ptrdiff_t;\n";
 
-const char* const kKernelName = "rtb_fused_mixed_scheme";
+const char* const kMixedName = "rtb_fused_mixed_scheme";
+const char* const kFp64Name = "rtb_fused_fp64_scheme";
 
 struct Nvrtc {
     bool ok = false;
@@ -98,7 +101,7 @@ std::mutex g_mu;
 std::map<std::string, std::vector<char>> g_cubins;  // compiled kernels, by source
 std::map<std::string, cudaKernel_t> g_kernels;      // loaded kernels, by source
 
-int compile_to_cubin(const std::string& src, std::vector<char>& cubin, std::string& log) {
+int compile_to_cubin(const std::string& src, bool fmad, std::vector<char>& cubin, std::string& log) {
     const Nvrtc& n = nvrtc();
     std::vector<const char*> names, texts;
     for (const char* t : {"cstdint", "stdint.h", "stddef.h"}) {
@@ -112,13 +115,14 @@ int compile_to_cubin(const std::string& src, std::vector<char>& cubin, std::stri
         texts.push_back(h.text);
     }
     nvrtcProgram prog = nullptr;
-    if (n.create(&prog, src.c_str(), "rtb_fused_mixed_scheme.cu", (int)names.size(), texts.data(), names.data()) !=
+    if (n.create(&prog, src.c_str(), "rtb_fused_scheme.cu", (int)names.size(), texts.data(), names.data()) !=
         NVRTC_SUCCESS)
         return RTB_FAILED;
-    // the options of kernels_mixed.cu; -default-device: the host function
-    // declarations of the headers are compiled as (unused) device functions
-    const char* opts[] = {"--gpu-architecture=sm_100a", "-std=c++17", "--fmad=true", "-lineinfo",
-                          "-default-device"};
+    // the options of kernels_mixed.cu (FMA contraction) or kernels_fp64.cu
+    // (none); -default-device: the host function declarations of the headers
+    // are compiled as (unused) device functions
+    const char* opts[] = {"--gpu-architecture=sm_100a", "-std=c++17", fmad ? "--fmad=true" : "--fmad=false",
+                          "-lineinfo", "-default-device"};
     nvrtcResult r = n.compile(prog, (int)(sizeof(opts) / sizeof(opts[0])), opts);
     size_t ls = 0;
     if (n.log_size(prog, &ls) == NVRTC_SUCCESS && ls > 1) {
@@ -136,35 +140,54 @@ int compile_to_cubin(const std::string& src, std::vector<char>& cubin, std::stri
 
 }  // namespace
 
-std::string mixed_scheme_source(const DevScheme& sch) {
-    std::string calls;
-    char line[320];
-    for (int k = 0; k < sch.n_surfaces; ++k) {
-        const DevSurface& s = sch.s[k];
-        std::snprintf(line, sizeof(line),
-                      "        if (stage == -1) stage = mx_surface<mx::FixedShape<%d, %d, %d, %d, %d, %d, %d, %d, %d, "
-                      "%d, %d>>(sch->s[%d], %d, sch->fixes, knots, beams, b, lam, memo, r);\n",
-                      (int)s.kind, (int)s.type, (int)s.cls, (int)s.shape, (int)s.gr_type, s.translate != 0 ? 1 : 0,
-                      (int)s.rot_mask, (int)s.n_poly, s.non_aux != 0 ? 1 : 0, s.sag_cull != 0 ? 1 : 0,
-                      s.c == 0.0 ? 1 : 0, k, k);
-        calls += line;
+// FixedShape<...> of surface s: the fields RtShape reads.
+static std::string fixed_shape(const DevSurface& s) {
+    char t[200];
+    std::snprintf(t, sizeof(t), "FixedShape<%d, %d, %d, %d, %d, %d, %d, %d, %d, %d, %d>", (int)s.kind, (int)s.type,
+                  (int)s.cls, (int)s.shape, (int)s.gr_type, s.translate != 0 ? 1 : 0, (int)s.rot_mask, (int)s.n_poly,
+                  s.non_aux != 0 ? 1 : 0, s.sag_cull != 0 ? 1 : 0, s.c == 0.0 ? 1 : 0);
+    return t;
+}
+
+static const char* const kParams =
+    "        const rtb::DevScheme* __restrict__ g_sch, const double* knots, const rtb::DevBeam* beams,\n"
+    "        int n_beams, rtb::DevRays in, rtb::DevRays out, unsigned long long* counts, unsigned* err,\n"
+    "        int state_out, rtb::FrameArgs frame, rtb::TileSched ts) {\n";
+
+std::string scheme_source(const DevScheme& sch, int precision) {
+    std::string src;
+    if (precision == RTB_MIXED) {
+        src = "#include \"mixed.cuh\"\n"
+              "namespace rtb {\n"
+              "struct SchemeSurfaces {\n"
+              "    __device__ __forceinline__ static void run(const DevScheme* sch, const double* knots,\n"
+              "        const DevBeam* beams, int b, double lam, mx::TableMemo& memo, mx::Ray& r, int& stage) {\n";
+        for (int k = 0; k < sch.n_surfaces; ++k) {
+            const std::string ks = std::to_string(k);
+            src += "        if (stage == -1) stage = mx_surface<" + fixed_shape(sch.s[k]) + ">(sch->s[" + ks + "], " +
+                   ks + ", sch->fixes, knots, beams, b, lam, memo, r);\n";
+        }
+        src += std::string("    }\n};\n}  // namespace rtb\n"
+                           "extern \"C\" __global__ void __maxnreg__(64) ") + kMixedName + "(\n" + kParams +
+               "    rtb::fused_mixed<rtb::SchemeSurfaces>(g_sch, knots, beams, n_beams, in, out, counts, err,\n"
+               "                                        state_out, frame, ts);\n}\n";
+    } else {
+        src = "#include \"fused_fp64.cuh\"\n"
+              "namespace rtb {\n"
+              "struct SchemeSurfacesF64 {\n"
+              "    __device__ __forceinline__ static void run(const DevScheme* sch, const double* knots,\n"
+              "        const DevBeam* beams, int b, double lam, unsigned* err, f64::Ray& r, int& stage) {\n";
+        for (int k = 0; k < sch.n_surfaces; ++k) {
+            const std::string ks = std::to_string(k);
+            src += "        if (stage == -1) f64_surface<" + fixed_shape(sch.s[k]) + ">(sch->s[" + ks + "], " + ks +
+                   ", sch->fixes, knots, beams, b, lam, err, r, stage);\n        __syncthreads();\n";
+        }
+        src += std::string("    }\n};\n}  // namespace rtb\n"
+                           "extern \"C\" __global__ void __maxnreg__(64) ") + kFp64Name + "(\n" + kParams +
+               "    rtb::fused_fp64<rtb::SchemeSurfacesF64>(g_sch, knots, beams, n_beams, in, out, counts, err,\n"
+               "                                          state_out, frame, ts);\n}\n";
     }
-    return std::string("#include \"mixed.cuh\"\n"
-                       "namespace rtb {\n"
-                       "struct SchemeSurfaces {\n"
-                       "    __device__ __forceinline__ static void run(const DevScheme* sch, const double* knots,\n"
-                       "        const DevBeam* beams, int b, double lam, mx::TableMemo& memo, mx::Ray& r, int& stage) {\n") +
-           calls +
-           "    }\n"
-           "};\n"
-           "}  // namespace rtb\n"
-           "extern \"C\" __global__ void __maxnreg__(64) rtb_fused_mixed_scheme(\n"
-           "        const rtb::DevScheme* __restrict__ g_sch, const double* knots, const rtb::DevBeam* beams,\n"
-           "        int n_beams, rtb::DevRays in, rtb::DevRays out, unsigned long long* counts, unsigned* err,\n"
-           "        int state_out, rtb::FrameArgs frame, rtb::TileSched ts) {\n"
-           "    rtb::fused_mixed<rtb::SchemeSurfaces>(g_sch, knots, beams, n_beams, in, out, counts, err,\n"
-           "                                        state_out, frame, ts);\n"
-           "}\n";
+    return src;
 }
 
 std::string nvrtc_info() {
@@ -181,7 +204,7 @@ bool specialize_enabled() {
 
 // The compiled kernel for `src` (g_mu held), compiled on first use when
 // `compile`, else only when compiled before.
-static const std::vector<char>* cubin_for(const std::string& src, std::string* why, bool compile = true) {
+static const std::vector<char>* cubin_for(const std::string& src, bool fmad, std::string* why, bool compile) {
     auto it = g_cubins.find(src);
     if (it != g_cubins.end()) return &it->second;
     if (!compile) {
@@ -195,33 +218,33 @@ static const std::vector<char>* cubin_for(const std::string& src, std::string* w
     }
     std::vector<char> cubin;
     std::string log;
-    if (compile_to_cubin(src, cubin, log) != RTB_OK) {
+    if (compile_to_cubin(src, fmad, cubin, log) != RTB_OK) {
         if (why) *why = "NVRTC failed: " + log.substr(0, 2000);
         return nullptr;
     }
     return &g_cubins.emplace(src, std::move(cubin)).first->second;
 }
 
-int compile_mixed_scheme(const DevScheme& sch, std::string* why) {
+int compile_scheme(const DevScheme& sch, int precision, std::string* why) {
     std::lock_guard<std::mutex> g(g_mu);
-    return cubin_for(mixed_scheme_source(sch), why) ? RTB_OK : RTB_FAILED;
+    return cubin_for(scheme_source(sch, precision), precision == RTB_MIXED, why, true) ? RTB_OK : RTB_FAILED;
 }
 
-int mixed_scheme_kernel(const DevScheme& sch, const void** kernel, std::string* why, bool compile) {
+int scheme_kernel(const DevScheme& sch, int precision, const void** kernel, std::string* why, bool compile) {
     *kernel = nullptr;
-    const std::string src = mixed_scheme_source(sch);
+    const std::string src = scheme_source(sch, precision);
     std::lock_guard<std::mutex> g(g_mu);
     auto it = g_kernels.find(src);
     if (it != g_kernels.end()) {
         *kernel = reinterpret_cast<const void*>(it->second);
         return RTB_OK;
     }
-    const std::vector<char>* cubin = cubin_for(src, why, compile);
+    const std::vector<char>* cubin = cubin_for(src, precision == RTB_MIXED, why, compile);
     if (!cubin) return RTB_OK;
     cudaLibrary_t lib = nullptr;
     cudaKernel_t k = nullptr;
     cudaError_t e = cudaLibraryLoadData(&lib, cubin->data(), nullptr, nullptr, 0, nullptr, nullptr, 0);
-    if (e == cudaSuccess) e = cudaLibraryGetKernel(&k, lib, kKernelName);
+    if (e == cudaSuccess) e = cudaLibraryGetKernel(&k, lib, precision == RTB_MIXED ? kMixedName : kFp64Name);
     if (e != cudaSuccess) {
         if (lib) cudaLibraryUnload(lib);
         return cuda_status(e);
@@ -235,13 +258,15 @@ int mixed_scheme_kernel(const DevScheme& sch, const void** kernel, std::string* 
 
 using namespace rtb;
 
-int rtb_specialize(const rtb_surface* surfaces, size_t n_surfaces, uint32_t fixes, char* note, size_t note_len) {
+int rtb_specialize(const rtb_surface* surfaces, size_t n_surfaces, uint32_t fixes, int32_t precision, char* note,
+                   size_t note_len) {
     if (note && note_len > 0) note[0] = 0;
+    if (precision != RTB_FP64 && precision != RTB_MIXED) return RTB_BAD_VALUE;
     PreparedScheme ps;
     int st = prepare_scheme(surfaces, n_surfaces, fixes, 0, ps);
     if (st != RTB_OK) return st;
     std::string why;
-    st = compile_mixed_scheme(ps.sch, &why);
+    st = compile_scheme(ps.sch, precision, &why);
     if (note && note_len > 0) std::snprintf(note, note_len, "%s", why.c_str());
     return st;
 }

@@ -1,4 +1,4 @@
-// jit.h -- scheme-specialised fused mixed-precision kernels (jit.cpp).
+// jit.h -- fused trace kernels specialised to a scheme's structure (jit.cpp).
 #pragma once
 
 #include <string>
@@ -7,9 +7,9 @@
 
 namespace rtb {
 
-// The CUDA source of the fused mixed kernel specialised to the structure of
-// `sch` (one FixedShape per surface).
-std::string mixed_scheme_source(const DevScheme& sch);
+// The CUDA source of the fused kernel of `precision` (RTB_MIXED or RTB_FP64)
+// specialised to the structure of `sch` (one FixedShape per surface).
+std::string scheme_source(const DevScheme& sch, int precision);
 
 // NVRTC's version, or why it is unavailable (rtb_info).
 std::string nvrtc_info();
@@ -17,15 +17,15 @@ std::string nvrtc_info();
 // False when RTB_SPECIALIZE=0 is set in the environment.
 bool specialize_enabled();
 
-// Compile (without loading) the specialised kernel for `sch`: RTB_OK, or
-// RTB_FAILED with `why`.  Needs no device.
-int compile_mixed_scheme(const DevScheme& sch, std::string* why);
+// Compile (without loading) the specialised kernel: RTB_OK, or RTB_FAILED
+// with `why`.  Needs no device.
+int compile_scheme(const DevScheme& sch, int precision, std::string* why);
 
-// The specialised kernel for `sch` (compiled on first use when `compile`,
-// then cached), as a function handle for cudaLaunchKernel; *kernel is NULL,
-// and `why` says why, when NVRTC is unavailable or fails, or when the kernel
-// was not compiled before and `compile` is false.  Error status only for CUDA
+// The specialised kernel (compiled on first use when `compile`, then
+// cached), as a function handle for cudaLaunchKernel; *kernel is NULL, and
+// `why` says why, when NVRTC is unavailable or fails, or when the kernel was
+// not compiled before and `compile` is false.  Error status only for CUDA
 // errors of loading a compiled kernel.
-int mixed_scheme_kernel(const DevScheme& sch, const void** kernel, std::string* why, bool compile = true);
+int scheme_kernel(const DevScheme& sch, int precision, const void** kernel, std::string* why, bool compile = true);
 
 }  // namespace rtb

@@ -44,7 +44,7 @@ struct rtb_plan {
     bool ran = false;
     int32_t block = 256, rpt = kDefaultRpt;
     uint64_t key = 0;
-    std::string jit_note;            // why the generic mixed kernel is launched ("" if specialised)
+    std::string jit_note;            // why the generic kernel is launched ("" if specialised)
 };
 
 namespace {
@@ -65,7 +65,7 @@ uint64_t plan_key(const rtb_plan& p) {
     h = fnv1a(h, &p.ps.sch, sizeof(DevScheme));
     h = fnv1a(h, p.ps.knots.data(), p.ps.knots.size() * sizeof(double));
     h = fnv1a(h, &p.n_rays, sizeof(p.n_rays));
-    int32_t tags[4] = {p.opts.precision, p.has_frame ? 1 : 0, p.opts.ray_order, p.ps.mixed_kernel ? 1 : 0};
+    int32_t tags[4] = {p.opts.precision, p.has_frame ? 1 : 0, p.opts.ray_order, p.ps.scheme_kernel ? 1 : 0};
     return fnv1a(h, tags, sizeof(tags));
 }
 
@@ -219,15 +219,11 @@ int rtb_plan_create(const rtb_surface* surfaces, size_t n_surfaces, const rtb_be
         delete p;
         return st;
     }
-    if (opts->precision == RTB_MIXED) {
-        if (!specialize_enabled()) {
-            p->jit_note = "RTB_SPECIALIZE=0";
-        } else if ((st = mixed_scheme_kernel(p->ps.sch, &p->ps.mixed_kernel, &p->jit_note)) != RTB_OK) {
-            delete p;
-            return st;
-        }
-    } else {
-        p->jit_note = "FP64 plan";
+    if (!specialize_enabled()) {
+        p->jit_note = "RTB_SPECIALIZE=0";
+    } else if ((st = scheme_kernel(p->ps.sch, opts->precision, &p->ps.scheme_kernel, &p->jit_note)) != RTB_OK) {
+        delete p;
+        return st;
     }
     if (opts->block_size > 0 || opts->rays_per_thread > 0) {
         p->block = opts->block_size > 0 ? opts->block_size : 256;
@@ -444,7 +440,7 @@ int rtb_plan_autotune(rtb_plan* p, int reps, rtb_tune_entry* table, size_t capac
 
 int rtb_plan_specialized(const rtb_plan* p, int32_t* specialized, char* note, size_t note_len) {
     if (!p || !specialized) return RTB_BAD_VALUE;
-    *specialized = p->ps.mixed_kernel ? 1 : 0;
+    *specialized = p->ps.scheme_kernel ? 1 : 0;
     if (note && note_len > 0) std::snprintf(note, note_len, "%s", p->jit_note.c_str());
     return RTB_OK;
 }

@@ -9,6 +9,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "shape.cuh"
 
 namespace rtb {
 namespace f64 {
@@ -61,28 +62,30 @@ struct CycleSkip {
 };
 
 // conic_derivs (rt_cuda_engine_surface.cu:45-61)
+template <class Sh = RtShape>
 __device__ __forceinline__ void conic_derivs(const DevSurface& s, double X, double Y, double& dFdX, double& dFdY) {
     double r2 = X * X + Y * Y;
     double E = s.c / sqrt(1.0 - s.k1 * s.c * s.c * r2);
     double sum = 0.0, rr = 1.0;
-    for (int i = 1; i <= s.n_poly; ++i, rr *= r2) sum += (double)i * s.poly[i - 1] * rr;
+    for (int i = 1; i <= Sh::n_poly(s); ++i, rr *= r2) sum += (double)i * s.poly[i - 1] * rr;
     E += 2.0 * sum;
     dFdX = -E * X;
     dFdY = -E * Y;
 }
 
 // toric_derivs (rt_cuda_engine_surface.cu:65-94)
+template <class Sh = RtShape>
 __device__ __forceinline__ void toric_derivs(const DevSurface& s, double X, double Y, double Z, double& dFdX,
                                              double& dFdY, double& dFdZ) {
     double Y2 = Y * Y;
     double Fy = s.c * Y2 / (1.0 + sqrt(1.0 - s.k1 * s.c * s.c * Y2));
     double sum = 0.0, rr = Y2;
-    for (int i = 0; i < s.n_poly; ++i, rr *= Y2) sum += s.poly[i] * rr;
+    for (int i = 0; i < Sh::n_poly(s); ++i, rr *= Y2) sum += s.poly[i] * rr;
     Fy += sum;
     double dFy = s.c * Y / sqrt(1.0 - s.k1 * s.c * s.c * Y2);
     sum = 0.0;
     rr = 1.0;
-    for (int i = 1; i <= s.n_poly; ++i, rr *= Y2) sum += (double)i * s.poly[i - 1] * rr;
+    for (int i = 1; i <= Sh::n_poly(s); ++i, rr *= Y2) sum += (double)i * s.poly[i - 1] * rr;
     dFy += 2.0 * sum;
     dFdX = -s.cR * X;
     dFdY = (s.cR * Fy - 1.0) * dFy;
@@ -131,6 +134,7 @@ __device__ __forceinline__ bool conic_isect(const DevSurface& s, Ray& r) {
 
 // iterative_conic_intersection (rt_cuda_engine_surface.cu:257-333); the
 // iteration count is per ray and bounded by K_ITER_MAX.
+template <class Sh = RtShape>
 __device__ __forceinline__ bool iter_conic_isect(const DevSurface& s, bool fix_root, Ray& r) {
     double s0 = -r.Z / r.cZ;
     if (!(s0 >= 0)) return false;
@@ -146,12 +150,12 @@ __device__ __forceinline__ bool iter_conic_isect(const DevSurface& s, bool fix_r
         double r2 = Xi * Xi + Yi * Yi;
         double F = Zi - s.c * r2 / (1.0 + sqrt(1.0 - s.k1 * s.c * s.c * r2));
         double sum = 0.0, rr = r2;
-        for (int i = 0; i < s.n_poly; ++i, rr *= r2) sum += s.poly[i] * rr;
+        for (int i = 0; i < Sh::n_poly(s); ++i, rr *= r2) sum += s.poly[i] * rr;
         F -= sum;
         double E = s.c / sqrt(1.0 - s.k1 * s.c * s.c * r2);
         sum = 0.0;
         rr = 1.0;
-        for (int i = 1; i <= s.n_poly; ++i, rr *= r2) sum += (double)i * s.poly[i - 1] * rr;
+        for (int i = 1; i <= Sh::n_poly(s); ++i, rr *= r2) sum += (double)i * s.poly[i - 1] * rr;
         E += 2.0 * sum;
         double dF = -E * Xi * r.cX - E * Yi * r.cY + r.cZ;
         if (fabs(dF) < K_ITER_EPS) { good = false; break; }
@@ -172,6 +176,7 @@ __device__ __forceinline__ bool iter_conic_isect(const DevSurface& s, bool fix_r
 }
 
 // iterative_poly_intersection (rt_cuda_engine_surface.cu:497-561)
+template <class Sh = RtShape>
 __device__ __forceinline__ bool iter_poly_isect(const DevSurface& s, bool fix_root, Ray& r) {
     double s0 = -r.Z / r.cZ;
     if (!(s0 > 0)) return false;
@@ -186,11 +191,11 @@ __device__ __forceinline__ bool iter_poly_isect(const DevSurface& s, bool fix_ro
         Zi = s1 * r.cZ;
         double r2 = Xi * Xi + Yi * Yi;
         double F = 0.0, rr = r2;
-        for (int i = 0; i < s.n_poly; ++i, rr *= r2) F += s.poly[i] * rr;
+        for (int i = 0; i < Sh::n_poly(s); ++i, rr *= r2) F += s.poly[i] * rr;
         F = Zi - F;
         double dF = 0.0;
         rr = 1.0;
-        for (int i = 1; i <= s.n_poly; ++i, rr *= r2) dF += (double)i * s.poly[i - 1] * rr;
+        for (int i = 1; i <= Sh::n_poly(s); ++i, rr *= r2) dF += (double)i * s.poly[i - 1] * rr;
         dF = -Xi * dF - Yi * dF + 1.0;
         if (fabs(dF) < K_ITER_EPS) { good = false; break; }
         s2 = s1 - F / dF;
@@ -247,32 +252,34 @@ __device__ __forceinline__ bool toric_isect(const DevSurface& s, uint32_t fixes,
     return true;
 }
 
+template <class Sh = RtShape>
 __device__ __forceinline__ bool intersect(const DevSurface& s, uint32_t fixes, Ray& r) {
-    switch (s.kind) {
+    switch (Sh::kind(s)) {
         case IS_PLANE: return plane_isect(r);
         case IS_PARABOLOID: return paraboloid_isect(s, r);
         case IS_CONIC: return conic_isect(s, r);
-        case IS_ITER_POLY: return iter_poly_isect(s, (fixes & RTB_FIX_ASPHERE_ROOT) != 0, r);
-        case IS_ITER_CONIC: return iter_conic_isect(s, (fixes & RTB_FIX_ASPHERE_ROOT) != 0, r);
+        case IS_ITER_POLY: return iter_poly_isect<Sh>(s, (fixes & RTB_FIX_ASPHERE_ROOT) != 0, r);
+        case IS_ITER_CONIC: return iter_conic_isect<Sh>(s, (fixes & RTB_FIX_ASPHERE_ROOT) != 0, r);
         case IS_TORIC: return toric_isect(s, fixes, r);
         default: return true;
     }
 }
 
 // ---- reflection (rt_cuda_engine_surface.cu:771-827) -----------------------
+template <class Sh = RtShape>
 __device__ __forceinline__ void reflect(const DevSurface& s, Ray& r) {
-    if (s.cls == RTB_PLANE) {
+    if (Sh::cls(s) == RTB_PLANE) {
         r.cZ = -r.cZ;
-    } else if (s.cls == RTB_CONIC) {
+    } else if (Sh::cls(s) == RTB_CONIC) {
         double dFdX, dFdY;
-        conic_derivs(s, r.X, r.Y, dFdX, dFdY);
+        conic_derivs<Sh>(s, r.X, r.Y, dFdX, dFdY);
         double a2 = 2.0 * (r.cX * dFdX + r.cY * dFdY + r.cZ) / (dFdX * dFdX + dFdY * dFdY + 1.0);
         r.cX -= a2 * dFdX;
         r.cY -= a2 * dFdY;
         r.cZ -= a2;
-    } else if (s.cls == RTB_TORIC) {
+    } else if (Sh::cls(s) == RTB_TORIC) {
         double dFdX, dFdY, dFdZ;
-        toric_derivs(s, r.X, r.Y, r.Z, dFdX, dFdY, dFdZ);
+        toric_derivs<Sh>(s, r.X, r.Y, r.Z, dFdX, dFdY, dFdZ);
         double a2 = 2.0 * (r.cX * dFdX + r.cY * dFdY + r.cZ * dFdZ) / (dFdX * dFdX + dFdY * dFdY + dFdZ * dFdZ);
         r.cX -= a2 * dFdX;
         r.cY -= a2 * dFdY;
@@ -281,8 +288,9 @@ __device__ __forceinline__ void reflect(const DevSurface& s, Ray& r) {
 }
 
 // ---- refraction (rt_cuda_engine_surface.cu:956-1066) ----------------------
+template <class Sh = RtShape>
 __device__ __forceinline__ bool refract(const DevSurface& s, double mu, Ray& r) {
-    if (s.cls == RTB_PLANE) {
+    if (Sh::cls(s) == RTB_PLANE) {
         double a = mu * r.cZ;
         double b = mu * mu - 1.0;
         double a2 = a * a;
@@ -294,9 +302,9 @@ __device__ __forceinline__ bool refract(const DevSurface& s, double mu, Ray& r) 
         r.cZ = mu * r.cZ + G;
         return true;
     }
-    if (s.cls == RTB_CONIC) {
+    if (Sh::cls(s) == RTB_CONIC) {
         double dFdX, dFdY;
-        conic_derivs(s, r.X, r.Y, dFdX, dFdY);
+        conic_derivs<Sh>(s, r.X, r.Y, dFdX, dFdY);
         double G = dFdX * dFdX + dFdY * dFdY + 1.0;
         double a = mu * (r.cX * dFdX + r.cY * dFdY + r.cZ) / G;
         double b = (mu * mu - 1.0) / G;
@@ -309,9 +317,9 @@ __device__ __forceinline__ bool refract(const DevSurface& s, double mu, Ray& r) 
         r.cZ = mu * r.cZ + G;
         return true;
     }
-    if (s.cls == RTB_TORIC) {
+    if (Sh::cls(s) == RTB_TORIC) {
         double dFdX, dFdY, dFdZ;
-        toric_derivs(s, r.X, r.Y, r.Z, dFdX, dFdY, dFdZ);
+        toric_derivs<Sh>(s, r.X, r.Y, r.Z, dFdX, dFdY, dFdZ);
         double G = dFdX * dFdX + dFdY * dFdY + dFdZ * dFdZ;
         double a = mu * (r.cX * dFdX + r.cY * dFdY + r.cZ * dFdZ) / G;
         double b = (mu * mu - 1.0) / G;
@@ -328,9 +336,10 @@ __device__ __forceinline__ bool refract(const DevSurface& s, double mu, Ray& r) 
 }
 
 // ---- diffraction (rt_cuda_engine_surface.cu:1247-1520) --------------------
+template <class Sh = RtShape>
 __device__ __forceinline__ bool diffract(const DevSurface& s, double mu, double L, Ray& r) {
-    if (s.gr_type == RTB_TRANSPARENT) {
-        if (s.cls == RTB_PLANE) {  // plane_diffr_trans_kernel
+    if (Sh::gr_type(s) == RTB_TRANSPARENT) {
+        if (Sh::cls(s) == RTB_PLANE) {  // plane_diffr_trans_kernel
             double a = mu * r.cZ;
             double b = mu * mu - 1.0 + L * L - 2.0 * mu * L * r.cX;
             double a2 = a * a;
@@ -342,9 +351,9 @@ __device__ __forceinline__ bool diffract(const DevSurface& s, double mu, double 
             r.cZ = mu * r.cZ + G;
             return true;
         }
-        if (s.cls == RTB_CONIC) {  // conic_diffr_trans_kernel
+        if (Sh::cls(s) == RTB_CONIC) {  // conic_diffr_trans_kernel
             double dFdX, dFdY;
-            conic_derivs(s, r.X, r.Y, dFdX, dFdY);
+            conic_derivs<Sh>(s, r.X, r.Y, dFdX, dFdY);
             double G = dFdX / (dFdY * dFdY + 1.0);
             double u = 1.0 / sqrt(1.0 + dFdX * G);
             double v = -dFdY * u * G;
@@ -361,9 +370,9 @@ __device__ __forceinline__ bool diffract(const DevSurface& s, double mu, double 
             r.cZ = mu * r.cZ - L * w + G;
             return true;
         }
-        if (s.cls == RTB_TORIC) {  // toric_diffr_trans_kernel
+        if (Sh::cls(s) == RTB_TORIC) {  // toric_diffr_trans_kernel
             double dFdX, dFdY, dFdZ;
-            toric_derivs(s, r.X, r.Y, r.Z, dFdX, dFdY, dFdZ);
+            toric_derivs<Sh>(s, r.X, r.Y, r.Z, dFdX, dFdY, dFdZ);
             double G = dFdX / (dFdY * dFdY + dFdZ + dFdZ);
             double u = 1.0 / sqrt(1.0 + dFdX * G);
             double v = -dFdY * u * G;
@@ -382,7 +391,7 @@ __device__ __forceinline__ bool diffract(const DevSurface& s, double mu, double 
         }
         return true;
     }
-    if (s.cls == RTB_PLANE) {  // plane_diffr_refl_kernel
+    if (Sh::cls(s) == RTB_PLANE) {  // plane_diffr_refl_kernel
         double a = r.cZ;
         double b = L * L - 2.0 * L * r.cX;
         double a2 = a * a;
@@ -393,9 +402,9 @@ __device__ __forceinline__ bool diffract(const DevSurface& s, double mu, double 
         r.cZ += G;
         return true;
     }
-    if (s.cls == RTB_CONIC) {  // conic_diffr_refl_kernel
+    if (Sh::cls(s) == RTB_CONIC) {  // conic_diffr_refl_kernel
         double dFdX, dFdY;
-        conic_derivs(s, r.X, r.Y, dFdX, dFdY);
+        conic_derivs<Sh>(s, r.X, r.Y, dFdX, dFdY);
         double G = dFdX / (dFdY * dFdY + 1.0);
         double u = 1.0 / sqrt(1.0 + dFdX * G);
         double v = -dFdY * u * G;
@@ -412,9 +421,9 @@ __device__ __forceinline__ bool diffract(const DevSurface& s, double mu, double 
         r.cZ = r.cZ - L * w + G;
         return true;
     }
-    if (s.cls == RTB_TORIC) {  // toric_diffr_refl_kernel
+    if (Sh::cls(s) == RTB_TORIC) {  // toric_diffr_refl_kernel
         double dFdX, dFdY, dFdZ;
-        toric_derivs(s, r.X, r.Y, r.Z, dFdX, dFdY, dFdZ);
+        toric_derivs<Sh>(s, r.X, r.Y, r.Z, dFdX, dFdY, dFdZ);
         double G = dFdX / (dFdY * dFdY + dFdZ + dFdZ);
         double u = 1.0 / sqrt(1.0 + dFdX * G);
         double v = -dFdY * u * G;
@@ -495,15 +504,16 @@ __device__ __forceinline__ void rotate_pair(double sA, double cA, double& v1, do
 }
 
 // beam_transform: translation then rotations about y, x, z (rt_cuda_engine_beam.cu:416-579)
+template <class Sh = RtShape>
 __device__ __forceinline__ void transform(const DevSurface& s, Ray& r) {
-    if (s.translate) {
+    if (Sh::translate(s)) {
         r.X -= s.dist[0];
         r.Y -= s.dist[1];
         r.Z -= s.dist[2];
     }
-    if (s.rot_mask & 1) rotate_pair(s.sinA[0], s.cosA[0], r.X, r.Z, r.cX, r.cZ);
-    if (s.rot_mask & 2) rotate_pair(s.sinA[1], s.cosA[1], r.Y, r.Z, r.cY, r.cZ);
-    if (s.rot_mask & 4) rotate_pair(s.sinA[2], s.cosA[2], r.X, r.Y, r.cX, r.cY);
+    if (Sh::rot_mask(s) & 1) rotate_pair(s.sinA[0], s.cosA[0], r.X, r.Z, r.cX, r.cZ);
+    if (Sh::rot_mask(s) & 2) rotate_pair(s.sinA[1], s.cosA[1], r.Y, r.Z, r.cY, r.cZ);
+    if (Sh::rot_mask(s) & 4) rotate_pair(s.sinA[2], s.cosA[2], r.X, r.Y, r.cX, r.cY);
 }
 
 // TabulatedFunction::operator[] (tabulated_function.cpp:173-204); knots at
@@ -542,31 +552,32 @@ enum ActionResult { ACT_OK = 0, ACT_LOST = 1, ACT_RANGE = 2 };
 // Mirror/Lens/Grating ::Action on one ray (surface.cpp:385-396,453-472,563-585)
 // with n(lambda) evaluated on the device (the reference evaluates it on the
 // host per ray, surface.cu:1094-1097,1565-1569,1608-1610).
+template <class Sh = RtShape>
 __device__ __forceinline__ int action(const DevSurface& s, const double* knots, long long order, double lambda,
                                       Ray& r) {
-    if (s.type == RTB_MIRROR) {
-        reflect(s, r);
+    if (Sh::type(s) == RTB_MIRROR) {
+        reflect<Sh>(s, r);
         return ACT_OK;
     }
-    if (s.type == RTB_LENS) {
+    if (Sh::type(s) == RTB_LENS) {
         double a, b;
         if (!table_eval(knots + s.n1_off, s.n1_n, lambda, a) || !table_eval(knots + s.n2_off, s.n2_n, lambda, b))
             return ACT_RANGE;
         double mu = a;
         mu /= b;
-        return refract(s, mu, r) ? ACT_OK : ACT_LOST;
+        return refract<Sh>(s, mu, r) ? ACT_OK : ACT_LOST;
     }
-    if (s.type == RTB_GRATING) {
+    if (Sh::type(s) == RTB_GRATING) {
         double n2v, mu = 0.0;
         if (!table_eval(knots + s.n2_off, s.n2_n, lambda, n2v)) return ACT_RANGE;
-        if (s.gr_type == RTB_TRANSPARENT) {
+        if (Sh::gr_type(s) == RTB_TRANSPARENT) {
             double n1v;
             if (!table_eval(knots + s.n1_off, s.n1_n, lambda, n1v)) return ACT_RANGE;
             mu = n1v;
             mu /= n2v;
         }
         double L = (double)order * lambda / n2v / s.gr_const;
-        return diffract(s, mu, L, r) ? ACT_OK : ACT_LOST;
+        return diffract<Sh>(s, mu, L, r) ? ACT_OK : ACT_LOST;
     }
     return ACT_OK;
 }

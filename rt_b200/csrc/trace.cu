@@ -19,12 +19,14 @@ DevRays dev_rays(const rtb_rays* r) {
     return d;
 }
 
-// One-shot fused mixed traces launch the kernel specialised to the scheme's
+// One-shot fused traces launch the kernel specialised to the scheme's
 // structure when one was compiled already in this process (by a plan or
 // rtb_specialize); they never compile one themselves.
 int attach_compiled(PreparedScheme& ps, const rtb_trace_opts& o) {
-    if (o.engine != RTB_ENGINE_FUSED || o.precision != RTB_MIXED || !specialize_enabled()) return RTB_OK;
-    return mixed_scheme_kernel(ps.sch, &ps.mixed_kernel, nullptr, false);
+    if (o.engine != RTB_ENGINE_FUSED || (o.precision != RTB_MIXED && o.precision != RTB_FP64) ||
+        !specialize_enabled())
+        return RTB_OK;
+    return scheme_kernel(ps.sch, o.precision, &ps.scheme_kernel, nullptr, false);
 }
 
 int check_beams(const rtb_beam* beams, size_t n_beams, size_t n_rays, std::vector<DevBeam>& out) {
@@ -123,9 +125,9 @@ int launch_trace(const PreparedScheme& ps, TraceArgs& a, int n_beams, const rtb_
         if (rpt < 1 || rpt > 64) return RTB_BAD_VALUE;
         const size_t smem = fused_smem_bytes(ps.sch.n_knots);
         if (smem > (size_t)engine().max_smem_optin) return RTB_BAD_VALUE;
-        const void* kern = !mixed ? reinterpret_cast<const void*>(k_fused_fp64)
-                           : ps.mixed_kernel ? ps.mixed_kernel
-                                             : reinterpret_cast<const void*>(k_fused_mixed);
+        const void* kern = ps.scheme_kernel ? ps.scheme_kernel
+                           : mixed         ? reinterpret_cast<const void*>(k_fused_mixed)
+                                           : reinterpret_cast<const void*>(k_fused_fp64);
         RTB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int per_sm = 0;
         RTB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));

@@ -247,16 +247,18 @@ SPEC_SCHEMES = {
 }
 
 
+@pytest.mark.parametrize("precision", [ffi.MIXED, ffi.FP64])
 @pytest.mark.parametrize("name", sorted(SPEC_SCHEMES))
-def test_specialised_plan_equals_generic_kernel(name, monkeypatch):
-    """A mixed plan launches the kernel compiled for its scheme's structure;
-    it computes what the generic kernel (RTB_SPECIALIZE=0) computes: the same
-    lost flags, stages, counters and frame, and positions and cosines equal
-    to 1e-9 (mm, or of a unit vector) -- bit for bit on most schemes, a few
-    ulps apart where folding the scheme's branches lets the compiler
-    contract a product and a sum into an FMA that the generic kernel keeps
-    apart (the gratings scheme).  Both are far inside the mixed engine's
-    0.05 um budget against the FP64 oracle."""
+def test_specialised_plan_equals_generic_kernel(name, precision, monkeypatch):
+    """A plan launches the kernel compiled for its scheme's structure; it
+    computes what the generic kernel (RTB_SPECIALIZE=0) computes.  FP64: bit
+    for bit (no contraction either way).  Mixed: the same lost flags, stages,
+    counters and frame, and positions and cosines equal to 1e-9 (mm, or of a
+    unit vector) -- bit for bit on most schemes, a few ulps apart where
+    folding the scheme's branches lets the compiler contract a product and a
+    sum into an FMA that the generic kernel keeps apart (the gratings
+    scheme).  Both are far inside the mixed engine's 0.05 um budget against
+    the FP64 oracle."""
     make, kw, orders = SPEC_SCHEMES[name]
     beams = [S.make_beam(0, 3000, kw["n_lambda"], kw["radius"], kw["lam_range"], 11, orders=orders)]
     ccd = S.ccd(S.C1_CCD)
@@ -264,7 +266,7 @@ def test_specialised_plan_equals_generic_kernel(name, monkeypatch):
     res = []
     for spec in ("1", "0"):
         monkeypatch.setenv("RTB_SPECIALIZE", spec)
-        o, counts, outside = frame_opts(ffi.MIXED, ccd, state_out=1)
+        o, counts, outside = frame_opts(precision, ccd, state_out=1)
         plan = E.Plan(cs.surfaces, beams, o)
         on, note = plan.specialized()
         assert on == (spec == "1"), note
@@ -280,6 +282,8 @@ def test_specialised_plan_equals_generic_kernel(name, monkeypatch):
     same = 0
     for f in ("X", "Y", "Z", "cX", "cY", "cZ"):
         x, y = a[3][f], b[3][f]
+        if precision == ffi.FP64:
+            assert torch.equal(x.view(torch.int64), y.view(torch.int64)), f
         fin = torch.isfinite(x)
         assert torch.equal(fin, torch.isfinite(y)), f
         assert float((x[fin] - y[fin]).abs().max()) <= 1e-9, f
@@ -290,11 +294,17 @@ def test_specialised_plan_equals_generic_kernel(name, monkeypatch):
     assert np.array_equal(a[6], b[6])
 
 
-def test_fp64_plan_is_not_specialised():
+def test_plans_report_their_kernel(monkeypatch):
     cs = S.to_c(S.echelle(), E.spline_init)
-    plan = E.Plan(cs.surfaces, small_c3(n_beams=4), E.opts(engine=ffi.ENGINE_FUSED, precision=ffi.FP64, fixes=FIXES))
-    assert plan.specialized() == (False, "FP64 plan")
-    plan.destroy()
+    for prec in (ffi.FP64, ffi.MIXED):
+        monkeypatch.setenv("RTB_SPECIALIZE", "1")
+        plan = E.Plan(cs.surfaces, small_c3(n_beams=4), E.opts(engine=ffi.ENGINE_FUSED, precision=prec, fixes=FIXES))
+        assert plan.specialized() == (True, "")
+        plan.destroy()
+        monkeypatch.setenv("RTB_SPECIALIZE", "0")
+        plan = E.Plan(cs.surfaces, small_c3(n_beams=4), E.opts(engine=ffi.ENGINE_FUSED, precision=prec, fixes=FIXES))
+        assert plan.specialized() == (False, "RTB_SPECIALIZE=0")
+        plan.destroy()
 
 
 def test_one_shot_trace_uses_a_compiled_specialisation(monkeypatch):

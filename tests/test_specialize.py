@@ -1,7 +1,6 @@
-"""Scheme-specialised mixed kernels (jit.cpp) without a GPU: rtb_specialize
-compiles the fused mixed kernel for the structure of every benchmark and
-coverage scheme with NVRTC, and the generated source fixes one FixedShape
-per surface."""
+"""Scheme-specialised fused kernels (jit.cpp) without a GPU: rtb_specialize
+compiles the fused mixed and FP64 kernels for the structure of every
+benchmark and coverage scheme with NVRTC."""
 import ctypes as C
 
 import pytest
@@ -34,14 +33,18 @@ def _nvrtc_present():
 
 
 @pytest.mark.skipif(not _nvrtc_present(), reason="libnvrtc not present")
+@pytest.mark.parametrize("precision", [ffi.MIXED, ffi.FP64])
 @pytest.mark.parametrize("name", sorted(SCHEMES))
-def test_specialised_kernel_compiles(name):
+def test_specialised_kernel_compiles(name, precision):
     cs = S.to_c(SCHEMES[name](), O.spline_init)
-    st, note = E.specialize(list(cs.surfaces), ffi.FIX_TORIC_SIGN | ffi.FIX_TORIC_STEP)
+    st, note = E.specialize(list(cs.surfaces), ffi.FIX_TORIC_SIGN | ffi.FIX_TORIC_STEP, precision)
     assert st == ffi.OK, note
     assert note == ""
 
 
-def test_specialize_rejects_a_bad_scheme():
+def test_specialize_rejects_bad_requests():
     st, _ = E.specialize([], 0)
+    assert st == ffi.BAD_VALUE
+    cs = S.to_c(S.littrow_free(), O.spline_init)
+    st, _ = E.specialize(list(cs.surfaces), 0, 7)
     assert st == ffi.BAD_VALUE
