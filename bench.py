@@ -171,9 +171,22 @@ def cpu_baseline(specs_fn, beams_all, budget_s=6.0):
     rate = rs / dt
     m = int(min(max(2000, budget_s * rate / (len(beams_all) * 5.3)), int(beams_all[0].n_rays)))
     n, rs, dt = run(m)
+    # one core on a smaller sample, for the per-core figure
+    lib.oracle_set_threads(1)
+    m1 = max(200, m // max(1, threads))
+    n1, rs1, dt1 = run(m1)
+    lib.oracle_set_threads(threads)
+    model = ""
+    try:
+        with open("/proc/cpuinfo") as f:
+            model = next((ln.split(":", 1)[1].strip() for ln in f if ln.startswith("model name")), "")
+    except OSError:
+        pass
     return {"value": rs / dt, "unit": UNIT, "cores": threads, "kind": "port",
             "sample": f"first {m} rays of each of the {len(beams_all)} order beams ({n} rays, {rs} ray-surfaces), "
-                      f"CPU oracle (C++, OpenMP, FP64), {dt:.2f} s"}
+                      f"CPU oracle (C++, OpenMP, FP64), {dt:.2f} s",
+            "one_core": {"value": rs1 / dt1, "sample": f"first {m1} rays of each beam ({n1} rays), {dt1:.2f} s"},
+            "nproc": os.cpu_count(), "cpu_model": model}
 
 
 def dgemm_tflops(n=4096, reps=5):
