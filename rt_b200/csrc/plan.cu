@@ -190,6 +190,13 @@ int rtb_plan_create(const rtb_surface* surfaces, size_t n_surfaces, const rtb_be
     *plan = nullptr;
     if (opts->engine != RTB_ENGINE_FUSED) return RTB_BAD_VALUE;
     if (opts->precision != RTB_FP64 && opts->precision != RTB_MIXED) return RTB_BAD_VALUE;
+    // compile the kernel specialised to the scheme first, outside the engine
+    // lock (NVRTC takes up to a second or so; other calls need not wait)
+    if (specialize_enabled()) {
+        PreparedScheme pre;
+        if (prepare_scheme(surfaces, n_surfaces, opts->fixes, opts->renormalize_lost, pre) == RTB_OK)
+            compile_scheme(pre.sch, opts->precision, nullptr);
+    }
     Lock l;
     int st = ensure_init();
     if (st != RTB_OK) return st;
