@@ -178,16 +178,26 @@ __global__ void __launch_bounds__(kAdjThreads, 4) k_adj_backward(AdjArgs a, cons
                     ad::load_state(st, sd, r);
                     ad::surface_step(s, table[e], sch->fixes, a.knots, order_of(s, a.beams, b), lam, r);
                 }
-                // the last surface's output is the CCD-plane point: only X, Y carry adjoints
-                const ad::Dual<kAdjW>* out[6] = {&r.X, &r.Y, &r.Z, &r.cX, &r.cY, &r.cZ};
+                // the last surface's output is the CCD-plane point: only X, Y
+                // carry adjoints.  Components are picked with selects (run-time
+                // indices would keep the ray and the adjoints in local memory).
+#pragma unroll
                 for (int l = 0; l < kAdjW; ++l) {
                     const int d = d0 + l;
                     if (d >= ndir) break;
                     double v = 0.0;
-                    if (act)
-                        for (int c = 0; c < 6; ++c) v += adj[c] * out[c]->d[l];
+                    if (act) {
+                        v += adj[0] * r.X.d[l];
+                        v += adj[1] * r.Y.d[l];
+                        v += adj[2] * r.Z.d[l];
+                        v += adj[3] * r.cX.d[l];
+                        v += adj[4] * r.cY.d[l];
+                        v += adj[5] * r.cZ.d[l];
+                    }
                     if (d < 6) {
-                        adj_in[d] = v;
+#pragma unroll
+                        for (int c = 0; c < 6; ++c)
+                            if (d == c) adj_in[c] = v;
                     } else {
                         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
                         if (lane == 0) acc[warp][sd.param[l]] += v;

@@ -108,13 +108,27 @@ __device__ void make_surfd(const DevSurface& s, int k, const ParamRef* map, int 
     }
 }
 
+// The seeded component is chosen with selects, not by indexing: a run-time
+// index into the ray's fields would keep the whole ray in local memory.
 template <int W>
 __device__ __forceinline__ void load_state(const double st[6], const Seeds<W>& sd, RayD<W>& r) {
-    Dual<W>* f[6] = {&r.X, &r.Y, &r.Z, &r.cX, &r.cY, &r.cZ};
-    for (int c = 0; c < 6; ++c) *f[c] = cst<W>(st[c]);
+    r.X = cst<W>(st[0]);
+    r.Y = cst<W>(st[1]);
+    r.Z = cst<W>(st[2]);
+    r.cX = cst<W>(st[3]);
+    r.cY = cst<W>(st[4]);
+    r.cZ = cst<W>(st[5]);
     if (sd.dense) return;
-    for (int l = 0; l < W; ++l)
-        if (sd.state[l] >= 0) f[sd.state[l]]->d[l] = 1.0;
+#pragma unroll
+    for (int l = 0; l < W; ++l) {
+        const int c = sd.state[l];
+        r.X.d[l] = (c == 0) ? 1.0 : 0.0;
+        r.Y.d[l] = (c == 1) ? 1.0 : 0.0;
+        r.Z.d[l] = (c == 2) ? 1.0 : 0.0;
+        r.cX.d[l] = (c == 3) ? 1.0 : 0.0;
+        r.cY.d[l] = (c == 4) ? 1.0 : 0.0;
+        r.cZ.d[l] = (c == 5) ? 1.0 : 0.0;
+    }
 }
 
 // ---- surface derivatives --------------------------------------------------
