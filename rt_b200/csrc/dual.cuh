@@ -3,7 +3,8 @@
 // Dual<W> carries a value and W tangents.  The value is computed with the
 // same IEEE operation as plain double arithmetic (translation units that use
 // it are compiled with --fmad=false), so a trace in Dual<W> has exactly the
-// values of the plain FP64 engine; the tangents follow the chain rule.
+// values of the plain FP64 engine; the tangents follow the chain rule, their
+// divisions as products with one refined reciprocal (tangent_rcp).
 #pragma once
 
 #include <cmath>
@@ -100,35 +101,50 @@ __device__ __forceinline__ Dual<W> operator*(double a, const Dual<W>& b) {
     for (int i = 0; i < W; ++i) r.d[i] = a * b.d[i];
     return r;
 }
+// 1/x for the tangents: the reciprocal seed refined by two Newton steps (to
+// about an ulp).  The values keep IEEE division; a tangent's last bits do not
+// steer anything, and one reciprocal per operation replaces W divisions.
+__device__ __forceinline__ double tangent_rcp(double x) {
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+    double e = fma(-x, r, 1.0);
+    r = fma(r, e, r);
+    e = fma(-x, r, 1.0);
+    return fma(r, e, r);
+}
+
 template <int W>
 __device__ __forceinline__ Dual<W> operator/(const Dual<W>& a, const Dual<W>& b) {
     Dual<W> r;
     r.v = a.v / b.v;
+    const double ib = tangent_rcp(b.v);
 #pragma unroll
-    for (int i = 0; i < W; ++i) r.d[i] = (a.d[i] - r.v * b.d[i]) / b.v;
+    for (int i = 0; i < W; ++i) r.d[i] = (a.d[i] - r.v * b.d[i]) * ib;
     return r;
 }
 template <int W>
 __device__ __forceinline__ Dual<W> operator/(const Dual<W>& a, double b) {
     Dual<W> r;
     r.v = a.v / b;
+    const double ib = tangent_rcp(b);
 #pragma unroll
-    for (int i = 0; i < W; ++i) r.d[i] = a.d[i] / b;
+    for (int i = 0; i < W; ++i) r.d[i] = a.d[i] * ib;
     return r;
 }
 template <int W>
 __device__ __forceinline__ Dual<W> operator/(double a, const Dual<W>& b) {
     Dual<W> r;
     r.v = a / b.v;
+    const double ib = tangent_rcp(b.v);
 #pragma unroll
-    for (int i = 0; i < W; ++i) r.d[i] = -r.v * b.d[i] / b.v;
+    for (int i = 0; i < W; ++i) r.d[i] = -r.v * b.d[i] * ib;
     return r;
 }
 template <int W>
 __device__ __forceinline__ Dual<W> sqrt(const Dual<W>& a) {
     Dual<W> r;
     r.v = ::sqrt(a.v);
-    const double h = (r.v > 0.0) ? 0.5 / r.v : 0.0;
+    const double h = (r.v > 0.0) ? 0.5 * tangent_rcp(r.v) : 0.0;
 #pragma unroll
     for (int i = 0; i < W; ++i) r.d[i] = a.d[i] * h;
     return r;

@@ -334,8 +334,9 @@ __device__ __forceinline__ bool asphere_isect(const DevSurface& ds, const SurfD<
     const double Ft = rv.cZ - E * (X.v * rv.cX + Y.v * rv.cY);
     Dual<W> tsum;
     tsum.v = s1 + s0.v;
+    const double iFt = tangent_rcp(Ft);
 #pragma unroll
-    for (int l = 0; l < W; ++l) tsum.d[l] = -F.d[l] / Ft;
+    for (int l = 0; l < W; ++l) tsum.d[l] = -F.d[l] * iFt;
     Dual<W> Xi = r.X + tsum * r.cX;
     Dual<W> Yi = r.Y + tsum * r.cY;
     Dual<W> Zi = r.Z + tsum * r.cZ;
@@ -402,8 +403,9 @@ __device__ __forceinline__ bool toric_isect(const DevSurface& ds, const SurfD<W>
     const double Ft = rv.cZ - dFY * rv.cY - ds.cR * (X.v * rv.cX + Z.v * rv.cZ - FY * dFY * rv.cY);
     Dual<W> t;
     t.v = sn1;
+    const double iFt = tangent_rcp(Ft);
 #pragma unroll
-    for (int l = 0; l < W; ++l) t.d[l] = -F.d[l] / Ft;
+    for (int l = 0; l < W; ++l) t.d[l] = -F.d[l] * iFt;
     r.X += t * r.cX;  // values: X + sn1 * cX, as the plain engine
     r.Y += t * r.cY;
     r.Z += t * r.cZ;
