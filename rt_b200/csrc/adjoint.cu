@@ -99,8 +99,9 @@ __global__ void __launch_bounds__(256) k_adj_forward(AdjArgs a, DevRays in, unsi
         a.flag[i] = (stage == -1) ? 1 : 0;
         a.X[i] = r.X;
         a.Y[i] = r.Y;
-        if (stage >= 0) atomicAdd(counts + (size_t)b * (n_stages + 1) + stage, 1ull);
-        else if (stage == -1) atomicAdd(counts + (size_t)b * (n_stages + 1) + n_stages, 1ull);
+        // one atomic per distinct counter in the warp (the rays of a beam
+        // mostly share theirs)
+        count_event(stage != -2, b * (n_stages + 1) + (stage >= 0 ? stage : n_stages), counts);
     }
 }
 
