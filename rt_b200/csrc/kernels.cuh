@@ -22,6 +22,7 @@ struct FrameArgs {
     uint64_t xdim, ydim;
     unsigned* counts;               // device; NULL disables the frame
     unsigned long long* n_outside;  // device; may be NULL
+    double inv_xpix, inv_ypix;      // 1/xpix, 1/ypix (the mixed kernel's pixel coordinates)
 };
 
 #ifndef __CUDACC_RTC__

@@ -626,7 +626,7 @@ __device__ __forceinline__ void fused_mixed(const DevScheme* __restrict__ g_sch,
                 out.flag[i] = in.flag[ri];
             }
             count_event(ev, key, counts);
-            if (frame.counts) frame_add(good, outX, outY, frame);
+            if (frame.counts) frame_add<false>(good, outX, outY, frame);
         }
     }
 }

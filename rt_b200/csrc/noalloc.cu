@@ -224,6 +224,8 @@ extern "C" RTB_API int rtb_trace_out_noalloc(const rtb_surface* surfaces, size_t
         frame.ydim = opts->ccd->ydim;
         frame.counts = opts->counts;
         frame.n_outside = reinterpret_cast<unsigned long long*>(opts->n_outside);
+        frame.inv_xpix = 1.0 / frame.xpix;
+        frame.inv_ypix = 1.0 / frame.ypix;
     }
     DevRays ri, ro;
     ri.X = in->X; ri.Y = in->Y; ri.Z = in->Z; ri.cX = in->cX; ri.cY = in->cY; ri.cZ = in->cZ;

@@ -60,6 +60,8 @@ FrameArgs frame_args(const rtb_trace_opts* o) {
         f.ydim = o->ccd->ydim;
         f.counts = o->counts;
         f.n_outside = reinterpret_cast<unsigned long long*>(o->n_outside);
+        f.inv_xpix = 1.0 / f.xpix;
+        f.inv_ypix = 1.0 / f.ypix;
     }
     return f;
 }
@@ -278,6 +280,8 @@ int rtb_ccd_frame(const rtb_rays* rays, const rtb_ccd* ccd, uint32_t* counts, ui
     f.ydim = ccd->ydim;
     f.counts = counts;
     f.n_outside = reinterpret_cast<unsigned long long*>(n_outside);
+    f.inv_xpix = 1.0 / f.xpix;
+    f.inv_ypix = 1.0 / f.ypix;
     k_ccd_frame<<<grid_for(rays->n, 256, 8), 256, 0, s>>>(dev_rays(rays), f);
     RTB_CUDA_TRY(cudaGetLastError());
     return RTB_OK;

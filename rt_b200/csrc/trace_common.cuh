@@ -53,14 +53,24 @@ __device__ __forceinline__ void count_event(bool ev, int key, unsigned long long
 }
 
 // Frame counts of one good ray at the detector: warp-aggregated increments
-// of the pixel it lands on.  Non-finite coordinates count as outside.
+// of the pixel it lands on.  Non-finite coordinates count as outside.  The
+// FP64 kernels divide by the pixel size as the reference does; the mixed
+// kernel (kDivide false) multiplies by its reciprocal, which moves a ray to
+// the next pixel only when its coordinate lies within an ulp of a pixel edge,
+// and saves two FP64 division sequences per ray.
+template <bool kDivide = true>
 __device__ __forceinline__ void frame_add(bool good, double X, double Y, const FrameArgs& f) {
     unsigned active = __activemask();
     long long pix = -1;
     if (good) {
         if (isfinite(X) && isfinite(Y)) {
             unsigned ix, iy;
-            ccd_coords(X, Y, f.xsize, f.ysize, f.xpix, f.ypix, ix, iy);
+            if (kDivide) {
+                ccd_coords(X, Y, f.xsize, f.ysize, f.xpix, f.ypix, ix, iy);
+            } else {
+                ix = __double2uint_rz((X + 0.5 * f.xsize) * f.inv_xpix);
+                iy = __double2uint_rz((Y + 0.5 * f.ysize) * f.inv_ypix);
+            }
             if (ix < f.xdim && iy < f.ydim) pix = (long long)iy * (long long)f.xdim + ix;
         }
     }
