@@ -17,6 +17,8 @@ page-locked host arrays (copies in and out inside the timed region).
 `cpu_baseline` is the CPU oracle on the host cores over a bounded sample of
 the same rays.  `c3_batched` is C3: 512 beams of uneven size, wavelength,
 field angle and order through the same scheme in one graph launch.
+`c4_adjoint` is C4: the forward/backward pair that gives the gradient of
+the spot merit in 24 scheme parameters over 1e7 rays.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 """
@@ -68,6 +70,8 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-c3", action="store_true")
+    p.add_argument("--no-c4", action="store_true")
+    p.add_argument("--c4-rays-per-lambda", type=int, default=156250, help="C4 adjoint: rays per wavelength (x64)")
     p.add_argument("--no-autotune", action="store_true", help="default launch configuration (profiling runs)")
     p.add_argument("--engines", default="per_surface,fused_fp64,fused_mixed")
     return p.parse_args()
@@ -187,6 +191,57 @@ def cpu_baseline(specs_fn, beams_all, budget_s=6.0):
                       f"CPU oracle (C++, OpenMP, FP64), {dt:.2f} s",
             "one_core": {"value": rs1 / dt1, "sample": f"first {m1} rays of each beam ({n1} rays), {dt1:.2f} s"},
             "nproc": os.cpu_count(), "cpu_model": model}
+
+
+def c4_adjoint(npl, reps=3):
+    """C4: the adjoint pair on the C0 spectrograph with its asphere field
+    flattener, 64 wavelengths x npl rays, 24 parameters.  The merit
+    sum_lambda RMS_spot + 10 (x_mean - x_t(lambda))^2 and its per-ray seeds
+    come from rtb_adjoint_spot_merit; one forward with checkpoints, the merit
+    and one backward give its whole gradient.  Each call returns
+    synchronised: wall-clock times, best of reps."""
+    import torch
+    from rt_b200 import engine as E
+    from rt_b200 import ffi, schemes as S
+    cs = S.to_c(S.littrow_free_asphere(), E.spline_init)
+    beams = S.c4_beams(n_per_lambda=npl)
+    n = S.total_rays(beams)
+    rays = E.generate(beams, n)
+    torch.cuda.synchronize()
+    adj = E.Adjoint(cs.surfaces, S.c4_params(), beams, n, fixes=ffi.FIX_ASPHERE_ROOT)
+    theta = adj.theta()
+    lam = np.linspace(S.C4_LAMBDA[0], S.C4_LAMBDA[1], S.C4_NLAMBDA)
+    target = S.c4_target_x(lam)
+
+    def best(fn):
+        out, ts = None, []
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            out = fn()
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - t0)
+        return min(ts) * 1e3, out
+
+    t_fwd, (st, stats) = best(lambda: adj.forward(theta, rays))
+    ffi.check(st, "rtb_adjoint_forward")
+    t_mer, (merit, gX, gY) = best(lambda: adj.spot_merit(target, 10.0))
+    t_bwd, grad = best(lambda: adj.backward(gX, gY))
+    d = np.zeros(len(theta))
+    d[0] = 1.0
+    t_jvp, _ = best(lambda: adj.jvp(d))
+    P = len(theta)
+    res = {"n_rays": n, "n_good": stats.n_good, "n_params": P, "merit": merit,
+           "forward_ms": t_fwd, "merit_ms": t_mer, "backward_ms": t_bwd, "jvp_ms_per_direction": t_jvp,
+           "gradient_ms": t_fwd + t_mer + t_bwd, "central_differences_ms": 2 * P * t_fwd,
+           "grad_norm": float(np.linalg.norm(grad)),
+           "how": "rtb_adjoint_forward (checkpoints at surface inputs), rtb_adjoint_spot_merit, "
+                  "rtb_adjoint_backward (dual-number passes, 4 directions each), rtb_adjoint_jvp; "
+                  "wall clock of synchronous calls, best of 3"}
+    adj.destroy()
+    del rays
+    torch.cuda.empty_cache()
+    return res
 
 
 def dgemm_tflops(n=4096, reps=5):
@@ -418,6 +473,14 @@ def main():
               "how": "rtb_plan_run: one CUDA graph (counter clear, fused mixed kernel, counter copy) per run"}
         plan.destroy()
 
+    # C4: the adjoint pair (gradient of the spot merit in 24 parameters)
+    c4 = None
+    if not args.no_c4:
+        try:
+            c4 = c4_adjoint(args.c4_rays_per_lambda)
+        except RuntimeError as e:
+            c4 = {"error": str(e)}
+
     # roofline of the headline kernel (HBM view): algorithmic bytes per launch
     # = 57 B read (X,Y,Z,cX,cY,cZ,lambda,flag) + 18 B written (X,Y,flag,
     # lost_stage) per ray + 4 B per ray counted on the frame.
@@ -506,6 +569,7 @@ def main():
                 if "per_surface" in engines and "value" in engines["per_surface"] else None,
                 "accuracy_vs_fp64": accuracy,
                 "c3_batched": c3,
+                "c4_adjoint": c4,
                 "roofline": roofline, "roofline_fp64": roofline_fp64, "cpu_baseline": cpu, "e2e": e2e,
                 "clocks": clocks,
                 "gpu_launches": args.steps * 1}
