@@ -400,8 +400,10 @@ RTB_API int rtb_plan_specialized(const rtb_plan* plan, int32_t* specialized, cha
  * compiled, one-shot fused traces of that precision and a scheme of that
  * structure (rtb_trace, rtb_trace_out, rtb_trace_host) launch it too; they
  * never compile it themselves.  RTB_OK when compiled; RTB_FAILED with the
- * reason in note (may be NULL) when NVRTC is unavailable or fails.  No
- * counterpart in the reference. */
+ * reason in note (may be NULL) when NVRTC is unavailable or fails.  With
+ * RTB_JIT_CACHE=<directory> in the environment, compiled kernels are also
+ * kept in files there and later processes load them instead of compiling.
+ * No counterpart in the reference. */
 RTB_API int rtb_specialize(const rtb_surface* surfaces, size_t n_surfaces, uint32_t fixes, int32_t precision,
                            char* note, size_t note_len);
 /* Release everything the plan holds, after its work has finished. */

@@ -22,9 +22,12 @@
 #include <dlfcn.h>
 #include <nvrtc.h>
 
+#include <unistd.h>
+
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <fstream>
 #include <map>
 #include <mutex>
 #include <string>
@@ -202,11 +205,80 @@ bool specialize_enabled() {
     return !(e && std::strcmp(e, "0") == 0);
 }
 
-// The compiled kernel for `src` (g_mu held), compiled on first use when
-// `compile`, else only when compiled before.
+// Optional on-disk cache of compiled kernels, for processes that trace the
+// same scheme structures (RTB_JIT_CACHE=<directory>; off when unset or
+// empty).  A file holds its full key -- NVRTC's version, the options, the
+// device sources and the kernel's source -- and the cubin, and is used only
+// when that key equals this build's exactly.  Files are written under a
+// temporary name and renamed into place, so that a reader never sees half a
+// file.
+static std::string cache_dir() {
+    const char* e = std::getenv("RTB_JIT_CACHE");
+    return (e && *e) ? std::string(e) : std::string();
+}
+
+static std::string cache_key(const std::string& src, bool fmad) {
+    const Nvrtc& n = nvrtc();
+    std::string k = "rtb-jit 1\nnvrtc " + std::to_string(n.major) + "." + std::to_string(n.minor) +
+                    (fmad ? " fmad\n" : " no-fmad\n");
+    for (const JitHeader& h : kJitHeaders) {
+        k += h.name;
+        k += '\n';
+        k += h.text;
+        k += '\n';
+    }
+    return k + src;
+}
+
+static std::string cache_path(const std::string& dir, const std::string& key) {
+    uint64_t h = 1469598103934665603ull;
+    for (unsigned char c : key) h = (h ^ c) * 1099511628211ull;
+    char name[40];
+    std::snprintf(name, sizeof(name), "/rtb-%016llx.cubin", (unsigned long long)h);
+    return dir + name;
+}
+
+static bool disk_load(const std::string& dir, const std::string& key, std::vector<char>& cubin) {
+    std::ifstream f(cache_path(dir, key), std::ios::binary);
+    uint64_t kn = 0, cn = 0;
+    if (!f.read(reinterpret_cast<char*>(&kn), 8) || kn != key.size()) return false;
+    std::string k(kn, '\0');
+    if (!f.read(&k[0], (std::streamsize)kn) || k != key) return false;
+    if (!f.read(reinterpret_cast<char*>(&cn), 8) || cn == 0 || cn > (1ull << 30)) return false;
+    cubin.resize(cn);
+    return (bool)f.read(cubin.data(), (std::streamsize)cn);
+}
+
+static void disk_store(const std::string& dir, const std::string& key, const std::vector<char>& cubin) {
+    const std::string path = cache_path(dir, key);
+    const std::string tmp = path + ".tmp." + std::to_string((long long)getpid());
+    {
+        std::ofstream f(tmp, std::ios::binary | std::ios::trunc);
+        const uint64_t kn = key.size(), cn = cubin.size();
+        f.write(reinterpret_cast<const char*>(&kn), 8);
+        f.write(key.data(), (std::streamsize)kn);
+        f.write(reinterpret_cast<const char*>(&cn), 8);
+        f.write(cubin.data(), (std::streamsize)cn);
+        if (!f) {
+            f.close();
+            std::remove(tmp.c_str());
+            return;
+        }
+    }
+    if (std::rename(tmp.c_str(), path.c_str()) != 0) std::remove(tmp.c_str());
+}
+
+// The compiled kernel for `src` (g_mu held): from memory, else from the
+// disk cache, else compiled (when `compile`).
 static const std::vector<char>* cubin_for(const std::string& src, bool fmad, std::string* why, bool compile) {
     auto it = g_cubins.find(src);
     if (it != g_cubins.end()) return &it->second;
+    const std::string dir = nvrtc().ok ? cache_dir() : std::string();
+    const std::string key = dir.empty() ? std::string() : cache_key(src, fmad);
+    if (!dir.empty()) {
+        std::vector<char> cubin;
+        if (disk_load(dir, key, cubin)) return &g_cubins.emplace(src, std::move(cubin)).first->second;
+    }
     if (!compile) {
         if (why) *why = "not compiled yet";
         return nullptr;
@@ -222,6 +294,7 @@ static const std::vector<char>* cubin_for(const std::string& src, bool fmad, std
         if (why) *why = "NVRTC failed: " + log.substr(0, 2000);
         return nullptr;
     }
+    if (!dir.empty()) disk_store(dir, key, cubin);
     return &g_cubins.emplace(src, std::move(cubin)).first->second;
 }
 
@@ -239,14 +312,26 @@ int scheme_kernel(const DevScheme& sch, int precision, const void** kernel, std:
         *kernel = reinterpret_cast<const void*>(it->second);
         return RTB_OK;
     }
-    const std::vector<char>* cubin = cubin_for(src, precision == RTB_MIXED, why, compile);
-    if (!cubin) return RTB_OK;
     cudaLibrary_t lib = nullptr;
     cudaKernel_t k = nullptr;
-    cudaError_t e = cudaLibraryLoadData(&lib, cubin->data(), nullptr, nullptr, 0, nullptr, nullptr, 0);
-    if (e == cudaSuccess) e = cudaLibraryGetKernel(&k, lib, precision == RTB_MIXED ? kMixedName : kFp64Name);
-    if (e != cudaSuccess) {
+    cudaError_t e = cudaSuccess;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        const std::vector<char>* cubin = cubin_for(src, precision == RTB_MIXED, why, compile);
+        if (!cubin) return RTB_OK;
+        lib = nullptr;
+        e = cudaLibraryLoadData(&lib, cubin->data(), nullptr, nullptr, 0, nullptr, nullptr, 0);
+        if (e == cudaSuccess) e = cudaLibraryGetKernel(&k, lib, precision == RTB_MIXED ? kMixedName : kFp64Name);
+        if (e == cudaSuccess) break;
         if (lib) cudaLibraryUnload(lib);
+        // a cubin that does not load (a damaged cache file): compile afresh once
+        g_cubins.erase(src);
+        const std::string dir = cache_dir();
+        if (!dir.empty()) std::remove(cache_path(dir, cache_key(src, precision == RTB_MIXED)).c_str());
+        if (!compile) break;
+    }
+    if (e != cudaSuccess) {
+        cudaGetLastError();  // handled here: not to be reported by a later launch check
+        if (!compile) return RTB_OK;  // one-shot traces run the generic kernel
         return cuda_status(e);
     }
     g_kernels.emplace(src, k);

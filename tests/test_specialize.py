@@ -48,3 +48,42 @@ def test_specialize_rejects_bad_requests():
     cs = S.to_c(S.littrow_free(), O.spline_init)
     st, _ = E.specialize(list(cs.surfaces), 0, 7)
     assert st == ffi.BAD_VALUE
+
+
+def _specialize_in_subprocess(cache_dir):
+    """rtb_specialize of C1's structure in a fresh process with the disk
+    cache at cache_dir: (status, seconds)."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = ("import sys, time; sys.path[:0] = [%r, %r]\n"
+            "import pyoracle as O\n"
+            "from rt_b200 import engine as E, ffi, schemes as S\n"
+            "cs = S.to_c(S.echelle(), O.spline_init)\n"
+            "t = time.perf_counter(); st, note = E.specialize(list(cs.surfaces), 3, ffi.MIXED)\n"
+            "print(st, time.perf_counter() - t)\n") % (root, os.path.join(root, "oracle"))
+    env = dict(os.environ, RTB_JIT_CACHE=str(cache_dir))
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env, timeout=300)
+    assert out.returncode == 0, out.stderr
+    st, dt = out.stdout.split()
+    return int(st), float(dt)
+
+
+@pytest.mark.skipif(not _nvrtc_present(), reason="libnvrtc not present")
+def test_jit_disk_cache(tmp_path):
+    """With RTB_JIT_CACHE set, the first process compiles and stores the
+    kernel, a second one loads it instead of compiling; a file whose key does
+    not match is ignored and replaced."""
+    st, t_compile = _specialize_in_subprocess(tmp_path)
+    assert st == ffi.OK
+    files = list(tmp_path.glob("rtb-*.cubin"))
+    assert len(files) == 1 and not list(tmp_path.glob("*.tmp.*"))
+    st, t_cached = _specialize_in_subprocess(tmp_path)
+    assert st == ffi.OK and t_cached < t_compile and len(list(tmp_path.glob("rtb-*.cubin"))) == 1
+    # damage the stored key: the next process compiles again and rewrites it
+    data = bytearray(files[0].read_bytes())
+    data[20] ^= 0xFF
+    files[0].write_bytes(bytes(data))
+    st, _ = _specialize_in_subprocess(tmp_path)
+    assert st == ffi.OK and files[0].read_bytes() != bytes(data)
