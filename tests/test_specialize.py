@@ -87,3 +87,29 @@ def test_jit_disk_cache(tmp_path):
     files[0].write_bytes(bytes(data))
     st, _ = _specialize_in_subprocess(tmp_path)
     assert st == ffi.OK and files[0].read_bytes() != bytes(data)
+
+
+@pytest.mark.skipif(not _nvrtc_present(), reason="libnvrtc not present")
+def test_kernels_are_shared_by_structure(tmp_path):
+    """A kernel is specialised to a scheme's structure, not to its numbers:
+    C0 with another collimator curvature and camera distance compiles to the
+    same kernel (one cache file), C0 with an asphere camera to another."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = ("import sys; sys.path[:0] = [%r, %r]\n"
+            "import pyoracle as O\n"
+            "from rt_b200 import engine as E, ffi, schemes as S\n"
+            "a = S.littrow_free()\n"
+            "b = S.littrow_free(); b[0].params = (-1 / 750.0, -1.0, 0); b[2].distance = (1.0, 2.0, 3.0)\n"
+            "c = S.c0_asphere_camera()\n"
+            "for specs in (a, b, c):\n"
+            "    st, note = E.specialize(list(S.to_c(specs, O.spline_init).surfaces), 0, ffi.FP64)\n"
+            "    assert st == ffi.OK, note\n"
+            "    print(len([f for f in __import__('os').listdir(%r) if f.endswith('.cubin')]))\n"
+            ) % (root, os.path.join(root, "oracle"), str(tmp_path))
+    env = dict(os.environ, RTB_JIT_CACHE=str(tmp_path))
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env, timeout=300)
+    assert out.returncode == 0, out.stderr
+    assert out.stdout.split() == ["1", "1", "2"]
