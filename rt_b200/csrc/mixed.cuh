@@ -3,20 +3,26 @@
 // Same per-ray algorithm as the plain engine (ray_fp64.cuh) with the
 // precision of each step chosen for cost against its effect on the CCD
 // position:
-//   * ray state, transforms, intersection roots (quadratic in a
-//     cancellation-safe form, Newton on the asphere sag to 1e-12 mm in at most
-//     six steps from the base-conic root, the toric Steffensen iteration),
-//     the grating equation and the detector coordinate: FP64, contracted to FMA;
+//   * ray state, transforms, intersection roots (the conic quadratic in a
+//     cancellation-safe form; Newton for the even asphere from the base-conic
+//     root and for the toric from the plane point, until a step falls below
+//     1e-6 mm, the root then good to ~1e-14 mm), the grating equation and the
+//     detector coordinate: FP64, contracted to FMA;
 //   * every division and square root: a MUFU seed (rcp/rsqrt.approx.f64)
 //     refined by Newton steps in FP64 instead of the IEEE FP64 division and
-//     square root sequences of the plain engine;
+//     square root sequences of the plain engine; the inverse of a Newton
+//     derivative from the seed alone; 1/c and 1/(grating constant) from the
+//     host;
 //   * surface normals and their polynomial terms (the sqrt/div-heavy
-//     derivatives of conic_derivs / toric_derivs, surface.cu:45-94): FP32,
-//     promoted to FP64 before they act on the direction cosines.  Their
-//     transverse components are small, so the FP32 rounding moves a direction
-//     by ~1e-9 rad.
+//     derivatives of conic_derivs / toric_derivs, surface.cu:45-94): FP32
+//     (from FP32 copies of the surface constants), promoted to FP64 before
+//     they act on the direction cosines.  Their transverse components are
+//     small, so the FP32 rounding moves a direction by ~1e-9 rad.
 // Compiled with FMA contraction.  Accuracy is measured against the FP64
 // oracle (median, p99.9 and max CCD error in um; target p99.9 <= 0.05 um).
+// The surface code reads each surface's structure through a shape policy
+// (shape.cuh): at run time in k_fused_mixed, fixed at compile time in the
+// copies compiled for one scheme (jit.cpp).
 #pragma once
 
 #include "trace_common.cuh"
