@@ -292,15 +292,20 @@ RTB_API int rtb_trace_out(const rtb_surface* surfaces, size_t n_surfaces, const 
 
 /* rtb_trace_out for callers that cannot allocate memory (no counterpart in
  * the reference).  Runs the fused kernel (opts->engine must be
- * RTB_ENGINE_FUSED) with its scratch -- prepared scheme, tables, beam table,
- * loss counters -- in a file-scope device array of RTB_NOALLOC_SCRATCH_BYTES
- * per device and host-side staging in file-scope host arrays: no cudaMalloc,
+ * RTB_ENGINE_FUSED; block_size and rays_per_thread as rtb_trace_out takes
+ * them) with its scratch -- prepared scheme, tables, beam table, loss
+ * counters -- in a file-scope device array of RTB_NOALLOC_SCRATCH_BYTES per
+ * device and host-side staging in file-scope host arrays: no cudaMalloc,
  * cudaFree, pool or heap allocation.  Requests that do not fit (more than
- * RTB_NOALLOC_MAX_KNOTS table values, or too many beams x stages for the
- * counters) return RTB_BAD_VALUE before any work is queued.  The first call on
- * a device looks up the array's address with that device current; make it
- * before any stream capture.  All calls share the array: calls that overlap
- * on the GPU race.  Synchronous on `stream`. */
+ * RTB_NOALLOC_MAX_KNOTS table values, too many beams x stages for the
+ * counters, or more shared memory than a block may have) return
+ * RTB_BAD_VALUE before any work is queued; with the largest tables the array
+ * holds the counters of 1,100 beams of a 32-surface scheme.  The first call
+ * on a device looks up the array's address with that device current; make it
+ * before any stream capture.  A NULL stream (the library's own) is valid only
+ * on the device the library was first used on.  Calls run one at a time and
+ * each returns with `stream` synchronised; all calls share the array, so
+ * other GPU work that wrote it during a call would race with that call. */
 #define RTB_NOALLOC_SCRATCH_BYTES 1048576
 #define RTB_NOALLOC_MAX_KNOTS 8192
 RTB_API int rtb_trace_out_noalloc(const rtb_surface* surfaces, size_t n_surfaces, const rtb_beam* beams,

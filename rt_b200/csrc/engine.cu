@@ -106,24 +106,36 @@ int surface_from_params(int cls, const double* params, DevSurface& s) {
     return RTB_OK;
 }
 
-// Append a table to the knot buffer: [x(n) y(n) y2(n)], or [0, y0] for a
-// single value.
-int add_table(const rtb_table* t, std::vector<double>& knots, int32_t& off, int32_t& cnt) {
+bool KnotBuf::append(const double* v, size_t k) {
+    if (vec) {
+        vec->insert(vec->end(), v, v + k);
+        return true;
+    }
+    if (n + k > cap) return false;
+    for (size_t i = 0; i < k; ++i) fixed[n + i] = v[i];
+    n += k;
+    return true;
+}
+
+// Append a table to the knot buffer: [x(n) y(n) y2(n)], or [0, y0, 0] for a
+// single value.  RTB_BAD_VALUE for a malformed table or a full fixed buffer.
+int add_table(const rtb_table* t, KnotBuf& knots, int32_t& off, int32_t& cnt) {
     if (!t || t->n == 0 || !t->y) return RTB_BAD_VALUE;
     off = (int32_t)knots.size();
     if (t->n == 1) {
         cnt = 1;
-        knots.push_back(0.0);
-        knots.push_back(t->y[0]);
-        knots.push_back(0.0);
-        return RTB_OK;
+        const double v[3] = {0.0, t->y[0], 0.0};
+        return knots.append(v, 3) ? RTB_OK : RTB_BAD_VALUE;
     }
     if (t->n < 4 || t->n > RTB_MAX_KNOTS || !t->x || !t->y2) return RTB_BAD_VALUE;
     cnt = (int32_t)t->n;
-    knots.insert(knots.end(), t->x, t->x + t->n);
-    knots.insert(knots.end(), t->y, t->y + t->n);
-    knots.insert(knots.end(), t->y2, t->y2 + t->n);
+    if (!knots.append(t->x, t->n) || !knots.append(t->y, t->n) || !knots.append(t->y2, t->n)) return RTB_BAD_VALUE;
     return RTB_OK;
+}
+
+int add_table(const rtb_table* t, std::vector<double>& knots, int32_t& off, int32_t& cnt) {
+    KnotBuf kb(knots);
+    return add_table(t, kb, off, cnt);
 }
 
 // The sag range of an even asphere over its circular pass aperture, for the
@@ -183,7 +195,7 @@ void mixed_constants(DevSurface& s) {
     }
 }
 
-int prepare_surface(const rtb_surface& in, DevSurface& s, std::vector<double>& knots) {
+int prepare_surface(const rtb_surface& in, DevSurface& s, KnotBuf& knots) {
     bool non_aux = in.type != RTB_AUX_TYPE;
     int st = surface_from_params(non_aux ? in.cls : RTB_AUX_CLASS, in.params, s);
     if (st != RTB_OK) return st;
@@ -220,17 +232,16 @@ int prepare_surface(const rtb_surface& in, DevSurface& s, std::vector<double>& k
     return RTB_OK;
 }
 
-int prepare_scheme(const rtb_surface* surf, size_t n, uint32_t fixes, int renorm_lost, PreparedScheme& out) {
+int prepare_scheme_into(const rtb_surface* surf, size_t n, uint32_t fixes, int renorm_lost, DevScheme& sch,
+                        KnotBuf& knots) {
     if (!surf || n == 0 || n > RTB_MAX_SURFACES) return RTB_BAD_VALUE;
-    std::memset(&out.sch, 0, sizeof(out.sch));
-    out.knots.clear();
-    out.knots.push_back(0.0);  // offset 0: a harmless single value for unused tables
-    out.knots.push_back(1.0);
-    out.knots.push_back(0.0);
+    std::memset(&sch, 0, sizeof(sch));
+    const double unit[3] = {0.0, 1.0, 0.0};  // offset 0: a harmless single value for unused tables
+    if (!knots.append(unit, 3)) return RTB_BAD_VALUE;
     int ng = 0, nonaux = 0;
     for (size_t k = 0; k < n; ++k) {
-        DevSurface& s = out.sch.s[k];
-        int st = prepare_surface(surf[k], s, out.knots);
+        DevSurface& s = sch.s[k];
+        int st = prepare_surface(surf[k], s, knots);
         if (st != RTB_OK) return st;
         s.grating_index = (s.type == RTB_GRATING) ? ng++ : -1;
         if (s.non_aux) ++nonaux;
@@ -238,22 +249,23 @@ int prepare_scheme(const rtb_surface* surf, size_t n, uint32_t fixes, int renorm
     }
     if (ng > RTB_MAX_GRATINGS) return RTB_BAD_VALUE;
     for (size_t k = 0; k < n; ++k) {
-        int cnt = out.sch.s[k].non_aux ? 1 : 0;
-        for (size_t j = k + 1; j < n; ++j) cnt += 1 + (out.sch.s[j].non_aux ? 1 : 0);
-        out.sch.s[k].renorm_after = cnt;
+        int cnt = sch.s[k].non_aux ? 1 : 0;
+        for (size_t j = k + 1; j < n; ++j) cnt += 1 + (sch.s[j].non_aux ? 1 : 0);
+        sch.s[k].renorm_after = cnt;
     }
+    const double* kn = knots.data();
     // identical tables share one copy (a lens's glass is the index after its
     // front surface and before its back surface), and a table on a uniform
     // grid records its inverse spacing for the mixed engine's direct lookup
     auto same = [&](int32_t o1, int32_t o2, int32_t cnt) {
         const int32_t len = (cnt == 1) ? 3 : 3 * cnt;
         for (int32_t i = 0; i < len; ++i)
-            if (out.knots[o1 + i] != out.knots[o2 + i]) return false;
+            if (kn[o1 + i] != kn[o2 + i]) return false;
         return true;
     };
     auto inv_spacing = [&](int32_t off, int32_t cnt) {
         if (cnt < 2) return 0.0;
-        const double* x = out.knots.data() + off;
+        const double* x = kn + off;
         const double h = (x[cnt - 1] - x[0]) / (cnt - 1);
         if (!(h > 0)) return 0.0;
         for (int32_t i = 0; i < cnt; ++i)
@@ -261,12 +273,12 @@ int prepare_scheme(const rtb_surface* surf, size_t n, uint32_t fixes, int renorm
         return 1.0 / h;
     };
     for (size_t k = 0; k < n; ++k) {
-        DevSurface& s = out.sch.s[k];
+        DevSurface& s = sch.s[k];
         int32_t* offs[2] = {&s.n1_off, &s.n2_off};
         int32_t cnts[2] = {s.n1_n, s.n2_n};
         for (int t = 0; t < 2; ++t) {
             for (size_t j = 0; j <= k; ++j) {
-                const DevSurface& e = out.sch.s[j];
+                const DevSurface& e = sch.s[j];
                 const int32_t eo[2] = {e.n1_off, e.n2_off}, ec[2] = {e.n1_n, e.n2_n};
                 bool done = false;
                 for (int u = 0; u < 2 && !done; ++u) {
@@ -282,11 +294,17 @@ int prepare_scheme(const rtb_surface* surf, size_t n, uint32_t fixes, int renorm
         s.n1_invh = inv_spacing(s.n1_off, s.n1_n);
         s.n2_invh = inv_spacing(s.n2_off, s.n2_n);
     }
-    out.sch.n_surfaces = (int32_t)n;
-    out.sch.n_knots = (int32_t)out.knots.size();
-    out.sch.fixes = fixes;
-    out.sch.renorm_lost = renorm_lost;
+    sch.n_surfaces = (int32_t)n;
+    sch.n_knots = (int32_t)knots.size();
+    sch.fixes = fixes;
+    sch.renorm_lost = renorm_lost;
     return RTB_OK;
+}
+
+int prepare_scheme(const rtb_surface* surf, size_t n, uint32_t fixes, int renorm_lost, PreparedScheme& out) {
+    out.knots.clear();
+    KnotBuf kb(out.knots);
+    return prepare_scheme_into(surf, n, fixes, renorm_lost, out.sch, kb);
 }
 
 // Natural cubic spline second derivatives: the sequential algorithm of

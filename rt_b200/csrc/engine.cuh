@@ -31,9 +31,29 @@ struct PreparedScheme {
     const void* scheme_kernel = nullptr;
 };
 
-int prepare_surface(const rtb_surface& in, DevSurface& out, std::vector<double>& knots);
+// The knot buffer a scheme's tables are packed into: a growing vector, or a
+// fixed array of `cap` doubles (the no-allocation trace), which refuses what
+// does not fit.
+struct KnotBuf {
+    std::vector<double>* vec = nullptr;
+    double* fixed = nullptr;
+    size_t cap = 0, n = 0;
+    explicit KnotBuf(std::vector<double>& v) : vec(&v) {}
+    KnotBuf(double* p, size_t capacity) : fixed(p), cap(capacity) {}
+    bool append(const double* v, size_t k);
+    size_t size() const { return vec ? vec->size() : n; }
+    const double* data() const { return vec ? vec->data() : fixed; }
+};
+
+int prepare_surface(const rtb_surface& in, DevSurface& out, KnotBuf& knots);
+// Every launch of a scheme reads what this prepares: the surfaces' constants,
+// the packed tables (identical tables sharing one copy, the inverse spacing
+// of tables on a uniform grid) and the counts that follow from the sequence.
+int prepare_scheme_into(const rtb_surface* s, size_t n, uint32_t fixes, int renorm_lost, DevScheme& sch,
+                        KnotBuf& knots);
 int prepare_scheme(const rtb_surface* s, size_t n, uint32_t fixes, int renorm_lost, PreparedScheme& out);
 int surface_from_params(int cls, const double* params, DevSurface& s);
+int add_table(const rtb_table* t, KnotBuf& knots, int32_t& off, int32_t& cnt);
 int add_table(const rtb_table* t, std::vector<double>& knots, int32_t& off, int32_t& cnt);
 // Sag range of an even asphere over its circular aperture (DevSurface::sag_*).
 void asphere_sag_bounds(DevSurface& s);

@@ -13,16 +13,18 @@
 //
 // Limits: RTB_NOALLOC_SCRATCH_BYTES (1 MiB) of device scratch per device,
 // which holds the scheme (<= RTB_MAX_SURFACES surfaces), up to
-// RTB_NOALLOC_MAX_KNOTS table values, and n_beams * (3 * n_surfaces + 1) loss
-// counters plus the beam table; larger requests return RTB_BAD_VALUE before
-// any work is queued.
+// RTB_NOALLOC_MAX_KNOTS table values, the beam table and n_beams *
+// (3 * n_surfaces + 1) loss counters; requests that do not fit, or whose
+// launch needs more shared memory than a block may have, return
+// RTB_BAD_VALUE before any work is queued.  With the largest tables the
+// counters leave room for 1,100 beams of a 32-surface scheme.
 //
 // The array is set up once per device, on the first call made with that
-// device current (cudaGetSymbolAddress); that first call should come before any
-// stream capture.  Every call on a device shares the array and leaves its
-// contents behind; each call clears the counters it uses.  Calls that overlap
-// on the GPU (concurrent streams, or a second call issued from another thread
-// before the first has returned) race on the array.
+// device current (cudaGetSymbolAddress).  Every call on a device shares the
+// array and leaves its contents behind; each call clears the counters it
+// uses.  Calls run one at a time (the engine lock) and each returns with its
+// stream synchronised, so calls of this library do not overlap on the GPU;
+// other work that writes the array while a call runs would race with it.
 #include <cstring>
 
 #include "engine.cuh"
@@ -69,90 +71,6 @@ int scratch_address(void** out) {
     return RTB_OK;
 }
 
-// A table appended to a fixed buffer, laid out as add_table() lays it out.
-int put_table(const rtb_table* t, double* knots, size_t cap, size_t& used, int32_t& off, int32_t& cnt) {
-    if (!t || t->n == 0 || !t->y) return RTB_BAD_VALUE;
-    size_t need = (t->n == 1) ? 3 : 3 * t->n;
-    if (t->n != 1 && (t->n < 4 || t->n > RTB_MAX_KNOTS || !t->x || !t->y2)) return RTB_BAD_VALUE;
-    if (used + need > cap) return RTB_BAD_VALUE;
-    off = (int32_t)used;
-    if (t->n == 1) {
-        cnt = 1;
-        knots[used] = 0.0;
-        knots[used + 1] = t->y[0];
-        knots[used + 2] = 0.0;
-    } else {
-        cnt = (int32_t)t->n;
-        std::memcpy(knots + used, t->x, t->n * sizeof(double));
-        std::memcpy(knots + used + t->n, t->y, t->n * sizeof(double));
-        std::memcpy(knots + used + 2 * t->n, t->y2, t->n * sizeof(double));
-    }
-    used += need;
-    return RTB_OK;
-}
-
-// The scheme preparation of prepare_scheme() into fixed buffers.
-int prepare_fixed(const rtb_surface* surf, size_t n, uint32_t fixes, int renorm_lost, DevScheme& out, double* knots,
-                  size_t cap, size_t& n_knots) {
-    if (!surf || n == 0 || n > RTB_MAX_SURFACES) return RTB_BAD_VALUE;
-    std::memset(&out, 0, sizeof(out));
-    n_knots = 0;
-    int32_t o, c;
-    rtb_table unit = {1, nullptr, nullptr, nullptr};
-    double one = 1.0;
-    unit.y = &one;
-    if (put_table(&unit, knots, cap, n_knots, o, c) != RTB_OK) return RTB_BAD_VALUE;
-    int ng = 0, nonaux = 0;
-    for (size_t k = 0; k < n; ++k) {
-        const rtb_surface& in = surf[k];
-        DevSurface& s = out.s[k];
-        bool non_aux = in.type != RTB_AUX_TYPE;
-        int st = surface_from_params(non_aux ? in.cls : RTB_AUX_CLASS, in.params, s);
-        if (st != RTB_OK) return st;
-        if (in.type < RTB_MIRROR || in.type > RTB_AUX_TYPE) return RTB_BAD_VALUE;
-        if (in.shape != RTB_CIRCLE && in.shape != RTB_RECTANGLE) return RTB_BAD_VALUE;
-        if (in.type == RTB_GRATING && in.grating_type != RTB_REFLECTIVE && in.grating_type != RTB_TRANSPARENT)
-            return RTB_BAD_VALUE;
-        s.cls = in.cls;
-        s.type = in.type;
-        s.shape = in.shape;
-        s.gr_type = in.grating_type;
-        s.non_aux = non_aux;
-        if (!non_aux) s.kind = IS_NONE;
-        s.order = in.order;
-        s.gr_const = in.gr_const;
-        double ang[3];
-        for (int i = 0; i < 3; ++i) ang[i] = scheme_angle_rad(in.angles_deg[i]);
-        transform_constants(ang, in.distance, s);
-        for (int i = 0; i < 2; ++i) {
-            s.size[i] = in.size[i];
-            s.center[i] = in.center[i];
-        }
-        mixed_constants(s);
-        s.n1_off = s.n2_off = 0;
-        s.n1_n = s.n2_n = 1;
-        if (in.type == RTB_LENS || in.type == RTB_GRATING) {
-            if ((st = put_table(&in.n2, knots, cap, n_knots, s.n2_off, s.n2_n)) != RTB_OK) return st;
-            if (in.type == RTB_LENS || in.grating_type == RTB_TRANSPARENT)
-                if ((st = put_table(&in.n1, knots, cap, n_knots, s.n1_off, s.n1_n)) != RTB_OK) return st;
-        }
-        s.grating_index = (s.type == RTB_GRATING) ? ng++ : -1;
-        if (s.non_aux) ++nonaux;
-        s.surfaces_upto = nonaux;
-    }
-    if (ng > RTB_MAX_GRATINGS) return RTB_BAD_VALUE;
-    for (size_t k = 0; k < n; ++k) {
-        int cnt = out.s[k].non_aux ? 1 : 0;
-        for (size_t j = k + 1; j < n; ++j) cnt += 1 + (out.s[j].non_aux ? 1 : 0);
-        out.s[k].renorm_after = cnt;
-    }
-    out.n_surfaces = (int32_t)n;
-    out.n_knots = (int32_t)n_knots;
-    out.fixes = fixes;
-    out.renorm_lost = renorm_lost;
-    return RTB_OK;
-}
-
 }  // namespace
 
 }  // namespace rtb
@@ -166,27 +84,36 @@ extern "C" RTB_API int rtb_trace_out_noalloc(const rtb_surface* surfaces, size_t
     if (opts->engine != RTB_ENGINE_FUSED) return RTB_BAD_VALUE;
     if (opts->precision != RTB_FP64 && opts->precision != RTB_MIXED) return RTB_BAD_VALUE;
     if (!beams || n_beams == 0 || n_surfaces == 0 || n_surfaces > RTB_MAX_SURFACES) return RTB_BAD_VALUE;
+    const bool mixed = opts->precision == RTB_MIXED;
+    // the launch configuration rtb_trace_out accepts (launch_trace)
+    const int threads = (opts->block_size > 0) ? opts->block_size : 256;
+    if (threads != 128 && threads != 256 && !(mixed && threads == 512)) return RTB_BAD_VALUE;
+    const int rpt = (opts->rays_per_thread > 0) ? opts->rays_per_thread : kDefaultRpt;
+    if (rpt < 1 || rpt > 64) return RTB_BAD_VALUE;
     const size_t ns1 = 3 * n_surfaces + 1;
-    // size checks before anything is written
-    {
-        Layout worst = layout(RTB_NOALLOC_MAX_KNOTS, n_beams, n_beams * ns1);
-        if (worst.total > RTB_NOALLOC_SCRATCH_BYTES) return RTB_BAD_VALUE;
-    }
+    if (layout(0, n_beams, n_beams * ns1).total > RTB_NOALLOC_SCRATCH_BYTES) return RTB_BAD_VALUE;
     std::lock_guard<std::mutex> lock(engine().mu);
     int st = ensure_init();
     if (st != RTB_OK) return st;
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) return RTB_FAILED;
+    // the library's own stream belongs to the device it was set up on
+    if (!stream && dev != engine().device) return RTB_BAD_VALUE;
     cudaStream_t s = stream ? (cudaStream_t)stream : engine().stream;
-    void* base = nullptr;
-    if ((st = scratch_address(&base)) != RTB_OK) return st;
 
-    Layout l0 = layout(RTB_NOALLOC_MAX_KNOTS, n_beams, n_beams * ns1);
-    double* knots_h = reinterpret_cast<double*>(h_stage + l0.knots);
-    size_t n_knots = 0;
-    if ((st = prepare_fixed(surfaces, n_surfaces, opts->fixes, opts->renormalize_lost, h_scheme, knots_h,
-                            RTB_NOALLOC_MAX_KNOTS, n_knots)) != RTB_OK)
+    // everything is prepared and checked in the host staging before the
+    // first copy is queued: the scheme by the same code as every other trace
+    // (prepare_scheme_into), its tables packed at their final offset
+    const size_t knots_at = layout(0, 0, 0).knots;
+    KnotBuf kb(reinterpret_cast<double*>(h_stage + knots_at), RTB_NOALLOC_MAX_KNOTS);
+    if ((st = prepare_scheme_into(surfaces, n_surfaces, opts->fixes, opts->renormalize_lost, h_scheme, kb)) !=
+        RTB_OK)
         return st;
+    const size_t n_knots = kb.size();
     const Layout l = layout(n_knots, n_beams, n_beams * ns1);
-    // the packed tables move to their final offset (l.knots == l0.knots)
+    if (l.total > RTB_NOALLOC_SCRATCH_BYTES) return RTB_BAD_VALUE;
+    const size_t smem = fused_smem_bytes((int)n_knots);
+    if (smem > (size_t)engine().max_smem_optin) return RTB_BAD_VALUE;
     std::memcpy(h_stage, &h_scheme, sizeof(DevScheme));
     DevBeam* beams_h = reinterpret_cast<DevBeam*>(h_stage + l.beams);
     uint64_t prev_end = 0;
@@ -201,18 +128,17 @@ extern "C" RTB_API int rtb_trace_out_noalloc(const rtb_surface* surfaces, size_t
         beams_h[b].n_orders = bi.n_orders;
         for (int g = 0; g < RTB_MAX_GRATINGS; ++g) beams_h[b].orders[g] = bi.orders[g];
     }
-    unsigned char* d = static_cast<unsigned char*>(base);
-    RTB_CUDA_TRY(cudaMemcpyAsync(d, h_stage, l.counts, cudaMemcpyHostToDevice, s));
-    RTB_CUDA_TRY(cudaMemsetAsync(d + l.counts, 0, l.total - l.counts, s));
-
-    const bool mixed = opts->precision == RTB_MIXED;
-    size_t smem = fused_smem_bytes((int)n_knots);
-    if (smem > (size_t)engine().max_smem_optin) return RTB_BAD_VALUE;
     auto kern = mixed ? k_fused_mixed : k_fused_fp64;
     RTB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
-    RTB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem));
+    RTB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
     if (per_sm < 1) per_sm = 1;
+    void* base = nullptr;
+    if ((st = scratch_address(&base)) != RTB_OK) return st;
+
+    unsigned char* d = static_cast<unsigned char*>(base);
+    RTB_CUDA_TRY(cudaMemcpyAsync(d, h_stage, l.counts, cudaMemcpyHostToDevice, s));
+    RTB_CUDA_TRY(cudaMemsetAsync(d + l.counts, 0, l.total - l.counts, s));
     FrameArgs frame;
     std::memset(&frame, 0, sizeof(frame));
     if (opts->ccd && opts->counts) {
@@ -236,10 +162,10 @@ extern "C" RTB_API int rtb_trace_out_noalloc(const rtb_surface* surfaces, size_t
     unsigned* err_d = reinterpret_cast<unsigned*>(d + l.err);
     // the tile counter shares the zeroed 256-byte error slot
     unsigned long long* tiles_d = reinterpret_cast<unsigned long long*>(d + l.err + 64);
-    kern<<<grid_for(in->n, 256 * kDefaultRpt, per_sm), 256, smem, s>>>(
+    kern<<<grid_for(in->n, threads * rpt, per_sm), threads, smem, s>>>(
         reinterpret_cast<const DevScheme*>(d), reinterpret_cast<const double*>(d + l.knots),
         reinterpret_cast<const DevBeam*>(d + l.beams), (int)n_beams, ri, ro, counts_d, err_d,
-        opts->state_out ? 1 : 0, frame, TileSched{tiles_d, kDefaultRpt});
+        opts->state_out ? 1 : 0, frame, TileSched{tiles_d, rpt, nullptr, 0});
     RTB_CUDA_TRY(cudaGetLastError());
     unsigned long long* counts_h = reinterpret_cast<unsigned long long*>(h_stage + l.counts);
     unsigned err = 0;

@@ -6,7 +6,8 @@ memory budget where no allocator may be called.  rtb_trace_out_noalloc keeps
 the fused kernel's scratch in a fixed 1 MiB device array instead.  These GPU
 tests call it through the C ABI and check that two calls in a row give what
 rtb_trace_out gives on the same inputs (bit for bit: the same kernel runs on
-the same rays), and that requests beyond its limits are refused.  The file
+the same rays, with the scheme prepared by the same code), and that requests
+beyond its limits are refused.  The file
 is named so that pytest collects it last.
 """
 import ctypes as C
@@ -57,6 +58,9 @@ def test_noalloc_matches_trace_out_on_two_calls(precision):
     cases = [
         (S.echelle(), S.c1_beams(n_per_lambda=120)[:6], 3),      # several beams with per-beam orders
         (S.littrow_free(), S.c0_beams(n_per_lambda=3000), 0),    # smaller scheme: leftovers must not leak
+        # wavelengths on the knots of the lens glass's uniform grid (0.35 + 0.01 i):
+        # the table lookups of both entry points must pick the same intervals
+        (S.echelle(), [S.make_beam(0, 200, 51, S.C1_RADIUS, (0.40, 0.90), 7, orders=(40, 1))], 3),
     ]
     for specs, beams, fixes in cases:
         cs = S.to_c(specs, E.spline_init)
@@ -65,11 +69,12 @@ def test_noalloc_matches_trace_out_on_two_calls(precision):
         out_ref, out_na = E.DeviceRays(n), E.DeviceRays(n)
         o = E.opts(engine=ffi.ENGINE_FUSED, precision=precision, fixes=fixes)
         st_r, stats_r = _call(L.rtb_trace_out, cs.surfaces, beams, o, rin, out_ref)
-        st_n, stats_n = _call(L.rtb_trace_out_noalloc, cs.surfaces, beams, o, rin, out_na)
-        assert st_r == st_n == ffi.OK
-        assert (stats_n.ray_surfaces, stats_n.n_good, stats_n.failed_beam, stats_n.failed_stage) == \
-            (stats_r.ray_surfaces, stats_r.n_good, stats_r.failed_beam, stats_r.failed_stage)
-        _same(out_na, out_ref)
+        for _ in range(2):  # the second call must not see the first one's scratch
+            st_n, stats_n = _call(L.rtb_trace_out_noalloc, cs.surfaces, beams, o, rin, out_na)
+            assert st_r == st_n == ffi.OK
+            assert (stats_n.ray_surfaces, stats_n.n_good, stats_n.failed_beam, stats_n.failed_stage) == \
+                (stats_r.ray_surfaces, stats_r.n_good, stats_r.failed_beam, stats_r.failed_stage)
+            _same(out_na, out_ref)
 
 
 def test_noalloc_rejects_requests_beyond_its_limit():
@@ -85,3 +90,9 @@ def test_noalloc_rejects_requests_beyond_its_limit():
     o = E.opts(engine=ffi.ENGINE_PER_SURFACE)
     st, _ = _call(L.rtb_trace_out_noalloc, cs.surfaces, beams[:1], o, rin, out)
     assert st == ffi.BAD_VALUE
+    # launch configurations rtb_trace_out refuses are refused here too
+    for block, rpt in ((96, 2), (512, 2), (256, 65)):
+        o = E.opts(engine=ffi.ENGINE_FUSED, precision=ffi.FP64)
+        o.block_size, o.rays_per_thread = block, rpt
+        st, _ = _call(L.rtb_trace_out_noalloc, cs.surfaces, beams[:1], o, rin, out)
+        assert st == ffi.BAD_VALUE, (block, rpt)
