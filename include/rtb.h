@@ -56,7 +56,14 @@ enum { RTB_REFLECTIVE = 0, RTB_TRANSPARENT = 1 };                              /
 
 /* ---- engine options ----------------------------------------------------- */
 enum { RTB_ENGINE_PER_SURFACE = 0, RTB_ENGINE_FUSED = 1 };
-enum { RTB_FP64 = 0, RTB_MIXED = 1 };
+/* RTB_FP64: the plain engine, IEEE FP64 (bit-exact with the reference's
+ * arithmetic).  RTB_MIXED: FP64 ray state, FP32 surface normals, MUFU-seeded
+ * divisions and square roots.  RTB_MIXED32: FP32 ray state and bulk
+ * arithmetic (transforms, normals, reflection, refraction, renormalisation),
+ * FP64 for the intersection roots, the grating equation and the detector
+ * coordinate.  Both mixed engines are fused only; neither has a counterpart
+ * in the reference, whose only scalar type is FP64 (num_defs.h:14). */
+enum { RTB_FP64 = 0, RTB_MIXED = 1, RTB_MIXED32 = 2 };
 /* Quirk fixes: 0 reproduces the reference; each bit selects the correct form. */
 enum {
     RTB_FIX_TORIC_SIGN = 1,   /* iter_toric's 1+k1c^2Y^2 becomes 1-k1c^2Y^2 (cuda_engine/rt_cuda_engine_surface.cu:350) */
@@ -142,10 +149,16 @@ typedef struct rtb_ccd {
  * arrays rtb_plan_rays returns do not reach them; 62 bytes more per ray);
  * RTB_ORDER_INDEX takes the rays in index order from those arrays. */
 enum { RTB_ORDER_COHERENT = 0, RTB_ORDER_INDEX = 1 };
+/* Where a plan's fused kernel stores each ray's results: at the ray's index
+ * (RTB_OUT_INDEX), or at its tracing slot (RTB_OUT_SLOT), so that the stores
+ * of a warp are coalesced; rtb_plan_order gives the slot -> index map.  Frame
+ * counts and statistics do not depend on it.  Traces other than plans store
+ * at the index. */
+enum { RTB_OUT_INDEX = 0, RTB_OUT_SLOT = 1 };
 
 typedef struct rtb_trace_opts {
     int32_t engine;                 /* RTB_ENGINE_PER_SURFACE / RTB_ENGINE_FUSED */
-    int32_t precision;              /* RTB_FP64 / RTB_MIXED */
+    int32_t precision;              /* RTB_FP64 / RTB_MIXED / RTB_MIXED32 */
     uint32_t fixes;                 /* RTB_FIX_* bits */
     int32_t renormalize_lost;       /* apply the reference's trailing Normalize calls to lost rays (beam.cpp:527-571) */
     int32_t block_size;             /* 0: tuned default */
@@ -155,6 +168,8 @@ typedef struct rtb_trace_opts {
     const rtb_ccd* ccd;             /* optional: add good rays to frame counts (see rtb_ccd_frame) */
     uint32_t* counts;               /* device, ccd->xdim*ccd->ydim pixels; not cleared */
     uint64_t* n_outside;            /* device, may be NULL */
+    int32_t out_order;              /* plans: RTB_OUT_INDEX (0) or RTB_OUT_SLOT */
+    int32_t reserved;
 } rtb_trace_opts;
 
 /* Per-call statistics of a trace. */
@@ -384,6 +399,10 @@ RTB_API int rtb_plan_counts(rtb_plan* plan, uint64_t* counts, size_t capacity, s
  * last run (X, Y, flag, lost_stage; every state array with opts->state_out;
  * out->lambda is in->lambda).  Either may be NULL. */
 RTB_API int rtb_plan_rays(const rtb_plan* plan, rtb_rays* in, rtb_rays* out);
+/* The plan's tracing order (device, n_rays entries: slot -> ray index), or
+ * NULL for a plan in index order (slot == index).  With RTB_OUT_SLOT, output
+ * slot s holds the results of ray order[s].  No reference counterpart. */
+RTB_API int rtb_plan_order(const rtb_plan* plan, const uint32_t** order);
 /* Time block_size {128, 256, 512 (RTB_MIXED only)} x rays_per_thread
  * {1, 2, 4, 8}: one untimed run, then `reps` runs, each configuration into a
  * private frame so the plan's frame is untouched.  The fastest becomes the

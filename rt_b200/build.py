@@ -41,6 +41,8 @@ JIT_HEADERS = {
     "trace_common.cuh": os.path.join(CSRC, "trace_common.cuh"),
     "ray_fp64.cuh": os.path.join(CSRC, "ray_fp64.cuh"),
     "mixed.cuh": os.path.join(CSRC, "mixed.cuh"),
+    "mixed32.cuh": os.path.join(CSRC, "mixed32.cuh"),
+    "rowpipe.cuh": os.path.join(CSRC, "rowpipe.cuh"),
     "shape.cuh": os.path.join(CSRC, "shape.cuh"),
     "fused_fp64.cuh": os.path.join(CSRC, "fused_fp64.cuh"),
     "../../include/rtb.h": os.path.join(HERE, "..", "include", "rtb.h"),

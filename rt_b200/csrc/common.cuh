@@ -23,7 +23,9 @@ constexpr unsigned K_ITER_MAX = 100000;
 enum IsectKind : int32_t { IS_NONE = 0, IS_PLANE, IS_PARABOLOID, IS_CONIC, IS_ITER_POLY, IS_ITER_CONIC, IS_TORIC };
 
 // Error bits a kernel raises for the host (the reference throws instead).
-enum DevError : uint32_t { DEV_ERR_OUT_OF_RANGE = 1u, DEV_ERR_BAD_VALUE = 2u };
+// DEV_ERR_TIMEOUT: a bounded wait of a kernel ran out (the staged copy of a
+// ray row never completed); the call fails with RTB_FAILED.
+enum DevError : uint32_t { DEV_ERR_OUT_OF_RANGE = 1u, DEV_ERR_BAD_VALUE = 2u, DEV_ERR_TIMEOUT = 4u };
 
 // One surface as the kernels consume it: everything the reference's host
 // code derives before a kernel launch (copy_surf_params, the transform's
@@ -60,6 +62,15 @@ struct DevSurface {
     float f_c, f_k1, f_cR, f_inv_c;
     float f_poly[RTB_MAX_POLY], f_ipoly[RTB_MAX_POLY];
     float f_sag_lo, f_sag_hi, f_size0, f_pad;  // sag range and aperture radius
+    // FP32-state engine (RTB_MIXED32): the transform from the frame of the
+    // previous non-Aux surface (the entrance frame for the first), with the
+    // Aux surfaces in between folded in, as P' = M P + off32 and D' = M D:
+    // M in FP32 (rows), off32 in FP64.  rot32: M is not the identity;
+    // first32: the first non-Aux surface, whose offset comes from the ray's
+    // beam (DevBeam::off0).  Set on non-Aux surfaces only.
+    float m32[9];
+    int32_t rot32, first32, pad32;
+    double off32[3];
 };
 
 // A prepared scheme in device memory; the fused kernels copy it to shared
@@ -71,6 +82,12 @@ struct DevScheme {
     int32_t renorm_lost;
     int32_t pad[4];
     DevSurface s[RTB_MAX_SURFACES];
+    // FP32-state engine: the first non-Aux surface's transform in FP64 (from
+    // the entrance frame), from which each beam's offset is made, and the
+    // transform of the Aux surfaces after the last non-Aux one (tail_on).
+    double m0[9], off0[3];
+    double tail_m[9], tail_off[3];
+    int32_t tail_on, pad_tail[3];
 };
 static_assert(sizeof(DevScheme) % 16 == 0, "DevScheme is copied to shared memory in 16-byte words");
 
@@ -81,6 +98,10 @@ struct DevBeam {
     int64_t orders[RTB_MAX_GRATINGS];
     int32_t n_orders;
     int32_t pad;
+    // FP32-state engine: the beam's origin (rtb_beam::center), to which its
+    // rays' FP32 positions are relative, and the offset of the first non-Aux
+    // surface's transform for those positions (DevScheme m0 origin + off0)
+    double origin[3], off0[3];
 };
 
 struct DevRays {

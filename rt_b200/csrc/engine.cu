@@ -232,6 +232,82 @@ int prepare_surface(const rtb_surface& in, DevSurface& s, KnotBuf& knots) {
     return RTB_OK;
 }
 
+// The rotations of one surface's transform applied to v, in the kernels'
+// order: about y (X,Z), about x (Y,Z), about z (X,Y) (beam.cu:437-518).
+static void rotate_by(const DevSurface& s, double v[3]) {
+    if (s.rot_mask & 1) {
+        const double e = v[0] * s.cosA[0] - v[2] * s.sinA[0];
+        v[2] = v[0] * s.sinA[0] + v[2] * s.cosA[0];
+        v[0] = e;
+    }
+    if (s.rot_mask & 2) {
+        const double e = v[1] * s.cosA[1] - v[2] * s.sinA[1];
+        v[2] = v[1] * s.sinA[1] + v[2] * s.cosA[1];
+        v[1] = e;
+    }
+    if (s.rot_mask & 4) {
+        const double e = v[0] * s.cosA[2] - v[1] * s.sinA[2];
+        v[1] = v[0] * s.sinA[2] + v[1] * s.cosA[2];
+        v[0] = e;
+    }
+}
+
+// The FP32-state engine's transforms: from the frame of one non-Aux surface
+// to the next (P' = M P + off, D' = M D), each surface's translation and
+// rotations and those of the Aux surfaces in between composed in FP64 here.
+static void fp32_transforms(DevScheme& sch) {
+    double M[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1}, off[3] = {0, 0, 0};
+    bool first = true;
+    for (int k = 0; k < sch.n_surfaces; ++k) {
+        DevSurface& s = sch.s[k];
+        // P -> R_k (M P + off - d_k): the columns of M and the offset rotate
+        for (int c = 0; c < 3; ++c) {
+            double v[3] = {M[c], M[3 + c], M[6 + c]};
+            rotate_by(s, v);
+            M[c] = v[0];
+            M[3 + c] = v[1];
+            M[6 + c] = v[2];
+        }
+        double o[3] = {off[0] - s.dist[0], off[1] - s.dist[1], off[2] - s.dist[2]};
+        rotate_by(s, o);
+        for (int i = 0; i < 3; ++i) off[i] = o[i];
+        if (!s.non_aux) continue;
+        bool ident = true;
+        for (int i = 0; i < 9; ++i) {
+            s.m32[i] = (float)M[i];
+            ident = ident && M[i] == ((i % 4 == 0) ? 1.0 : 0.0);
+        }
+        s.rot32 = ident ? 0 : 1;
+        s.first32 = first ? 1 : 0;
+        for (int i = 0; i < 3; ++i) s.off32[i] = off[i];
+        if (first) {
+            for (int i = 0; i < 9; ++i) sch.m0[i] = M[i];
+            for (int i = 0; i < 3; ++i) sch.off0[i] = off[i];
+            first = false;
+        }
+        for (int i = 0; i < 9; ++i) M[i] = (i % 4 == 0) ? 1.0 : 0.0;
+        off[0] = off[1] = off[2] = 0.0;
+    }
+    bool tail = false;
+    for (int i = 0; i < 9; ++i) {
+        sch.tail_m[i] = M[i];
+        tail = tail || M[i] != ((i % 4 == 0) ? 1.0 : 0.0);
+    }
+    for (int i = 0; i < 3; ++i) {
+        sch.tail_off[i] = off[i];
+        tail = tail || off[i] != 0.0;
+    }
+    sch.tail_on = tail ? 1 : 0;
+}
+
+void beam_frame(const DevScheme& sch, const double center[3], DevBeam& d) {
+    for (int i = 0; i < 3; ++i) {
+        d.origin[i] = center[i];
+        d.off0[i] = sch.m0[3 * i] * center[0] + sch.m0[3 * i + 1] * center[1] + sch.m0[3 * i + 2] * center[2] +
+                    sch.off0[i];
+    }
+}
+
 int prepare_scheme_into(const rtb_surface* surf, size_t n, uint32_t fixes, int renorm_lost, DevScheme& sch,
                         KnotBuf& knots) {
     if (!surf || n == 0 || n > RTB_MAX_SURFACES) return RTB_BAD_VALUE;
@@ -298,6 +374,7 @@ int prepare_scheme_into(const rtb_surface* surf, size_t n, uint32_t fixes, int r
     sch.n_knots = (int32_t)knots.size();
     sch.fixes = fixes;
     sch.renorm_lost = renorm_lost;
+    fp32_transforms(sch);
     return RTB_OK;
 }
 

@@ -143,16 +143,25 @@ struct TraceArgs {
 
 DevRays dev_rays(const rtb_rays* r);
 // Beam table for the trace kernels; rays of beam b are [first_ray, first_ray + n_rays) < n_rays, in order.
-int check_beams(const rtb_beam* beams, size_t n_beams, size_t n_rays, std::vector<DevBeam>& out);
+// With `sch`, each beam also gets its origin and first-surface offset for the
+// FP32-state engine (beam_frame).
+int check_beams(const rtb_beam* beams, size_t n_beams, size_t n_rays, std::vector<DevBeam>& out,
+                const DevScheme* sch = nullptr);
+// A beam's origin (its centre: FP32 positions are relative to it) and the
+// offset of the first non-Aux surface's transform for such positions.
+void beam_frame(const DevScheme& sch, const double center[3], DevBeam& d);
 // Beam table for the generator; *total is the end of the last beam.
 int gen_beams(const rtb_beam* beams, size_t n_beams, size_t n_rays, std::vector<GenBeam>& out, uint64_t* total);
 FrameArgs frame_args(const rtb_trace_opts* o);
 // Launch the trace kernels of one call (no synchronisation).
 // `order` (fused kernels; may be NULL): the order in which the rays are
 // traced; in_by_slot: `in` holds the rays in that order.
+// `rows` (mixed kernels; may be NULL): the rays in tracing order as row
+// blocks (Row64 / Row32 of rowpipe.cuh), read in place of `in`;
+// out_by_slot: outputs at the tracing slot instead of the ray's index.
 int launch_trace(const PreparedScheme& ps, TraceArgs& a, int n_beams, const rtb_trace_opts& o, const DevRays& in,
                  const DevRays& out, const FrameArgs& frame, cudaStream_t st, const uint32_t* order = nullptr,
-                 bool in_by_slot = false);
+                 bool in_by_slot = false, const void* rows = nullptr, bool out_by_slot = false);
 // The coherent tracing order (beam, chunk, wavelength, Morton code of the
 // entrance position) of n <= 2^32 generated rays, as a permutation in
 // `order` (device, n).

@@ -86,6 +86,7 @@ __device__ __forceinline__ void fused_fp64(const DevScheme* __restrict__ g_sch, 
             const size_t slot = tile * block_rays + (size_t)j * blockDim.x + threadIdx.x;
             const size_t i = (ts.order && slot < in.n) ? (size_t)ts.order[slot] : slot;
             const size_t ri = ts.in_by_slot ? slot : i;
+            const size_t oi = ts.out_by_slot ? slot : i;  // where its results go
             bool ev = false, good = false;
             int key = 0;
             double outX = 0, outY = 0;
@@ -98,7 +99,7 @@ __device__ __forceinline__ void fused_fp64(const DevScheme* __restrict__ g_sch, 
                 if (!(b + 1 >= n_beams || i < beams[b + 1].first_ray) || i < beams[b].first_ray)
                     b = beam_of(beams, n_beams, i);
             } else if (slot < in.n && in.flag != out.flag) {
-                out.flag[i] = in.flag[ri];
+                out.flag[oi] = in.flag[ri];
             }
             int stage = have ? -1 : -3;
             Surfaces::run(sch, s_knots, beams, b, lam, err, r, stage);
@@ -106,25 +107,25 @@ __device__ __forceinline__ void fused_fp64(const DevScheme* __restrict__ g_sch, 
                 if (stage >= 0) {
                     ev = true;
                     if (sch->renorm_lost) f64::renormalize(r, sch->s[stage / 3].renorm_after);
-                    out.flag[i] = 0;
-                    out.lost_stage[i] = (uint8_t)stage;
+                    out.flag[oi] = 0;
+                    out.lost_stage[oi] = (uint8_t)stage;
                     key = b * (n_stages + 1) + stage;
                 } else if (stage == -1) {
                     ev = good = true;
                     key = b * (n_stages + 1) + n_stages;
                     if (in.flag != out.flag) {
-                        out.flag[i] = 1;
-                        out.lost_stage[i] = RTB_NOT_LOST;
+                        out.flag[oi] = 1;
+                        out.lost_stage[oi] = RTB_NOT_LOST;
                     }
                 }
                 if (stage != -2) {
-                    out.X[i] = r.X;
-                    out.Y[i] = r.Y;
+                    out.X[oi] = r.X;
+                    out.Y[oi] = r.Y;
                     if (state_out) {
-                        out.Z[i] = r.Z;
-                        out.cX[i] = r.cX;
-                        out.cY[i] = r.cY;
-                        out.cZ[i] = r.cZ;
+                        out.Z[oi] = r.Z;
+                        out.cX[oi] = r.cX;
+                        out.cY[oi] = r.cY;
+                        out.cZ[oi] = r.cZ;
                     }
                 }
                 outX = r.X;

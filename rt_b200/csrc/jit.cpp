@@ -55,7 +55,12 @@ const char* const kTypes =
     "typedef unsigned long uint64_t; typedef unsigned long size_t; typedef long ptrdiff_t;\n";
 
 const char* const kMixedName = "rtb_fused_mixed_scheme";
+const char* const kMixed32Name = "rtb_fused_mixed32_scheme";
 const char* const kFp64Name = "rtb_fused_fp64_scheme";
+
+const char* kernel_name(int precision) {
+    return precision == RTB_MIXED ? kMixedName : precision == RTB_MIXED32 ? kMixed32Name : kFp64Name;
+}
 
 struct Nvrtc {
     bool ok = false;
@@ -146,9 +151,10 @@ int compile_to_cubin(const std::string& src, bool fmad, std::vector<char>& cubin
 // FixedShape<...> of surface s: the fields RtShape reads.
 static std::string fixed_shape(const DevSurface& s) {
     char t[200];
-    std::snprintf(t, sizeof(t), "FixedShape<%d, %d, %d, %d, %d, %d, %d, %d, %d, %d, %d>", (int)s.kind, (int)s.type,
-                  (int)s.cls, (int)s.shape, (int)s.gr_type, s.translate != 0 ? 1 : 0, (int)s.rot_mask, (int)s.n_poly,
-                  s.non_aux != 0 ? 1 : 0, s.sag_cull != 0 ? 1 : 0, s.c == 0.0 ? 1 : 0);
+    std::snprintf(t, sizeof(t), "FixedShape<%d, %d, %d, %d, %d, %d, %d, %d, %d, %d, %d, %d, %d>", (int)s.kind,
+                  (int)s.type, (int)s.cls, (int)s.shape, (int)s.gr_type, s.translate != 0 ? 1 : 0, (int)s.rot_mask,
+                  (int)s.n_poly, s.non_aux != 0 ? 1 : 0, s.sag_cull != 0 ? 1 : 0, s.c == 0.0 ? 1 : 0,
+                  s.rot32 != 0 ? 1 : 0, s.first32 != 0 ? 1 : 0);
     return t;
 }
 
@@ -157,33 +163,76 @@ static const char* const kParams =
     "        int n_beams, rtb::DevRays in, rtb::DevRays out, unsigned long long* counts, unsigned* err,\n"
     "        int state_out, rtb::FrameArgs frame, rtb::TileSched ts) {\n";
 
+// The surfaces' constants baked into the kernel: a __constant__ image of
+// sch.s[0 .. n_surfaces), which the surface code reads at addresses known at
+// compile time -- constant-bank operands of its instructions instead of
+// shared-memory loads and their address arithmetic.  The run time fields of
+// the scheme (the knot tables, the beams) are read as before.
+static std::string surface_constants(const DevScheme& sch) {
+    static_assert(sizeof(DevSurface) % 8 == 0, "DevSurface is baked as 64-bit words");
+    const size_t words = (size_t)sch.n_surfaces * sizeof(DevSurface) / 8;
+    std::vector<unsigned long long> w(words);
+    std::memcpy(w.data(), sch.s, words * 8);
+    std::string t = "namespace rtb {\nstatic __constant__ const unsigned long long k_surface_words[" +
+                    std::to_string(words) + "] = {";
+    char buf[32];
+    for (size_t i = 0; i < words; ++i) {
+        std::snprintf(buf, sizeof(buf), "%s0x%llxull", (i % 6) ? ", " : ",\n    ", w[i]);
+        t += (i == 0) ? buf + 1 : buf;
+    }
+    t += "};\n__device__ __forceinline__ const DevSurface* k_surfaces() {\n"
+         "    return reinterpret_cast<const DevSurface*>(k_surface_words);\n}\n"
+         "constexpr uint32_t k_fixes = " + std::to_string(sch.fixes) + "u;\n}  // namespace rtb\n";
+    return t;
+}
+
 std::string scheme_source(const DevScheme& sch, int precision) {
     std::string src;
+    const bool bake = bake_values();
+    const std::string S = bake ? "k_surfaces()[" : "sch->s[";
+    const std::string F = bake ? "k_fixes" : "sch->fixes";
     if (precision == RTB_MIXED) {
-        src = "#include \"mixed.cuh\"\n"
+        src = "#include \"mixed.cuh\"\n" + (bake ? surface_constants(sch) : std::string()) +
               "namespace rtb {\n"
               "struct SchemeSurfaces {\n"
               "    __device__ __forceinline__ static void run(const DevScheme* sch, const double* knots,\n"
               "        const DevBeam* beams, int b, double lam, mx::TableMemo& memo, mx::Ray& r, int& stage) {\n";
         for (int k = 0; k < sch.n_surfaces; ++k) {
             const std::string ks = std::to_string(k);
-            src += "        if (stage == -1) stage = mx_surface<" + fixed_shape(sch.s[k]) + ">(sch->s[" + ks + "], " +
-                   ks + ", sch->fixes, knots, beams, b, lam, memo, r);\n";
+            src += "        if (stage == -1) stage = mx_surface<" + fixed_shape(sch.s[k]) + ">(" + S + ks + "], " +
+                   ks + ", " + F + ", knots, beams, b, lam, memo, r);\n";
         }
         src += std::string("    }\n};\n}  // namespace rtb\n"
                            "extern \"C\" __global__ void __maxnreg__(64) ") + kMixedName + "(\n" + kParams +
                "    rtb::fused_mixed<rtb::SchemeSurfaces>(g_sch, knots, beams, n_beams, in, out, counts, err,\n"
                "                                        state_out, frame, ts);\n}\n";
+    } else if (precision == RTB_MIXED32) {
+        src = "#include \"mixed32.cuh\"\n" + (bake ? surface_constants(sch) : std::string()) +
+              "namespace rtb {\n"
+              "struct SchemeSurfaces32 {\n"
+              "    __device__ __forceinline__ static void run(const DevScheme* sch, const double* knots,\n"
+              "        const DevBeam* beams, int b, double lam, mx::TableMemo& memo, m32::Ray& r, mx::Ray& q,\n"
+              "        int& stage) {\n";
+        for (int k = 0; k < sch.n_surfaces; ++k) {
+            if (!sch.s[k].non_aux) continue;  // folded into the next surface's transform
+            const std::string ks = std::to_string(k);
+            src += "        if (stage == -1) stage = m32_surface<" + fixed_shape(sch.s[k]) + ">(" + S + ks + "], " +
+                   ks + ", " + F + ", knots, beams, b, lam, memo, r, q);\n";
+        }
+        src += std::string("    }\n};\n}  // namespace rtb\n"
+                           "extern \"C\" __global__ void __maxnreg__(64) ") + kMixed32Name + "(\n" + kParams +
+               "    rtb::fused_mixed32<rtb::SchemeSurfaces32>(g_sch, knots, beams, n_beams, in, out, counts, err,\n"
+               "                                            state_out, frame, ts);\n}\n";
     } else {
-        src = "#include \"fused_fp64.cuh\"\n"
+        src = "#include \"fused_fp64.cuh\"\n" + (bake ? surface_constants(sch) : std::string()) +
               "namespace rtb {\n"
               "struct SchemeSurfacesF64 {\n"
               "    __device__ __forceinline__ static void run(const DevScheme* sch, const double* knots,\n"
               "        const DevBeam* beams, int b, double lam, unsigned* err, f64::Ray& r, int& stage) {\n";
         for (int k = 0; k < sch.n_surfaces; ++k) {
             const std::string ks = std::to_string(k);
-            src += "        if (stage == -1) f64_surface<" + fixed_shape(sch.s[k]) + ">(sch->s[" + ks + "], " + ks +
-                   ", sch->fixes, knots, beams, b, lam, err, r, stage);\n        __syncthreads();\n";
+            src += "        if (stage == -1) f64_surface<" + fixed_shape(sch.s[k]) + ">(" + S + ks + "], " + ks + ", " +
+                   F + ", knots, beams, b, lam, err, r, stage);\n        __syncthreads();\n";
         }
         src += std::string("    }\n};\n}  // namespace rtb\n"
                            "extern \"C\" __global__ void __maxnreg__(64) ") + kFp64Name + "(\n" + kParams +
@@ -198,6 +247,11 @@ std::string nvrtc_info() {
     if (!n.ok) return "unavailable (" + n.why + ")";
     return std::to_string(n.major) + "." + std::to_string(n.minor) +
            (specialize_enabled() ? "" : " (RTB_SPECIALIZE=0)");
+}
+
+bool bake_values() {
+    const char* e = std::getenv("RTB_SPECIALIZE");
+    return !(e && std::strcmp(e, "structure") == 0);
 }
 
 bool specialize_enabled() {
@@ -300,7 +354,7 @@ static const std::vector<char>* cubin_for(const std::string& src, bool fmad, std
 
 int compile_scheme(const DevScheme& sch, int precision, std::string* why) {
     std::lock_guard<std::mutex> g(g_mu);
-    return cubin_for(scheme_source(sch, precision), precision == RTB_MIXED, why, true) ? RTB_OK : RTB_FAILED;
+    return cubin_for(scheme_source(sch, precision), precision != RTB_FP64, why, true) ? RTB_OK : RTB_FAILED;
 }
 
 int scheme_kernel(const DevScheme& sch, int precision, const void** kernel, std::string* why, bool compile) {
@@ -316,17 +370,17 @@ int scheme_kernel(const DevScheme& sch, int precision, const void** kernel, std:
     cudaKernel_t k = nullptr;
     cudaError_t e = cudaSuccess;
     for (int attempt = 0; attempt < 2; ++attempt) {
-        const std::vector<char>* cubin = cubin_for(src, precision == RTB_MIXED, why, compile);
+        const std::vector<char>* cubin = cubin_for(src, precision != RTB_FP64, why, compile);
         if (!cubin) return RTB_OK;
         lib = nullptr;
         e = cudaLibraryLoadData(&lib, cubin->data(), nullptr, nullptr, 0, nullptr, nullptr, 0);
-        if (e == cudaSuccess) e = cudaLibraryGetKernel(&k, lib, precision == RTB_MIXED ? kMixedName : kFp64Name);
+        if (e == cudaSuccess) e = cudaLibraryGetKernel(&k, lib, kernel_name(precision));
         if (e == cudaSuccess) break;
         if (lib) cudaLibraryUnload(lib);
         // a cubin that does not load (a damaged cache file): compile afresh once
         g_cubins.erase(src);
         const std::string dir = cache_dir();
-        if (!dir.empty()) std::remove(cache_path(dir, cache_key(src, precision == RTB_MIXED)).c_str());
+        if (!dir.empty()) std::remove(cache_path(dir, cache_key(src, precision != RTB_FP64)).c_str());
         if (!compile) break;
     }
     if (e != cudaSuccess) {
@@ -346,7 +400,7 @@ using namespace rtb;
 int rtb_specialize(const rtb_surface* surfaces, size_t n_surfaces, uint32_t fixes, int32_t precision, char* note,
                    size_t note_len) {
     if (note && note_len > 0) note[0] = 0;
-    if (precision != RTB_FP64 && precision != RTB_MIXED) return RTB_BAD_VALUE;
+    if (precision != RTB_FP64 && precision != RTB_MIXED && precision != RTB_MIXED32) return RTB_BAD_VALUE;
     PreparedScheme ps;
     int st = prepare_scheme(surfaces, n_surfaces, fixes, 0, ps);
     if (st != RTB_OK) return st;

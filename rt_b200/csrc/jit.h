@@ -7,7 +7,8 @@
 
 namespace rtb {
 
-// The CUDA source of the fused kernel of `precision` (RTB_MIXED or RTB_FP64)
+// The CUDA source of the fused kernel of `precision` (RTB_MIXED, RTB_MIXED32
+// or RTB_FP64)
 // specialised to the structure of `sch` (one FixedShape per surface).
 std::string scheme_source(const DevScheme& sch, int precision);
 
@@ -16,6 +17,10 @@ std::string nvrtc_info();
 
 // False when RTB_SPECIALIZE=0 is set in the environment.
 bool specialize_enabled();
+
+// Whether specialised kernels bake the surfaces' constants in (default), or
+// only their structure (RTB_SPECIALIZE=structure).
+bool bake_values();
 
 // Compile (without loading) the specialised kernel: RTB_OK, or RTB_FAILED
 // with `why`.  Needs no device.

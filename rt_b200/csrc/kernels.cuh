@@ -33,17 +33,22 @@ inline size_t fused_smem_bytes(int n_knots) {
 #endif
 
 // Scheduling of the persistent fused kernels: `next` is a counter of tiles
-// (zeroed before each launch) handed out to warps, 32*rpt rays each
-// (k_fused_mixed), or to blocks, blockDim*rpt rays each (k_fused_fp64).  Slot s
-// of the tiles traces ray order[s] (a permutation of the rays), or ray s when
-// order is NULL; its input is read at s when in_by_slot (the input arrays
-// hold the rays in tracing order), else at the ray's index.  Outputs go to
-// the ray's index.
+// (zeroed before each launch) handed out to warps, 32*rpt rays each (the
+// mixed kernels), or to blocks, blockDim*rpt rays each (k_fused_fp64).  Slot
+// s of the tiles traces ray order[s] (a permutation of the rays), or ray s
+// when order is NULL; its input is read at s when in_by_slot (the input
+// arrays hold the rays in tracing order), else at the ray's index.  Outputs
+// go to the ray's index unless out_by_slot.
+// `rows` (mixed kernels, may be NULL): the rays in tracing order as row
+// blocks (Row64 for RTB_MIXED, Row32 for RTB_MIXED32, rowpipe.cuh), read in
+// place of `in`.  out_by_slot: outputs go to the tracing slot instead.
 struct TileSched {
     unsigned long long* next;
     int rpt;
     const uint32_t* order;
     int in_by_slot;
+    const void* rows;
+    int out_by_slot;
 };
 constexpr int kDefaultRpt = 2;
 
@@ -91,6 +96,12 @@ __global__ void k_order_keys(const GenBeam* beams, int n_beams, uint64_t total, 
                              unsigned long long* keys, uint32_t* idx, int chunk_shift);
 // dst[s] = src[order[s]] for X..lambda and flag
 __global__ void k_gather_rays(const uint32_t* order, uint64_t n, DevRays src, DevRays dst);
+// the same into row blocks of 32 rays (rowpipe.cuh): FP64 (Row64), or FP32
+// positions relative to the beam's origin and FP32 cosines (Row32); slots
+// past n up to a whole row get flag 0
+__global__ void k_gather_rows64(const uint32_t* order, uint64_t n, DevRays src, void* rows);
+__global__ void k_gather_rows32(const uint32_t* order, uint64_t n, DevRays src, const DevBeam* beams, int n_beams,
+                                void* rows);
 __global__ void k_ccd_frame(DevRays rays, FrameArgs f);
 
 // ---- trace kernels ----
@@ -103,7 +114,10 @@ __global__ void k_surface_step(const DevScheme* sch, int k, const double* knots,
 __global__ void k_fused_fp64(const DevScheme* sch, const double* knots, const DevBeam* beams, int n_beams,
                              DevRays in, DevRays out, unsigned long long* counts, unsigned* err, int state_out,
                              FrameArgs frame, TileSched ts);
-// kernels_mixed.cu
+// kernels_mixed.cu: FP64 state (RTB_MIXED) and FP32 state (RTB_MIXED32)
+__global__ void k_fused_mixed32(const DevScheme* sch, const double* knots, const DevBeam* beams, int n_beams,
+                                DevRays in, DevRays out, unsigned long long* counts, unsigned* err, int state_out,
+                                FrameArgs frame, TileSched ts);
 __global__ void k_fused_mixed(const DevScheme* sch, const double* knots, const DevBeam* beams, int n_beams,
                               DevRays in, DevRays out, unsigned long long* counts, unsigned* err, int state_out,
                               FrameArgs frame, TileSched ts);

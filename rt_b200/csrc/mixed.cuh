@@ -6,7 +6,7 @@
 //   * ray state, transforms, intersection roots (the conic quadratic in a
 //     cancellation-safe form; Newton for the even asphere from the base-conic
 //     root and for the toric from the plane point, until a step falls below
-//     1e-6 mm, the root then good to ~1e-14 mm), the grating equation and the
+//     1e-5 mm, the root then good to ~1e-12 mm), the grating equation and the
 //     detector coordinate: FP64, contracted to FMA;
 //   * every division and square root: a MUFU seed (rcp/rsqrt.approx.f64)
 //     refined by Newton steps in FP64 instead of the IEEE FP64 division and
@@ -27,6 +27,7 @@
 
 #include "trace_common.cuh"
 #include "ray_fp64.cuh"
+#include "rowpipe.cuh"
 
 namespace rtb {
 namespace mx {
@@ -207,9 +208,10 @@ __device__ __forceinline__ bool conic_isect(const DevSurface& s, Ray& r) {
 // no square root per step) from the base-conic root, the derivative's inverse
 // taken from the reciprocal seed (rcp_seed).  Newton converges
 // quadratically, the next correction being about |G''/2G'| dt^2 (< 1e-2 dt^2
-// for these surfaces), so the loop stops after a step below 1e-6 mm: the root
-// is then good to ~1e-14 mm.  One or two steps from the conic root; at most
-// eight for rays that start far from the surface (far outside the aperture).
+// for these surfaces) plus the seed's 2^-22 dt, so the loop stops after a
+// step below 1e-5 mm: the root is then good to ~1e-12 mm.  One step from the
+// conic root for most rays; at most eight for rays that start far from the
+// surface (far outside the aperture).
 //
 // Rays far outside the aperture take most of those steps, and their lanes
 // hold the warp: a ray that within the slab sag_lo <= Z <= sag_hi (every
@@ -276,7 +278,7 @@ __device__ __forceinline__ int asphere_isect(const DevSurface& s, Ray& r) {
         }
         const double dt = G * rcp_seed(dG);
         t -= dt;
-        if (!(fabs(dt) >= 1e-6)) break;
+        if (!(fabs(dt) >= 1e-5)) break;
     }
     if (!isfinite(t)) return 1;  // no root near the ray (far outside any aperture)
     x = fma(t, r.cX, r.X);
@@ -308,8 +310,9 @@ __device__ __forceinline__ int asphere_isect(const DevSurface& s, Ray& r) {
 // its inverse from the reciprocal seed, rcp_seed)
 //   dF/dt = cZ - FY' cY - cR (X cX + Z cZ - FY FY' cY),  FY' = c Y / s,
 // s = sqrt(1 -+ k1 c^2 Y^2) (FY = c Y^2 / (1 + s) has this derivative for
-// either sign), until a step falls below 1e-6 mm (quadratic convergence: the
-// root is then good to ~1e-14 mm), at most six steps.  As in the reference, a
+// either sign), until a step falls below 1e-5 mm (quadratic convergence: the
+// next correction, |F''/2F'| dt^2 plus the seed's 2^-22 dt, is ~1e-12 mm), at
+// most six steps.  As in the reference, a
 // ray is lost only when the plane point lies behind it.
 __device__ __forceinline__ bool toric_isect(const DevSurface& s, uint32_t fixes, Ray& r) {
     const double sgn = (fixes & RTB_FIX_TORIC_SIGN) ? -1.0 : 1.0;
@@ -326,7 +329,7 @@ __device__ __forceinline__ bool toric_isect(const DevSurface& s, uint32_t fixes,
         double dF = r.cZ - dFY * r.cY - s.cR * (fma(X, r.cX, Z * r.cZ) - FY * dFY * r.cY);
         double dt = F * rcp_seed(dF);
         t -= dt;
-        if (!(fabs(dt) >= 1e-6)) break;  // next correction ~|F''/2F'| dt^2 << 1e-12 mm
+        if (!(fabs(dt) >= 1e-5)) break;  // next correction ~|F''/2F'| dt^2 + 2^-22 dt ~ 1e-12 mm
     }
     r.X = fma(t, r.cX, r.X);
     r.Y = fma(t, r.cY, r.Y);
@@ -562,14 +565,17 @@ struct RtSurfaces {
     }
 };
 
-// Fused mixed-precision trace: one ray per thread at a time, the whole scheme
+// Fused mixed-precision trace: one ray per lane at a time, the whole scheme
 // in registers, the scheme and knot tables in shared memory, a persistent
-// grid whose warps take tiles of rays (next_tile).  The kernels that run it
-// (k_fused_mixed and the scheme-specialised ones) are launched with blocks of
-// up to 512 threads and 64 registers a thread, which keeps 32 warps resident
-// per SM and hides the FP64 dependency chains better than more registers
-// would (C1: 11.5 ms per step at 64 registers, 13.0 at 80, 16.1 at 96; below
-// 64 the spills cost more).
+// grid whose warps take tiles of rpt rows of 32 rays (rowpipe.cuh).  Plans
+// feed it Row64 blocks in tracing order through the row pipeline (each row's
+// bulk copy in flight while the warp traces the row before); one-shot traces
+// read the SoA arrays.  The kernels that run it (k_fused_mixed and the
+// scheme-specialised ones) are launched with blocks of up to 512 threads and
+// 64 registers a thread, which keeps 32 warps resident per SM and hides the
+// FP64 dependency chains better than more registers would (C1: 11.5 ms per
+// step at 64 registers, 13.0 at 80, 16.1 at 96; below 64 the spills cost
+// more).
 template <class Surfaces>
 __device__ __forceinline__ void fused_mixed(const DevScheme* __restrict__ g_sch, const double* knots,
                                             const DevBeam* beams, int n_beams, DevRays in, DevRays out,
@@ -577,63 +583,75 @@ __device__ __forceinline__ void fused_mixed(const DevScheme* __restrict__ g_sch,
                                             FrameArgs frame, TileSched ts) {
     const double* s_knots;
     const DevScheme* sch = stage_scheme(g_sch, knots, s_knots);
-    const int ns = sch->n_surfaces;
-    const int n_stages = 3 * ns;
-    const uint64_t tile_rays = 32ull * (uint64_t)ts.rpt;
-    const uint64_t n_tiles = (in.n + tile_rays - 1) / tile_rays;
-    uint64_t tile;
+    const int n_stages = 3 * sch->n_surfaces;
+    RowLoop rows(ts, in.n, warp_row_buffer<Row64>(sch->n_knots), (unsigned)sizeof(Row64), err);
+    const int lane = threadIdx.x & 31;
     int b = 0;
-    while (next_tile(ts, n_tiles, tile)) {
-        for (int j = 0; j < ts.rpt; ++j) {
-            const size_t slot = tile * tile_rays + (size_t)j * 32 + (threadIdx.x & 31);
-            const size_t i = (ts.order && slot < in.n) ? (size_t)ts.order[slot] : slot;  // the ray (outputs)
-            const size_t ri = ts.in_by_slot ? slot : i;                                  // its input
-            bool ev = false, good = false;
-            int key = 0;
-            double outX = 0, outY = 0;
-            if (slot < in.n && in.flag[ri] == 1) {
-                mx::Ray r{in.X[ri], in.Y[ri], in.Z[ri], in.cX[ri], in.cY[ri], in.cZ[ri]};
-                mx::normalize(r);
-                const double lam = in.lambda[ri];
-                // rays come in increasing order per thread: the previous
-                // ray's beam is usually this one's
-                if (!(b + 1 >= n_beams || i < beams[b + 1].first_ray) || i < beams[b].first_ray)
-                    b = beam_of(beams, n_beams, i);
-                mx::TableMemo memo;
-                int stage = -1;
-                Surfaces::run(sch, s_knots, beams, b, lam, memo, r, stage);
-                if (stage == -2) atomicOr(err, DEV_ERR_OUT_OF_RANGE);
-                if (stage >= 0) {
-                    ev = true;
-                    out.flag[i] = 0;
-                    out.lost_stage[i] = (uint8_t)stage;
-                    key = b * (n_stages + 1) + stage;
-                } else if (stage == -1) {
-                    ev = good = true;
-                    key = b * (n_stages + 1) + n_stages;
-                    if (in.flag != out.flag) {
-                        out.flag[i] = 1;
-                        out.lost_stage[i] = RTB_NOT_LOST;
-                    }
-                }
-                if (stage != -2) {
-                    out.X[i] = r.X;
-                    out.Y[i] = r.Y;
-                    if (state_out) {
-                        out.Z[i] = r.Z;
-                        out.cX[i] = r.cX;
-                        out.cY[i] = r.cY;
-                        out.cZ[i] = r.cZ;
-                    }
-                }
-                outX = r.X;
-                outY = r.Y;
-            } else if (slot < in.n && in.flag != out.flag) {
-                out.flag[i] = in.flag[ri];
+    while (rows.begin()) {
+        const size_t slot = rows.slot();
+        const bool valid = slot < in.n;
+        const size_t i = (ts.order && valid) ? (size_t)ts.order[slot] : slot;  // the ray
+        const size_t oi = ts.out_by_slot ? slot : i;                           // where its results go
+        mx::Ray r{0, 0, 0, 0, 0, 0};
+        double lam = 0.0;
+        char f = 0;
+        if (rows.packed) {
+            const Row64& w = rows.row<Row64>();
+            f = w.flag[lane];
+            r = mx::Ray{w.X[lane], w.Y[lane], w.Z[lane], w.cX[lane], w.cY[lane], w.cZ[lane]};
+            lam = w.lambda[lane];
+        } else if (valid) {
+            const size_t ri = ts.in_by_slot ? slot : i;
+            f = in.flag[ri];
+            if (f == 1) {
+                r = mx::Ray{in.X[ri], in.Y[ri], in.Z[ri], in.cX[ri], in.cY[ri], in.cZ[ri]};
+                lam = in.lambda[ri];
             }
-            count_event(ev, key, counts);
-            if (frame.counts) frame_add<false>(good, outX, outY, frame);
         }
+        rows.prefetch();
+        bool ev = false, good = false;
+        int key = 0;
+        double outX = 0, outY = 0;
+        if (valid && f == 1) {
+            mx::normalize(r);
+            // rays come in increasing order per warp: the previous ray's
+            // beam is usually this one's
+            if (!(b + 1 >= n_beams || i < beams[b + 1].first_ray) || i < beams[b].first_ray)
+                b = beam_of(beams, n_beams, i);
+            mx::TableMemo memo;
+            int stage = -1;
+            Surfaces::run(sch, s_knots, beams, b, lam, memo, r, stage);
+            if (stage == -2) atomicOr(err, DEV_ERR_OUT_OF_RANGE);
+            if (stage >= 0) {
+                ev = true;
+                out.flag[oi] = 0;
+                out.lost_stage[oi] = (uint8_t)stage;
+                key = b * (n_stages + 1) + stage;
+            } else if (stage == -1) {
+                ev = good = true;
+                key = b * (n_stages + 1) + n_stages;
+                if (rows.packed || in.flag != out.flag) {
+                    out.flag[oi] = 1;
+                    out.lost_stage[oi] = RTB_NOT_LOST;
+                }
+            }
+            if (stage != -2) {
+                out.X[oi] = r.X;
+                out.Y[oi] = r.Y;
+                if (state_out) {
+                    out.Z[oi] = r.Z;
+                    out.cX[oi] = r.cX;
+                    out.cY[oi] = r.cY;
+                    out.cZ[oi] = r.cZ;
+                }
+            }
+            outX = r.X;
+            outY = r.Y;
+        } else if (valid && (rows.packed || in.flag != out.flag)) {
+            out.flag[oi] = f;
+        }
+        count_event(ev, key, counts);
+        if (frame.counts) frame_add<false>(good, outX, outY, frame);
     }
 }
 

@@ -13,6 +13,7 @@
 #include <cub/cub.cuh>
 
 #include "engine.cuh"
+#include "rowpipe.cuh"
 
 namespace rtb {
 
@@ -294,6 +295,63 @@ __global__ void k_gather_rays(const uint32_t* order, uint64_t n, DevRays src, De
         dst.cZ[t] = src.cZ[i];
         dst.lambda[t] = src.lambda[i];
         dst.flag[t] = src.flag[i];
+    }
+}
+
+// Row blocks of the tracing order (rowpipe.cuh): slot t goes to element
+// t % 32 of row t / 32; the slots after the last ray, up to a whole row, get
+// flag 0.  Each thread writes one slot, so a warp writes 32 consecutive
+// elements of each component.
+__global__ void k_gather_rows64(const uint32_t* order, uint64_t n, DevRays src, void* rows) {
+    Row64* dst = static_cast<Row64*>(rows);
+    const uint64_t total = (n + 31) / 32 * 32;
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < total;
+         t += (uint64_t)blockDim.x * gridDim.x) {
+        Row64& w = dst[t >> 5];
+        const int l = (int)(t & 31);
+        if (t < n) {
+            const uint64_t i = order ? order[t] : t;
+            w.X[l] = src.X[i];
+            w.Y[l] = src.Y[i];
+            w.Z[l] = src.Z[i];
+            w.cX[l] = src.cX[i];
+            w.cY[l] = src.cY[i];
+            w.cZ[l] = src.cZ[i];
+            w.lambda[l] = src.lambda[i];
+            w.flag[l] = src.flag[i];
+        } else {
+            w.X[l] = w.Y[l] = w.Z[l] = w.cX[l] = w.cY[l] = w.cZ[l] = w.lambda[l] = 0.0;
+            w.flag[l] = 0;
+        }
+    }
+}
+
+// The same with FP32 positions relative to the ray's beam's origin
+// (DevBeam::origin) and FP32 cosines; the wavelength stays FP64.
+__global__ void k_gather_rows32(const uint32_t* order, uint64_t n, DevRays src, const DevBeam* beams, int n_beams,
+                                void* rows) {
+    Row32* dst = static_cast<Row32*>(rows);
+    const uint64_t total = (n + 31) / 32 * 32;
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < total;
+         t += (uint64_t)blockDim.x * gridDim.x) {
+        Row32& w = dst[t >> 5];
+        const int l = (int)(t & 31);
+        if (t < n) {
+            const uint64_t i = order ? order[t] : t;
+            const DevBeam& b = beams[beam_of(beams, n_beams, i)];
+            w.X[l] = (float)(src.X[i] - b.origin[0]);
+            w.Y[l] = (float)(src.Y[i] - b.origin[1]);
+            w.Z[l] = (float)(src.Z[i] - b.origin[2]);
+            w.cX[l] = (float)src.cX[i];
+            w.cY[l] = (float)src.cY[i];
+            w.cZ[l] = (float)src.cZ[i];
+            w.lambda[l] = src.lambda[i];
+            w.flag[l] = src.flag[i];
+        } else {
+            w.X[l] = w.Y[l] = w.Z[l] = w.cX[l] = w.cY[l] = w.cZ[l] = 0.0f;
+            w.lambda[l] = 0.0;
+            w.flag[l] = 0;
+        }
     }
 }
 

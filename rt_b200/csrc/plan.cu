@@ -17,6 +17,7 @@
 
 #include "engine.cuh"
 #include "jit.h"
+#include "rowpipe.cuh"
 
 using namespace rtb;
 
@@ -33,8 +34,9 @@ struct rtb_plan {
     void* in_mem = nullptr;          // generated rays
     void* out_mem = nullptr;         // output arrays
     uint32_t* order = nullptr;       // coherent tracing order (device), or NULL for index order
-    void* slot_mem = nullptr;        // the input rays in tracing order (with `order`)
+    void* slot_mem = nullptr;        // the input rays in tracing order (with `order`): SoA (FP64 plans)
     DevRays in_slot{};
+    void* rows = nullptr;            // or row blocks (mixed plans: Row64, Row32 for RTB_MIXED32)
     DevRays in{}, out{};
     unsigned long long* h_counts = nullptr;  // page-locked: counters, then the error word
     cudaStream_t stream = nullptr;
@@ -65,12 +67,13 @@ uint64_t plan_key(const rtb_plan& p) {
     h = fnv1a(h, &p.ps.sch, sizeof(DevScheme));
     h = fnv1a(h, p.ps.knots.data(), p.ps.knots.size() * sizeof(double));
     h = fnv1a(h, &p.n_rays, sizeof(p.n_rays));
-    int32_t tags[4] = {p.opts.precision, p.has_frame ? 1 : 0, p.opts.ray_order, p.ps.scheme_kernel ? 1 : 0};
+    int32_t tags[5] = {p.opts.precision, p.has_frame ? 1 : 0, p.opts.ray_order, p.ps.scheme_kernel ? 1 : 0,
+                       p.opts.out_order};
     return fnv1a(h, tags, sizeof(tags));
 }
 
 bool config_ok(const rtb_plan& p, int32_t block, int32_t rpt) {
-    const bool mixed = p.opts.precision == RTB_MIXED;
+    const bool mixed = p.opts.precision == RTB_MIXED || p.opts.precision == RTB_MIXED32;
     if (block != 128 && block != 256 && !(mixed && block == 512)) return false;
     return rpt >= 1 && rpt <= 64;
 }
@@ -110,8 +113,12 @@ int enqueue_run(rtb_plan* p, const FrameArgs& frame, cudaStream_t s) {
     rtb_trace_opts o = p->opts;
     o.block_size = p->block;
     o.rays_per_thread = p->rpt;
-    int st = p->order ? launch_trace(p->ps, p->args, (int)p->n_beams, o, p->in_slot, p->out, frame, s, p->order, true)
-                      : launch_trace(p->ps, p->args, (int)p->n_beams, o, p->in, p->out, frame, s);
+    const bool by_slot = p->opts.out_order == RTB_OUT_SLOT;
+    int st = p->rows    ? launch_trace(p->ps, p->args, (int)p->n_beams, o, p->in, p->out, frame, s, p->order, true,
+                                       p->rows, by_slot)
+             : p->order ? launch_trace(p->ps, p->args, (int)p->n_beams, o, p->in_slot, p->out, frame, s, p->order,
+                                       true, nullptr, by_slot)
+                        : launch_trace(p->ps, p->args, (int)p->n_beams, o, p->in, p->out, frame, s);
     if (st != RTB_OK) return st;
     RTB_CUDA_TRY(cudaMemcpyAsync(p->h_counts, p->args.counts, p->args.counts_len * 8, cudaMemcpyDeviceToHost, s));
     RTB_CUDA_TRY(cudaMemcpyAsync(p->h_counts + p->args.counts_len, p->args.err, 4, cudaMemcpyDeviceToHost, s));
@@ -163,6 +170,7 @@ void release(rtb_plan* p) {
     if (p->out_mem) cudaFree(p->out_mem);
     if (p->order) cudaFree(p->order);
     if (p->slot_mem) cudaFree(p->slot_mem);
+    if (p->rows) cudaFree(p->rows);
     if (p->h_counts) cudaFreeHost(p->h_counts);
     if (p->done) cudaEventDestroy(p->done);
     if (p->stream) cudaStreamDestroy(p->stream);
@@ -189,7 +197,9 @@ int rtb_plan_create(const rtb_surface* surfaces, size_t n_surfaces, const rtb_be
     if (!plan || !opts || !beams || n_beams == 0) return RTB_BAD_VALUE;
     *plan = nullptr;
     if (opts->engine != RTB_ENGINE_FUSED) return RTB_BAD_VALUE;
-    if (opts->precision != RTB_FP64 && opts->precision != RTB_MIXED) return RTB_BAD_VALUE;
+    if (opts->precision != RTB_FP64 && opts->precision != RTB_MIXED && opts->precision != RTB_MIXED32)
+        return RTB_BAD_VALUE;
+    if (opts->out_order != RTB_OUT_INDEX && opts->out_order != RTB_OUT_SLOT) return RTB_BAD_VALUE;
     // compile the kernel specialised to the scheme first, outside the engine
     // lock (NVRTC takes up to a second or so; other calls need not wait)
     if (specialize_enabled()) {
@@ -221,7 +231,7 @@ int rtb_plan_create(const rtb_surface* surfaces, size_t n_surfaces, const rtb_be
     std::vector<GenBeam> gb;
     uint64_t total = 0;
     if ((st = prepare_scheme(surfaces, n_surfaces, opts->fixes, opts->renormalize_lost, p->ps)) != RTB_OK ||
-        (st = check_beams(beams, n_beams, p->n_rays, p->beams_h)) != RTB_OK ||
+        (st = check_beams(beams, n_beams, p->n_rays, p->beams_h, &p->ps.sch)) != RTB_OK ||
         (st = gen_beams(beams, n_beams, p->n_rays, gb, &total)) != RTB_OK) {
         delete p;
         return st;
@@ -289,17 +299,32 @@ int rtb_plan_create(const rtb_surface* surfaces, size_t n_surfaces, const rtb_be
     // costs the mixed kernel 0.8 ms of its 5.3 on C1 against coalesced stores;
     // chunks small enough to stage a block's stores in shared memory lose
     // more in coherence than that.
+    // The mixed kernels read the ordered copy as row blocks of 32 rays
+    // (rowpipe.cuh: one bulk copy per row into shared memory, issued a row
+    // ahead), the FP32-state kernel with FP32 positions relative to each
+    // beam's origin: 57 and 33 bytes per ray.
+    const bool mixed = opts->precision != RTB_FP64;
     if (e == cudaSuccess && opts->ray_order == RTB_ORDER_COHERENT && p->n_rays <= 0xffffffffull) {
         e = cudaMalloc(&p->order, p->n_rays * sizeof(uint32_t));
-        if (e == cudaSuccess) e = cudaMalloc(&p->slot_mem, rays_bytes(p->n_rays, true));
+        const size_t n_rows = (p->n_rays + 31) / 32;
+        const size_t row_size = opts->precision == RTB_MIXED32 ? sizeof(Row32) : sizeof(Row64);
+        if (e == cudaSuccess)
+            e = mixed ? cudaMalloc(&p->rows, n_rows * row_size) : cudaMalloc(&p->slot_mem, rays_bytes(p->n_rays, true));
         if (e == cudaSuccess) {
-            p->in_slot = carve(p->slot_mem, p->n_rays, true);
-            const int chunk_shift = opts->precision == RTB_MIXED ? 20 : 30;
+            if (!mixed) p->in_slot = carve(p->slot_mem, p->n_rays, true);
+            const int chunk_shift = mixed ? 20 : 30;
             st = coherent_order(gbuf.as<GenBeam>(), (int)n_beams, p->n_rays, p->in, p->order, chunk_shift,
                                 p->stream);
             if (st == RTB_OK) {
-                k_gather_rays<<<grid_for(p->n_rays, 256, 8), 256, 0, p->stream>>>(p->order, p->n_rays, p->in,
-                                                                                  p->in_slot);
+                const unsigned g = grid_for(n_rows * 32, 256, 8);
+                if (opts->precision == RTB_MIXED32)
+                    k_gather_rows32<<<g, 256, 0, p->stream>>>(p->order, p->n_rays, p->in, p->args.beams,
+                                                              (int)n_beams, p->rows);
+                else if (mixed)
+                    k_gather_rows64<<<g, 256, 0, p->stream>>>(p->order, p->n_rays, p->in, p->rows);
+                else
+                    k_gather_rays<<<grid_for(p->n_rays, 256, 8), 256, 0, p->stream>>>(p->order, p->n_rays, p->in,
+                                                                                      p->in_slot);
                 e = cudaGetLastError();
             }
             if (st != RTB_OK) {
@@ -345,6 +370,12 @@ int rtb_plan_counts(rtb_plan* p, uint64_t* counts, size_t capacity, size_t* n_en
     const size_t n = p->args.counts_len;
     if (n_entries) *n_entries = n;
     if (counts) std::memcpy(counts, p->h_counts, (capacity < n ? capacity : n) * sizeof(uint64_t));
+    return RTB_OK;
+}
+
+int rtb_plan_order(const rtb_plan* p, const uint32_t** order) {
+    if (!p || !order) return RTB_BAD_VALUE;
+    *order = p->order;
     return RTB_OK;
 }
 

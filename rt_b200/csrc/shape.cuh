@@ -21,10 +21,12 @@ struct RtShape {
     __device__ __forceinline__ static bool non_aux(const DevSurface& s) { return s.non_aux != 0; }
     __device__ __forceinline__ static bool sag_cull(const DevSurface& s) { return s.sag_cull != 0; }
     __device__ __forceinline__ static bool poly_only(const DevSurface& s) { return s.c == 0.0; }
+    __device__ __forceinline__ static bool rot32(const DevSurface& s) { return s.rot32 != 0; }
+    __device__ __forceinline__ static bool first32(const DevSurface& s) { return s.first32 != 0; }
 };
 
 template <int KIND, int TYPE, int CLS, int SHAPE, int GRT, int TRANS, int ROT, int NPOLY, int NONAUX, int SAG,
-          int POLYONLY>
+          int POLYONLY, int ROT32 = 0, int FIRST32 = 0>
 struct FixedShape {
     __device__ __forceinline__ static constexpr int kind(const DevSurface&) { return KIND; }
     __device__ __forceinline__ static constexpr int type(const DevSurface&) { return TYPE; }
@@ -37,6 +39,8 @@ struct FixedShape {
     __device__ __forceinline__ static constexpr bool non_aux(const DevSurface&) { return NONAUX != 0; }
     __device__ __forceinline__ static constexpr bool sag_cull(const DevSurface&) { return SAG != 0; }
     __device__ __forceinline__ static constexpr bool poly_only(const DevSurface&) { return POLYONLY != 0; }
+    __device__ __forceinline__ static constexpr bool rot32(const DevSurface&) { return ROT32 != 0; }
+    __device__ __forceinline__ static constexpr bool first32(const DevSurface&) { return FIRST32 != 0; }
 };
 
 }  // namespace rtb

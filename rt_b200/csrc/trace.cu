@@ -6,6 +6,7 @@
 
 #include "engine.cuh"
 #include "jit.h"
+#include "rowpipe.cuh"
 
 namespace rtb {
 
@@ -23,13 +24,14 @@ DevRays dev_rays(const rtb_rays* r) {
 // structure when one was compiled already in this process (by a plan or
 // rtb_specialize); they never compile one themselves.
 int attach_compiled(PreparedScheme& ps, const rtb_trace_opts& o) {
-    if (o.engine != RTB_ENGINE_FUSED || (o.precision != RTB_MIXED && o.precision != RTB_FP64) ||
-        !specialize_enabled())
+    if (o.engine != RTB_ENGINE_FUSED ||
+        (o.precision != RTB_MIXED && o.precision != RTB_MIXED32 && o.precision != RTB_FP64) || !specialize_enabled())
         return RTB_OK;
     return scheme_kernel(ps.sch, o.precision, &ps.scheme_kernel, nullptr, false);
 }
 
-int check_beams(const rtb_beam* beams, size_t n_beams, size_t n_rays, std::vector<DevBeam>& out) {
+int check_beams(const rtb_beam* beams, size_t n_beams, size_t n_rays, std::vector<DevBeam>& out,
+                const DevScheme* sch) {
     if (!beams || n_beams == 0 || n_beams > (1u << 20)) return RTB_BAD_VALUE;
     out.resize(n_beams);
     uint64_t prev_end = 0;
@@ -44,6 +46,7 @@ int check_beams(const rtb_beam* beams, size_t n_beams, size_t n_rays, std::vecto
         d.n_rays = in.n_rays;
         d.n_orders = in.n_orders;
         for (int g = 0; g < RTB_MAX_GRATINGS; ++g) d.orders[g] = in.orders[g];
+        if (sch) beam_frame(*sch, in.center, d);
     }
     return RTB_OK;
 }
@@ -108,7 +111,7 @@ int gen_beams(const rtb_beam* beams, size_t n_beams, size_t n_rays, std::vector<
 
 int launch_trace(const PreparedScheme& ps, TraceArgs& a, int n_beams, const rtb_trace_opts& o, const DevRays& in,
                  const DevRays& out, const FrameArgs& frame, cudaStream_t st, const uint32_t* order,
-                 bool in_by_slot) {
+                 bool in_by_slot, const void* rows, bool out_by_slot) {
     if (o.engine == RTB_ENGINE_PER_SURFACE) {
         if (o.precision != RTB_FP64) return RTB_BAD_VALUE;
         unsigned grid = grid_for(in.n, 256, 8);
@@ -119,15 +122,20 @@ int launch_trace(const PreparedScheme& ps, TraceArgs& a, int n_beams, const rtb_
                                                  a.counts, a.err);
         if (frame.counts) k_ccd_frame<<<grid, 256, 0, st>>>(out, frame);
     } else if (o.engine == RTB_ENGINE_FUSED) {
-        const bool mixed = o.precision == RTB_MIXED;
+        const bool m32 = o.precision == RTB_MIXED32;
+        const bool mixed = o.precision == RTB_MIXED || m32;
         if (!mixed && o.precision != RTB_FP64) return RTB_BAD_VALUE;
+        if (rows && !mixed) return RTB_BAD_VALUE;
         const int threads = (o.block_size > 0) ? o.block_size : 256;
         if (threads != 128 && threads != 256 && !(mixed && threads == 512)) return RTB_BAD_VALUE;
         const int rpt = (o.rays_per_thread > 0) ? o.rays_per_thread : kDefaultRpt;
         if (rpt < 1 || rpt > 64) return RTB_BAD_VALUE;
-        const size_t smem = fused_smem_bytes(ps.sch.n_knots);
+        size_t smem = fused_smem_bytes(ps.sch.n_knots);
+        if (rows) smem = (smem + 127) / 128 * 128 + (m32 ? row_buffers_bytes<Row32>(threads)
+                                                         : row_buffers_bytes<Row64>(threads));
         if (smem > (size_t)engine().max_smem_optin) return RTB_BAD_VALUE;
         const void* kern = ps.scheme_kernel ? ps.scheme_kernel
+                           : m32           ? reinterpret_cast<const void*>(k_fused_mixed32)
                            : mixed         ? reinterpret_cast<const void*>(k_fused_mixed)
                                            : reinterpret_cast<const void*>(k_fused_fp64);
         RTB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -145,7 +153,7 @@ int launch_trace(const PreparedScheme& ps, TraceArgs& a, int n_beams, const rtb_
         unsigned* err = a.err;
         int state_out = o.state_out ? 1 : 0;
         FrameArgs fr = frame;
-        TileSched ts{a.tiles, rpt, order, in_by_slot ? 1 : 0};
+        TileSched ts{a.tiles, rpt, order, in_by_slot ? 1 : 0, rows, out_by_slot ? 1 : 0};
         void* params[] = {&sch, &knots, &beams, &nb, &rin, &rout, &counts, &err, &state_out, &fr, &ts};
         RTB_CUDA_TRY(cudaLaunchKernel(kern, dim3(grid), dim3(threads), params, smem, st));
     } else {
@@ -182,6 +190,7 @@ int trace_result(const PreparedScheme& ps, const unsigned long long* counts, uns
         stats->failed_beam = failed_beam;
         stats->failed_stage = failed_stage;
     }
+    if (err & DEV_ERR_TIMEOUT) return RTB_FAILED;
     if (err & DEV_ERR_OUT_OF_RANGE) return RTB_OUT_OF_RANGE;
     if (err) return RTB_BAD_VALUE;
     if (failed_beam >= 0) return (failed_stage % 3 == 2) ? RTB_NO_GOOD_RAYS : RTB_NO_INTERSECTIONS;
@@ -224,7 +233,7 @@ int rtb_trace(const rtb_surface* surfaces, size_t n_surfaces, const rtb_beam* be
         (st = attach_compiled(ps, *opts)) != RTB_OK)
         return st;
     std::vector<DevBeam> db;
-    if ((st = check_beams(beams, n_beams, rays->n, db)) != RTB_OK) return st;
+    if ((st = check_beams(beams, n_beams, rays->n, db, &ps.sch)) != RTB_OK) return st;
     TraceArgs a;
     if ((st = a.init(ps, db, s)) != RTB_OK) return st;
     FrameArgs frame = frame_args(opts);
@@ -251,7 +260,7 @@ int rtb_trace_out(const rtb_surface* surfaces, size_t n_surfaces, const rtb_beam
         (st = attach_compiled(ps, *opts)) != RTB_OK)
         return st;
     std::vector<DevBeam> db;
-    if ((st = check_beams(beams, n_beams, in->n, db)) != RTB_OK) return st;
+    if ((st = check_beams(beams, n_beams, in->n, db, &ps.sch)) != RTB_OK) return st;
     TraceArgs a;
     if ((st = a.init(ps, db, s)) != RTB_OK) return st;
     FrameArgs frame = frame_args(opts);
@@ -343,7 +352,7 @@ int trace_host_impl(const rtb_surface* surfaces, size_t n_surfaces, const rtb_be
     if (st == RTB_OK) st = attach_compiled(ps, *opts);
     if (st != RTB_OK) return st;
     std::vector<DevBeam> db;
-    if ((st = check_beams(beams, n_beams, h->n, db)) != RTB_OK) return st;
+    if ((st = check_beams(beams, n_beams, h->n, db, &ps.sch)) != RTB_OK) return st;
     const uint64_t n = h->n;
     if (n == 0) return RTB_OK;
     if (chunk == 0) chunk = (size_t)1 << 22;

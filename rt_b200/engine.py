@@ -39,6 +39,7 @@ def lib() -> C.CDLL:
         L.rtb_plan_run.argtypes = [vp, vp]
         L.rtb_plan_result.argtypes = [vp, P(ffi.TraceStats)]
         L.rtb_plan_rays.argtypes = [vp, P(ffi.Rays), P(ffi.Rays)]
+        L.rtb_plan_order.argtypes = [vp, P(vp)]
         L.rtb_plan_counts.argtypes = [vp, vp, C.c_size_t, P(C.c_size_t)]
         L.rtb_plan_autotune.argtypes = [vp, C.c_int, P(ffi.TuneEntry), C.c_size_t, P(C.c_size_t)]
         L.rtb_plan_set_config.argtypes = [vp, C.c_int32, C.c_int32]
@@ -151,17 +152,24 @@ def _beams(beams):
 
 
 def generate(beams, n: int, stream=None) -> DeviceRays:
+    """Seeded rays of `beams` on the device.  Without a stream the generator
+    runs on the library's own stream, which is not ordered with torch's, so
+    the call waits for it: the rays are complete when it returns."""
     rays = DeviceRays(n)
     st = lib().rtb_generate_beams(_beams(beams), len(beams), C.byref(rays.struct()), stream)
     ffi.check(st, "rtb_generate_beams")
+    if stream is None:
+        import torch
+        torch.cuda.synchronize()
     return rays
 
 
 def opts(engine=ffi.ENGINE_FUSED, precision=ffi.FP64, fixes=0, renorm_lost=1, state_out=1, block=0, rpt=0,
-         ccd=None, counts=None, n_outside=None) -> ffi.TraceOpts:
+         ccd=None, counts=None, n_outside=None, out_order=ffi.OUT_INDEX) -> ffi.TraceOpts:
     o = ffi.TraceOpts()
     o.engine, o.precision, o.fixes, o.renormalize_lost = engine, precision, fixes, renorm_lost
     o.block_size, o.rays_per_thread, o.state_out = block, rpt, state_out
+    o.out_order = out_order
     if ccd is not None:
         o._ccd = ccd  # keep alive
         o.ccd = C.pointer(ccd)
@@ -250,6 +258,16 @@ class Plan:
         i, o = ffi.Rays(), ffi.Rays()
         ffi.check(lib().rtb_plan_rays(self.h, C.byref(i), C.byref(o)), "rtb_plan_rays")
         return i, o
+
+    def order(self, n: int):
+        """The tracing order (slot -> ray index) as a device tensor of n int64,
+        or None for a plan in index order."""
+        import torch
+        p = C.c_void_p()
+        ffi.check(lib().rtb_plan_order(self.h, C.byref(p)), "rtb_plan_order")
+        if not p.value:
+            return None
+        return torch.as_tensor(_DevArray(p.value, n, "<i4"), device="cuda").to(torch.int64) & 0xFFFFFFFF
 
     def autotune(self, reps=3):
         table = (ffi.TuneEntry * 16)()

@@ -28,11 +28,12 @@ MIRROR, LENS, GRATING, STOP, SHADE, DETECTOR, AUX_TYPE = range(7)
 CIRCLE, RECTANGLE = range(2)
 REFLECTIVE, TRANSPARENT = range(2)
 ENGINE_PER_SURFACE, ENGINE_FUSED = range(2)
-FP64, MIXED = range(2)
+FP64, MIXED, MIXED32 = range(3)
 FIX_TORIC_SIGN = 1
 FIX_TORIC_STEP = 2
 FIX_ASPHERE_ROOT = 4
 ORDER_COHERENT, ORDER_INDEX = 0, 1
+OUT_INDEX, OUT_SLOT = 0, 1
 
 MAX_POLY = 10
 MAX_PARAMS = 16
@@ -76,7 +77,8 @@ class TraceOpts(C.Structure):
     _fields_ = [("engine", C.c_int32), ("precision", C.c_int32), ("fixes", C.c_uint32),
                 ("renormalize_lost", C.c_int32), ("block_size", C.c_int32), ("rays_per_thread", C.c_int32),
                 ("state_out", C.c_int32), ("ray_order", C.c_int32), ("ccd", C.POINTER(CCD)),
-                ("counts", C.c_void_p), ("n_outside", C.c_void_p)]
+                ("counts", C.c_void_p), ("n_outside", C.c_void_p), ("out_order", C.c_int32),
+                ("reserved", C.c_int32)]
 
 
 class TraceStats(C.Structure):

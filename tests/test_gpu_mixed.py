@@ -1,5 +1,6 @@
-"""Accuracy of the fused mixed-precision kernel against the FP64 engine
-(GPU tests): CCD position error p99.9 <= 0.05 um, and the same rays lost."""
+"""Accuracy of the fused mixed-precision kernels (FP64 state, RTB_MIXED; FP32
+state, RTB_MIXED32) against the FP64 engine (GPU tests): CCD position error
+p99.9 <= 0.05 um, and the same rays lost."""
 import numpy as np
 import pytest
 import torch
@@ -10,18 +11,19 @@ from rt_b200 import ffi, metrics, schemes as S
 pytestmark = pytest.mark.gpu
 
 
-def _trace_pair(specs, beams, n, fixes):
+def _trace_pair(specs, beams, n, fixes, precision):
     cs = S.to_c(specs, E.spline_init)
     rays = E.generate(beams, n)
     ref = rays.copy()
-    st_m, stats_m = E.trace(cs.surfaces, beams, rays, E.opts(precision=ffi.MIXED, fixes=fixes))
+    st_m, stats_m = E.trace(cs.surfaces, beams, rays, E.opts(precision=precision, fixes=fixes))
     st_r, stats_r = E.trace(cs.surfaces, beams, ref, E.opts(precision=ffi.FP64, fixes=fixes))
     assert st_m == st_r == ffi.OK
     return rays, ref, stats_m, stats_r
 
 
+@pytest.mark.parametrize("precision", [ffi.MIXED, ffi.MIXED32])
 @pytest.mark.parametrize("case", ["c0", "c4", "c1"])
-def test_mixed_ccd_error(case):
+def test_mixed_ccd_error(case, precision):
     if case == "c1":
         specs, beams, ccd = S.echelle(), S.c1_beams(n_per_lambda=800), S.C1_CCD
     elif case == "c4":
@@ -29,10 +31,10 @@ def test_mixed_ccd_error(case):
     else:
         specs, beams, ccd = S.littrow_free(), S.c0_beams(n_per_lambda=40000), S.C0_CCD
     n = S.total_rays(beams)
-    rays, ref, sm, sr = _trace_pair(specs, beams, n, fixes=3)
+    rays, ref, sm, sr = _trace_pair(specs, beams, n, 3, precision)
     m = metrics.ccd_error(rays.X, rays.Y, rays.flag, ref.X, ref.Y, ref.flag, ccd["xsize"], ccd["ysize"],
                           ccd["xpix"], ccd["ypix"])
-    print(case, m)
+    print(case, precision, m)
     assert m["rays_compared"] > 0.2 * n
     assert m["p99_9_um"] <= 0.05
     assert m["pixel_mismatch_rate"] < 1e-3

@@ -33,7 +33,7 @@ def _nvrtc_present():
 
 
 @pytest.mark.skipif(not _nvrtc_present(), reason="libnvrtc not present")
-@pytest.mark.parametrize("precision", [ffi.MIXED, ffi.FP64])
+@pytest.mark.parametrize("precision", [ffi.MIXED, ffi.MIXED32, ffi.FP64])
 @pytest.mark.parametrize("name", sorted(SCHEMES))
 def test_specialised_kernel_compiles(name, precision):
     cs = S.to_c(SCHEMES[name](), O.spline_init)
@@ -90,10 +90,13 @@ def test_jit_disk_cache(tmp_path):
 
 
 @pytest.mark.skipif(not _nvrtc_present(), reason="libnvrtc not present")
-def test_kernels_are_shared_by_structure(tmp_path):
-    """A kernel is specialised to a scheme's structure, not to its numbers:
-    C0 with another collimator curvature and camera distance compiles to the
-    same kernel (one cache file), C0 with an asphere camera to another."""
+@pytest.mark.parametrize("mode", ["values", "structure"])
+def test_kernels_are_shared_by_what_they_bake(tmp_path, mode):
+    """By default a kernel bakes in its scheme's surface constants: C0 with
+    another collimator curvature and camera distance compiles to a kernel of
+    its own.  With RTB_SPECIALIZE=structure only the structure is fixed: the
+    two compile to the same kernel (one cache file), C0 with an asphere
+    camera to another."""
     import os
     import subprocess
     import sys
@@ -110,6 +113,8 @@ def test_kernels_are_shared_by_structure(tmp_path):
             "    print(len([f for f in __import__('os').listdir(%r) if f.endswith('.cubin')]))\n"
             ) % (root, os.path.join(root, "oracle"), str(tmp_path))
     env = dict(os.environ, RTB_JIT_CACHE=str(tmp_path))
+    if mode == "structure":
+        env["RTB_SPECIALIZE"] = "structure"
     out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env, timeout=300)
     assert out.returncode == 0, out.stderr
-    assert out.stdout.split() == ["1", "1", "2"]
+    assert out.stdout.split() == (["1", "2", "3"] if mode == "values" else ["1", "1", "2"])
