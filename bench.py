@@ -44,15 +44,19 @@ WORKLOAD = ("C1 cross-dispersed echelle: 1.0e8 rays (31 echelle orders 30..60 x 
             "x 50404 rays, disk r=25 mm), OAP + echelle + cross-disperser + toric fold + 2 even-asphere lens "
             "surfaces + CCD 4096^2, frame counts accumulated")
 FIXES = 3  # RTB_FIX_TORIC_SIGN | RTB_FIX_TORIC_STEP: the toric fold's Steffensen step divides 0/0 otherwise
-# DRAM bytes per ray of the headline kernel (rtb_fused_mixed_scheme, the
-# mixed kernel compiled for C1's structure): ncu dram__bytes_read + write of
-# one launch on C1 at 1,984,000 rays
-TRAFFIC_PER_RAY_MIXED = (143.441920e6 + 27.038208e6) / 1_984_000
-# FP64 / FP32 floating-point operations it executes per ray on C1 (ncu
-# sm__sass_thread_inst_executed_op_{dfma x2, dadd, dmul} and the f32 ones,
-# same capture workload): the compute side of its roofline
-F64_FLOPS_PER_RAY_MIXED = 717.75
-F32_FLOPS_PER_RAY_MIXED = 57.91
+# Per-ray figures of the two mixed kernels (compiled for C1 with its surface
+# constants baked in) from one ncu capture each of one launch on C1 at
+# 1,001,728 rays per 0.1 of the workload (31 x 64 x 5,049 rays, 1.0e7 rays:
+# inputs 4x the L2): DRAM bytes read + written, and the executed FP64 / FP32
+# floating-point operations (ncu op counters, FMA = 2, FFMA2 = 4).  None
+# where no capture of the current kernel exists.
+KERNEL_PROFILE = {
+    "fused_mixed": {"traffic_per_ray": None, "f64_flops_per_ray": None, "f32_flops_per_ray": None},
+    "fused_mixed32": {"traffic_per_ray": None, "f64_flops_per_ray": None, "f32_flops_per_ray": None},
+}
+# bytes of input per ray the mixed kernels read: a plan's 32-ray row blocks
+# (Row64: 1824 B, Row32: 1056 B per 32 rays)
+ROW_BYTES_PER_RAY = {"fused_mixed": 1824 / 32, "fused_mixed32": 1056 / 32}
 # bytes per ray-surface of a minimal per-surface FP64 pass: read X..cZ, lambda,
 # flag (57 B), write X..cZ, flag (49 B)
 ALG_BYTES_PER_RAY_SURFACE = 106
@@ -73,7 +77,7 @@ def parse():
     p.add_argument("--no-c4", action="store_true")
     p.add_argument("--c4-rays-per-lambda", type=int, default=156250, help="C4 adjoint: rays per wavelength (x64)")
     p.add_argument("--no-autotune", action="store_true", help="default launch configuration (profiling runs)")
-    p.add_argument("--engines", default="per_surface,fused_fp64,fused_mixed")
+    p.add_argument("--engines", default="per_surface,fused_fp64,fused_mixed,fused_mixed32")
     return p.parse_args()
 
 
@@ -348,8 +352,29 @@ def main():
         return ms / K, stats
 
     engines = {}
-    mk = lambda eng, prec: E.opts(engine=eng, precision=prec, fixes=FIXES, state_out=0, ccd=ccd, counts=counts,
-                                  n_outside=outside)
+    mk = lambda eng, prec, out_order=ffi.OUT_INDEX: E.opts(engine=eng, precision=prec, fixes=FIXES, state_out=0,  # noqa
+                                                          ccd=ccd, counts=counts, n_outside=outside,
+                                                          out_order=out_order)
+    FUSED = (("fused_fp64", ffi.FP64), ("fused_mixed", ffi.MIXED), ("fused_mixed32", ffi.MIXED32))
+    MIXED_ENGINES = {"fused_mixed": ffi.MIXED, "fused_mixed32": ffi.MIXED32}
+    PREC = dict(FUSED)
+    KERNELS = {ffi.FP64: ("rtb_fused_fp64_scheme", "k_fused_fp64"),
+               ffi.MIXED: ("rtb_fused_mixed_scheme", "k_fused_mixed"),
+               ffi.MIXED32: ("rtb_fused_mixed32_scheme", "k_fused_mixed32")}
+
+    def by_index(plan, n_rays):
+        """A plan's X, Y and flags at the rays' indices (its outputs are at
+        the tracing slots)."""
+        out = E.device_view(plan.rays()[1])
+        order = plan.order(n_rays)
+        if order is None:
+            return out
+        res = {}
+        for k in ("X", "Y", "flag"):
+            t = torch.empty_like(out[k])
+            t[order] = out[k]
+            res[k] = t
+        return res
 
     def traced(st):
         # beams whose every ray is lost are reported (first one in stats), the
@@ -391,86 +416,109 @@ def main():
         except RuntimeError as e:
             engines["per_surface"] = {"error": str(e)}
     # the fused kernels: a plan each (rays generated in HBM once, one graph
-    # launch per step, launch configuration from the autotuner)
-    for name, prec in (("fused_fp64", ffi.FP64), ("fused_mixed", ffi.MIXED)):
+    # launch per step, launch configuration from the autotuner), outputs
+    # stored at the tracing slot (RTB_OUT_SLOT; rtb_plan_order maps them to
+    # the rays)
+    clocks_of = {}
+    for name, prec in FUSED:
         if name not in want:
             continue
         try:
             torch.cuda.synchronize()
             t_create = time.perf_counter()
-            plan = E.Plan(surf, beams, mk(ffi.ENGINE_FUSED, prec))
+            plan = E.Plan(surf, beams, mk(ffi.ENGINE_FUSED, prec, out_order=ffi.OUT_SLOT))
             torch.cuda.synchronize()
             t_create = time.perf_counter() - t_create
             table = [] if args.no_autotune else plan.autotune(reps=2)
             block, rpt, _ = plan.config()
-            if name == "fused_mixed" or "fused_mixed" not in want:
+            if prec != ffi.FP64 or not (want & set(MIXED_ENGINES)):
                 with Clocks(local) as ck:
                     ms, stats = timed_plan(plan, args.steps, args.warmup)
-                clocks = ck.summary()
+                clocks_of[name] = ck.summary()
             else:
                 ms, stats = timed_plan(plan, max(2, args.steps // 4), 1)
-            # the same plan in index order: what the coherent tracing order gains
-            o_idx = mk(ffi.ENGINE_FUSED, prec)
-            o_idx.ray_order = ffi.ORDER_INDEX
-            p_idx = E.Plan(surf, beams, o_idx)
-            ffi.check(p_idx.set_config(block, rpt), "rtb_plan_set_config")
-            ms_idx, _ = timed_plan(p_idx, max(2, args.steps // 4), 1)
-            p_idx.destroy()
+            # the same plan storing at the rays' indices, and in index order:
+            # what the slot-order stores and the coherent order gain
+            variants = {}
+            for key, ro, oo in (("index_outputs", ffi.ORDER_COHERENT, ffi.OUT_INDEX),
+                                ("index_order", ffi.ORDER_INDEX, ffi.OUT_INDEX)):
+                o_v = mk(ffi.ENGINE_FUSED, prec, out_order=oo)
+                o_v.ray_order = ro
+                p_v = E.Plan(surf, beams, o_v)
+                ffi.check(p_v.set_config(block, rpt), "rtb_plan_set_config")
+                ms_v, _ = timed_plan(p_v, max(2, args.steps // 4), 1)
+                variants[key] = {"ms_per_step": ms_v, "value": stats.rs / (ms_v * 1e-3)}
+                p_v.destroy()
         except RuntimeError as e:
             engines[name] = {"error": str(e)}
             continue
         plans[name] = plan
         spec_on, spec_note = plan.specialized()
+        kname, generic = KERNELS[prec]
         engines[name] = {"ms_per_step": ms, "value": stats.rs / (ms * 1e-3),
-                         "kernel": ((("rtb_fused_mixed_scheme (k_fused_mixed" if prec == ffi.MIXED else
-                                     "rtb_fused_fp64_scheme (k_fused_fp64") +
-                                    " compiled for the scheme's structure with NVRTC when the plan is made)")
-                                   if spec_on else ("k_fused_mixed" if prec == ffi.MIXED else "k_fused_fp64")),
+                         "kernel": (f"{kname} ({generic} compiled with NVRTC for the scheme when the plan is "
+                                    "made: structure fixed, surface constants baked in)") if spec_on else generic,
                          "specialised": spec_on, "specialise_note": spec_note,
                          "ray_surfaces_per_step": stats.ray_surfaces, "n_good": stats.n_good,
                          "launch": f"rtb_plan_run (CUDA graph), block {block} x {rpt} rays/thread"
                                    + ("" if args.no_autotune else " (autotuned)"),
                          "ray_order": "coherent (beam, wavelength, Morton code of the entrance position), "
                                       "sorted once when the plan is made",
-                         "plan_create_s": t_create,
-                         "index_order": {"ms_per_step": ms_idx,
-                                         "value": stats.rs / (ms_idx * 1e-3)},
+                         "outputs": "at the tracing slot (RTB_OUT_SLOT)",
+                         "plan_create_s": t_create, **variants,
                          "autotune_ms": {f"{b}x{r}": round(t, 4) for b, r, t in table}}
-        head = name if (head is None or name == "fused_mixed") else head
+
+    # accuracy of each mixed engine against the FP64 plan on the same rays
+    # (the plans generate identical rays from the same beam table)
+    accuracy = {}
+    if "fused_fp64" in plans:
+        from rt_b200 import metrics
+        ref = by_index(plans["fused_fp64"], n)
+        for name in MIXED_ENGINES:
+            if name in plans:
+                a = by_index(plans[name], n)
+                accuracy[name] = metrics.ccd_error(a["X"], a["Y"], a["flag"], ref["X"], ref["Y"], ref["flag"],
+                                                   ccd.xsize, ccd.ysize, ccd.xpix, ccd.ypix)
+                engines[name]["accuracy_vs_fp64"] = accuracy[name]
+    for p_ in plans.values():
+        p_.destroy()
+    plans.clear()
+    # the headline: the faster mixed engine within 0.05 um at p99.9
+    for name in MIXED_ENGINES:
+        e = engines.get(name, {})
+        ok = "value" in e and (name not in accuracy or accuracy[name].get("p99_9_um", 1e9) <= 0.05)
+        if ok and (head is None or e["ms_per_step"] < engines[head]["ms_per_step"]):
+            head = name
+    if head is None and "value" in engines.get("fused_fp64", {}):
+        head = "fused_fp64"
+    clocks = clocks_of.get(head)
     if head is None and "value" in engines.get("per_surface", {}):
         head = "per_surface"
     if head is None:
         raise SystemExit("no engine ran")
     hv = engines[head]
 
-    # accuracy of the mixed kernel against the FP64 kernel on the same rays
-    # (the two plans generate identical rays from the same beam table)
-    accuracy = None
-    if "fused_mixed" in plans and "fused_fp64" in plans:
-        from rt_b200 import metrics
-        a = E.device_view(plans["fused_mixed"].rays()[1])
-        b = E.device_view(plans["fused_fp64"].rays()[1])
-        accuracy = metrics.ccd_error(a["X"], a["Y"], a["flag"], b["X"], b["Y"], b["flag"], ccd.xsize, ccd.ysize,
-                                     ccd.xpix, ccd.ypix)
-    for p_ in plans.values():
-        p_.destroy()
-    plans.clear()
-
+    head_prec = PREC.get(head, ffi.FP64)
     # C3: 512 beams of uneven size, wavelength, field angle and order in one
-    # graph launch of the mixed kernel, launch configuration autotuned
+    # graph launch of the headline kernel, launch configuration autotuned.
+    # Most of C3's rays are lost early (random order x wavelength: 192 of the
+    # 512 beams reach the CCD), so its ray-surfaces/s is not comparable with
+    # C1's.
     c3 = None
-    if not args.no_c3 and "fused_mixed" in want:
+    if not args.no_c3 and head in MIXED_ENGINES:
         b3 = S.c3_beams()
-        plan = E.Plan(surf, b3, mk(ffi.ENGINE_FUSED, ffi.MIXED))
+        plan = E.Plan(surf, b3, mk(ffi.ENGINE_FUSED, head_prec, out_order=ffi.OUT_SLOT))
         table = [] if args.no_autotune else plan.autotune(reps=3)
         block, rpt, n3 = plan.config()
         ms3, st3 = timed_plan(plan, args.steps, args.warmup)
         cnt = plan.counts()
-        c3 = {"beams": len(b3), "n_rays": n3, "beams_with_good_rays": int((cnt[:, -1] > 0).sum()), "ray_surfaces_per_run": st3.ray_surfaces, "n_good": st3.n_good,
-              "ms_per_run": ms3, "value": st3.rs / (ms3 * 1e-3), "unit": UNIT,
+        c3 = {"beams": len(b3), "n_rays": n3, "beams_with_good_rays": int((cnt[:, -1] > 0).sum()),
+              "ray_surfaces_per_run": st3.ray_surfaces, "n_good": st3.n_good,
+              "ms_per_run": ms3, "value": st3.rs / (ms3 * 1e-3), "unit": UNIT, "engine": head,
               "config": {"block_size": block, "rays_per_thread": rpt},
               "autotune_ms": {f"{b}x{r}": round(t, 4) for b, r, t in table},
-              "how": "rtb_plan_run: one CUDA graph (counter clear, fused mixed kernel, counter copy) per run"}
+              "note": "most rays are lost early (192 of 512 beams reach the CCD): not comparable with C1",
+              "how": "rtb_plan_run: one CUDA graph (counter clear, fused kernel, counter copy) per run"}
         plan.destroy()
 
     # C4: the adjoint pair (gradient of the spot merit in 24 parameters)
@@ -482,9 +530,12 @@ def main():
             c4 = {"error": str(e)}
 
     # roofline of the headline kernel (HBM view): algorithmic bytes per launch
-    # = 57 B read (X,Y,Z,cX,cY,cZ,lambda,flag) + 18 B written (X,Y,flag,
-    # lost_stage) per ray + 4 B per ray counted on the frame.
-    alg_bytes = n * (57 + 18) + hv["n_good"] * 4
+    # = its input rows (Row64: 57 B, Row32: 33 B per ray) + 18 B written per
+    # ray (X, Y, flag, lost_stage at the tracing slot) + 4 B per ray counted
+    # on the frame
+    prof = KERNEL_PROFILE.get(head, {})
+    in_bytes = ROW_BYTES_PER_RAY.get(head, 57 + 4)
+    alg_bytes = n * (in_bytes + 18) + hv["n_good"] * 4
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -492,28 +543,26 @@ def main():
         pass
     peak = peaks.get("hbm_gbs", 6650.0)
     achieved = alg_bytes / (hv["ms_per_step"] * 1e-3) / 1e9
-    # DRAM traffic of the headline kernel from an ncu capture of the same
-    # workload at 1,984,000 rays (143.4 MB read + 27.0 MB written, the
-    # tracing-order index included), scaled by rays
-    traffic = TRAFFIC_PER_RAY_MIXED * n if head == "fused_mixed" else None
+    tpr = prof.get("traffic_per_ray")
+    traffic = tpr * n if tpr else None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "traffic_per_ray_bytes": TRAFFIC_PER_RAY_MIXED if traffic else None,
-                "alg_bytes": alg_bytes,
-                "kernel": (hv.get("kernel", "k_fused_mixed").split(" ")[0]) if head == "fused_mixed" else "k_fused_fp64",
+                "traffic": traffic, "traffic_per_ray_bytes": tpr, "alg_bytes": alg_bytes,
+                "alg_bytes_per_ray": alg_bytes / n,
+                "kernel": hv.get("kernel", "").split(" ")[0],
                 "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "fallback",
-                "note": "HBM view of a kernel bound by instruction issue and FP64 latency: ncu shows issue "
-                        "slots 57% busy, FP64 pipe 45% active, 29.2/32 threads active per instruction, "
-                        "DRAM 14% of peak"}
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch on C1 at "
+                                  "1.0e7 rays, per ray, times the rays of a step" if tpr else None,
+                "note": "HBM view of a kernel bound by instruction issue (no FP64, FP32 or memory pipe "
+                        "saturated): the compute roofline is roofline_fp64"}
 
-    # end to end through the C ABI on host arrays: every rank its own rays,
-    # each step started together, the slowest rank's wall time
     # compute roofline of the headline kernel: executed FP64 flops per second
     # against cuBLAS DGEMM measured here
     fp64_peak = dgemm_tflops()
-    f64_achieved = F64_FLOPS_PER_RAY_MIXED * n / (hv["ms_per_step"] * 1e-3) / 1e12 if head == "fused_mixed" else None
+    f64pr = prof.get("f64_flops_per_ray")
+    f64_achieved = f64pr * n / (hv["ms_per_step"] * 1e-3) / 1e12 if f64pr else None
     roofline_fp64 = {"bound": "fp64", "achieved": f64_achieved, "peak": fp64_peak, "unit": "TFLOP/s",
                      "frac": (f64_achieved / fp64_peak) if (f64_achieved and fp64_peak) else None,
-                     "flops_per_ray": F64_FLOPS_PER_RAY_MIXED, "f32_flops_per_ray": F32_FLOPS_PER_RAY_MIXED,
+                     "executed_flops_per_ray": f64pr, "f32_executed_flops_per_ray": prof.get("f32_flops_per_ray"),
                      "peak_source": "cuBLAS DGEMM 4096^3 measured in this run (best of 5)",
                      "note": "executed FP64 operations (FMA = 2) from ncu op counters, Newton refinements of "
                              "reciprocals and square roots included"}
@@ -527,13 +576,11 @@ def main():
     if not args.no_e2e:
         h = E.PinnedRays(n)
         src_cpu = {f: getattr(rays_in, f).cpu().numpy() for f in E.FIELDS}
-        o = mk(ffi.ENGINE_FUSED, ffi.MIXED if head == "fused_mixed" else ffi.FP64)
+        o = mk(ffi.ENGINE_FUSED, head_prec)
         # the kernel compiled for the scheme (cached from the plan above;
         # rtb_specialize is the call a user makes ahead of one-shot traces)
         st_s, note = E.specialize(surf, FIXES, o.precision)
-        mixed = head == "fused_mixed"
-        spec = (("rtb_fused_mixed_scheme" if mixed else "rtb_fused_fp64_scheme") if st_s == ffi.OK else
-                ("k_fused_mixed" if mixed else "k_fused_fp64") + f" ({note})")
+        spec = KERNELS[head_prec][0] if st_s == ffi.OK else KERNELS[head_prec][1] + f" ({note})"
         times = []
         for it in range(2 + max(1, args.steps // 3)):
             for f in E.FIELDS:
@@ -560,10 +607,10 @@ def main():
     if rank == 0:
         line = {"metric": METRIC, "value": hv["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": hv["ms_per_step"], "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if head == "fused_mixed" else "f64",
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if head in MIXED_ENGINES else "f64",
                 "data": "synthetic",
                 "config": {"workload": WORKLOAD, "n_rays": n, "engine": head, "beams": len(beams),
-                           "l2": "inputs (5.7 GB) larger than L2", "toric_fixes": FIXES},
+                           "l2": "inputs (3.3-5.7 GB) larger than L2", "toric_fixes": FIXES},
                 "engines": engines,
                 "speedup_vs_plain_fp64": (hv["value"] / engines["per_surface"]["value"])
                 if "per_surface" in engines and "value" in engines["per_surface"] else None,

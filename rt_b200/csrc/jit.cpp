@@ -186,8 +186,17 @@ static std::string surface_constants(const DevScheme& sch) {
     return t;
 }
 
+// Register cap of the specialised kernels: 64 (32 warps per SM), or
+// RTB_JIT_MAXNREG (32..128) to measure other occupancies.
+static std::string jit_maxnreg() {
+    const char* e = std::getenv("RTB_JIT_MAXNREG");
+    const int v = e ? std::atoi(e) : 0;
+    return std::to_string((v >= 32 && v <= 128) ? v : 64);
+}
+
 std::string scheme_source(const DevScheme& sch, int precision) {
     std::string src;
+    const std::string maxnreg = jit_maxnreg();
     const bool bake = bake_values();
     const std::string S = bake ? "k_surfaces()[" : "sch->s[";
     const std::string F = bake ? "k_fixes" : "sch->fixes";
@@ -196,14 +205,14 @@ std::string scheme_source(const DevScheme& sch, int precision) {
               "namespace rtb {\n"
               "struct SchemeSurfaces {\n"
               "    __device__ __forceinline__ static void run(const DevScheme* sch, const double* knots,\n"
-              "        const DevBeam* beams, int b, double lam, mx::TableMemo& memo, mx::Ray& r, int& stage) {\n";
+              "        const BeamCtx& bc, double lam, mx::TableMemo& memo, mx::Ray& r, int& stage) {\n";
         for (int k = 0; k < sch.n_surfaces; ++k) {
             const std::string ks = std::to_string(k);
             src += "        if (stage == -1) stage = mx_surface<" + fixed_shape(sch.s[k]) + ">(" + S + ks + "], " +
-                   ks + ", " + F + ", knots, beams, b, lam, memo, r);\n";
+                   ks + ", " + F + ", knots, bc, lam, memo, r);\n";
         }
         src += std::string("    }\n};\n}  // namespace rtb\n"
-                           "extern \"C\" __global__ void __maxnreg__(64) ") + kMixedName + "(\n" + kParams +
+                           "extern \"C\" __global__ void __maxnreg__(" + maxnreg + ") ") + kMixedName + "(\n" + kParams +
                "    rtb::fused_mixed<rtb::SchemeSurfaces>(g_sch, knots, beams, n_beams, in, out, counts, err,\n"
                "                                        state_out, frame, ts);\n}\n";
     } else if (precision == RTB_MIXED32) {
@@ -211,16 +220,16 @@ std::string scheme_source(const DevScheme& sch, int precision) {
               "namespace rtb {\n"
               "struct SchemeSurfaces32 {\n"
               "    __device__ __forceinline__ static void run(const DevScheme* sch, const double* knots,\n"
-              "        const DevBeam* beams, int b, double lam, mx::TableMemo& memo, m32::Ray& r, mx::Ray& q,\n"
-              "        int& stage) {\n";
+              "        const BeamCtx& bc, const double* off0, double lam, mx::TableMemo& memo, m32::Ray& r,\n"
+              "        mx::Ray& q, int& stage) {\n";
         for (int k = 0; k < sch.n_surfaces; ++k) {
             if (!sch.s[k].non_aux) continue;  // folded into the next surface's transform
             const std::string ks = std::to_string(k);
             src += "        if (stage == -1) stage = m32_surface<" + fixed_shape(sch.s[k]) + ">(" + S + ks + "], " +
-                   ks + ", " + F + ", knots, beams, b, lam, memo, r, q);\n";
+                   ks + ", " + F + ", knots, bc, off0, lam, memo, r, q);\n";
         }
         src += std::string("    }\n};\n}  // namespace rtb\n"
-                           "extern \"C\" __global__ void __maxnreg__(64) ") + kMixed32Name + "(\n" + kParams +
+                           "extern \"C\" __global__ void __maxnreg__(" + maxnreg + ") ") + kMixed32Name + "(\n" + kParams +
                "    rtb::fused_mixed32<rtb::SchemeSurfaces32>(g_sch, knots, beams, n_beams, in, out, counts, err,\n"
                "                                            state_out, frame, ts);\n}\n";
     } else {
@@ -235,7 +244,7 @@ std::string scheme_source(const DevScheme& sch, int precision) {
                    F + ", knots, beams, b, lam, err, r, stage);\n        __syncthreads();\n";
         }
         src += std::string("    }\n};\n}  // namespace rtb\n"
-                           "extern \"C\" __global__ void __maxnreg__(64) ") + kFp64Name + "(\n" + kParams +
+                           "extern \"C\" __global__ void __maxnreg__(" + maxnreg + ") ") + kFp64Name + "(\n" + kParams +
                "    rtb::fused_fp64<rtb::SchemeSurfacesF64>(g_sch, knots, beams, n_beams, in, out, counts, err,\n"
                "                                          state_out, frame, ts);\n}\n";
     }

@@ -538,15 +538,14 @@ __device__ __forceinline__ int action(const DevSurface& s, const double* knots, 
 // unit vector, so here the cosines are normalised once, when a ray is loaded.
 template <class Sh = RtShape>
 __device__ __forceinline__ int mx_surface(const DevSurface& s, int k, uint32_t fixes, const double* knots,
-                                          const DevBeam* beams, int b, double lam, mx::TableMemo& memo, mx::Ray& r) {
+                                          const BeamCtx& bc, double lam, mx::TableMemo& memo, mx::Ray& r) {
     mx::transform<Sh>(s, r);
     if (!Sh::non_aux(s)) return -1;
     const int hit = mx::intersect<Sh>(s, fixes, r);
     if (hit == 1) return 3 * k;
     if (hit == 2) return 3 * k + 1;
     if (!f64::aperture_pass(Sh::type(s) == RTB_SHADE, Sh::shape(s), s.size, s.center, r.X, r.Y)) return 3 * k + 1;
-    long long order = s.order;
-    if (Sh::type(s) == RTB_GRATING && beams[b].n_orders > 0) order = beams[b].orders[s.grating_index];
+    const long long order = (Sh::type(s) == RTB_GRATING) ? bc.order(s) : s.order;
     int a = mx::action<Sh>(s, knots, order, lam, memo, r);
     if (a == 2) return -2;
     if (a == 1) return 3 * k + 2;
@@ -558,10 +557,10 @@ __device__ __forceinline__ int mx_surface(const DevSurface& s, int k, uint32_t f
 // scheme (jit.cpp) passes a policy whose run() calls mx_surface with each
 // surface's FixedShape in turn.
 struct RtSurfaces {
-    __device__ __forceinline__ static void run(const DevScheme* sch, const double* knots, const DevBeam* beams,
-                                               int b, double lam, mx::TableMemo& memo, mx::Ray& r, int& stage) {
+    __device__ __forceinline__ static void run(const DevScheme* sch, const double* knots, const BeamCtx& bc,
+                                               double lam, mx::TableMemo& memo, mx::Ray& r, int& stage) {
         for (int k = 0; k < sch->n_surfaces && stage == -1; ++k)
-            stage = mx_surface(sch->s[k], k, sch->fixes, knots, beams, b, lam, memo, r);
+            stage = mx_surface(sch->s[k], k, sch->fixes, knots, bc, lam, memo, r);
     }
 };
 
@@ -586,12 +585,15 @@ __device__ __forceinline__ void fused_mixed(const DevScheme* __restrict__ g_sch,
     const int n_stages = 3 * sch->n_surfaces;
     RowLoop rows(ts, in.n, warp_row_buffer<Row64>(sch->n_knots), (unsigned)sizeof(Row64), err);
     const int lane = threadIdx.x & 31;
-    int b = 0;
+    BeamCursor cur;
     while (rows.begin()) {
         const size_t slot = rows.slot();
         const bool valid = slot < in.n;
-        const size_t i = (ts.order && valid) ? (size_t)ts.order[slot] : slot;  // the ray
-        const size_t oi = ts.out_by_slot ? slot : i;                           // where its results go
+        // the ray's index, read only when its results go there; its beam: the
+        // beam of its slot in a plan's (beam-major) tracing order
+        const size_t i = (ts.order && valid && !(rows.packed && ts.out_by_slot)) ? (size_t)ts.order[slot] : slot;
+        const size_t oi = ts.out_by_slot ? slot : i;
+        const size_t bi = rows.packed ? slot : i;
         mx::Ray r{0, 0, 0, 0, 0, 0};
         double lam = 0.0;
         char f = 0;
@@ -612,15 +614,14 @@ __device__ __forceinline__ void fused_mixed(const DevScheme* __restrict__ g_sch,
         bool ev = false, good = false;
         int key = 0;
         double outX = 0, outY = 0;
+        int b = 0;
         if (valid && f == 1) {
+            b = cur.at(beams, n_beams, bi);
+            const BeamCtx bc = beam_ctx(beams, b);
             mx::normalize(r);
-            // rays come in increasing order per warp: the previous ray's
-            // beam is usually this one's
-            if (!(b + 1 >= n_beams || i < beams[b + 1].first_ray) || i < beams[b].first_ray)
-                b = beam_of(beams, n_beams, i);
             mx::TableMemo memo;
             int stage = -1;
-            Surfaces::run(sch, s_knots, beams, b, lam, memo, r, stage);
+            Surfaces::run(sch, s_knots, bc, lam, memo, r, stage);
             if (stage == -2) atomicOr(err, DEV_ERR_OUT_OF_RANGE);
             if (stage >= 0) {
                 ev = true;

@@ -12,8 +12,8 @@
 //   * the intersection root: the ray's start in the new frame is the FP32
 //     rotated position plus the FP64 vertex offset, and the roots of
 //     mixed.cuh (cancellation-safe conic quadratic, Newton on the even
-//     asphere and the toric, stopping a step below 1e-6 mm with the root
-//     good to ~1e-14 mm) run in FP64 on it; the aperture test runs on the
+//     asphere and the toric, stopping after a step below 1e-5 mm with the
+//     root good to ~1e-12 mm) run in FP64 on it; the aperture test runs on the
 //     FP64 point before it is rounded to the FP32 state;
 //   * the grating equation (mx::diffract);
 //   * the detector coordinate: the last surface's FP64 intersection point
@@ -153,14 +153,14 @@ __device__ __forceinline__ bool refract(float mu, float nx, float ny, float nz, 
 // surface; the point where it was lost otherwise).
 template <class Sh = RtShape>
 __device__ __forceinline__ int m32_surface(const DevSurface& s, int k, uint32_t fixes, const double* knots,
-                                           const DevBeam* beams, int b, double lam, mx::TableMemo& memo,
-                                           m32::Ray& r, mx::Ray& q) {
+                                           const BeamCtx& bc, const double* off0, double lam,
+                                           mx::TableMemo& memo, m32::Ray& r, mx::Ray& q) {
     if (!Sh::non_aux(s)) return -1;  // its transform is folded into the next surface's
     if (Sh::rot32(s)) {
         m32::rotate(s.m32, r.X, r.Y, r.Z);
         m32::rotate(s.m32, r.cX, r.cY, r.cZ);
     }
-    const double* off = Sh::first32(s) ? beams[b].off0 : s.off32;
+    const double* off = Sh::first32(s) ? off0 : s.off32;
     q = mx::Ray{(double)r.X + off[0], (double)r.Y + off[1], (double)r.Z + off[2],
                 (double)r.cX,         (double)r.cY,         (double)r.cZ};
     const int hit = mx::intersect<Sh>(s, fixes, q);
@@ -205,8 +205,7 @@ __device__ __forceinline__ int m32_surface(const DevSurface& s, int k, uint32_t 
         return -1;
     }
     // the grating equation in FP64 on the FP64 cosines
-    long long order = s.order;
-    if (beams[b].n_orders > 0) order = beams[b].orders[s.grating_index];
+    const long long order = bc.order(s);
     const double mu = (gr_type == RTB_TRANSPARENT) ? n1v * in2 : 0.0;
     const double L = (double)order * lam * in2 * s.inv_gr;
     if (!mx::diffract<Sh>(s, mu, L, (double)nx, (double)ny, (double)nz, q)) return 3 * k + 2;
@@ -220,11 +219,11 @@ __device__ __forceinline__ int m32_surface(const DevSurface& s, int k, uint32_t 
 // surface's structure read from the scheme; jit.cpp writes the same with a
 // FixedShape per surface).
 struct Rt32Surfaces {
-    __device__ __forceinline__ static void run(const DevScheme* sch, const double* knots, const DevBeam* beams,
-                                               int b, double lam, mx::TableMemo& memo, m32::Ray& r, mx::Ray& q,
-                                               int& stage) {
+    __device__ __forceinline__ static void run(const DevScheme* sch, const double* knots, const BeamCtx& bc,
+                                               const double* off0, double lam, mx::TableMemo& memo, m32::Ray& r,
+                                               mx::Ray& q, int& stage) {
         for (int k = 0; k < sch->n_surfaces && stage == -1; ++k)
-            stage = m32_surface(sch->s[k], k, sch->fixes, knots, beams, b, lam, memo, r, q);
+            stage = m32_surface(sch->s[k], k, sch->fixes, knots, bc, off0, lam, memo, r, q);
     }
 };
 
@@ -242,14 +241,16 @@ __device__ __forceinline__ void fused_mixed32(const DevScheme* __restrict__ g_sc
     const int n_stages = 3 * sch->n_surfaces;
     RowLoop rows(ts, in.n, warp_row_buffer<Row32>(sch->n_knots), (unsigned)sizeof(Row32), err);
     const int lane = threadIdx.x & 31;
-    int b = 0;
+    BeamCursor cur;
     while (rows.begin()) {
         const size_t slot = rows.slot();
         const bool valid = slot < in.n;
-        const size_t i = (ts.order && valid) ? (size_t)ts.order[slot] : slot;  // the ray
-        const size_t oi = ts.out_by_slot ? slot : i;                           // where its results go
-        if (valid && (!(b + 1 >= n_beams || i < beams[b + 1].first_ray) || i < beams[b].first_ray))
-            b = beam_of(beams, n_beams, i);
+        // the ray's index, read only when its results go there; its beam: the
+        // beam of its slot in a plan's (beam-major) tracing order
+        const size_t i = (ts.order && valid && !(rows.packed && ts.out_by_slot)) ? (size_t)ts.order[slot] : slot;
+        const size_t oi = ts.out_by_slot ? slot : i;
+        const size_t bi = rows.packed ? slot : i;
+        const int b = valid ? cur.at(beams, n_beams, bi) : 0;
         m32::Ray r{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         double lam = 0.0;
         char f = 0;
@@ -274,11 +275,13 @@ __device__ __forceinline__ void fused_mixed32(const DevScheme* __restrict__ g_sc
         int key = 0;
         double outX = 0, outY = 0;
         if (valid && f == 1) {
+            const BeamCtx bc = beam_ctx(beams, b);
+            const double off0[3] = {bc.bm->off0[0], bc.bm->off0[1], bc.bm->off0[2]};
             m32::normalize(r);
             mx::TableMemo memo;
             mx::Ray q{0, 0, 0, 0, 0, 0};
             int stage = -1;
-            Surfaces::run(sch, s_knots, beams, b, lam, memo, r, q, stage);
+            Surfaces::run(sch, s_knots, bc, off0, lam, memo, r, q, stage);
             if (stage == -1 && sch->tail_on) {  // Aux surfaces after the last one, in FP64
                 const double* m = sch->tail_m;
                 const double* o = sch->tail_off;

@@ -299,7 +299,9 @@ int rtb_plan_create(const rtb_surface* surfaces, size_t n_surfaces, const rtb_be
     // costs the mixed kernel 0.8 ms of its 5.3 on C1 against coalesced stores;
     // chunks small enough to stage a block's stores in shared memory lose
     // more in coherence than that.
-    // The mixed kernels read the ordered copy as row blocks of 32 rays
+    // The order is beam-major (k_order_keys): the slots of beam b are the
+    // range of its ray indices, so a kernel reading rows finds a ray's beam
+    // from its slot.  The mixed kernels read the ordered copy as row blocks of 32 rays
     // (rowpipe.cuh: one bulk copy per row into shared memory, issued a row
     // ahead), the FP32-state kernel with FP32 positions relative to each
     // beam's origin: 57 and 33 bytes per ray.
