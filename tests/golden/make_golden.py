@@ -4,7 +4,8 @@ Runs oracle/_ref/harness_refgpu -- the reference's Beam/Surface/
 TabulatedFunction host classes over the reference's own cuda_engine compiled
 for sm_100a (oracle/Makefile) -- on small seeded beams through the benchmark
 and coverage schemes, and stores input and output of each case in
-tests/golden/<case>.npz.  Needs a GPU; the fixtures are committed so that the
+tests/golden/<case>.npz.  The *_nofma cases run the same sources built
+without FMA contraction (harness_refgpu_nofma).  Needs a GPU; the fixtures are committed so that the
 CPU tests can pin the oracle to the reference engine without one.
 
 Lens and grating refractive indices are single values in these cases: the
@@ -76,7 +77,19 @@ def cases():
         "mirrors_tagged": (cov["mirrors"], small, (), 400),
         "lenses": (scalarize(cov["lenses"]), small, (), 400),
         "gratings": (scalarize(cov["gratings"]), small, (), 400),
+        # C1 with its toric fold, through the reference built without FMA
+        # contraction (HARNESS): the same rays meet the toric step's 0/0 as
+        # in the oracle, so the fold is pinned ray by ray
+        "c1_m38_nofma": (scalarize(S.echelle()), c1, (38, 1), 40),
+        "c1_m52_nofma": (scalarize(S.echelle()), c1, (52, 1), 40),
     }
+
+
+# The reference build each case runs through (oracle/_ref/harness_<kind>):
+# refgpu is the cuda_engine built for sm_100a with its own flags (FMA
+# contraction on, as nvcc defaults), refgpu_nofma the same sources with
+# --fmad=false.
+HARNESS = {"c1_m38_nofma": "refgpu_nofma", "c1_m52_nofma": "refgpu_nofma"}
 
 
 def spec_arrays(specs):
@@ -92,17 +105,18 @@ def spec_arrays(specs):
 
 def main(out_dir=HERE, only=None):
     os.makedirs(out_dir, exist_ok=True)
-    if H.harness("refgpu") is None:
-        raise SystemExit("oracle/_ref/harness_refgpu is not built")
     for name, (specs, kw, orders, n_per) in cases().items():
         if only and name not in only:
             continue
+        kind = HARNESS.get(name, "refgpu")
+        if H.harness(kind) is None:
+            raise SystemExit(f"oracle/_ref/harness_{kind} is not built")
         beam = S.make_beam(0, n_per, kw["n_lambda"], kw["radius"], kw["lam_range"], 20141203, orders=orders)
         rays = O.generate([beam], beam.n_rays)
         if name.endswith("_tagged"):
             # mirrors only: the wavelength is free, so it carries the ray index
             rays.lambda_[:] = 0.4 + 1e-7 * np.arange(rays.n)
-        rc, out = H.run_trace("refgpu", specs, list(orders), rays)
+        rc, out = H.run_trace(kind, specs, list(orders), rays)
         inp = np.stack([rays.X, rays.Y, rays.Z, rays.cX, rays.cY, rays.cZ, rays.lambda_])
         payload = dict(rc=rc, input=inp, scheme=spec_arrays(specs), orders=np.array(orders, dtype=np.int64))
         if out is not None:

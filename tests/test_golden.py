@@ -8,10 +8,13 @@ tolerances (positions 1e-9 mm, direction cosines 1e-12) and flags, counts
 and wavelengths exactly.
 
 Schemes with a toric surface are compared ray by ray only where the rays can
-be identified (mirrors_tagged: the wavelength carries the ray index): the
-reference's toric iteration divides 0/0 for rays that converge exactly
-(rt_cuda_engine_surface.cu:390), which rays do depends on FMA contraction,
-and Beam::Rearrange then orders the two outputs differently.
+be identified (mirrors_tagged: the wavelength carries the ray index), or
+where the reference ran without FMA contraction (the *_nofma cases, C1's
+toric fold): the reference's toric iteration divides 0/0 for rays that
+converge exactly (rt_cuda_engine_surface.cu:390), which rays do depends on
+FMA contraction, and Beam::Rearrange then orders the two outputs
+differently.  Without contraction the reference rounds every operation as
+the oracle does, and the *_nofma outputs equal the oracle's bit for bit.
 """
 import os
 
@@ -65,6 +68,8 @@ def test_oracle_matches_reference_engine(name):
     fin = ~np.isnan(ref)
     assert np.all(np.abs(ours[:3] - ref[:3])[fin[:3]] <= POS_TOL)
     assert np.all(np.abs(ours[3:6] - ref[3:6])[fin[3:6]] <= COS_TOL)
+    if G.HARNESS.get(name) == "refgpu_nofma":
+        assert np.array_equal(ours[fin], ref[fin]), "the reference without FMA contraction differs in bits"
 
 
 def test_toric_rays_match_by_tag():

@@ -102,3 +102,84 @@ def test_reference_cuda_engine_speed(variant):
     else:
         assert abs(res["per_surface_fp64"][1] - ref_good) <= 0.3 * n
     assert res["per_surface_fp64"][0] < ref_s
+
+
+@pytest.mark.skipif(os.environ.get("RTB_REF_C1") != "1", reason="minutes of GPU time: set RTB_REF_C1=1")
+@pytest.mark.skipif(H.harness("refgpu") is None or H.harness("refgpu_ptx") is None,
+                    reason="reference cuda_engine harnesses not built")
+def test_reference_cuda_engine_whole_c1(tmp_path):
+    """The reference's cuda_engine over the whole C1 workload -- all 31 echelle
+    order ranges, 1.0e8 rays, the fold as a sphere (with the toric, its
+    per-ray device printf and cycling rays take ~140 s per range) -- built as
+    the reference ships it (compute_50 PTX, compiled by the driver at load,
+    CMakeLists.txt:115) and for sm_100a, each range through Scheme::run's
+    loop in its own process as the reference runs ranges; this engine's
+    per-surface FP64, fused FP64 and fused mixed paths on the same rays, with
+    the SM clocks sampled meanwhile.  Prints one JSON line and writes it to
+    $RTB_REF_C1_OUT when set."""
+    from rt_b200.clocks import Clocks
+    specs = sphere_fold(S.echelle())
+    beams = S.c1_beams()
+    n = S.total_rays(beams)
+    line = {"workload": "C1, fold as a sphere: 31 ranges (orders 30..60) x 64 wavelengths x 50404 rays",
+            "rays": n, "builds": {}}
+    spec_dir = str(tmp_path)
+    for kind, label in (("refgpu_ptx", "compute_50 PTX as shipped, JIT"), ("refgpu", "sm_100a")):
+        total_s, good, per_range = 0.0, 0, []
+        with Clocks(0) as ck:
+            for b in beams:
+                m = int(b.orders[0])
+                one = S.make_beam(0, int(b.disk[0]), S.C1_NLAMBDA, S.C1_RADIUS, S.C1_LAMBDA, int(b.seed),
+                                  orders=(m, 1))
+                rays = O.generate([one], one.n_rays)
+                spec = H.write_spec(specs, [m, 1], spec_dir)
+                bin_path = H.write_beam(rays, spec_dir)
+                out = subprocess.run([H.harness(kind), "trace", spec, bin_path, spec_dir + "/out.dat"],
+                                     capture_output=True, text=True, timeout=600)
+                mm = re.search(r"trace_seconds=([0-9.]+) good=(\d+)", out.stderr)
+                assert out.returncode in (0, 5, 6) and mm, out.stderr[-2000:]
+                total_s += float(mm.group(1))
+                good += int(mm.group(2))
+                per_range.append(round(float(mm.group(1)), 4))
+        line["builds"][label] = {"trace_seconds": total_s, "good": good, "per_range_s": per_range,
+                                 "clocks": ck.summary()}
+    # this engine on the same rays (one call or one plan run for all ranges)
+    cs = S.to_c(specs, E.spline_init)
+    rays = E.generate(beams, n)
+    ours = {}
+    o_ps = E.opts(engine=ffi.ENGINE_PER_SURFACE, precision=ffi.FP64, state_out=0)
+    best = 1e9
+    for _ in range(3):
+        r = rays.copy()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        st, stats = E.trace(cs.surfaces, beams, r, o_ps)
+        torch.cuda.synchronize()
+        best = min(best, time.perf_counter() - t0)
+        del r
+    rs, ours["per_surface_fp64"] = stats.ray_surfaces, {"seconds": best, "good": stats.n_good}
+    for name, prec in (("fused_fp64", ffi.FP64), ("fused_mixed", ffi.MIXED), ("fused_mixed32", ffi.MIXED32)):
+        plan = E.Plan(cs.surfaces, beams, E.opts(engine=ffi.ENGINE_FUSED, precision=prec, state_out=0,
+                                                  out_order=ffi.OUT_SLOT))
+        plan.run()
+        plan.result()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(5):
+            plan.run()
+        st, stats = plan.result()
+        ours[name] = {"seconds": (time.perf_counter() - t0) / 5, "good": stats.n_good}
+        plan.destroy()
+    line["ray_surfaces"] = rs
+    for k, v in line["builds"].items():
+        v["rate"] = rs / v["trace_seconds"]
+    for k, v in ours.items():
+        v["rate"] = rs / v["seconds"]
+    line["this_engine"] = ours
+    print(json.dumps(line))
+    if os.environ.get("RTB_REF_C1_OUT"):
+        with open(os.environ["RTB_REF_C1_OUT"], "w") as f:
+            f.write(json.dumps(line) + "\n")
+    sm = line["builds"]["sm_100a"]
+    assert abs(ours["per_surface_fp64"]["good"] - sm["good"]) <= 1e-4 * n
+    assert ours["per_surface_fp64"]["seconds"] < sm["trace_seconds"]
