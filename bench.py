@@ -9,10 +9,13 @@ CCD frame counts accumulated.  A ray-surface is one ray through one non-Aux
 surface; lost rays count up to the surface that loses them.
 
 Engines timed: the plain FP64 per-surface engine (one kernel per surface,
-rtb_trace_out), the fused FP64 kernel and the fused mixed-precision kernel
-(the headline `value`), each fused kernel as a plan (rtb_plan_*: rays
-resident in HBM, one CUDA graph launch per step, launch configuration chosen
-by the autotuner first).  `e2e` runs the same trace through rtb_trace_host on
+rtb_trace_out), the fused FP64 kernel and the two fused mixed-precision
+kernels (FP64 ray state, RTB_MIXED; FP32 ray state, RTB_MIXED32), each fused
+kernel as a plan (rtb_plan_*: rays resident in HBM as 32-ray row blocks in a
+coherent tracing order, outputs stored at the tracing slots, one CUDA graph
+launch per step, launch configuration chosen by the autotuner first).  The
+headline `value` is the faster mixed kernel whose p99.9 CCD error against
+the FP64 plan is within 0.05 um.  `e2e` runs the same trace through rtb_trace_host on
 page-locked host arrays (copies in and out inside the timed region).
 `cpu_baseline` is the CPU oracle on the host cores over a bounded sample of
 the same rays.  `c3_batched` is C3: 512 beams of uneven size, wavelength,
@@ -47,14 +50,13 @@ WORKLOAD = ("C1 cross-dispersed echelle: 1.0e8 rays (31 echelle orders 30..60 x 
             "surfaces + CCD 4096^2, frame counts accumulated")
 FIXES = 3  # RTB_FIX_TORIC_SIGN | RTB_FIX_TORIC_STEP: the toric fold's Steffensen step divides 0/0 otherwise
 # Per-ray figures of the two mixed kernels (compiled for C1 with its surface
-# constants baked in) from one ncu capture each of one launch on C1 at
-# 1,001,728 rays per 0.1 of the workload (31 x 64 x 5,049 rays, 1.0e7 rays:
-# inputs 4x the L2): DRAM bytes read + written, and the executed FP64 / FP32
-# floating-point operations (ncu op counters, FMA = 2, FFMA2 = 4).  None
-# where no capture of the current kernel exists.
+# constants baked in; plans with slot outputs), from ncu captures of one
+# launch each: DRAM bytes read + written on this workload (1.0e8 rays, one
+# pass), and the executed FP64 / FP32 floating-point operations on C1 at
+# 1.0e7 rays (31 x 64 x 5041; ncu op counters, FMA = 2, FFMA2 = 4).
 KERNEL_PROFILE = {
-    "fused_mixed": {"traffic_per_ray": None, "f64_flops_per_ray": None, "f32_flops_per_ray": None},
-    "fused_mixed32": {"traffic_per_ray": None, "f64_flops_per_ray": None, "f32_flops_per_ray": None},
+    "fused_mixed": {"traffic_per_ray": 76.92, "f64_flops_per_ray": 628.69, "f32_flops_per_ray": 50.84},
+    "fused_mixed32": {"traffic_per_ray": 52.06, "f64_flops_per_ray": 455.10, "f32_flops_per_ray": 238.15},
 }
 # bytes of input per ray the mixed kernels read: a plan's 32-ray row blocks
 # (Row64: 1824 B, Row32: 1056 B per 32 rays)
@@ -493,8 +495,8 @@ def main():
                 "alg_bytes_per_ray": alg_bytes / n,
                 "kernel": hv.get("kernel", "").split(" ")[0],
                 "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "fallback",
-                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch on C1 at "
-                                  "1.0e7 rays, per ray, times the rays of a step" if tpr else None,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of this "
+                                  "workload, per ray, times the rays of a step" if tpr else None,
                 "note": "HBM view of a kernel bound by instruction issue (no FP64, FP32 or memory pipe "
                         "saturated): the compute roofline is roofline_fp64"}
 

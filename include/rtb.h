@@ -333,6 +333,14 @@ RTB_API int rtb_trace_host(const rtb_surface* surfaces, size_t n_surfaces, const
                    size_t n_beams, const rtb_trace_opts* opts, const rtb_rays* host_rays,
                    rtb_trace_stats* stats);
 
+/* Fault hook for tests (no reference counterpart): after the library's next
+ * `after` device allocations, the `count` following ones fail as if the
+ * device were out of memory, so that the calls making them return
+ * RTB_BAD_ALLOC (the reference's ENGINE_ERROR_BAD_ALLOC,
+ * rt_engine_errors.h:4) and release what they had allocated.  count 0
+ * clears it. */
+RTB_API int rtb_fail_allocations(uint32_t after, uint32_t count);
+
 /* Frame counts: counts[iy*xdim + ix] += 1 for every good ray whose pixel
  * (ccd_coordinates, ccd.cu:30-45) lies on the CCD; *n_outside (device, may be
  * NULL) counts the good rays that do not.  counts is not cleared. */

@@ -534,7 +534,7 @@ int rtb_adjoint_create(const rtb_surface* surfaces, size_t n_surfaces, const rtb
     const size_t o_y = off; off += al(n_rays * sizeof(double));
     const size_t o_fl = off; off += al(n_rays);
     cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaMalloc(&c->mem, off);
+    if (e == cudaSuccess) e = dev_malloc((void**)&c->mem, off);
     if (e != cudaSuccess) {
         if (c->stream) cudaStreamDestroy(c->stream);
         delete c;

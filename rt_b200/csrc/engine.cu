@@ -7,6 +7,7 @@
 // stream-ordered pool (no cudaMalloc/cudaFree per call as in
 // rt_cuda_engine_common.cu:72-155).
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -20,6 +21,31 @@ namespace rtb {
 Engine& engine() {
     static Engine e;
     return e;
+}
+
+// The fault hook (rtb_fail_allocations): allocations to let through, then
+// allocations to fail.
+static std::atomic<int> g_alloc_skip{0}, g_alloc_fail{0};
+
+static bool take_one(std::atomic<int>& c) {
+    int n = c.load();
+    while (n > 0)
+        if (c.compare_exchange_weak(n, n - 1)) return true;
+    return false;
+}
+
+bool injected_alloc_failure() {
+    if (g_alloc_fail.load() <= 0) return false;
+    if (take_one(g_alloc_skip)) return false;
+    return take_one(g_alloc_fail);
+}
+
+cudaError_t dev_malloc(void** p, size_t bytes) {
+    if (injected_alloc_failure()) {
+        *p = nullptr;
+        return cudaErrorMemoryAllocation;
+    }
+    return cudaMalloc(p, bytes);
 }
 
 int ensure_init() {
@@ -195,7 +221,24 @@ void mixed_constants(DevSurface& s) {
     }
 }
 
+// Every number a surface contributes to a trace is finite: a NaN or an
+// infinity in the scheme is a bad request, refused before any launch (the
+// reference would trace it into NaN rays).
+static bool surface_finite(const rtb_surface& in) {
+    const double nn = in.params[2];
+    if (!std::isfinite(in.params[0]) || !std::isfinite(in.params[1]) || !std::isfinite(nn)) return false;
+    const int used = 3 + ((nn >= 0 && nn <= RTB_MAX_POLY) ? (int)nn : 0) + (in.cls == RTB_TORIC ? 1 : 0);
+    for (int i = 3; i < used && i < RTB_MAX_PARAMS; ++i)
+        if (!std::isfinite(in.params[i])) return false;
+    for (int i = 0; i < 3; ++i)
+        if (!std::isfinite(in.distance[i]) || !std::isfinite(in.angles_deg[i])) return false;
+    for (int i = 0; i < 2; ++i)
+        if (!std::isfinite(in.size[i]) || !std::isfinite(in.center[i])) return false;
+    return in.type != RTB_GRATING || std::isfinite(in.gr_const);
+}
+
 int prepare_surface(const rtb_surface& in, DevSurface& s, KnotBuf& knots) {
+    if (in.type != RTB_AUX_TYPE && !surface_finite(in)) return RTB_BAD_VALUE;
     bool non_aux = in.type != RTB_AUX_TYPE;
     int st = surface_from_params(non_aux ? in.cls : RTB_AUX_CLASS, in.params, s);
     if (st != RTB_OK) return st;
@@ -463,6 +506,13 @@ int finish(cudaStream_t st, const unsigned* d_err, size_t* n_bad, const unsigned
 }  // namespace rtb
 
 using namespace rtb;
+
+extern "C" RTB_API int rtb_fail_allocations(uint32_t after, uint32_t count) {
+    rtb::g_alloc_fail.store(0);
+    rtb::g_alloc_skip.store((int)(after > 1000000u ? 1000000u : after));
+    rtb::g_alloc_fail.store((int)(count > 1000000u ? 1000000u : count));
+    return RTB_OK;
+}
 
 extern "C" {
 

@@ -20,6 +20,11 @@ struct Engine {
 Engine& engine();
 int ensure_init();
 
+// Fault hook (rtb_fail_allocations): true for the allocations it makes fail.
+bool injected_alloc_failure();
+// cudaMalloc, failing as out of memory while the fault hook says so.
+cudaError_t dev_malloc(void** p, size_t bytes);
+
 // Host-side scheme preparation (what the reference's host code computes
 // before its launches).
 struct PreparedScheme {
@@ -86,7 +91,8 @@ struct DevBuf {
     int alloc(size_t bytes, cudaStream_t st) {
         release();
         s = st;
-        cudaError_t e = cudaMallocAsync(&p, bytes ? bytes : 16, st);
+        cudaError_t e = injected_alloc_failure() ? cudaErrorMemoryAllocation
+                                                 : cudaMallocAsync(&p, bytes ? bytes : 16, st);
         if (e != cudaSuccess) {
             p = nullptr;
             return cuda_status(e);

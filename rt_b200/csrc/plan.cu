@@ -262,8 +262,8 @@ int rtb_plan_create(const rtb_surface* surfaces, size_t n_surfaces, const rtb_be
     const bool full_out = opts->state_out != 0;
     cudaError_t e = cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->done, cudaEventDisableTiming);
-    if (e == cudaSuccess) e = cudaMalloc(&p->in_mem, rays_bytes(p->n_rays, true));
-    if (e == cudaSuccess) e = cudaMalloc(&p->out_mem, rays_bytes(p->n_rays, full_out));
+    if (e == cudaSuccess) e = dev_malloc((void**)&p->in_mem, rays_bytes(p->n_rays, true));
+    if (e == cudaSuccess) e = dev_malloc((void**)&p->out_mem, rays_bytes(p->n_rays, full_out));
     if (e == cudaSuccess)
         e = cudaMallocHost(&p->h_counts, (n_beams * (3 * n_surfaces + 1) + 1) * sizeof(unsigned long long));
     if (e != cudaSuccess) {
@@ -307,11 +307,11 @@ int rtb_plan_create(const rtb_surface* surfaces, size_t n_surfaces, const rtb_be
     // beam's origin: 57 and 33 bytes per ray.
     const bool mixed = opts->precision != RTB_FP64;
     if (e == cudaSuccess && opts->ray_order == RTB_ORDER_COHERENT && p->n_rays <= 0xffffffffull) {
-        e = cudaMalloc(&p->order, p->n_rays * sizeof(uint32_t));
+        e = dev_malloc((void**)&p->order, p->n_rays * sizeof(uint32_t));
         const size_t n_rows = (p->n_rays + 31) / 32;
         const size_t row_size = opts->precision == RTB_MIXED32 ? sizeof(Row32) : sizeof(Row64);
         if (e == cudaSuccess)
-            e = mixed ? cudaMalloc(&p->rows, n_rows * row_size) : cudaMalloc(&p->slot_mem, rays_bytes(p->n_rays, true));
+            e = mixed ? dev_malloc((void**)&p->rows, n_rows * row_size) : dev_malloc((void**)&p->slot_mem, rays_bytes(p->n_rays, true));
         if (e == cudaSuccess) {
             if (!mixed) p->in_slot = carve(p->slot_mem, p->n_rays, true);
             const int chunk_shift = mixed ? 20 : 30;
@@ -424,7 +424,7 @@ int rtb_plan_autotune(rtb_plan* p, int reps, rtb_tune_entry* table, size_t capac
     const int32_t saved_block = p->block, saved_rpt = p->rpt;
     void* frame_mem = nullptr;
     if (p->has_frame) {
-        RTB_CUDA_TRY(cudaMalloc(&frame_mem, p->ccd.xdim * p->ccd.ydim * sizeof(uint32_t) + 256));
+        RTB_CUDA_TRY(dev_malloc((void**)&frame_mem, p->ccd.xdim * p->ccd.ydim * sizeof(uint32_t) + 256));
         p->opts.counts = static_cast<uint32_t*>(frame_mem);
         p->opts.n_outside = reinterpret_cast<uint64_t*>(static_cast<char*>(frame_mem) +
                                                         p->ccd.xdim * p->ccd.ydim * sizeof(uint32_t));

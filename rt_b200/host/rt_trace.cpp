@@ -1,8 +1,8 @@
 // rt_trace -- the reference's ray-tracing program (ray-tracing/main.cpp with
 // Scheme::run, common-lib/scheme.cpp:878-1099) on the B200 engine.
 //
-//   rt_trace scheme_file rt_files_file [log_file] [--precision fp64|mixed]
-//            [--fixes N] [--seed S]
+//   rt_trace scheme_file rt_files_file [log_file] [--precision fp64|mixed|mixed32]
+//            [--fixes N] [--seed S] [--bench K]
 //
 // Loads the scheme file (rtb_scheme_load), writes the input beam as
 // <result_file>_input_beam.dat, traces every wavelength range -- one range,
@@ -19,7 +19,15 @@
 // here every range draws its positions from Philox4x32-10 keyed by
 // seed + range index, so a run can be repeated.  The engine is the fused FP64
 // kernel by default (the same bits as the reference's per-surface loop on the
-// CPU oracle); --precision mixed selects the mixed-precision kernel.
+// CPU oracle); --precision mixed selects the mixed-precision kernel (FP64
+// ray state), mixed32 the one with FP32 ray state.
+//
+// --bench K times the trace instead of writing results: every range becomes
+// one beam of a plan (rtb_plan_*: rays generated on the device, coherent
+// tracing order, outputs at the tracing slots, launch configuration from the
+// autotuner), and K plan runs are timed with CUDA events on the plan's stream,
+// after three untimed ones; the program prints ms per run and ray-surfaces
+// per second.  This timing goes through the C ABI alone.
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -82,17 +90,98 @@ const char* scheme_error_text(int e) {
 
 }  // namespace
 
+// --bench: every range one beam of a plan, K timed runs.
+int run_bench(const rtb_surface* surf, size_t ns, size_t n_rows, int K, int precision, uint32_t fixes,
+              uint64_t seed, uint64_t n_per, uint64_t n_lambda, uint64_t n_rays, const rtb_scheme_beam& bd,
+              const double* rows, size_t row_len, int n_gratings) {
+    std::vector<rtb_beam> beams(n_rows);
+    for (size_t r = 0; r < n_rows; ++r) {
+        rtb_beam& b = beams[r];
+        std::memset(&b, 0, sizeof(b));
+        b.first_ray = r * n_rays;
+        b.n_rays = n_rays;
+        b.shape = RTB_CIRCLE;
+        b.disk[0] = (double)n_per;
+        b.disk[1] = bd.params[1];
+        b.disk[2] = bd.params[2];
+        for (int i = 0; i < 3; ++i) b.center[i] = bd.center[i];
+        const double* row = rows + r * row_len;
+        b.range[0] = row[0];
+        b.range[1] = (bd.range_distr == RTB_RANGE_MONOCHROMATIC) ? row[0] : row[1];
+        b.n_lambda = n_lambda;
+        b.seed = seed + r;
+        if (n_rows > 1 && (int)row_len >= 2 + n_gratings) {
+            b.n_orders = n_gratings;
+            for (int g = 0; g < n_gratings && g < RTB_MAX_GRATINGS; ++g) b.orders[g] = (int64_t)row[2 + g];
+        }
+    }
+    rtb_trace_opts o;
+    std::memset(&o, 0, sizeof(o));
+    o.engine = RTB_ENGINE_FUSED;
+    o.precision = precision;
+    o.fixes = fixes;
+    o.renormalize_lost = 1;
+    o.state_out = 0;
+    o.out_order = RTB_OUT_SLOT;
+    rtb_plan* plan = nullptr;
+    int st = rtb_plan_create(surf, ns, beams.data(), beams.size(), &o, &plan);
+    if (st != RTB_OK) return fail("plan creation failed", 2);
+    rtb_tune_entry tune[16];
+    size_t n_tune = 0;
+    cudaStream_t s = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (rtb_plan_autotune(plan, 2, tune, 16, &n_tune) != RTB_OK ||
+        cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess || cudaEventCreate(&e0) != cudaSuccess ||
+        cudaEventCreate(&e1) != cudaSuccess) {
+        rtb_plan_destroy(plan);
+        return fail("bench set-up failed", 2);
+    }
+    int rc = 0;
+    for (int i = 0; i < 3 && !rc; ++i) rc = rtb_plan_run(plan, s) != RTB_OK;
+    cudaEventRecord(e0, s);
+    for (int i = 0; i < K && !rc; ++i) rc = rtb_plan_run(plan, s) != RTB_OK;
+    cudaEventRecord(e1, s);
+    float ms = 0.f;
+    rtb_trace_stats stats;
+    if (!rc && (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess)) rc = 1;
+    const int rs = rc ? RTB_FAILED : rtb_plan_result(plan, &stats);
+    int32_t block = 0, rpt = 0;
+    uint64_t n = 0;
+    rtb_plan_config(plan, &block, &rpt, &n);
+    int32_t spec = 0;
+    rtb_plan_specialized(plan, &spec, nullptr, 0);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaStreamDestroy(s);
+    rtb_plan_destroy(plan);
+    if (rc || (rs != RTB_OK && rs != RTB_NO_INTERSECTIONS && rs != RTB_NO_GOOD_RAYS))
+        return fail("bench run failed", 2);
+    const double per = (double)ms / K;
+    std::printf("rt_trace bench: %llu rays in %zu ranges, %llu ray-surfaces and %llu good rays per run; "
+                "%s kernel%s, block %d x %d rays per thread; %.4f ms per run, %.4g ray-surfaces/s\n",
+                (unsigned long long)n, n_rows, (unsigned long long)stats.ray_surfaces,
+                (unsigned long long)stats.n_good,
+                precision == RTB_FP64 ? "fused FP64" : (precision == RTB_MIXED ? "fused mixed" : "fused mixed32"),
+                spec ? " (specialised)" : "", block, rpt, per, (double)stats.ray_surfaces / (per * 1e-3));
+    return 0;
+}
+
 int main(int argc, char** argv) {
     std::vector<std::string> pos;
     int precision = RTB_FP64;
     uint32_t fixes = 0;
     uint64_t seed = 20141203;
+    int bench = 0;
     for (int i = 1; i < argc; ++i) {
         std::string a = argv[i];
         if (a == "--precision" && i + 1 < argc) {
             std::string v = argv[++i];
             if (v == "mixed") precision = RTB_MIXED;
-            else if (v != "fp64") return fail("--precision is fp64 or mixed");
+            else if (v == "mixed32") precision = RTB_MIXED32;
+            else if (v != "fp64") return fail("--precision is fp64, mixed or mixed32");
+        } else if (a == "--bench" && i + 1 < argc) {
+            bench = std::atoi(argv[++i]);
+            if (bench < 1) return fail("--bench takes a number of runs");
         } else if (a == "--fixes" && i + 1 < argc) {
             fixes = (uint32_t)std::strtoul(argv[++i], nullptr, 0);
         } else if (a == "--seed" && i + 1 < argc) {
@@ -103,7 +192,7 @@ int main(int argc, char** argv) {
     }
     if (pos.size() < 2) {
         std::fprintf(stderr, "Usage: rt_trace scheme_filename rt_files_filename [log_file] "
-                             "[--precision fp64|mixed] [--fixes N] [--seed S]\n");
+                             "[--precision fp64|mixed|mixed32] [--fixes N] [--seed S] [--bench K]\n");
         return 1;
     }
     std::ofstream logf;
@@ -142,6 +231,12 @@ int main(int argc, char** argv) {
     int n_gratings = 0;
     for (size_t k = 0; k < ns; ++k) n_gratings += surf[k].type == RTB_GRATING;
 
+    if (bench > 0) {
+        const int rc = run_bench(surf, ns, n_rows, bench, precision, fixes, seed, n_per, n_lambda, n_rays, bd, rows,
+                                 row_len, n_gratings);
+        rtb_scheme_free(sc);
+        return rc;
+    }
     DeviceRays rays;
     uint32_t* order = nullptr;
     if (!rays.alloc(n_rays) || cudaMalloc(&order, n_rays * sizeof(uint32_t)) != cudaSuccess) {
