@@ -215,6 +215,32 @@ def dgemm_tflops(n=4096, reps=5):
         return None
 
 
+def sgemm_tflops(n=8192, reps=5):
+    """cuBLAS FP32 GEMM throughput with TF32 off (the FP32 pipes), TFLOP/s."""
+    import torch
+    prev = torch.backends.cuda.matmul.allow_tf32
+    try:
+        torch.backends.cuda.matmul.allow_tf32 = False
+        a = torch.randn(n, n, dtype=torch.float32, device="cuda")
+        b = torch.randn(n, n, dtype=torch.float32, device="cuda")
+        torch.matmul(a, b)
+        torch.cuda.synchronize()
+        best = 1e30
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch.matmul(a, b)
+            e1.record()
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        del a, b
+        return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+    except RuntimeError:
+        return None
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = prev
+
+
 def reference_arm(args):
     # rank 0 alone runs (on the host cores) and prints; the other ranks exit
     from rt_b200 import replicas
@@ -398,6 +424,9 @@ def main():
             engines[name] = {"error": str(e)}
             continue
         plans[name] = plan
+        cnt = plan.counts().sum(axis=0).astype(np.int64)  # per stage: rays lost there; last: rays at the end
+        lost_before = np.concatenate([[0], np.cumsum(cnt[:-1])])
+        reaching = [int(n - lost_before[3 * k]) for k in range(len(surf))]
         spec_on, spec_note = plan.specialized()
         kname, generic = KERNELS[prec]
         engines[name] = {"ms_per_step": ms, "value": stats.rs / (ms * 1e-3),
@@ -410,6 +439,7 @@ def main():
                          "ray_order": "coherent (beam, wavelength, Morton code of the entrance position), "
                                       "sorted once when the plan is made",
                          "outputs": "at the tracing slot (RTB_OUT_SLOT)",
+                         "rays_reaching_surfaces": reaching,
                          "plan_create_s": t_create, **variants,
                          "autotune_ms": {f"{b}x{r}": round(t, 4) for b, r, t in table}}
 
@@ -500,17 +530,40 @@ def main():
                 "note": "HBM view of a kernel bound by instruction issue (no FP64, FP32 or memory pipe "
                         "saturated): the compute roofline is roofline_fp64"}
 
-    # compute roofline of the headline kernel: executed FP64 flops per second
-    # against cuBLAS DGEMM measured here
-    fp64_peak = dgemm_tflops()
-    f64pr = prof.get("f64_flops_per_ray")
-    f64_achieved = f64pr * n / (hv["ms_per_step"] * 1e-3) / 1e12 if f64pr else None
-    roofline_fp64 = {"bound": "fp64", "achieved": f64_achieved, "peak": fp64_peak, "unit": "TFLOP/s",
-                     "frac": (f64_achieved / fp64_peak) if (f64_achieved and fp64_peak) else None,
-                     "executed_flops_per_ray": f64pr, "f32_executed_flops_per_ray": prof.get("f32_flops_per_ray"),
-                     "peak_source": "cuBLAS DGEMM 4096^3 measured in this run (best of 5)",
-                     "note": "executed FP64 operations (FMA = 2) from ncu op counters, Newton refinements of "
-                             "reciprocals and square roots included"}
+    # compute roofline of the headline kernel.  Algorithmic flops: the
+    # reference algorithm's operations per ray at each surface (the CPU
+    # oracle on the counting scalar, oracle/count_flops.py ->
+    # rt_b200/data/flops_c1.json) times the rays this step sent to that
+    # surface; executed flops: ncu op counters of the kernel (KERNEL_PROFILE).
+    # Peaks: cuBLAS DGEMM and SGEMM (TF32 off) measured in this run.
+    fp64_peak, fp32_peak = dgemm_tflops(), sgemm_tflops()
+    sec = hv["ms_per_step"] * 1e-3
+    alg = None
+    try:
+        tab = json.load(open(os.path.join(ROOT, "rt_b200", "data", "flops_c1.json")))
+        reach = hv.get("rays_reaching_surfaces")
+        if reach and len(reach) == len(tab["surfaces"]) and not args.surfaces:
+            alg = sum(r * row["ops_per_ray"] for r, row in zip(reach, tab["surfaces"]))
+            alg += tab["lost_ray_renormalize_ops"] / tab["sample_rays"] * n
+    except (OSError, KeyError, ValueError):
+        alg = None
+    f64pr, f32pr = prof.get("f64_flops_per_ray"), prof.get("f32_flops_per_ray")
+    tf = lambda flops: flops / sec / 1e12 if flops else None  # noqa: E731
+    frac = lambda a, p: (a / p) if (a and p) else None  # noqa: E731
+    roofline_fp64 = {"bound": "fp64", "achieved": tf(alg), "peak": fp64_peak, "unit": "TFLOP/s",
+                     "frac": frac(tf(alg), fp64_peak),
+                     "alg_flops_per_ray": (alg / n) if alg else None,
+                     "executed_flops_per_ray": f64pr,
+                     "executed_achieved": tf(f64pr * n if f64pr else None),
+                     "executed_frac": frac(tf(f64pr * n if f64pr else None), fp64_peak),
+                     "f32_executed_flops_per_ray": f32pr,
+                     "f32_executed_achieved": tf(f32pr * n if f32pr else None), "f32_peak": fp32_peak,
+                     "f32_executed_frac": frac(tf(f32pr * n if f32pr else None), fp32_peak),
+                     "peak_source": "cuBLAS DGEMM / SGEMM (TF32 off) 4096^3 measured in this run (best of 5)",
+                     "note": "achieved = the reference algorithm's FP64 operations (oracle op count per "
+                             "surface x rays reaching it) per second; executed = the kernel's own FP64 "
+                             "operations (ncu, FMA = 2), Newton refinements of its reciprocals and square "
+                             "roots included"}
     if "per_surface" in engines and "value" in engines["per_surface"]:
         ps = engines["per_surface"]
         gbs = ALG_BYTES_PER_RAY_SURFACE * ps["value"] / 1e9

@@ -15,6 +15,7 @@
 // Tests check that the two agree once oracle_reference_order permutes the
 // first one.
 #include "rt_oracle.hpp"
+#include "flop_count.hpp"
 #include "../include/rtb.h"
 
 #include <atomic>
@@ -78,14 +79,16 @@ int prepare(const rtb_surface* s, size_t n, std::vector<Prepared>& out) {
     return OK;
 }
 
-inline bool eval_table(const rtb_table& t, double x, double& v) {
+template <class T>
+inline bool eval_table(const rtb_table& t, T x, T& v) {
     return table_eval(t.n, t.x, t.y, t.y2, x, v);
 }
 
 // Normalize a lost ray `count` times; stops at the fixed point.
-inline void renormalize(Ray& r, int count) {
+template <class T>
+inline void renormalize(RayT<T>& r, int count) {
     for (int i = 0; i < count; ++i) {
-        double a = r.cX, b = r.cY, c = r.cZ;
+        T a = r.cX, b = r.cY, c = r.cZ;
         normalize(a, b, c);
         if (a == r.cX && b == r.cY && c == r.cZ) break;
         r.cX = a; r.cY = b; r.cZ = c;
@@ -95,55 +98,68 @@ inline void renormalize(Ray& r, int count) {
 // Action of a surface on one ray (Mirror/Lens/Grating ::Action,
 // surface.cpp:385-396,453-472,563-585).  Returns OK, OUT_OF_RANGE, or
 // NO_GOOD_RAYS meaning "this ray is lost".
-inline int action(const Prepared& p, const long* orders, int n_orders, double lambda, Ray& r) {
+template <class T>
+inline int action(const Prepared& p, const SurfConstT<T>& sc, const long* orders, int n_orders, T lambda,
+                  RayT<T>& r) {
     switch (p.type) {
-        case Mirror: reflect(p.cls, p.sc, r); return OK;
+        case Mirror: reflect(p.cls, sc, r); return OK;
         case Lens: {
-            double a, b;
+            T a, b;
             if (!eval_table(p.n1, lambda, a) || !eval_table(p.n2, lambda, b)) return OUT_OF_RANGE;
-            double mu = a;
+            T mu = a;
             mu /= b;
-            return refract(p.cls, p.sc, mu, r) ? OK : NO_GOOD_RAYS;
+            return refract(p.cls, sc, mu, r) ? OK : NO_GOOD_RAYS;
         }
         case Grating: {
             long ord = (n_orders > 0) ? orders[p.grating_index] : p.order;
-            double n2v, mu = 0.0;
+            T n2v, mu = 0.0;
             if (!eval_table(p.n2, lambda, n2v)) return OUT_OF_RANGE;
             if (p.gr_type == Transparent) {
-                double n1v;
+                T n1v;
                 if (!eval_table(p.n1, lambda, n1v)) return OUT_OF_RANGE;
                 mu = n1v;
                 mu /= n2v;
             } else if (p.gr_type != Reflective) {
                 return BAD_VALUE;
             }
-            double L = ord * lambda / n2v / p.gr_const;
-            return diffract(p.cls, p.gr_type, p.sc, mu, L, r) ? OK : NO_GOOD_RAYS;
+            T L = T((double)ord) * lambda / n2v / p.gr_const;
+            return diffract(p.cls, p.gr_type, sc, mu, L, r) ? OK : NO_GOOD_RAYS;
         }
         default: return OK;
     }
 }
 
 // Trace one ray through all surfaces.  Returns a status; sets lost_stage.
-inline int trace_ray(const std::vector<Prepared>& S, const long* orders, int n_orders, double lambda,
-                     int renorm_lost, uint32_t fixes, Ray& r, int& lost_stage) {
+// `at(k)` is called as the ray enters surface k and, with k = S.size(),
+// after its last one (the operation counter attributes by it).
+template <class T, class At>
+inline int trace_ray(const std::vector<Prepared>& S, const SurfConstT<T>* SC, const long* orders, int n_orders,
+                     T lambda, int renorm_lost, uint32_t fixes, RayT<T>& r, int& lost_stage, At&& at) {
     lost_stage = RTB_NOT_LOST;
     for (size_t k = 0; k < S.size(); ++k) {
         const Prepared& p = S[k];
+        at(k);
         transform(p.tc, r);
         normalize(r.cX, r.cY, r.cZ);
         if (!p.non_aux) continue;
         int stage = (int)(3 * k);
-        if (!intersect(p.kind, p.sc, fixes, r)) { lost_stage = stage; break; }
+        if (!intersect(p.kind, SC[k], fixes, r)) { lost_stage = stage; break; }
         bool shade = p.type == Shade;
         if (!aperture_pass(shade, p.shape, p.size, p.center, r.X, r.Y)) { lost_stage = stage + 1; break; }
-        int st = action(p, orders, n_orders, lambda, r);
+        int st = action(p, SC[k], orders, n_orders, lambda, r);
         if (st == NO_GOOD_RAYS) { lost_stage = stage + 2; break; }
         if (st != OK) return st;
         normalize(r.cX, r.cY, r.cZ);
     }
+    at(S.size());
     if (lost_stage != RTB_NOT_LOST && renorm_lost) renormalize(r, S[lost_stage / 3].renorm_after);
     return OK;
+}
+
+inline std::vector<SurfConst> surface_constants(const std::vector<Prepared>& S) {
+    std::vector<SurfConst> sc(S.size());
+    for (size_t k = 0; k < S.size(); ++k) sc[k] = S[k].sc;
+    return sc;
 }
 
 }  // namespace
@@ -507,6 +523,7 @@ int oracle_trace(const rtb_surface* surfaces, size_t n_surfaces, const rtb_beam*
     std::vector<Prepared> S;
     int st = prepare(surfaces, n_surfaces, S);
     if (st != OK) return st;
+    const std::vector<SurfConst> SC = surface_constants(S);
     const size_t n_stages = 3 * n_surfaces;
     std::vector<uint64_t> counts(n_beams * n_stages, 0);
     uint64_t ray_surfaces = 0, n_good = 0;
@@ -527,7 +544,8 @@ int oracle_trace(const rtb_surface* surfaces, size_t n_surfaces, const rtb_beam*
                 size_t i = bm.first_ray + (size_t)ii;
                 Ray r{rays->X[i], rays->Y[i], rays->Z[i], rays->cX[i], rays->cY[i], rays->cZ[i]};
                 int ls;
-                int s2 = trace_ray(S, orders, bm.n_orders, rays->lambda[i], renorm_lost, fixes, r, ls);
+                int s2 = trace_ray(S, SC.data(), orders, bm.n_orders, rays->lambda[i], renorm_lost, fixes, r, ls,
+                                   [](size_t) {});
                 if (s2 != OK) { err = s2; continue; }
                 rays->X[i] = r.X; rays->Y[i] = r.Y; rays->Z[i] = r.Z;
                 rays->cX[i] = r.cX; rays->cY[i] = r.cY; rays->cZ[i] = r.cZ;
@@ -565,6 +583,64 @@ int oracle_trace(const rtb_surface* surfaces, size_t n_surfaces, const rtb_beam*
         stats->failed_stage = failed_stage;
     }
     if (failed_beam >= 0) return (failed_stage % 3 == 2) ? NO_GOOD_RAYS : NO_INTERSECTIONS;
+    return OK;
+}
+
+// Algorithmic operation count of the reference's per-ray arithmetic
+// (flop_count.hpp): every ray of `rays` (not modified) traced with the
+// counting scalar, as oracle_trace traces it.  ops[k] (k < n_surfaces) sums
+// the operations of surface k -- its transform, Normalize, intersection,
+// aperture, action and Normalize -- over the rays that reach it, reached[k]
+// counts those rays; ops[n_surfaces] holds the trailing Normalize calls of
+// lost rays (renorm_lost).
+int oracle_count_flops(const rtb_surface* surfaces, size_t n_surfaces, const rtb_beam* beams, size_t n_beams,
+                       uint32_t fixes, int renorm_lost, const rtb_rays* rays, uint64_t* ops, uint64_t* reached) {
+    std::vector<Prepared> S;
+    int st = prepare(surfaces, n_surfaces, S);
+    if (st != OK) return st;
+    std::vector<SurfConstT<Flop>> SC(S.size());
+    for (size_t k = 0; k < S.size(); ++k) SC[k] = SurfConstT<Flop>(S[k].sc);
+    std::vector<uint64_t> tot_ops(n_surfaces + 1, 0), tot_reached(n_surfaces + 1, 0);
+    std::atomic<int> err{0};
+    for (size_t b = 0; b < n_beams; ++b) {
+        const rtb_beam& bm = beams[b];
+        if (bm.first_ray + bm.n_rays > rays->n) return BAD_VALUE;
+        long orders[RTB_MAX_GRATINGS];
+        for (int g = 0; g < RTB_MAX_GRATINGS; ++g) orders[g] = (long)bm.orders[g];
+#pragma omp parallel
+        {
+            std::vector<uint64_t> my_ops(n_surfaces + 1, 0), my_reached(n_surfaces + 1, 0);
+#pragma omp for schedule(static)
+            for (long long ii = 0; ii < (long long)bm.n_rays; ++ii) {
+                const size_t i = bm.first_ray + (size_t)ii;
+                if (rays->flag && rays->flag[i] != 1) continue;
+                RayT<Flop> r{rays->X[i], rays->Y[i], rays->Z[i], rays->cX[i], rays->cY[i], rays->cZ[i]};
+                int ls;
+                size_t cur = 0;
+                uint64_t mark = Flop::n;
+                auto at = [&](size_t k) {
+                    if (k > 0) my_ops[cur] += Flop::n - mark;
+                    mark = Flop::n;
+                    cur = k;
+                    ++my_reached[k];
+                };
+                int s2 = trace_ray(S, SC.data(), orders, bm.n_orders, Flop(rays->lambda[i]), renorm_lost, fixes, r,
+                                   ls, at);
+                my_ops[cur] += Flop::n - mark;
+                if (s2 != OK) err = s2;
+            }
+#pragma omp critical
+            for (size_t k = 0; k <= n_surfaces; ++k) {
+                tot_ops[k] += my_ops[k];
+                tot_reached[k] += my_reached[k];
+            }
+        }
+    }
+    if (err) return err;
+    for (size_t k = 0; k <= n_surfaces; ++k) {
+        if (ops) ops[k] = tot_ops[k];
+        if (reached) reached[k] = tot_reached[k];
+    }
     return OK;
 }
 
@@ -616,7 +692,7 @@ int oracle_trace_literal(const rtb_surface* surfaces, size_t n_surfaces, const r
         bad = 0;
         for (size_t i = 0; i < ng; ++i) {
             Ray r{X[i], Y[i], Z[i], cX[i], cY[i], cZ[i]};
-            int a = action(p, orders, beam->n_orders, lambda[i], r);
+            int a = action(p, p.sc, orders, beam->n_orders, lambda[i], r);
             if (a == NO_GOOD_RAYS) { flag[i] = 0; ++bad; }
             else if (a != OK) { *n_good_out = ng; return a; }
             cX[i] = r.cX; cY[i] = r.cY; cZ[i] = r.cZ;

@@ -102,6 +102,22 @@ def trace(surfaces, beams, rays: HostRays, fixes: int = 0, renorm_lost: int = 1)
     return st, stats, counts
 
 
+def count_flops(surfaces, beams, rays: HostRays, fixes: int = 0, renorm_lost: int = 1):
+    """Algorithmic operation count of the reference's per-ray arithmetic over
+    `rays` (not modified): (ops per surface, rays reaching each surface),
+    the last entry of ops the trailing Normalize calls of lost rays."""
+    L = load()
+    L.oracle_count_flops.argtypes = [C.POINTER(ffi.Surface), C.c_size_t, C.POINTER(ffi.Beam), C.c_size_t,
+                                     C.c_uint32, C.c_int, C.POINTER(ffi.Rays), C.c_void_p, C.c_void_p]
+    n_s = len(surfaces)
+    ops = np.zeros(n_s + 1, dtype=np.uint64)
+    reached = np.zeros(n_s + 1, dtype=np.uint64)
+    st = L.oracle_count_flops((ffi.Surface * n_s)(*surfaces), n_s, (ffi.Beam * len(beams))(*beams), len(beams),
+                              fixes, renorm_lost, C.byref(rays.struct()), ffi.vptr(ops), ffi.vptr(reached))
+    ffi.check(st, "oracle_count_flops")
+    return ops, reached
+
+
 def trace_literal(surfaces, beam, rays: HostRays, fixes: int = 0):
     """Reference-order replica for one beam covering all of `rays`; returns (status, n_good)."""
     n_s = len(surfaces)

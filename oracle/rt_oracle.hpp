@@ -66,11 +66,21 @@ enum QuirkFix : uint32_t {
 // ---------------------------------------------------------------------------
 // Surface constants as copy_surf_params() stages them
 // (cuda_engine/rt_cuda_engine_surface.cu:108-148).
-struct SurfConst {
-    double c = 0, k1 = 1, cR = 0;
+// T is the scalar type of the per-ray arithmetic: double for the oracle
+// proper; other types (the operation counter of flop_count.hpp) take the
+// same statements.
+template <class T>
+struct SurfConstT {
+    T c = 0, k1 = 1, cR = 0;
     size_t n_poly = 0;
-    double poly[RTO_MAX_POLY] = {0};
+    T poly[RTO_MAX_POLY] = {};
+    SurfConstT() = default;
+    template <class U>
+    explicit SurfConstT(const SurfConstT<U>& o) : c(o.c), k1(o.k1), cR(o.cR), n_poly(o.n_poly) {
+        for (int i = 0; i < RTO_MAX_POLY; ++i) poly[i] = o.poly[i];
+    }
 };
+using SurfConst = SurfConstT<double>;
 
 inline Status make_surf_const(int cls, const double* params, SurfConst& s) {
     s.c = params[0];
@@ -85,19 +95,25 @@ inline Status make_surf_const(int cls, const double* params, SurfConst& s) {
 
 // ---------------------------------------------------------------------------
 // Ray state (one ray of the SoA beam, common-lib/beam.h:96-99).
-struct Ray {
-    double X, Y, Z, cX, cY, cZ;
+template <class T>
+struct RayT {
+    T X, Y, Z, cX, cY, cZ;
 };
+using Ray = RayT<double>;
+
+using std::fabs;
+using std::sqrt;
 
 // ===========================================================================
 // Surface derivatives
 // ===========================================================================
 
 // conic_derivs (cuda_engine/rt_cuda_engine_surface.cu:45-61)
-inline void conic_derivs(const SurfConst& s, double X, double Y, double& dFdX, double& dFdY) {
-    double r2 = X * X + Y * Y;
-    double E = s.c / std::sqrt(1.0 - s.k1 * s.c * s.c * r2);
-    double sum = 0.0, rr = 1.0;
+template <class T>
+inline void conic_derivs(const SurfConstT<T>& s, T X, T Y, T& dFdX, T& dFdY) {
+    T r2 = X * X + Y * Y;
+    T E = s.c / sqrt(1.0 - s.k1 * s.c * s.c * r2);
+    T sum = 0.0, rr = 1.0;
     for (size_t i = 1; i <= s.n_poly; ++i, rr *= r2) sum += i * s.poly[i - 1] * rr;
     E += 2.0 * sum;
     dFdX = -E * X;
@@ -105,14 +121,15 @@ inline void conic_derivs(const SurfConst& s, double X, double Y, double& dFdX, d
 }
 
 // toric_derivs (cuda_engine/rt_cuda_engine_surface.cu:65-94)
-inline void toric_derivs(const SurfConst& s, double X, double Y, double Z,
-                         double& dFdX, double& dFdY, double& dFdZ) {
-    double Y2 = Y * Y;
-    double Fy = s.c * Y2 / (1.0 + std::sqrt(1.0 - s.k1 * s.c * s.c * Y2));
-    double sum = 0.0, rr = Y2;
+template <class T>
+inline void toric_derivs(const SurfConstT<T>& s, T X, T Y, T Z,
+                         T& dFdX, T& dFdY, T& dFdZ) {
+    T Y2 = Y * Y;
+    T Fy = s.c * Y2 / (1.0 + sqrt(1.0 - s.k1 * s.c * s.c * Y2));
+    T sum = 0.0, rr = Y2;
     for (size_t i = 0; i < s.n_poly; ++i, rr *= Y2) sum += s.poly[i] * rr;
     Fy += sum;
-    double dFy = s.c * Y / std::sqrt(1.0 - s.k1 * s.c * s.c * Y2);
+    T dFy = s.c * Y / sqrt(1.0 - s.k1 * s.c * s.c * Y2);
     sum = 0.0; rr = 1.0;
     for (size_t i = 1; i <= s.n_poly; ++i, rr *= Y2) sum += i * s.poly[i - 1] * rr;
     dFy += 2.0 * sum;
@@ -126,8 +143,9 @@ inline void toric_derivs(const SurfConst& s, double X, double Y, double Z,
 // ===========================================================================
 
 // plane_intersection (surface.cu:154-178)
-inline bool plane_intersection(Ray& r) {
-    double s0 = -r.Z / r.cZ;
+template <class T>
+inline bool plane_intersection(RayT<T>& r) {
+    T s0 = -r.Z / r.cZ;
     if (s0 < 0.0) return false;
     r.X += r.cX * s0;
     r.Y += r.cY * s0;
@@ -136,10 +154,11 @@ inline bool plane_intersection(Ray& r) {
 }
 
 // paraboloid_intersection (surface.cu:183-213): linear root, A ignored.
-inline bool paraboloid_intersection(const SurfConst& s, Ray& r) {
-    double B = 2.0 * (s.k1 * r.Z * r.cZ + r.X * r.cX + r.Y * r.cY - r.cZ / s.c);
-    double C = s.k1 * r.Z * r.Z + r.X * r.X + r.Y * r.Y - 2.0 * r.Z / s.c;
-    double t = -C / B;
+template <class T>
+inline bool paraboloid_intersection(const SurfConstT<T>& s, RayT<T>& r) {
+    T B = 2.0 * (s.k1 * r.Z * r.cZ + r.X * r.cX + r.Y * r.cY - r.cZ / s.c);
+    T C = s.k1 * r.Z * r.Z + r.X * r.X + r.Y * r.Y - 2.0 * r.Z / s.c;
+    T t = -C / B;
     if (t < 0.0) return false;
     r.X += t * r.cX;
     r.Y += t * r.cY;
@@ -148,15 +167,16 @@ inline bool paraboloid_intersection(const SurfConst& s, Ray& r) {
 }
 
 // conic_intersection (surface.cu:216-253): root chosen by sign(c), no t>=0 check.
-inline bool conic_intersection(const SurfConst& s, Ray& r) {
-    double A = s.k1 * r.cZ * r.cZ + r.cX * r.cX + r.cY * r.cY;
-    double B = 2.0 * (s.k1 * r.Z * r.cZ + r.X * r.cX + r.Y * r.cY - r.cZ / s.c);
-    double C = s.k1 * r.Z * r.Z + r.X * r.X + r.Y * r.Y - 2.0 * r.Z / s.c;
-    double D = B * B - 4.0 * A * C;
+template <class T>
+inline bool conic_intersection(const SurfConstT<T>& s, RayT<T>& r) {
+    T A = s.k1 * r.cZ * r.cZ + r.cX * r.cX + r.cY * r.cY;
+    T B = 2.0 * (s.k1 * r.Z * r.cZ + r.X * r.cX + r.Y * r.cY - r.cZ / s.c);
+    T C = s.k1 * r.Z * r.Z + r.X * r.X + r.Y * r.Y - 2.0 * r.Z / s.c;
+    T D = B * B - 4.0 * A * C;
     if (D < 0.0) return false;
-    double t;
-    if (s.c > 0) t = (-B - std::sqrt(D)) / 2.0 / A;
-    else         t = (-B + std::sqrt(D)) / 2.0 / A;
+    T t;
+    if (s.c > 0) t = (-B - sqrt(D)) / 2.0 / A;
+    else         t = (-B + sqrt(D)) / 2.0 / A;
     r.X += t * r.cX;
     r.Y += t * r.cY;
     r.Z += t * r.cZ;
@@ -169,10 +189,11 @@ inline bool conic_intersection(const SurfConst& s, Ray& r) {
 // with `fix_root`, the point of the last update (s2) once converged.
 // The iteration counter is reset per ray (the reference keeps it per thread
 // across its grid-stride loop, which only matters after ~1e5 iterations).
-inline bool iterative_conic_intersection(const SurfConst& s, bool fix_root, Ray& r) {
-    double s0 = -r.Z / r.cZ;
+template <class T>
+inline bool iterative_conic_intersection(const SurfConstT<T>& s, bool fix_root, RayT<T>& r) {
+    T s0 = -r.Z / r.cZ;
     if (!(s0 >= 0)) return false;
-    double s1, s2 = 0.0, Xi = 0, Yi = 0, Zi = 0;
+    T s1, s2 = 0.0, Xi = 0, Yi = 0, Zi = 0;
     size_t Niter = 0;
     bool good = true;
     do {
@@ -180,20 +201,20 @@ inline bool iterative_conic_intersection(const SurfConst& s, bool fix_root, Ray&
         Xi = r.X + (s1 + s0) * r.cX;
         Yi = r.Y + (s1 + s0) * r.cY;
         Zi = s1 * r.cZ;
-        double r2 = Xi * Xi + Yi * Yi;
-        double F = Zi - s.c * r2 / (1.0 + std::sqrt(1.0 - s.k1 * s.c * s.c * r2));
-        double sum = 0.0, rr = r2;
+        T r2 = Xi * Xi + Yi * Yi;
+        T F = Zi - s.c * r2 / (1.0 + sqrt(1.0 - s.k1 * s.c * s.c * r2));
+        T sum = 0.0, rr = r2;
         for (size_t i = 0; i < s.n_poly; ++i, rr *= r2) sum += s.poly[i] * rr;
         F -= sum;
-        double E = s.c / std::sqrt(1.0 - s.k1 * s.c * s.c * r2);
+        T E = s.c / sqrt(1.0 - s.k1 * s.c * s.c * r2);
         sum = 0.0; rr = 1.0;
         for (size_t i = 1; i <= s.n_poly; ++i, rr *= r2) sum += i * s.poly[i - 1] * rr;
         E += 2.0 * sum;
-        double dF = -E * Xi * r.cX - E * Yi * r.cY + r.cZ;
-        if (std::fabs(dF) < ITER_EPS) { good = false; break; }
+        T dF = -E * Xi * r.cX - E * Yi * r.cY + r.cZ;
+        if (fabs(dF) < ITER_EPS) { good = false; break; }
         s2 = s1 - F / dF;
         ++Niter;
-    } while ((std::fabs(s2 - s1) >= ITER_EPS) && (Niter <= ITER_MAX));
+    } while ((fabs(s2 - s1) >= ITER_EPS) && (Niter <= ITER_MAX));
     if (fix_root && good && Niter <= ITER_MAX) {  // the point of the last update
         Xi = r.X + (s2 + s0) * r.cX;
         Yi = r.Y + (s2 + s0) * r.cY;
@@ -206,10 +227,11 @@ inline bool iterative_conic_intersection(const SurfConst& s, bool fix_root, Ray&
 
 // iterative_poly_intersection (surface.cu:497-561): c == 0 with a polynomial;
 // requires s0 > 0 and uses (-X-Y)*sum in the derivative, as the reference.
-inline bool iterative_poly_intersection(const SurfConst& s, bool fix_root, Ray& r) {
-    double s0 = -r.Z / r.cZ;
+template <class T>
+inline bool iterative_poly_intersection(const SurfConstT<T>& s, bool fix_root, RayT<T>& r) {
+    T s0 = -r.Z / r.cZ;
     if (!(s0 > 0)) return false;
-    double s1, s2 = 0.0, Xi = 0, Yi = 0, Zi = 0;
+    T s1, s2 = 0.0, Xi = 0, Yi = 0, Zi = 0;
     size_t Niter = 0;
     bool good = true;
     do {
@@ -217,18 +239,18 @@ inline bool iterative_poly_intersection(const SurfConst& s, bool fix_root, Ray& 
         Xi = r.X + (s1 + s0) * r.cX;
         Yi = r.Y + (s1 + s0) * r.cY;
         Zi = s1 * r.cZ;
-        double r2 = Xi * Xi + Yi * Yi;
-        double F = 0.0, rr = r2;
+        T r2 = Xi * Xi + Yi * Yi;
+        T F = 0.0, rr = r2;
         for (size_t i = 0; i < s.n_poly; ++i, rr *= r2) F += s.poly[i] * rr;
         F = Zi - F;
-        double dF = 0.0;
+        T dF = 0.0;
         rr = 1.0;
         for (size_t i = 1; i <= s.n_poly; ++i, rr *= r2) dF += i * s.poly[i - 1] * rr;
         dF = -Xi * dF - Yi * dF + 1.0;
-        if (std::fabs(dF) < ITER_EPS) { good = false; break; }
+        if (fabs(dF) < ITER_EPS) { good = false; break; }
         s2 = s1 - F / dF;
         ++Niter;
-    } while ((std::fabs(s2 - s1) >= ITER_EPS) && (Niter <= ITER_MAX));
+    } while ((fabs(s2 - s1) >= ITER_EPS) && (Niter <= ITER_MAX));
     if (fix_root && good && Niter <= ITER_MAX) {  // the point of the last update
         Xi = r.X + (s2 + s0) * r.cX;
         Yi = r.Y + (s2 + s0) * r.cY;
@@ -240,35 +262,37 @@ inline bool iterative_poly_intersection(const SurfConst& s, bool fix_root, Ray& 
 }
 
 // toric_func (surface.cu:338-356); `fix_sign` selects 1-k1c^2Y^2.
-inline double toric_func(const SurfConst& s, bool fix_sign, double t, const Ray& r) {
-    double X = r.X + t * r.cX;
-    double Y = r.Y + t * r.cY;
-    double Z = r.Z + t * r.cZ;
-    double Y2 = Y * Y;
-    double FY = fix_sign ? s.c * Y2 / (1.0 + std::sqrt(1.0 - s.k1 * s.c * s.c * Y2))
-                         : s.c * Y2 / (1.0 + std::sqrt(1.0 + s.k1 * s.c * s.c * Y2));
+template <class T>
+inline T toric_func(const SurfConstT<T>& s, bool fix_sign, T t, const RayT<T>& r) {
+    T X = r.X + t * r.cX;
+    T Y = r.Y + t * r.cY;
+    T Z = r.Z + t * r.cZ;
+    T Y2 = Y * Y;
+    T FY = fix_sign ? s.c * Y2 / (1.0 + sqrt(1.0 - s.k1 * s.c * s.c * Y2))
+                         : s.c * Y2 / (1.0 + sqrt(1.0 + s.k1 * s.c * s.c * Y2));
     return Z - FY - 0.5 * s.cR * (X * X + Z * Z - FY * FY);
 }
 
 // iter_toric (surface.cu:359-410): Steffensen iteration; a ray that runs out
 // of iterations is not flagged, as in the reference.  `fix_step` stops the
 // iteration where the reference's step divides by Fzn-Fxn == 0.
-inline bool iter_toric(const SurfConst& s, bool fix_sign, bool fix_step, Ray& r) {
-    double sn1 = -r.Z / r.cZ;
+template <class T>
+inline bool iter_toric(const SurfConstT<T>& s, bool fix_sign, bool fix_step, RayT<T>& r) {
+    T sn1 = -r.Z / r.cZ;
     if (!(sn1 >= 0)) return false;
     size_t Niter = 0;
-    double Fyn = 0.0, sn;
+    T Fyn = 0.0, sn;
     do {
         sn = sn1;
-        double Fxn = toric_func(s, fix_sign, sn, r);
-        if (std::fabs(Fyn - Fxn) <= ITER_EPS) break;
-        double zn = sn + Fxn;
-        double Fzn = toric_func(s, fix_sign, zn, r);
+        T Fxn = toric_func(s, fix_sign, sn, r);
+        if (fabs(Fyn - Fxn) <= ITER_EPS) break;
+        T zn = sn + Fxn;
+        T Fzn = toric_func(s, fix_sign, zn, r);
         if (fix_step && Fzn - Fxn == 0.0) { sn1 = sn; break; }
         sn1 = sn - Fxn * Fxn / (Fzn - Fxn);
         Fyn = Fxn;
         ++Niter;
-    } while ((std::fabs(sn1 - sn) >= ITER_EPS) && (Niter <= ITER_MAX));
+    } while ((fabs(sn1 - sn) >= ITER_EPS) && (Niter <= ITER_MAX));
     r.X += sn1 * r.cX;
     r.Y += sn1 * r.cY;
     r.Z += sn1 * r.cZ;
@@ -297,7 +321,8 @@ inline IsectKind intersection_kind(int cls, const double* params) {
     }
 }
 
-inline bool intersect(IsectKind kind, const SurfConst& s, uint32_t fixes, Ray& r) {
+template <class T>
+inline bool intersect(IsectKind kind, const SurfConstT<T>& s, uint32_t fixes, RayT<T>& r) {
     switch (kind) {
         case IS_PLANE: return plane_intersection(r);
         case IS_PARABOLOID: return paraboloid_intersection(s, r);
@@ -312,22 +337,23 @@ inline bool intersect(IsectKind kind, const SurfConst& s, uint32_t fixes, Ray& r
 // ===========================================================================
 // Reflection (surface.cu:771-827)
 // ===========================================================================
-inline void reflect(int cls, const SurfConst& s, Ray& r) {
+template <class T>
+inline void reflect(int cls, const SurfConstT<T>& s, RayT<T>& r) {
     switch (cls) {
         case Plane: r.cZ = -r.cZ; return;
         case Conic: {
-            double dFdX, dFdY;
+            T dFdX, dFdY;
             conic_derivs(s, r.X, r.Y, dFdX, dFdY);
-            double a2 = 2.0 * (r.cX * dFdX + r.cY * dFdY + r.cZ) / (dFdX * dFdX + dFdY * dFdY + 1.0);
+            T a2 = 2.0 * (r.cX * dFdX + r.cY * dFdY + r.cZ) / (dFdX * dFdX + dFdY * dFdY + 1.0);
             r.cX -= a2 * dFdX;
             r.cY -= a2 * dFdY;
             r.cZ -= a2;
             return;
         }
         case Toric: {
-            double dFdX, dFdY, dFdZ;
+            T dFdX, dFdY, dFdZ;
             toric_derivs(s, r.X, r.Y, r.Z, dFdX, dFdY, dFdZ);
-            double a2 = 2.0 * (r.cX * dFdX + r.cY * dFdY + r.cZ * dFdZ) /
+            T a2 = 2.0 * (r.cX * dFdX + r.cY * dFdY + r.cZ * dFdZ) /
                         (dFdX * dFdX + dFdY * dFdY + dFdZ * dFdZ);
             r.cX -= a2 * dFdX;
             r.cY -= a2 * dFdY;
@@ -341,45 +367,46 @@ inline void reflect(int cls, const SurfConst& s, Ray& r) {
 // ===========================================================================
 // Refraction (surface.cu:956-1066); mu = n1(lambda)/n2(lambda).
 // ===========================================================================
-inline bool refract(int cls, const SurfConst& s, double mu, Ray& r) {
+template <class T>
+inline bool refract(int cls, const SurfConstT<T>& s, T mu, RayT<T>& r) {
     switch (cls) {
         case Plane: {
-            double a = mu * r.cZ;
-            double b = mu * mu - 1.0;
-            double a2 = a * a;
+            T a = mu * r.cZ;
+            T b = mu * mu - 1.0;
+            T a2 = a * a;
             if (b > a2) return false;
             b = a2 - b;
-            double G = -a + std::sqrt(b);
+            T G = -a + sqrt(b);
             r.cX *= mu;
             r.cY *= mu;
             r.cZ = mu * r.cZ + G;
             return true;
         }
         case Conic: {
-            double dFdX, dFdY;
+            T dFdX, dFdY;
             conic_derivs(s, r.X, r.Y, dFdX, dFdY);
-            double G = dFdX * dFdX + dFdY * dFdY + 1.0;
-            double a = mu * (r.cX * dFdX + r.cY * dFdY + r.cZ) / G;
-            double b = (mu * mu - 1.0) / G;
-            double a2 = a * a;
+            T G = dFdX * dFdX + dFdY * dFdY + 1.0;
+            T a = mu * (r.cX * dFdX + r.cY * dFdY + r.cZ) / G;
+            T b = (mu * mu - 1.0) / G;
+            T a2 = a * a;
             if (b > a2) return false;
             b = a2 - b;
-            G = -a + std::sqrt(b);
+            G = -a + sqrt(b);
             r.cX = mu * r.cX + G * dFdX;
             r.cY = mu * r.cY + G * dFdY;
             r.cZ = mu * r.cZ + G;
             return true;
         }
         case Toric: {
-            double dFdX, dFdY, dFdZ;
+            T dFdX, dFdY, dFdZ;
             toric_derivs(s, r.X, r.Y, r.Z, dFdX, dFdY, dFdZ);
-            double G = dFdX * dFdX + dFdY * dFdY + dFdZ * dFdZ;
-            double a = mu * (r.cX * dFdX + r.cY * dFdY + r.cZ * dFdZ) / G;
-            double b = (mu * mu - 1.0) / G;
-            double a2 = a * a;
+            T G = dFdX * dFdX + dFdY * dFdY + dFdZ * dFdZ;
+            T a = mu * (r.cX * dFdX + r.cY * dFdY + r.cZ * dFdZ) / G;
+            T b = (mu * mu - 1.0) / G;
+            T a2 = a * a;
             if (b > a2) return false;
             b = a2 - b;
-            G = -a + std::sqrt(b);
+            G = -a + sqrt(b);
             r.cX = mu * r.cX + G * dFdX;
             r.cY = mu * r.cY + G * dFdY;
             r.cZ = mu * r.cZ + G * dFdZ;
@@ -392,54 +419,55 @@ inline bool refract(int cls, const SurfConst& s, double mu, Ray& r) {
 // ===========================================================================
 // Diffraction (surface.cu:1247-1520); L = m*lambda/n2(lambda)/d.
 // ===========================================================================
-inline bool diffract(int cls, int gr_type, const SurfConst& s, double mu, double L, Ray& r) {
+template <class T>
+inline bool diffract(int cls, int gr_type, const SurfConstT<T>& s, T mu, T L, RayT<T>& r) {
     if (gr_type == Transparent) {
         switch (cls) {
             case Plane: {  // plane_diffr_trans_kernel (surface.cu:1247-1282)
-                double a = mu * r.cZ;
-                double b = mu * mu - 1.0 + L * L - 2.0 * mu * L * r.cX;
-                double a2 = a * a;
+                T a = mu * r.cZ;
+                T b = mu * mu - 1.0 + L * L - 2.0 * mu * L * r.cX;
+                T a2 = a * a;
                 if (b > a2) return false;
                 b = a2 - b;
-                double G = -a + std::sqrt(b);
+                T G = -a + sqrt(b);
                 r.cX = mu * r.cX - L;
                 r.cY *= mu;
                 r.cZ = mu * r.cZ + G;
                 return true;
             }
             case Conic: {  // conic_diffr_trans_kernel (surface.cu:1320-1368)
-                double dFdX, dFdY;
+                T dFdX, dFdY;
                 conic_derivs(s, r.X, r.Y, dFdX, dFdY);
-                double G = dFdX / (dFdY * dFdY + 1.0);
-                double u = 1.0 / std::sqrt(1.0 + dFdX * G);
-                double v = -dFdY * u * G;
-                double w = -u * G;
+                T G = dFdX / (dFdY * dFdY + 1.0);
+                T u = 1.0 / sqrt(1.0 + dFdX * G);
+                T v = -dFdY * u * G;
+                T w = -u * G;
                 G = dFdX * dFdX + dFdY * dFdY + 1.0;
-                double a = mu * (r.cX * dFdX + r.cY * dFdY + r.cZ) / G;
-                double b = (mu * mu - 1.0 + L * L - 2.0 * L * mu * (r.cX * u + r.cY * v + r.cZ * w)) / G;
-                double a2 = a * a;
+                T a = mu * (r.cX * dFdX + r.cY * dFdY + r.cZ) / G;
+                T b = (mu * mu - 1.0 + L * L - 2.0 * L * mu * (r.cX * u + r.cY * v + r.cZ * w)) / G;
+                T a2 = a * a;
                 if (b > a2) return false;
                 b = a2 - b;
-                G = -a + std::sqrt(b);
+                G = -a + sqrt(b);
                 r.cX = mu * r.cX - L * u + G * dFdX;
                 r.cY = mu * r.cY - L * v + G * dFdY;
                 r.cZ = mu * r.cZ - L * w + G;
                 return true;
             }
             case Toric: {  // toric_diffr_trans_kernel (surface.cu:1423-1470)
-                double dFdX, dFdY, dFdZ;
+                T dFdX, dFdY, dFdZ;
                 toric_derivs(s, r.X, r.Y, r.Z, dFdX, dFdY, dFdZ);
-                double G = dFdX / (dFdY * dFdY + dFdZ + dFdZ);
-                double u = 1.0 / std::sqrt(1.0 + dFdX * G);
-                double v = -dFdY * u * G;
-                double w = -dFdZ * u * G;
+                T G = dFdX / (dFdY * dFdY + dFdZ + dFdZ);
+                T u = 1.0 / sqrt(1.0 + dFdX * G);
+                T v = -dFdY * u * G;
+                T w = -dFdZ * u * G;
                 G = dFdX * dFdX + dFdY * dFdY + dFdZ * dFdZ;
-                double a = mu * (r.cX * dFdX + r.cY * dFdY + r.cZ * dFdZ) / G;
-                double b = (mu * mu - 1.0 + L * L - 2.0 * L * mu * (r.cX * u + r.cY * v + r.cZ * w)) / G;
-                double a2 = a * a;
+                T a = mu * (r.cX * dFdX + r.cY * dFdY + r.cZ * dFdZ) / G;
+                T b = (mu * mu - 1.0 + L * L - 2.0 * L * mu * (r.cX * u + r.cY * v + r.cZ * w)) / G;
+                T a2 = a * a;
                 if (b > a2) return false;
                 b = a2 - b;
-                G = -a + std::sqrt(b);
+                G = -a + sqrt(b);
                 r.cX = mu * r.cX - L * u + G * dFdX;
                 r.cY = mu * r.cY - L * v + G * dFdY;
                 r.cZ = mu * r.cZ - L * w + G * dFdZ;
@@ -450,49 +478,49 @@ inline bool diffract(int cls, int gr_type, const SurfConst& s, double mu, double
     }
     switch (cls) {
         case Plane: {  // plane_diffr_refl_kernel (surface.cu:1284-1318)
-            double a = r.cZ;
-            double b = L * L - 2.0 * L * r.cX;
-            double a2 = a * a;
+            T a = r.cZ;
+            T b = L * L - 2.0 * L * r.cX;
+            T a2 = a * a;
             if (b > a2) return false;
             b = a2 - b;
-            double G = -a - std::sqrt(b);
+            T G = -a - sqrt(b);
             r.cX -= L;
             r.cZ += G;
             return true;
         }
         case Conic: {  // conic_diffr_refl_kernel (surface.cu:1370-1421)
-            double dFdX, dFdY;
+            T dFdX, dFdY;
             conic_derivs(s, r.X, r.Y, dFdX, dFdY);
-            double G = dFdX / (dFdY * dFdY + 1.0);
-            double u = 1.0 / std::sqrt(1.0 + dFdX * G);
-            double v = -dFdY * u * G;
-            double w = -u * G;
+            T G = dFdX / (dFdY * dFdY + 1.0);
+            T u = 1.0 / sqrt(1.0 + dFdX * G);
+            T v = -dFdY * u * G;
+            T w = -u * G;
             G = dFdX * dFdX + dFdY * dFdY + 1.0;
-            double a = (r.cX * dFdX + r.cY * dFdY + r.cZ) / G;
-            double b = (L * L - 2.0 * L * (r.cX * u + r.cY * v + r.cZ * w)) / G;
-            double a2 = a * a;
+            T a = (r.cX * dFdX + r.cY * dFdY + r.cZ) / G;
+            T b = (L * L - 2.0 * L * (r.cX * u + r.cY * v + r.cZ * w)) / G;
+            T a2 = a * a;
             if (b > a2) return false;
             b = a2 - b;
-            G = -a - std::sqrt(b);
+            G = -a - sqrt(b);
             r.cX = r.cX - L * u + G * dFdX;
             r.cY = r.cY - L * v + G * dFdY;
             r.cZ = r.cZ - L * w + G;
             return true;
         }
         case Toric: {  // toric_diffr_refl_kernel (surface.cu:1472-1520)
-            double dFdX, dFdY, dFdZ;
+            T dFdX, dFdY, dFdZ;
             toric_derivs(s, r.X, r.Y, r.Z, dFdX, dFdY, dFdZ);
-            double G = dFdX / (dFdY * dFdY + dFdZ + dFdZ);
-            double u = 1.0 / std::sqrt(1.0 + dFdX * G);
-            double v = -dFdY * u * G;
-            double w = -dFdZ * u * G;
+            T G = dFdX / (dFdY * dFdY + dFdZ + dFdZ);
+            T u = 1.0 / sqrt(1.0 + dFdX * G);
+            T v = -dFdY * u * G;
+            T w = -dFdZ * u * G;
             G = dFdX * dFdX + dFdY * dFdY + dFdZ * dFdZ;
-            double a = (r.cX * dFdX + r.cY * dFdY + r.cZ * dFdZ) / G;
-            double b = (L * L - 2.0 * L * (r.cX * u + r.cY * v + r.cZ * w)) / G;
-            double a2 = a * a;
+            T a = (r.cX * dFdX + r.cY * dFdY + r.cZ * dFdZ) / G;
+            T b = (L * L - 2.0 * L * (r.cX * u + r.cY * v + r.cZ * w)) / G;
+            T a2 = a * a;
             if (b > a2) return false;
             b = a2 - b;
-            G = -a - std::sqrt(b);
+            G = -a - sqrt(b);
             r.cX += -L * u + G * dFdX;
             r.cY += -L * v + G * dFdY;
             r.cZ += -L * w + G * dFdZ;
@@ -507,15 +535,16 @@ inline bool diffract(int cls, int gr_type, const SurfConst& s, double mu, double
 // ===========================================================================
 
 // Beam::Normalize body (common-lib/beam.cpp:541-569)
-inline void normalize(double& cX, double& cY, double& cZ) {
-    double acX = std::fabs(cX), acY = std::fabs(cY), acZ = std::fabs(cZ);
-    double norm;
+template <class T>
+inline void normalize(T& cX, T& cY, T& cZ) {
+    T acX = fabs(cX), acY = fabs(cY), acZ = fabs(cZ);
+    T norm;
     if (acX >= acY) {
-        if (acX >= acZ) norm = acX * std::sqrt(1.0 + acY * acY / acX / acX + acZ * acZ / acX / acX);
-        else norm = acZ * std::sqrt(1.0 + acX * acX / acZ / acZ + acY * acY / acZ / acZ);
+        if (acX >= acZ) norm = acX * sqrt(1.0 + acY * acY / acX / acX + acZ * acZ / acX / acX);
+        else norm = acZ * sqrt(1.0 + acX * acX / acZ / acZ + acY * acY / acZ / acZ);
     } else {
-        if (acY >= acZ) norm = acY * std::sqrt(1.0 + acX * acX / acY / acY + acZ * acZ / acY / acY);
-        else norm = acZ * std::sqrt(1.0 + acX * acX / acZ / acZ + acY * acY / acZ / acZ);
+        if (acY >= acZ) norm = acY * sqrt(1.0 + acX * acX / acY / acY + acZ * acZ / acY / acY);
+        else norm = acZ * sqrt(1.0 + acX * acX / acZ / acZ + acY * acY / acZ / acZ);
     }
     cX /= norm;
     cY /= norm;
@@ -525,26 +554,27 @@ inline void normalize(double& cX, double& cY, double& cZ) {
 // Aperture test of Surface::ApplyConstrains (common-lib/surface.cpp:264-321)
 // and Shade::ApplyConstrains (common-lib/surface.cpp:652-699); true = ray
 // survives.  `shade` selects the inverted test.
+template <class T>
 inline bool aperture_pass(bool shade, int shape, const double size[2], const double center[2],
-                          double X, double Y) {
-    double xr = X - center[0];
-    double yr = Y - center[1];
+                          T X, T Y) {
+    T xr = X - center[0];
+    T yr = Y - center[1];
     if (!shade) {
         if (shape == Circle) {
-            double R2 = size[0] * size[0];
-            double ray_R2 = xr * xr + yr * yr;
+            const double R2 = size[0] * size[0];  // once per surface in the reference
+            T ray_R2 = xr * xr + yr * yr;
             return !(ray_R2 > R2);
         }
-        return !((X < (center[0] - size[0] / 2.0)) || (X > (center[0] + size[0] / 2.0)) ||
-                 (Y < (center[1] - size[1] / 2.0)) || (Y > (center[1] + size[1] / 2.0)));
+        return !((X < (T(center[0]) - T(size[0]) / 2.0)) || (X > (T(center[0]) + T(size[0]) / 2.0)) ||
+                 (Y < (T(center[1]) - T(size[1]) / 2.0)) || (Y > (T(center[1]) + T(size[1]) / 2.0)));
     }
     if (shape == Circle) {
-        double R2 = size[0] * size[0];
-        double ray_R2 = xr * xr + yr * yr;
+        const double R2 = size[0] * size[0];
+        T ray_R2 = xr * xr + yr * yr;
         return !(ray_R2 <= R2);
     }
-    return !((xr >= -size[0] / 2.0) && (xr <= size[0] / 2.0) &&
-             (yr >= -size[1] / 2.0) && (yr <= size[1] / 2.0));
+    return !((xr >= -T(size[0]) / 2.0) && (xr <= T(size[0]) / 2.0) &&
+             (yr >= -T(size[1]) / 2.0) && (yr <= T(size[1]) / 2.0));
 }
 
 // Beam::Rearrange (common-lib/beam.cpp:574-598): two-pointer partition of the
@@ -603,8 +633,9 @@ inline TransformConst make_transform(const double angles[3], const double dist[3
 }
 
 // rotation_kernel body (beam.cu:333-350)
-inline void rotate_pair(double sA, double cA, double& v1, double& v2, double& w1, double& w2) {
-    double e = v1 * cA - v2 * sA;
+template <class T>
+inline void rotate_pair(double sA, double cA, T& v1, T& v2, T& w1, T& w2) {
+    T e = v1 * cA - v2 * sA;
     v2 = v1 * sA + v2 * cA;
     v1 = e;
     e = w1 * cA - w2 * sA;
@@ -613,7 +644,8 @@ inline void rotate_pair(double sA, double cA, double& v1, double& v2, double& w1
 }
 
 // Translation then rotations about Y, X, Z (beam.cu:437-518).
-inline void transform(const TransformConst& t, Ray& r) {
+template <class T>
+inline void transform(const TransformConst& t, RayT<T>& r) {
     if (t.translate) {
         r.X -= t.dist[0];
         r.Y -= t.dist[1];
@@ -651,8 +683,8 @@ inline void spline_init(size_t N, const double* x, const double* y, double* y2) 
 
 // TabulatedFunction::operator[] (tabulated_function.cpp:173-204).  Returns
 // false where the reference throws (OutOfRange, BadArgument).
-inline bool table_eval(size_t n, const double* x, const double* y, const double* y2, double xval,
-                       double& out) {
+template <class T>
+inline bool table_eval(size_t n, const double* x, const double* y, const double* y2, T xval, T& out) {
     if (n == 0) return false;
     if (n == 1) { out = y[0]; return true; }
     if ((xval < x[0]) || (xval > x[n - 1])) return false;
@@ -662,10 +694,10 @@ inline bool table_eval(size_t n, const double* x, const double* y, const double*
         if (x[i] == xval) { out = y[i]; return true; }
         if (x[i] > xval) ir = i; else il = i;
     }
-    double h = x[ir] - x[il];
+    T h = T(x[ir]) - x[il];
     if (h == 0.0) return false;
-    double a = (x[ir] - xval) / h;
-    double b = (xval - x[il]) / h;
+    T a = (x[ir] - xval) / h;
+    T b = (xval - x[il]) / h;
     out = a * y[il] + b * y[ir] + ((a * a * a - a) * y2[il] + (b * b * b - b) * y2[ir]) * (h * h) / 6.0;
     return true;
 }
