@@ -111,14 +111,43 @@ __global__ void __launch_bounds__(256) k_adj_forward(AdjArgs a, DevRays in, unsi
 // The dual-number surface constants of pass (k, d0) of the backward sweep:
 // lane l differentiates state component d0 + l (< 6) or the surface's
 // parameter d0 + l - 6.
+// The state directions of surface k's backward passes.  The first surface's
+// input is the entrance ray, which no parameter moves: none.  A later
+// surface's input is the previous surface's output, whose cosines form a unit
+// vector: every perturbation of them lies in the plane orthogonal to the
+// direction, so the input adjoint is needed only there -- the three position
+// components and two tangent directions of the cosines, 5 instead of 6.
+__host__ __device__ __forceinline__ int backward_state_dirs(int k) { return k == 0 ? 0 : 5; }
+
+// Direction d of a pass: state seed 0..2 (X, Y, Z), 6 or 7 (the cosines'
+// tangent directions), or parameter d - n_state of the surface.
 __device__ __forceinline__ void backward_seeds(const AdjArgs& a, int k, int d0, ad::Seeds<kAdjW>& sd) {
-    const int ndir = 6 + a.surf_nparams[k];
+    const int ns = backward_state_dirs(k);
+    const int ndir = ns + a.surf_nparams[k];
     sd.dense = nullptr;
     for (int l = 0; l < kAdjW; ++l) {
         const int d = d0 + l;
-        sd.state[l] = (d < 6) ? d : -1;
-        sd.param[l] = (d >= 6 && d < ndir) ? a.surf_params[k * RTB_ADJ_MAX_PARAMS + (d - 6)] : -1;
+        sd.state[l] = (d < ns) ? (d < 3 ? d : 6 + (d - 3)) : -1;
+        sd.param[l] = (d >= ns && d < ndir) ? a.surf_params[k * RTB_ADJ_MAX_PARAMS + (d - ns)] : -1;
     }
+}
+
+// An orthonormal pair spanning the plane orthogonal to the unit vector c:
+// t1 = c x e / |c x e| with e the axis least aligned with c, t2 = c x t1.
+__device__ __forceinline__ void tangent_pair(const double c[3], double t1[3], double t2[3]) {
+    const double ax = fabs(c[0]), ay = fabs(c[1]), az = fabs(c[2]);
+    if (ax <= ay && ax <= az) {
+        t1[0] = 0.0; t1[1] = c[2]; t1[2] = -c[1];
+    } else if (ay <= az) {
+        t1[0] = -c[2]; t1[1] = 0.0; t1[2] = c[0];
+    } else {
+        t1[0] = c[1]; t1[1] = -c[0]; t1[2] = 0.0;
+    }
+    const double inv = 1.0 / sqrt(t1[0] * t1[0] + t1[1] * t1[1] + t1[2] * t1[2]);
+    t1[0] *= inv; t1[1] *= inv; t1[2] *= inv;
+    t2[0] = c[1] * t1[2] - c[2] * t1[1];
+    t2[1] = c[2] * t1[0] - c[0] * t1[2];
+    t2[2] = c[0] * t1[1] - c[1] * t1[0];
 }
 
 // One thread per table entry (k, d0).
@@ -172,14 +201,17 @@ __global__ void __launch_bounds__(kAdjThreads, 4) k_adj_backward(AdjArgs a, cons
             double st[6];
             if (act)
                 for (int c = 0; c < 6; ++c) st[c] = a.ckpt[((size_t)k * 6 + c) * a.n + i];
-            const int ndir = 6 + a.surf_nparams[k];
-            double adj_in[6] = {0, 0, 0, 0, 0, 0};
+            const int nst = backward_state_dirs(k);
+            const int ndir = nst + a.surf_nparams[k];
+            double t1[3] = {0, 0, 0}, t2[3] = {0, 0, 0};
+            if (act && nst) tangent_pair(st + 3, t1, t2);
+            double adj_in[6] = {0, 0, 0, 0, 0, 0}, a_t1 = 0.0, a_t2 = 0.0;
             for (int d0 = 0, e = first_entry[k]; d0 < ndir; d0 += kAdjW, ++e) {
                 ad::Seeds<kAdjW> sd;
                 backward_seeds(a, k, d0, sd);
                 ad::RayD<kAdjW> r;
                 if (act) {
-                    ad::load_state(st, sd, r);
+                    ad::load_state(st, sd, r, t1, t2);
                     ad::surface_step(s, table[e], sch->fixes, a.knots, order_of(s, a.beams, b), lam, r);
                 }
                 // the last surface's output is the CCD-plane point: only X, Y
@@ -198,16 +230,20 @@ __global__ void __launch_bounds__(kAdjThreads, 4) k_adj_backward(AdjArgs a, cons
                         v += adj[4] * r.cY.d[l];
                         v += adj[5] * r.cZ.d[l];
                     }
-                    if (d < 6) {
+                    if (d < nst) {
 #pragma unroll
-                        for (int c = 0; c < 6; ++c)
+                        for (int c = 0; c < 3; ++c)
                             if (d == c) adj_in[c] = v;
+                        if (d == 3) a_t1 = v;
+                        if (d == 4) a_t2 = v;
                     } else {
                         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
                         if (lane == 0) acc[warp][sd.param[l]] += v;
                     }
                 }
             }
+            // the cosines' adjoint, in the plane of their perturbations
+            for (int c = 0; c < 3; ++c) adj_in[3 + c] = a_t1 * t1[c] + a_t2 * t2[c];
             for (int c = 0; c < 6; ++c) adj[c] = adj_in[c];
         }
     }
@@ -635,7 +671,8 @@ int rtb_adjoint_backward(rtb_adjoint* c, const double* gX, const double* gY, dou
     std::vector<int> first(c->surf_nparams.size());
     for (size_t k = 0; k < c->surf_nparams.size(); ++k) {
         first[k] = (int)entries.size();
-        for (int d0 = 0; d0 < 6 + c->surf_nparams[k]; d0 += kAdjW) entries.push_back(make_int2((int)k, d0));
+        for (int d0 = 0; d0 < backward_state_dirs((int)k) + c->surf_nparams[k]; d0 += kAdjW)
+            entries.push_back(make_int2((int)k, d0));
     }
     const size_t ne = entries.size();
     auto al = [](size_t x) { return (x + 255) / 256 * 256; };

@@ -110,8 +110,11 @@ __device__ void make_surfd(const DevSurface& s, int k, const ParamRef* map, int 
 
 // The seeded component is chosen with selects, not by indexing: a run-time
 // index into the ray's fields would keep the whole ray in local memory.
+// State seeds: lane l differentiates component sd.state[l] (0..5), or the
+// cosines along t1 (6) or t2 (7).
 template <int W>
-__device__ __forceinline__ void load_state(const double st[6], const Seeds<W>& sd, RayD<W>& r) {
+__device__ __forceinline__ void load_state(const double st[6], const Seeds<W>& sd, RayD<W>& r,
+                                           const double* t1 = nullptr, const double* t2 = nullptr) {
     r.X = cst<W>(st[0]);
     r.Y = cst<W>(st[1]);
     r.Z = cst<W>(st[2]);
@@ -125,9 +128,9 @@ __device__ __forceinline__ void load_state(const double st[6], const Seeds<W>& s
         r.X.d[l] = (c == 0) ? 1.0 : 0.0;
         r.Y.d[l] = (c == 1) ? 1.0 : 0.0;
         r.Z.d[l] = (c == 2) ? 1.0 : 0.0;
-        r.cX.d[l] = (c == 3) ? 1.0 : 0.0;
-        r.cY.d[l] = (c == 4) ? 1.0 : 0.0;
-        r.cZ.d[l] = (c == 5) ? 1.0 : 0.0;
+        r.cX.d[l] = (c == 3) ? 1.0 : (c == 6 && t1) ? t1[0] : (c == 7 && t2) ? t2[0] : 0.0;
+        r.cY.d[l] = (c == 4) ? 1.0 : (c == 6 && t1) ? t1[1] : (c == 7 && t2) ? t2[1] : 0.0;
+        r.cZ.d[l] = (c == 5) ? 1.0 : (c == 6 && t1) ? t1[2] : (c == 7 && t2) ? t2[2] : 0.0;
     }
 }
 
