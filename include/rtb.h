@@ -605,7 +605,10 @@ RTB_API int rtb_adjoint_theta(const rtb_adjoint* ctx, double* theta);
 RTB_API int rtb_adjoint_forward(rtb_adjoint* ctx, const double* theta, const rtb_rays* rays, double* X, double* Y,
                                 char* flag, rtb_trace_stats* stats, void* stream);
 /* grad[j] = sum over rays of gX * dX/dtheta_j + gY * dY/dtheta_j for the last
- * forward (gX, gY device, n_rays; grad host, n_params).  Deterministic. */
+ * forward (gX, gY device, n_rays; grad host, n_params).  Deterministic.  One
+ * reverse sweep per ray through the surfaces, each surface recomputed from its
+ * checkpoint; with the environment variable RTB_ADJOINT_BACKWARD=passes, the
+ * same gradient (to rounding) by forward-mode dual-number passes. */
 RTB_API int rtb_adjoint_backward(rtb_adjoint* ctx, const double* gX, const double* gY, double* grad, void* stream);
 /* Forward-mode sensitivities of the last forward along dtheta (host, n_params):
  * dX, dY (device, n_rays) = sum_j dtheta_j dX/dtheta_j (0 for lost rays). */

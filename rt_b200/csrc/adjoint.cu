@@ -6,25 +6,32 @@
 // bits), storing each ray's state (X Y Z cX cY cZ) at the input of every
 // surface -- 48 bytes x surfaces per ray.
 //
-// Backward (k_adj_backward): per ray, surfaces last to first.  For surface k
-// the local Jacobian of its output state with respect to its input state and
-// to the parameters that live on it is recomputed from checkpoint k in
-// forward mode (dual numbers, W directions per pass); the adjoint of the
-// output state is carried back through it, and the parameter adjoints are
-// accumulated.  The surface's dual-number constants of every pass (which do
-// not depend on the ray) are built once per call into a table
-// (k_build_surfd) that all threads read.  Each warp sums a parameter's
-// contributions over its 32 lanes with a shuffle tree and adds them to its
-// row in shared memory; the block adds its warps' rows in order and the block
-// partials are summed in block order, so the gradient is reproducible.
+// Backward (k_adj_reverse): per ray, surfaces last to first.  Surface k is
+// recomputed from checkpoint k and the adjoint of its output state is carried
+// back through its stages in reverse order (ray_rev.cuh), giving the adjoint
+// of its input state and of the constants its parameters move, in one sweep.
+// Each warp sums a parameter's contributions over its 32 lanes with a
+// shuffle tree and adds them to its row in shared memory; the block adds its
+// warps' rows in order and the block partials are summed in block order, so
+// the gradient is reproducible.
+//
+// The same gradient by forward-mode passes (k_adj_backward, selected with
+// RTB_ADJOINT_BACKWARD=passes): for surface k the local Jacobian of its
+// output state with respect to its input state and to the parameters that
+// live on it is recomputed from checkpoint k with dual numbers, W directions
+// per pass, and contracted with the output adjoint.  The surface's
+// dual-number constants of every pass (which do not depend on the ray) are
+// built once per call into a table (k_build_surfd) that all threads read.
 //
 // Translation unit compiled with --fmad=false: the dual numbers' values are
 // the plain engine's.
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
 #include "engine.cuh"
 #include "ray_ad.cuh"
+#include "ray_rev.cuh"
 #include "trace_common.cuh"
 
 namespace rtb {
@@ -253,6 +260,63 @@ __global__ void __launch_bounds__(kAdjThreads, 4) k_adj_backward(AdjArgs a, cons
         for (int w = 0; w < kAdjWarps; ++w) sum += acc[w][p];
         partial[(size_t)blockIdx.x * P + p] = sum;
     }
+}
+
+// The reverse sweep (ray_rev.cuh).  Rays are taken 32 at a time per warp,
+// every lane of a warp the same number of steps, so the warp can sum each
+// parameter's contributions with shuffles.  The first surface's input
+// adjoint is not needed: a first surface without parameters is not swept.
+__global__ void __launch_bounds__(kAdjThreads, 4) k_adj_reverse(AdjArgs a, const double* gX, const double* gY,
+                                                             double* partial) {
+    __shared__ double acc[kAdjWarps][RTB_ADJ_MAX_PARAMS];
+    const DevScheme* sch = a.sch;
+    const int ns = sch->n_surfaces;
+    const int P = a.n_params;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int p = lane; p < P; p += 32) acc[warp][p] = 0.0;
+    __syncwarp();
+    for (size_t i0 = (size_t)blockIdx.x * blockDim.x + (size_t)warp * 32; i0 < a.n; i0 += gstride()) {
+        const size_t i = i0 + lane;
+        bool act = i < a.n && a.flag[i] == 1;
+        rv::RayA adj{act ? gX[i] : 0.0, act ? gY[i] : 0.0, 0.0, 0.0, 0.0, 0.0};
+        act = act && !(adj.X == 0.0 && adj.Y == 0.0);
+        if (!__any_sync(0xffffffffu, act)) continue;
+        const double lam = act ? a.lambda[i] : 0.0;
+        const int b = act ? beam_of(a.beams, a.n_beams, i) : 0;
+        for (int k = ns - 1; k >= 0; --k) {
+            const int np = a.surf_nparams[k];
+            if (k == 0 && np == 0) break;
+            const DevSurface& s = sch->s[k];
+            rv::SurfA pa;
+            rv::clear(pa);
+            if (act) {
+                const double* c = a.ckpt + (size_t)k * 6 * a.n + i;
+                const f64::Ray r0{c[0], c[a.n], c[2 * a.n], c[3 * a.n], c[4 * a.n], c[5 * a.n]};
+                if (!rv::surface_rev(s, sch->fixes, a.knots, order_of(s, a.beams, b), lam, r0, adj, pa)) {
+                    act = false;  // not reached: the recomputation is the forward's
+                    rv::clear(pa);
+                }
+            }
+            for (int q = 0; q < np; ++q) {
+                const int j = a.surf_params[k * RTB_ADJ_MAX_PARAMS + q];
+                double v = act ? rv::param_adjoint(s, a.map[j], pa) : 0.0;
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                if (lane == 0) acc[warp][j] += v;
+            }
+        }
+    }
+    __syncthreads();
+    for (int p = threadIdx.x; p < P; p += blockDim.x) {
+        double sum = 0.0;
+        for (int w = 0; w < kAdjWarps; ++w) sum += acc[w][p];
+        partial[(size_t)blockIdx.x * P + p] = sum;
+    }
+}
+
+// RTB_ADJOINT_BACKWARD=passes: the backward by forward-mode passes.
+bool backward_by_passes() {
+    const char* e = std::getenv("RTB_ADJOINT_BACKWARD");
+    return e && std::strcmp(e, "passes") == 0;
 }
 
 __global__ void k_adj_sum_partials(const double* partial, int n_blocks, int P, double* grad) {
@@ -666,6 +730,19 @@ int rtb_adjoint_backward(rtb_adjoint* c, const double* gX, const double* gY, dou
     cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
     const int P = (int)c->params.size();
     const unsigned grid = adj_grid(c->n, kAdjThreads);
+    AdjArgs a = adj_args(c);
+    if (!backward_by_passes()) {
+        DevBuf part;
+        int st = part.alloc((size_t)grid * P * sizeof(double), s);
+        if (st != RTB_OK) return st;
+        k_adj_reverse<<<grid, kAdjThreads, 0, s>>>(a, gX, gY, part.as<double>());
+        RTB_CUDA_TRY(cudaGetLastError());
+        k_adj_sum_partials<<<1, RTB_ADJ_MAX_PARAMS, 0, s>>>(part.as<double>(), (int)grid, P, c->d_grad);
+        RTB_CUDA_TRY(cudaGetLastError());
+        RTB_CUDA_TRY(cudaMemcpyAsync(grad, c->d_grad, P * sizeof(double), cudaMemcpyDeviceToHost, s));
+        RTB_CUDA_TRY(cudaStreamSynchronize(s));
+        return RTB_OK;
+    }
     // the passes of every surface: (k, first direction)
     std::vector<int2> entries;
     std::vector<int> first(c->surf_nparams.size());
@@ -688,7 +765,6 @@ int rtb_adjoint_backward(rtb_adjoint* c, const double* gX, const double* gY, dou
     double* partial = reinterpret_cast<double*>(p + o_part);
     RTB_CUDA_TRY(cudaMemcpyAsync(d_ent, entries.data(), ne * sizeof(int2), cudaMemcpyHostToDevice, s));
     RTB_CUDA_TRY(cudaMemcpyAsync(d_first, first.data(), first.size() * sizeof(int), cudaMemcpyHostToDevice, s));
-    AdjArgs a = adj_args(c);
     k_build_surfd<<<(unsigned)((ne + 63) / 64), 64, 0, s>>>(a, d_ent, (int)ne, table);
     RTB_CUDA_TRY(cudaGetLastError());
     k_adj_backward<<<grid, kAdjThreads, 0, s>>>(a, table, d_first, gX, gY, partial);

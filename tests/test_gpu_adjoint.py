@@ -4,8 +4,9 @@ parameters (GPU tests).
 
 * The forward is the plain FP64 engine: the same bits as rtb_trace's fused
   FP64 trace, also with the parameters moved.
-* The backward (reverse sweep over surfaces from checkpoints) equals the
-  contraction of the forward-mode sensitivities with the same seeds.
+* The backward (reverse sweep over the surfaces, and inside each surface,
+  from checkpoints) equals the contraction of the forward-mode sensitivities
+  with the same seeds.
 * Forward-mode sensitivities match central finite differences ray by ray.
 * The merit sum_lambda RMS + 10 (xbar - x_t(lambda))^2, differentiated
   through a torch.autograd.Function around forward/backward, matches central
