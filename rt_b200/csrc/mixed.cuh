@@ -524,7 +524,12 @@ __device__ __forceinline__ int action(const DevSurface& s, const double* knots, 
     if (type == RTB_GRATING) {
         const double mu = (gr_type == RTB_TRANSPARENT) ? n1v * in2 : 0.0;
         const double L = (double)order * lambda * in2 * s.inv_gr;
-        return diffract<Sh>(s, mu, L, nx, ny, nz, r) ? 0 : 1;
+        if (!diffract<Sh>(s, mu, L, nx, ny, nz, r)) return 1;
+        // the reference's rule direction on a toric (L^2+M+M) is neither a
+        // unit vector nor orthogonal to the normal, so the diffracted cosines
+        // are not a unit vector: the Normalize after the action matters here
+        if (cls == RTB_TORIC) normalize(r);
+        return 0;
     }
     return 0;
 }
@@ -534,8 +539,9 @@ __device__ __forceinline__ int action(const DevSurface& s, const double* knots, 
 // One surface of the mixed engine on one ray: -1 survived, a stage >= 0 that
 // lost it, -2 a wavelength outside a table.  The reference normalises the
 // direction cosines after every transform and action (beam.cpp:527-571);
-// rotations and the reflection, refraction and grating formulas preserve a
-// unit vector, so here the cosines are normalised once, when a ray is loaded.
+// rotations and the reflection, refraction and plane and conic grating
+// formulas preserve a unit vector, so here the cosines are normalised when a
+// ray is loaded and after a toric grating only.
 template <class Sh = RtShape>
 __device__ __forceinline__ int mx_surface(const DevSurface& s, int k, uint32_t fixes, const double* knots,
                                           const BeamCtx& bc, double lam, mx::TableMemo& memo, mx::Ray& r) {

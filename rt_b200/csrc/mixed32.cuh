@@ -209,6 +209,7 @@ __device__ __forceinline__ int m32_surface(const DevSurface& s, int k, uint32_t 
     const double mu = (gr_type == RTB_TRANSPARENT) ? n1v * in2 : 0.0;
     const double L = (double)order * lam * in2 * s.inv_gr;
     if (!mx::diffract<Sh>(s, mu, L, (double)nx, (double)ny, (double)nz, q)) return 3 * k + 2;
+    if (cls == RTB_TORIC) mx::normalize(q);  // the toric rule direction leaves the cosines off unit length
     r.cX = (float)q.cX;
     r.cY = (float)q.cY;
     r.cZ = (float)q.cZ;

@@ -14,9 +14,12 @@
 // loads thus cost one instruction per warp, issued a whole row of tracing
 // ahead, instead of a scoreboard wait per lane and array.
 //
-// Rows are handed out as TileSched tiles of rpt rows; a warp takes its next
-// tile from the counter when it starts the last row of the current one, so
-// the copy of the next tile's first row is in flight as early as any other.
+// Rows are handed out as TileSched tiles of rpt rows.  A warp draws its tiles
+// from the counter one tile ahead: the atomic that names the tile after next
+// is issued when a tile starts and its result is first used when that tile
+// ends, so its round trip to L2 is hidden behind a tile of tracing; the copy
+// of the next tile's first row starts with the last row of the current one,
+// as early as any other row's.
 // Every wait on the mbarrier is bounded: past kWaitLimit polls the kernel
 // raises DEV_ERR_TIMEOUT, waits (bounded again) for the copy it issued and
 // stops taking rows.  The copies read this GPU's own memory only and use no
@@ -94,6 +97,7 @@ struct RowLoop {
     const TileSched& ts;
     uint64_t n, n_tiles;
     uint64_t tile = 0, next_tile_ = 0;
+    unsigned long long ahead = 0;  // lane 0: the counter value drawn for the tile after next
     int j = 0, next_j = 0;
     bool have_next = false, packed;
     unsigned row_bytes;
@@ -112,7 +116,19 @@ struct RowLoop {
         }
         have_next = next_tile(ts, n_tiles, next_tile_);
         next_j = 0;
-        if (have_next) issue(next_tile_, 0);
+        if (have_next) {
+            issue(next_tile_, 0);
+            draw_ahead();
+        }
+    }
+    // Lane 0 draws a tile from the counter; the result is read at the next
+    // tile switch (take_ahead).
+    __device__ void draw_ahead() {
+        if ((threadIdx.x & 31) == 0) ahead = atomicAdd(ts.next, 1ull);
+    }
+    __device__ bool take_ahead(uint64_t& t) const {
+        t = __shfl_sync(0xffffffffu, ahead, 0);
+        return t < n_tiles;
     }
     __device__ uint64_t row_of(uint64_t t, int jj) const { return t * (uint64_t)ts.rpt + (uint64_t)jj; }
     __device__ void issue(uint64_t t, int jj) {
@@ -149,8 +165,9 @@ struct RowLoop {
             next_j = j + 1;
             have_next = true;
         } else {
-            have_next = next_tile(ts, n_tiles, next_tile_);
+            have_next = take_ahead(next_tile_);
             next_j = 0;
+            if (have_next) draw_ahead();
         }
         if (have_next) issue(next_tile_, next_j);
     }

@@ -39,3 +39,29 @@ def test_mixed_ccd_error(case, precision):
     assert m["p99_9_um"] <= 0.05
     assert m["pixel_mismatch_rate"] < 1e-3
     assert abs(int(sm.n_good) - int(sr.n_good)) <= 1e-4 * n + 2
+
+
+# FP32-state error bounds measured on the coverage schemes (p99.9, um): the
+# lenses scheme refracts part of its beam close to total internal reflection
+# at its tilted window, where the FP32 cosines' rounding (1e-7) is amplified
+# by 1 / cos of the refracted angle; the FP64-state engine keeps its 0.05 um
+# there.  RTB_MIXED32 is the faster engine only where it meets the budget
+# (bench.py picks the headline engine by that test on C1).
+MIXED32_COVERAGE_P999_UM = {"mirrors": 0.05, "gratings": 0.15, "lenses": 1.0}
+
+
+@pytest.mark.parametrize("precision", [ffi.MIXED, ffi.MIXED32])
+@pytest.mark.parametrize("name", ["mirrors", "lenses", "gratings"])
+def test_mixed_ccd_error_on_coverage_schemes(name, precision):
+    """Every surface class, type and grating form (toric gratings included,
+    whose rule direction leaves the diffracted cosines off unit length until
+    the Normalize that follows)."""
+    specs = S.coverage_schemes()[name]
+    beams = [S.make_beam(0, 20000, 5, 10.0, (0.4, 0.8), 11)]
+    n = S.total_rays(beams)
+    rays, ref, sm, sr = _trace_pair(specs, beams, n, 3, precision)
+    m = metrics.ccd_error(rays.X, rays.Y, rays.flag, ref.X, ref.Y, ref.flag, 80.0, 80.0, 0.015, 0.015)
+    print(name, precision, m)
+    assert m["rays_compared"] > 0.1 * n  # the mirrors scheme's apertures clip most of the beam
+    assert m["p99_9_um"] <= (0.05 if precision == ffi.MIXED else MIXED32_COVERAGE_P999_UM[name])
+    assert abs(int(sm.n_good) - int(sr.n_good)) <= 1e-4 * n + 2

@@ -260,9 +260,12 @@ def test_specialised_plan_equals_generic_kernel(name, precision, monkeypatch):
     sum into an FMA that the generic kernel keeps apart (the gratings
     scheme).  Both are far inside the mixed engine's 0.05 um budget against
     the FP64 oracle.  FP32 state: the contractions the compiler picks move
-    the FP32 state by a few ulps, the outputs by up to 1e-5 mm (0.01 um), and
-    a ray on an aperture edge may fall on the other side (at most one in
-    1e4)."""
+    the FP32 state by a few ulps, which the optics can amplify (a refraction
+    near total internal reflection, on the lenses scheme, by up to 1e-3 mm on
+    single rays): each kernel's CCD error against the FP64 engine (p99.9)
+    stays within the FP32-state engine's bound for the scheme (0.05 um; the
+    gratings scheme 0.15 um, the lenses scheme 1 um), and a ray on an aperture
+    edge may fall on the other side (at most one in 1e4)."""
     make, kw, orders = SPEC_SCHEMES[name]
     beams = [S.make_beam(0, 3000, kw["n_lambda"], kw["radius"], kw["lam_range"], 11, orders=orders)]
     ccd = S.ccd(S.C1_CCD)
@@ -284,12 +287,26 @@ def test_specialised_plan_equals_generic_kernel(name, precision, monkeypatch):
     assert a[0] == b[0] and a[0] in TRACED + (ffi.OUT_OF_RANGE,)
     assert a[2] > 0
     if precision == ffi.MIXED32:
-        both = (a[3]["flag"] == 1) & (b[3]["flag"] == 1)
         assert int((a[3]["flag"] != b[3]["flag"]).sum()) <= 1e-4 * a[3]["flag"].numel() + 1
         assert abs(a[2] - b[2]) <= 1e-4 * a[3]["flag"].numel() + 1
-        for f in ("X", "Y"):
-            x, y = a[3][f][both], b[3][f][both]
-            assert float((x - y).abs().max()) <= 1e-5, f
+        o, counts64, outside64 = frame_opts(ffi.FP64, ccd, state_out=1)  # the plan writes into these
+        plan = E.Plan(cs.surfaces, beams, o)
+        plan.run()
+        _, ref = plan_output(plan)
+        ref = {k: v.clone() for k, v in ref.items()}
+        plan.destroy()
+        torch.cuda.synchronize()
+        del counts64, outside64
+
+        def p999_um(out):
+            both = (out["flag"] == 1) & (ref["flag"] == 1)
+            d = torch.hypot(out["X"][both] - ref["X"][both], out["Y"][both] - ref["Y"][both]) * 1e3
+            return float(torch.quantile(d.float().cpu(), 0.999))
+
+        ea, eb = p999_um(a[3]), p999_um(b[3])
+        print(name, "FP32 state, p99.9 um against FP64: specialised", ea, "generic", eb)
+        bound = {"gratings": 0.15, "lenses": 1.0}.get(name, 0.05)
+        assert max(ea, eb) <= bound, (ea, eb)
         return
     assert a[:3] == b[:3]
     same = 0
