@@ -316,8 +316,8 @@ RTB_API int rtb_trace_out(const rtb_surface* surfaces, size_t n_surfaces, const 
  * counters, or more shared memory than a block may have) return
  * RTB_BAD_VALUE before any work is queued; with the largest tables the array
  * holds the counters of 1,100 beams of a 32-surface scheme.  The first call
- * on a device looks up the array's address with that device current; make it
- * before any stream capture.  A NULL stream (the library's own) is valid only
+ * on a device looks up the array's address with that device current.  A NULL
+ * stream (the library's own) is valid only
  * on the device the library was first used on.  Calls run one at a time and
  * each returns with `stream` synchronised; all calls share the array, so
  * other GPU work that wrote it during a call would race with that call. */
