@@ -185,7 +185,7 @@ def c4_adjoint(npl, reps=3):
            "gradient_ms": t_fwd + t_mer + t_bwd, "central_differences_ms": 2 * P * t_fwd,
            "grad_norm": float(np.linalg.norm(grad)),
            "how": "rtb_adjoint_forward (checkpoints at surface inputs), rtb_adjoint_spot_merit, "
-                  "rtb_adjoint_backward (reverse sweep inside each surface), rtb_adjoint_jvp; "
+                  "rtb_adjoint_backward (reverse sweep inside each surface, compiled for the scheme's structure), rtb_adjoint_jvp; "
                   "wall clock of synchronous calls, best of 3"}
     adj.destroy()
     del rays

@@ -623,6 +623,15 @@ RTB_API int rtb_adjoint_jvp(rtb_adjoint* ctx, const double* dtheta, double* dX, 
 RTB_API int rtb_adjoint_spot_merit(rtb_adjoint* ctx, const double* target_x, double weight, double* merit,
                                    double* gX, double* gY, void* stream);
 RTB_API int rtb_adjoint_destroy(rtb_adjoint* ctx);
+/* Compile the adjoint's reverse sweep for this scheme's structure ahead of
+ * rtb_adjoint_create (which compiles it otherwise, once per structure and
+ * process, and launches it from rtb_adjoint_backward; RTB_SPECIALIZE=0 keeps
+ * the generic kernel); needs no device.  One kernel serves every parameter
+ * value of the structure.  RTB_OK when compiled; RTB_FAILED with the reason
+ * in note (may be NULL) when NVRTC is unavailable or fails.  No counterpart
+ * in the reference. */
+RTB_API int rtb_adjoint_specialize(const rtb_surface* surfaces, size_t n_surfaces, uint32_t fixes, char* note,
+                                   size_t note_len);
 
 #ifdef __cplusplus
 }

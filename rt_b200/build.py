@@ -45,6 +45,10 @@ JIT_HEADERS = {
     "rowpipe.cuh": os.path.join(CSRC, "rowpipe.cuh"),
     "shape.cuh": os.path.join(CSRC, "shape.cuh"),
     "fused_fp64.cuh": os.path.join(CSRC, "fused_fp64.cuh"),
+    "dual.cuh": os.path.join(CSRC, "dual.cuh"),
+    "ray_ad.cuh": os.path.join(CSRC, "ray_ad.cuh"),
+    "ray_rev.cuh": os.path.join(CSRC, "ray_rev.cuh"),
+    "adjoint_rev.cuh": os.path.join(CSRC, "adjoint_rev.cuh"),
     "../../include/rtb.h": os.path.join(HERE, "..", "include", "rtb.h"),
 }
 

@@ -6,14 +6,11 @@
 // bits), storing each ray's state (X Y Z cX cY cZ) at the input of every
 // surface -- 48 bytes x surfaces per ray.
 //
-// Backward (k_adj_reverse): per ray, surfaces last to first.  Surface k is
-// recomputed from checkpoint k and the adjoint of its output state is carried
-// back through its stages in reverse order (ray_rev.cuh), giving the adjoint
-// of its input state and of the constants its parameters move, in one sweep.
-// Each warp sums a parameter's contributions over its 32 lanes with a
-// shuffle tree and adds them to its row in shared memory; the block adds its
-// warps' rows in order and the block partials are summed in block order, so
-// the gradient is reproducible.
+// Backward (adjoint_rev.cuh): per ray, surfaces last to first, each surface
+// recomputed from its checkpoint and its adjoint carried back through its
+// stages in one reverse sweep (ray_rev.cuh); the kernel compiled for the
+// scheme's structure when NVRTC is there (jit.cpp, rtb_adj_reverse_scheme;
+// RTB_SPECIALIZE=0 keeps the generic k_adj_reverse), its sums reproducible.
 //
 // The same gradient by forward-mode passes (k_adj_backward, selected with
 // RTB_ADJOINT_BACKWARD=passes): for surface k the local Jacobian of its
@@ -30,8 +27,9 @@
 #include <vector>
 
 #include "engine.cuh"
+#include "adjoint_rev.cuh"
+#include "jit.h"
 #include "ray_ad.cuh"
-#include "ray_rev.cuh"
 #include "trace_common.cuh"
 
 namespace rtb {
@@ -42,32 +40,8 @@ namespace {
 // surface's values (with their IEEE divisions) once for kAdjW tangents; on
 // C4 (1e7 rays, 24 parameters) 2, 3, 4, 6, 8 ran 53, 42, 42, 50, 59 ms
 constexpr int kAdjW = 4;
-constexpr int kAdjThreads = 128;
 constexpr int kMeritThreads = 256;
 constexpr int kMeritParts = 32;    // fixed split of each group's rays (deterministic sums)
-
-struct AdjArgs {
-    const DevScheme* sch;
-    const double* knots;
-    const DevBeam* beams;
-    int n_beams;
-    const ad::ParamRef* map;
-    int n_params;
-    const int* surf_params;  // [n_surfaces][RTB_ADJ_MAX_PARAMS]: parameter indices per surface
-    const int* surf_nparams; // [n_surfaces]
-    double* ckpt;            // [(k * 6 + c) * n + i]
-    double* lambda;          // copy of the wavelengths
-    char* flag;              // 1 = reached the end
-    double* X;
-    double* Y;
-    uint64_t n;
-};
-
-__device__ __forceinline__ long long order_of(const DevSurface& s, const DevBeam* beams, int b) {
-    long long order = s.order;
-    if (s.type == RTB_GRATING && beams[b].n_orders > 0) order = beams[b].orders[s.grating_index];
-    return order;
-}
 
 __global__ void __launch_bounds__(256) k_adj_forward(AdjArgs a, DevRays in, unsigned long long* counts,
                                                      unsigned* err) {
@@ -101,7 +75,7 @@ __global__ void __launch_bounds__(256) k_adj_forward(AdjArgs a, DevRays in, unsi
                 stage = 3 * k + 1;
                 break;
             }
-            int act = f64::action(s, a.knots, order_of(s, a.beams, b), lam, r);
+            int act = f64::action(s, a.knots, adj_order(s, a.beams, b), lam, r);
             if (act == f64::ACT_RANGE) { atomicOr(err, DEV_ERR_OUT_OF_RANGE); stage = -2; break; }
             if (act == f64::ACT_LOST) { stage = 3 * k + 2; break; }
             f64::normalize(r.cX, r.cY, r.cZ);
@@ -178,8 +152,6 @@ __global__ void k_build_surfd_dense(AdjArgs a, const double* dtheta, ad::SurfD<1
     ad::make_surfd(a.sch->s[k], k, a.map, a.n_params, sd, table[k]);
 }
 
-constexpr int kAdjWarps = kAdjThreads / 32;
-
 // Rays are taken 32 at a time per warp, every lane of a warp the same number
 // of steps, so the warp can sum each parameter's contributions with shuffles.
 // first_entry[k]: the table entry of surface k's first pass.  Four blocks per
@@ -219,7 +191,7 @@ __global__ void __launch_bounds__(kAdjThreads, 4) k_adj_backward(AdjArgs a, cons
                 ad::RayD<kAdjW> r;
                 if (act) {
                     ad::load_state(st, sd, r, t1, t2);
-                    ad::surface_step(s, table[e], sch->fixes, a.knots, order_of(s, a.beams, b), lam, r);
+                    ad::surface_step(s, table[e], sch->fixes, a.knots, adj_order(s, a.beams, b), lam, r);
                 }
                 // the last surface's output is the CCD-plane point: only X, Y
                 // carry adjoints.  Components are picked with selects (run-time
@@ -262,55 +234,10 @@ __global__ void __launch_bounds__(kAdjThreads, 4) k_adj_backward(AdjArgs a, cons
     }
 }
 
-// The reverse sweep (ray_rev.cuh).  Rays are taken 32 at a time per warp,
-// every lane of a warp the same number of steps, so the warp can sum each
-// parameter's contributions with shuffles.  The first surface's input
-// adjoint is not needed: a first surface without parameters is not swept.
+// The reverse sweep of any scheme (adjoint_rev.cuh).
 __global__ void __launch_bounds__(kAdjThreads, 4) k_adj_reverse(AdjArgs a, const double* gX, const double* gY,
                                                              double* partial) {
-    __shared__ double acc[kAdjWarps][RTB_ADJ_MAX_PARAMS];
-    const DevScheme* sch = a.sch;
-    const int ns = sch->n_surfaces;
-    const int P = a.n_params;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int p = lane; p < P; p += 32) acc[warp][p] = 0.0;
-    __syncwarp();
-    for (size_t i0 = (size_t)blockIdx.x * blockDim.x + (size_t)warp * 32; i0 < a.n; i0 += gstride()) {
-        const size_t i = i0 + lane;
-        bool act = i < a.n && a.flag[i] == 1;
-        rv::RayA adj{act ? gX[i] : 0.0, act ? gY[i] : 0.0, 0.0, 0.0, 0.0, 0.0};
-        act = act && !(adj.X == 0.0 && adj.Y == 0.0);
-        if (!__any_sync(0xffffffffu, act)) continue;
-        const double lam = act ? a.lambda[i] : 0.0;
-        const int b = act ? beam_of(a.beams, a.n_beams, i) : 0;
-        for (int k = ns - 1; k >= 0; --k) {
-            const int np = a.surf_nparams[k];
-            if (k == 0 && np == 0) break;
-            const DevSurface& s = sch->s[k];
-            rv::SurfA pa;
-            rv::clear(pa);
-            if (act) {
-                const double* c = a.ckpt + (size_t)k * 6 * a.n + i;
-                const f64::Ray r0{c[0], c[a.n], c[2 * a.n], c[3 * a.n], c[4 * a.n], c[5 * a.n]};
-                if (!rv::surface_rev(s, sch->fixes, a.knots, order_of(s, a.beams, b), lam, r0, adj, pa)) {
-                    act = false;  // not reached: the recomputation is the forward's
-                    rv::clear(pa);
-                }
-            }
-            for (int q = 0; q < np; ++q) {
-                const int j = a.surf_params[k * RTB_ADJ_MAX_PARAMS + q];
-                double v = act ? rv::param_adjoint(s, a.map[j], pa) : 0.0;
-                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-                if (lane == 0) acc[warp][j] += v;
-            }
-        }
-    }
-    __syncthreads();
-    for (int p = threadIdx.x; p < P; p += blockDim.x) {
-        double sum = 0.0;
-        for (int w = 0; w < kAdjWarps; ++w) sum += acc[w][p];
-        partial[(size_t)blockIdx.x * P + p] = sum;
-    }
+    adj_reverse<RtAdjSurfaces>(a, gX, gY, partial);
 }
 
 // RTB_ADJOINT_BACKWARD=passes: the backward by forward-mode passes.
@@ -352,7 +279,7 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_jvp(AdjArgs a, const ad::Su
         ad::load_state(st, sd, r);
         for (int k = 0; k < ns; ++k) {
             const DevSurface& s = sch->s[k];
-            ad::surface_step(s, table[k], sch->fixes, a.knots, order_of(s, a.beams, b), lam, r);
+            ad::surface_step(s, table[k], sch->fixes, a.knots, adj_order(s, a.beams, b), lam, r);
         }
         dX[i] = r.X.d[0];
         dY[i] = r.Y.d[0];
@@ -436,6 +363,7 @@ struct rtb_adjoint {
     uint32_t fixes = 0;
     PreparedScheme ps;
     bool have_forward = false;
+    const void* rev_kernel = nullptr;              // the reverse sweep compiled for the scheme, or NULL
     // device
     void* mem = nullptr;
     DevScheme* d_sch = nullptr;
@@ -670,6 +598,14 @@ int rtb_adjoint_create(const rtb_surface* surfaces, size_t n_surfaces, const rtb
         delete c;
         return cuda_status(e);
     }
+    // the reverse sweep compiled for the scheme's structure, which the
+    // parameters cannot change (check_param; rtb_adjoint_forward checks the
+    // intersection kinds); the generic kernel when NVRTC is unavailable
+    if (specialize_enabled()) {
+        std::string why;
+        const void* k = nullptr;
+        if (adjoint_kernel(c->ps.sch, &k, &why) == RTB_OK) c->rev_kernel = k;
+    }
     *out = c;
     return RTB_OK;
 }
@@ -735,7 +671,13 @@ int rtb_adjoint_backward(rtb_adjoint* c, const double* gX, const double* gY, dou
         DevBuf part;
         int st = part.alloc((size_t)grid * P * sizeof(double), s);
         if (st != RTB_OK) return st;
-        k_adj_reverse<<<grid, kAdjThreads, 0, s>>>(a, gX, gY, part.as<double>());
+        double* partial = part.as<double>();
+        if (c->rev_kernel) {
+            void* args[] = {&a, &gX, &gY, &partial};
+            RTB_CUDA_TRY(cudaLaunchKernel(c->rev_kernel, dim3(grid), dim3(kAdjThreads), args, 0, s));
+        } else {
+            k_adj_reverse<<<grid, kAdjThreads, 0, s>>>(a, gX, gY, partial);
+        }
         RTB_CUDA_TRY(cudaGetLastError());
         k_adj_sum_partials<<<1, RTB_ADJ_MAX_PARAMS, 0, s>>>(part.as<double>(), (int)grid, P, c->d_grad);
         RTB_CUDA_TRY(cudaGetLastError());

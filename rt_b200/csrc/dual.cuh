@@ -7,7 +7,9 @@
 // divisions as products with one refined reciprocal (tangent_rcp).
 #pragma once
 
+#ifndef __CUDACC_RTC__  // run-time compiled kernels take the device math built in
 #include <cmath>
+#endif
 
 namespace rtb {
 namespace ad {

@@ -366,9 +366,10 @@ int compile_scheme(const DevScheme& sch, int precision, std::string* why) {
     return cubin_for(scheme_source(sch, precision), precision != RTB_FP64, why, true) ? RTB_OK : RTB_FAILED;
 }
 
-int scheme_kernel(const DevScheme& sch, int precision, const void** kernel, std::string* why, bool compile) {
+// Load the kernel `name` of `src` (compiled when needed and `compile`).
+static int load_kernel(const std::string& src, bool fmad, const char* name, const void** kernel, std::string* why,
+                       bool compile) {
     *kernel = nullptr;
-    const std::string src = scheme_source(sch, precision);
     std::lock_guard<std::mutex> g(g_mu);
     auto it = g_kernels.find(src);
     if (it != g_kernels.end()) {
@@ -379,17 +380,17 @@ int scheme_kernel(const DevScheme& sch, int precision, const void** kernel, std:
     cudaKernel_t k = nullptr;
     cudaError_t e = cudaSuccess;
     for (int attempt = 0; attempt < 2; ++attempt) {
-        const std::vector<char>* cubin = cubin_for(src, precision != RTB_FP64, why, compile);
+        const std::vector<char>* cubin = cubin_for(src, fmad, why, compile);
         if (!cubin) return RTB_OK;
         lib = nullptr;
         e = cudaLibraryLoadData(&lib, cubin->data(), nullptr, nullptr, 0, nullptr, nullptr, 0);
-        if (e == cudaSuccess) e = cudaLibraryGetKernel(&k, lib, kernel_name(precision));
+        if (e == cudaSuccess) e = cudaLibraryGetKernel(&k, lib, name);
         if (e == cudaSuccess) break;
         if (lib) cudaLibraryUnload(lib);
         // a cubin that does not load (a damaged cache file): compile afresh once
         g_cubins.erase(src);
         const std::string dir = cache_dir();
-        if (!dir.empty()) std::remove(cache_path(dir, cache_key(src, precision != RTB_FP64)).c_str());
+        if (!dir.empty()) std::remove(cache_path(dir, cache_key(src, fmad)).c_str());
         if (!compile) break;
     }
     if (e != cudaSuccess) {
@@ -400,6 +401,45 @@ int scheme_kernel(const DevScheme& sch, int precision, const void** kernel, std:
     g_kernels.emplace(src, k);
     *kernel = reinterpret_cast<const void*>(k);
     return RTB_OK;
+}
+
+int scheme_kernel(const DevScheme& sch, int precision, const void** kernel, std::string* why, bool compile) {
+    return load_kernel(scheme_source(sch, precision), precision != RTB_FP64, kernel_name(precision), kernel, why,
+                       compile);
+}
+
+// AdjShape<...> of surface s (adjoint_rev.cuh).
+static std::string adj_shape(const DevSurface& s) {
+    char t[160];
+    std::snprintf(t, sizeof(t), "AdjShape<%d, %d, %d, %d, %d, %d, %d, %d>", (int)s.kind, (int)s.type, (int)s.cls,
+                  (int)s.shape, (int)s.gr_type, (int)s.n_poly, s.non_aux != 0 ? 1 : 0, s.c == 0.0 ? 1 : 0);
+    return t;
+}
+
+static const char* const kAdjReverseName = "rtb_adj_reverse_scheme";
+
+std::string adjoint_source(const DevScheme& sch) {
+    std::string src =
+        "#include \"adjoint_rev.cuh\"\n"
+        "namespace rtb {\n"
+        "struct SchemeAdjSurfaces {\n"
+        "    __device__ __forceinline__ static void sweep(const AdjArgs& a, RevRay& ray, int lane, double* acc_row) {\n";
+    for (int k = sch.n_surfaces - 1; k >= 0; --k)
+        src += "        rev_surface<" + adj_shape(sch.s[k]) + ">(a, " + std::to_string(k) + ", ray, lane, acc_row);\n";
+    src += std::string("    }\n};\n}  // namespace rtb\n"
+                       "extern \"C\" __global__ void __launch_bounds__(rtb::kAdjThreads, 4) ") + kAdjReverseName +
+           "(rtb::AdjArgs a,\n        const double* gX, const double* gY, double* partial) {\n"
+           "    rtb::adj_reverse<rtb::SchemeAdjSurfaces>(a, gX, gY, partial);\n}\n";
+    return src;
+}
+
+int adjoint_kernel(const DevScheme& sch, const void** kernel, std::string* why) {
+    return load_kernel(adjoint_source(sch), false, kAdjReverseName, kernel, why, true);
+}
+
+int compile_adjoint(const DevScheme& sch, std::string* why) {
+    std::lock_guard<std::mutex> g(g_mu);
+    return cubin_for(adjoint_source(sch), false, why, true) ? RTB_OK : RTB_FAILED;
 }
 
 }  // namespace rtb
@@ -415,6 +455,18 @@ int rtb_specialize(const rtb_surface* surfaces, size_t n_surfaces, uint32_t fixe
     if (st != RTB_OK) return st;
     std::string why;
     st = compile_scheme(ps.sch, precision, &why);
+    if (note && note_len > 0) std::snprintf(note, note_len, "%s", why.c_str());
+    return st;
+}
+
+int rtb_adjoint_specialize(const rtb_surface* surfaces, size_t n_surfaces, uint32_t fixes, char* note,
+                           size_t note_len) {
+    if (note && note_len > 0) note[0] = 0;
+    PreparedScheme ps;
+    int st = prepare_scheme(surfaces, n_surfaces, fixes, 0, ps);
+    if (st != RTB_OK) return st;
+    std::string why;
+    st = compile_adjoint(ps.sch, &why);
     if (note && note_len > 0) std::snprintf(note, note_len, "%s", why.c_str());
     return st;
 }

@@ -28,6 +28,7 @@
 
 #include "ray_ad.cuh"
 #include "ray_fp64.cuh"
+#include "shape.cuh"
 
 namespace rtb {
 namespace rv {
@@ -114,9 +115,10 @@ __device__ __forceinline__ void normalize_rev(double cX, double cY, double cZ, R
 // conic_derivs: dFdX = -E X, dFdY = -E Y with
 // E = c / w + 2 sum_{i=1..n} i a_i r2^(i-1), w = sqrt(1 - k1 c^2 r2).
 // In: the adjoints gX, gY of dFdX, dFdY.
+template <class Sh = RtShape>
 __device__ __forceinline__ void conic_derivs_rev(const DevSurface& s, double X, double Y, double gX, double gY,
                                                  RayA& a, SurfA& p) {
-    const int n = s.n_poly;
+    const int n = Sh::n_poly(s);
     const double r2 = X * X + Y * Y;
     const double iw = 1.0 / sqrt(1.0 - s.k1 * s.c * s.c * r2);
     const double iw3 = iw * iw * iw;
@@ -142,9 +144,10 @@ __device__ __forceinline__ void conic_derivs_rev(const DevSurface& s, double X, 
 // toric_derivs: dFdX = -cR X, dFdY = (cR Fy - 1) dFy, dFdZ = 1 - cR Z with
 // Fy = c Y2 / (1 + w) + sum_i a_i Y2^(i+1), dFy = c Y / w + 2 sum_{i=1..n} i a_i Y2^(i-1),
 // w = sqrt(1 - k1 c^2 Y2).  In: the adjoints gX, gY, gZ of dFdX, dFdY, dFdZ.
+template <class Sh = RtShape>
 __device__ __forceinline__ void toric_derivs_rev(const DevSurface& s, double X, double Y, double Z, double gX,
                                                  double gY, double gZ, RayA& a, SurfA& p) {
-    const int n = s.n_poly;
+    const int n = Sh::n_poly(s);
     const double c = s.c, k1 = s.k1, Y2 = Y * Y;
     const double w = sqrt(1.0 - k1 * c * c * Y2);
     const double iw = 1.0 / w, iw3 = iw * iw * iw, den = 1.0 + w, iden2 = 1.0 / (den * den);
@@ -184,20 +187,22 @@ __device__ __forceinline__ void toric_derivs_rev(const DevSurface& s, double X, 
 }
 
 // The slopes of a conic (dFdZ = 1) or toric surface at (X, Y, Z).
+template <class Sh = RtShape>
 __device__ __forceinline__ void slopes(const DevSurface& s, bool tor, double X, double Y, double Z, double& dX,
                                        double& dY, double& dZ) {
     if (tor) {
-        f64::toric_derivs(s, X, Y, Z, dX, dY, dZ);
+        f64::toric_derivs<Sh>(s, X, Y, Z, dX, dY, dZ);
     } else {
-        f64::conic_derivs(s, X, Y, dX, dY);
+        f64::conic_derivs<Sh>(s, X, Y, dX, dY);
         dZ = 1.0;
     }
 }
 
+template <class Sh = RtShape>
 __device__ __forceinline__ void slopes_rev(const DevSurface& s, bool tor, double X, double Y, double Z, double gX,
                                            double gY, double gZ, RayA& a, SurfA& p) {
-    if (tor) toric_derivs_rev(s, X, Y, Z, gX, gY, gZ, a, p);
-    else conic_derivs_rev(s, X, Y, gX, gY, a, p);
+    if (tor) toric_derivs_rev<Sh>(s, X, Y, Z, gX, gY, gZ, a, p);
+    else conic_derivs_rev<Sh>(s, X, Y, gX, gY, a, p);
 }
 
 // ---- intersections -----------------------------------------------------------
@@ -229,6 +234,7 @@ __device__ __forceinline__ void quadric_BC_rev(const DevSurface& s, const f64::R
 
 // Asphere surface function F = Z - sag(r2) - sum_i a_i r2^(i+1) at P = r + t c
 // (t held), sag = c r2 / (1 + w), w = sqrt(1 - k1 c^2 r2); gF its adjoint.
+template <class Sh = RtShape>
 __device__ __forceinline__ void asphere_F_rev(const DevSurface& s, bool poly_only, const f64::Ray& r, double t,
                                               double gF, RayA& a, SurfA& p) {
     const double PX = r.X + t * r.cX, PY = r.Y + t * r.cY;
@@ -244,7 +250,7 @@ __device__ __forceinline__ void asphere_F_rev(const DevSurface& s, bool poly_onl
     double rq = 1.0;  // r2^i
 #pragma unroll
     for (int i = 0; i < RTB_MAX_POLY; ++i) {
-        if (i >= s.n_poly) break;
+        if (i >= Sh::n_poly(s)) break;
         dsag += (i + 1) * s.poly[i] * rq;
         p.poly[i] += -gF * rq * r2;
         rq *= r2;
@@ -284,13 +290,14 @@ __device__ __forceinline__ void toric_F_rev(const DevSurface& s, bool fix_sign, 
 }
 
 // dF/dt along the ray at the reported point (the value ray_ad.cuh divides by).
+template <class Sh = RtShape>
 __device__ __forceinline__ double asphere_Ft(const DevSurface& s, bool poly_only, const f64::Ray& r, double t) {
     const double X = r.X + t * r.cX, Y = r.Y + t * r.cY;
     const double r2 = X * X + Y * Y;
     double E = 0.0;
     if (!poly_only) E = s.c / sqrt(1.0 - s.k1 * s.c * s.c * r2);
     double sum = 0.0, rr = 1.0;
-    for (int i = 1; i <= s.n_poly; ++i, rr *= r2) sum += (double)i * s.poly[i - 1] * rr;
+    for (int i = 1; i <= Sh::n_poly(s); ++i, rr *= r2) sum += (double)i * s.poly[i - 1] * rr;
     E += 2.0 * sum;
     return r.cZ - E * (X * r.cX + Y * r.cY);
 }
@@ -306,14 +313,15 @@ __device__ __forceinline__ double toric_Ft(const DevSurface& s, bool fix_sign, c
 
 // The intersection on the values, as f64::intersect computes it; t: the ray
 // parameter of the reported point for the iterative kinds.
+template <class Sh = RtShape>
 __device__ __forceinline__ bool isect_fwd(const DevSurface& s, uint32_t fixes, f64::Ray& r, double& t) {
     t = 0.0;
-    switch (s.kind) {
+    switch (Sh::kind(s)) {
         case IS_ITER_POLY:
         case IS_ITER_CONIC: {
             const double s0 = -r.Z / r.cZ;
             double s1;
-            if (!ad::asphere_values(s, r, s.kind == IS_ITER_POLY, (fixes & RTB_FIX_ASPHERE_ROOT) != 0, s1))
+            if (!ad::asphere_values(s, r, Sh::kind(s) == IS_ITER_POLY, (fixes & RTB_FIX_ASPHERE_ROOT) != 0, s1))
                 return false;
             t = s1 + s0;
             r.X = r.X + t * r.cX;  // iterative_*_intersection's Xi, Yi, Zi
@@ -328,14 +336,15 @@ __device__ __forceinline__ bool isect_fwd(const DevSurface& s, uint32_t fixes, f
             r.Z += t * r.cZ;
             return true;
         }
-        default: return f64::intersect(s, fixes, r);
+        default: return f64::intersect<Sh>(s, fixes, r);
     }
 }
 
 // r: the state before the intersection; in: the adjoint after it.
+template <class Sh = RtShape>
 __device__ __forceinline__ void isect_rev(const DevSurface& s, uint32_t fixes, const f64::Ray& r, double t, RayA& a,
                                           SurfA& p) {
-    switch (s.kind) {
+    switch (Sh::kind(s)) {
         case IS_PLANE: {
             const double s0 = -r.Z / r.cZ;
             const double g0 = a.X * r.cX + a.Y * r.cY;  // Z' = 0 carries nothing
@@ -378,9 +387,9 @@ __device__ __forceinline__ void isect_rev(const DevSurface& s, uint32_t fixes, c
         }
         case IS_ITER_POLY:
         case IS_ITER_CONIC: {
-            const bool po = s.kind == IS_ITER_POLY;
+            const bool po = Sh::kind(s) == IS_ITER_POLY;
             const double gt = along_rev(r, t, a);
-            asphere_F_rev(s, po, r, t, -gt / asphere_Ft(s, po, r, t), a, p);
+            asphere_F_rev<Sh>(s, po, r, t, -gt / asphere_Ft<Sh>(s, po, r, t), a, p);
             return;
         }
         case IS_TORIC: {
@@ -397,20 +406,21 @@ __device__ __forceinline__ void isect_rev(const DevSurface& s, uint32_t fixes, c
 
 // The refractive-index ratio and grating term of the action, as f64::action
 // computes them.  False where a table is out of range.
+template <class Sh = RtShape>
 __device__ __forceinline__ bool action_consts(const DevSurface& s, const double* knots, long long order,
                                               double lambda, double& mu, double& L) {
     mu = 0.0;
     L = 0.0;
-    if (s.type == RTB_LENS) {
+    if (Sh::type(s) == RTB_LENS) {
         double a, b;
         if (!f64::table_eval(knots + s.n1_off, s.n1_n, lambda, a) || !f64::table_eval(knots + s.n2_off, s.n2_n, lambda, b))
             return false;
         mu = a;
         mu /= b;
-    } else if (s.type == RTB_GRATING) {
+    } else if (Sh::type(s) == RTB_GRATING) {
         double n2v;
         if (!f64::table_eval(knots + s.n2_off, s.n2_n, lambda, n2v)) return false;
-        if (s.gr_type == RTB_TRANSPARENT) {
+        if (Sh::gr_type(s) == RTB_TRANSPARENT) {
             double n1v;
             if (!f64::table_eval(knots + s.n1_off, s.n1_n, lambda, n1v)) return false;
             mu = n1v;
@@ -421,21 +431,23 @@ __device__ __forceinline__ bool action_consts(const DevSurface& s, const double*
     return true;
 }
 
+template <class Sh = RtShape>
 __device__ __forceinline__ bool action_fwd(const DevSurface& s, double mu, double L, f64::Ray& r) {
-    if (s.type == RTB_MIRROR) {
-        f64::reflect(s, r);
+    if (Sh::type(s) == RTB_MIRROR) {
+        f64::reflect<Sh>(s, r);
         return true;
     }
-    if (s.type == RTB_LENS) return f64::refract(s, mu, r);
-    if (s.type == RTB_GRATING) return f64::diffract(s, mu, L, r);
+    if (Sh::type(s) == RTB_LENS) return f64::refract<Sh>(s, mu, r);
+    if (Sh::type(s) == RTB_GRATING) return f64::diffract<Sh>(s, mu, L, r);
     return true;
 }
 
 // Reflection about the curved surface's normal: c' = c - a2 dF,
 // a2 = 2 (c . dF) / |dF|^2.
+template <class Sh = RtShape>
 __device__ __forceinline__ void reflect_rev(const DevSurface& s, bool tor, const f64::Ray& r, RayA& a, SurfA& p) {
     double dX, dY, dZ;
-    slopes(s, tor, r.X, r.Y, r.Z, dX, dY, dZ);
+    slopes<Sh>(s, tor, r.X, r.Y, r.Z, dX, dY, dZ);
     const double num = r.cX * dX + r.cY * dY + r.cZ * dZ;
     const double den = dX * dX + dY * dY + dZ * dZ;
     const double a2 = 2.0 * num / den;
@@ -448,15 +460,16 @@ __device__ __forceinline__ void reflect_rev(const DevSurface& s, bool tor, const
     gX += gn * r.cX + 2.0 * gden * dX;
     gY += gn * r.cY + 2.0 * gden * dY;
     gZ += gn * r.cZ + 2.0 * gden * dZ;
-    slopes_rev(s, tor, r.X, r.Y, r.Z, gX, gY, gZ, a, p);
+    slopes_rev<Sh>(s, tor, r.X, r.Y, r.Z, gX, gY, gZ, a, p);
 }
 
 // Refraction at a curved surface: G0 = |dF|^2, a = mu (c . dF) / G0,
 // b = (mu^2 - 1) / G0, G = -a + sqrt(a^2 - b), c' = mu c + G dF.
+template <class Sh = RtShape>
 __device__ __forceinline__ void refract_rev(const DevSurface& s, bool tor, double mu, const f64::Ray& r, RayA& a,
                                             SurfA& p) {
     double dX, dY, dZ;
-    slopes(s, tor, r.X, r.Y, r.Z, dX, dY, dZ);
+    slopes<Sh>(s, tor, r.X, r.Y, r.Z, dX, dY, dZ);
     const double G0 = dX * dX + dY * dY + dZ * dZ;
     const double num = r.cX * dX + r.cY * dY + r.cZ * dZ;
     const double av = mu * num / G0, bv = (mu * mu - 1.0) / G0;
@@ -476,7 +489,7 @@ __device__ __forceinline__ void refract_rev(const DevSurface& s, bool tor, doubl
     gX += gn * r.cX + 2.0 * gG0 * dX;
     gY += gn * r.cY + 2.0 * gG0 * dY;
     gZ += gn * r.cZ + 2.0 * gG0 * dZ;
-    slopes_rev(s, tor, r.X, r.Y, r.Z, gX, gY, gZ, a, p);
+    slopes_rev<Sh>(s, tor, r.X, r.Y, r.Z, gX, gY, gZ, a, p);
 }
 
 // Diffraction at a curved grating (transparent: m = mu, K = mu^2 - 1, sign +;
@@ -486,10 +499,11 @@ __device__ __forceinline__ void refract_rev(const DevSurface& s, bool tor, doubl
 // a = m (c . dF) / G0, b = (K + L^2 - 2 L m (c . uvw)) / G0,
 // G = -a + sign sqrt(a^2 - b), c' = m c - L uvw + G dF.  Returns the
 // adjoint of L.
+template <class Sh = RtShape>
 __device__ __forceinline__ double diffract_curved_rev(const DevSurface& s, bool tor, bool trans, double mu, double L,
                                                       const f64::Ray& r, RayA& a, SurfA& p) {
     double dX, dY, dZ;
-    slopes(s, tor, r.X, r.Y, r.Z, dX, dY, dZ);
+    slopes<Sh>(s, tor, r.X, r.Y, r.Z, dX, dY, dZ);
     const double m = trans ? mu : 1.0, K = trans ? mu * mu - 1.0 : 0.0, sg = trans ? 1.0 : -1.0;
     const double den1 = tor ? dY * dY + dZ + dZ : dY * dY + 1.0;
     const double g1 = dX / den1;
@@ -549,36 +563,37 @@ __device__ __forceinline__ double diffract_curved_rev(const DevSurface& s, bool 
     const double gden1 = -gg1 * g1 / den1;
     gY += 2.0 * gden1 * dY;
     if (tor) gZ += 2.0 * gden1;
-    slopes_rev(s, tor, r.X, r.Y, r.Z, gX, gY, gZ, a, p);
+    slopes_rev<Sh>(s, tor, r.X, r.Y, r.Z, gX, gY, gZ, a, p);
     return gL;
 }
 
 // r: the state before the action; in: the adjoint after it.
+template <class Sh = RtShape>
 __device__ __forceinline__ void action_rev(const DevSurface& s, double mu, double L, const f64::Ray& r, RayA& a,
                                            SurfA& p) {
-    const bool tor = s.cls == RTB_TORIC;
-    if (s.type == RTB_MIRROR) {
-        if (s.cls == RTB_PLANE) a.cZ = -a.cZ;
-        else if (s.cls == RTB_CONIC || tor) reflect_rev(s, tor, r, a, p);
+    const bool tor = Sh::cls(s) == RTB_TORIC;
+    if (Sh::type(s) == RTB_MIRROR) {
+        if (Sh::cls(s) == RTB_PLANE) a.cZ = -a.cZ;
+        else if (Sh::cls(s) == RTB_CONIC || tor) reflect_rev<Sh>(s, tor, r, a, p);
         return;
     }
-    if (s.type == RTB_LENS) {
-        if (s.cls == RTB_PLANE) {  // a = mu cZ, G = -a + sqrt(a^2 - (mu^2 - 1)), c' = (mu cX, mu cY, mu cZ + G)
+    if (Sh::type(s) == RTB_LENS) {
+        if (Sh::cls(s) == RTB_PLANE) {  // a = mu cZ, G = -a + sqrt(a^2 - (mu^2 - 1)), c' = (mu cX, mu cY, mu cZ + G)
             const double av = mu * r.cZ;
             const double sq = sqrt(av * av - (mu * mu - 1.0));
             const double gG = a.cZ;
             a.cX *= mu;
             a.cY *= mu;
             a.cZ = mu * a.cZ + mu * (-gG + gG * av / sq);
-        } else if (s.cls == RTB_CONIC || tor) {
-            refract_rev(s, tor, mu, r, a, p);
+        } else if (Sh::cls(s) == RTB_CONIC || tor) {
+            refract_rev<Sh>(s, tor, mu, r, a, p);
         }
         return;
     }
-    if (s.type != RTB_GRATING) return;
-    const bool trans = s.gr_type == RTB_TRANSPARENT;
+    if (Sh::type(s) != RTB_GRATING) return;
+    const bool trans = Sh::gr_type(s) == RTB_TRANSPARENT;
     double gL = 0.0;
-    if (s.cls == RTB_PLANE) {
+    if (Sh::cls(s) == RTB_PLANE) {
         // transparent: a = mu cZ, b = mu^2 - 1 + L^2 - 2 mu L cX, G = -a + sqrt(a^2 - b),
         //   c' = (mu cX - L, mu cY, mu cZ + G);
         // reflective: a = cZ, b = L^2 - 2 L cX, G = -a - sqrt(a^2 - b), c' = (cX - L, cY, cZ + G)
@@ -594,8 +609,8 @@ __device__ __forceinline__ void action_rev(const DevSurface& s, double mu, doubl
         gL += gb * (2.0 * L - 2.0 * m * r.cX);
         a.cX += gb * (-2.0 * m * L);
         a.cZ += ga * m;
-    } else if (s.cls == RTB_CONIC || tor) {
-        gL = diffract_curved_rev(s, tor, trans, mu, L, r, a, p);
+    } else if (Sh::cls(s) == RTB_CONIC || tor) {
+        gL = diffract_curved_rev<Sh>(s, tor, trans, mu, L, r, a, p);
     }
     p.gr += gL * (-L / s.gr_const);  // L = (order lambda / n2) / gr
 }
@@ -606,24 +621,25 @@ __device__ __forceinline__ void action_rev(const DevSurface& s, double mu, doubl
 // surface's output state; out, the adjoint of its input state, with the
 // constants' adjoints added to p.  False if the recomputation loses the ray
 // (it does not for a ray the forward traced through).
+template <class Sh = RtShape>
 __device__ __forceinline__ bool surface_rev(const DevSurface& s, uint32_t fixes, const double* knots,
                                             long long order, double lambda, const f64::Ray& r0, RayA& a,
                                             SurfA& p) {
     f64::Ray r1 = r0;
-    f64::transform(s, r1);
+    f64::transform<Sh>(s, r1);
     f64::Ray r2 = r1;
     f64::normalize(r2.cX, r2.cY, r2.cZ);
-    if (s.non_aux) {
+    if (Sh::non_aux(s)) {
         f64::Ray r3 = r2;
         double t;
-        if (!isect_fwd(s, fixes, r3, t)) return false;
+        if (!isect_fwd<Sh>(s, fixes, r3, t)) return false;
         double mu, L;
-        if (!action_consts(s, knots, order, lambda, mu, L)) return false;
+        if (!action_consts<Sh>(s, knots, order, lambda, mu, L)) return false;
         f64::Ray r4 = r3;
-        if (!action_fwd(s, mu, L, r4)) return false;
+        if (!action_fwd<Sh>(s, mu, L, r4)) return false;
         normalize_rev(r4.cX, r4.cY, r4.cZ, a);
-        action_rev(s, mu, L, r3, a, p);
-        isect_rev(s, fixes, r2, t, a, p);
+        action_rev<Sh>(s, mu, L, r3, a, p);
+        isect_rev<Sh>(s, fixes, r2, t, a, p);
     }
     normalize_rev(r1.cX, r1.cY, r1.cZ, a);
     transform_rev(s, r0, a, p);

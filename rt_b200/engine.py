@@ -47,6 +47,7 @@ def lib() -> C.CDLL:
         L.rtb_plan_destroy.argtypes = [vp]
         L.rtb_plan_specialized.argtypes = [vp, P(C.c_int32), C.c_char_p, C.c_size_t]
         L.rtb_specialize.argtypes = [P(ffi.Surface), C.c_size_t, C.c_uint32, C.c_int32, C.c_char_p, C.c_size_t]
+        L.rtb_adjoint_specialize.argtypes = [P(ffi.Surface), C.c_size_t, C.c_uint32, C.c_char_p, C.c_size_t]
         L.rtb_adjoint_create.argtypes = [P(ffi.Surface), C.c_size_t, P(ffi.Param), C.c_size_t, P(ffi.Beam),
                                          C.c_size_t, C.c_uint64, C.c_uint32, P(vp)]
         L.rtb_adjoint_theta.argtypes = [vp, vp]
@@ -222,6 +223,15 @@ def specialize(surfaces, fixes=0, precision=ffi.MIXED):
     arr = (ffi.Surface * len(surfaces))(*surfaces)
     note = C.create_string_buffer(4096)
     st = lib().rtb_specialize(arr, len(surfaces), fixes, precision, note, len(note))
+    return st, note.value.decode()
+
+
+def adjoint_specialize(surfaces, fixes=0):
+    """Compile the adjoint's reverse sweep for this scheme's structure
+    (rtb_adjoint_specialize; no device needed): (status, note)."""
+    arr = (ffi.Surface * len(surfaces))(*surfaces)
+    note = C.create_string_buffer(4096)
+    st = lib().rtb_adjoint_specialize(arr, len(surfaces), fixes, note, len(note))
     return st, note.value.decode()
 
 

@@ -105,3 +105,46 @@ def test_reverse_equals_passes_and_jvp_on_every_kind(name, fixes, monkeypatch):
         assert err <= tol, (params[j], g_rev[j], g_pas[j], dot, scale)
     print(name, fixes, P, "parameters, worst error / sum |contributions|:", worst)
     adj.destroy()
+
+
+@pytest.mark.parametrize("name", ["c4", "mirrors", "lenses", "gratings"])
+def test_reverse_sweep_compiled_for_the_scheme_equals_generic(name, monkeypatch):
+    """rtb_adjoint_create compiles the reverse sweep for the scheme's
+    structure (RTB_SPECIALIZE=0: the generic kernel); both run the same
+    IEEE operations in the same order: the same gradient bits, also with
+    the parameters moved off their create-time values (angles and distances
+    away from zero change which transforms apply, which the compiled kernel
+    reads at run time)."""
+    if name == "c4":
+        specs, params, fixes = S.littrow_free_asphere(), S.c4_params(), ffi.FIX_ASPHERE_ROOT
+    else:
+        specs = S.coverage_schemes()[name]
+        params, fixes = all_params(specs), ffi.FIX_TORIC_SIGN | ffi.FIX_TORIC_STEP
+    beams = [S.make_beam(0, 400, 5, 10.0, (0.4, 0.8), 23)]
+    n = S.total_rays(beams)
+    cs = S.to_c(specs, E.spline_init)
+    rays = E.generate(beams, n)
+    grads = []
+    for spec in ("1", "0"):
+        monkeypatch.setenv("RTB_SPECIALIZE", spec)
+        adj = E.Adjoint(cs.surfaces, params, beams, n, fixes=fixes)
+        theta = adj.theta()
+        out = []
+        for move in (0.0, 1e-3):
+            th = theta + move * np.where(np.arange(len(theta)) % 2 == 0, 1.0, -1.0) * np.maximum(np.abs(theta), 1.0)
+            if move:
+                # groove densities stay positive; everything else moves by 1e-3 (relative, or absolute at 0)
+                th = np.where(theta > 0, np.maximum(th, 0.5 * theta), th)
+            st, _ = adj.forward(th, rays)
+            assert st == ffi.OK
+            gen = torch.Generator(device="cuda").manual_seed(3)
+            gX = torch.randn(n, dtype=torch.float64, device="cuda", generator=gen)
+            gY = torch.randn(n, dtype=torch.float64, device="cuda", generator=gen)
+            finite = torch.isfinite(adj.X) & torch.isfinite(adj.Y)
+            gX, gY = torch.where(finite, gX, 0.0), torch.where(finite, gY, 0.0)
+            monkeypatch.delenv("RTB_ADJOINT_BACKWARD", raising=False)
+            out.append(adj.backward(gX, gY))
+        grads.append(out)
+        adj.destroy()
+    for a, b in zip(*grads):
+        assert np.array_equal(a, b), np.max(np.abs(a - b))

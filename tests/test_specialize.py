@@ -42,6 +42,17 @@ def test_specialised_kernel_compiles(name, precision):
     assert note == ""
 
 
+@pytest.mark.skipif(not _nvrtc_present(), reason="libnvrtc not present")
+@pytest.mark.parametrize("name", sorted(SCHEMES))
+def test_adjoint_reverse_sweep_compiles(name):
+    """The adjoint's reverse sweep compiled for each scheme's structure
+    (rtb_adjoint_specialize, adjoint_rev.cuh with one AdjShape per surface)."""
+    cs = S.to_c(SCHEMES[name](), O.spline_init)
+    st, note = E.adjoint_specialize(list(cs.surfaces), ffi.FIX_TORIC_SIGN | ffi.FIX_TORIC_STEP)
+    assert st == ffi.OK, note
+    assert note == ""
+
+
 def test_specialize_rejects_bad_requests():
     st, _ = E.specialize([], 0)
     assert st == ffi.BAD_VALUE
