@@ -2,9 +2,9 @@
 // parameters: forward with checkpoints, reverse sweep over surfaces,
 // forward-mode sensitivities, and the spot merit's per-ray seeds.
 //
-// Forward (k_adj_forward): the fused FP64 engine's per-ray loop (the same
-// bits), storing each ray's state (X Y Z cX cY cZ) at the input of every
-// surface -- 48 bytes x surfaces per ray.
+// Forward (adjoint_rev.cuh): the fused FP64 engine's per-ray loop (the same
+// bits), storing each ray's state at the input of every surface; compiled
+// for the scheme's structure like the backward.
 //
 // Backward (adjoint_rev.cuh): per ray, surfaces last to first, each surface
 // recomputed from its checkpoint and its adjoint carried back through its
@@ -43,50 +43,10 @@ constexpr int kAdjW = 4;
 constexpr int kMeritThreads = 256;
 constexpr int kMeritParts = 32;    // fixed split of each group's rays (deterministic sums)
 
+// The forward through any scheme (adjoint_rev.cuh).
 __global__ void __launch_bounds__(256) k_adj_forward(AdjArgs a, DevRays in, unsigned long long* counts,
                                                      unsigned* err) {
-    const DevScheme* sch = a.sch;
-    const int ns = sch->n_surfaces;
-    const int n_stages = 3 * ns;
-    for (size_t i = gtid(); i < a.n; i += gstride()) {
-        a.lambda[i] = in.lambda[i];
-        if (in.flag[i] != 1) {
-            a.flag[i] = 0;
-            continue;
-        }
-        f64::Ray r{in.X[i], in.Y[i], in.Z[i], in.cX[i], in.cY[i], in.cZ[i]};
-        const double lam = in.lambda[i];
-        const int b = beam_of(a.beams, a.n_beams, i);
-        int stage = -1;
-        for (int k = 0; k < ns; ++k) {
-            double* c = a.ckpt + (size_t)k * 6 * a.n + i;
-            c[0] = r.X;
-            c[a.n] = r.Y;
-            c[2 * a.n] = r.Z;
-            c[3 * a.n] = r.cX;
-            c[4 * a.n] = r.cY;
-            c[5 * a.n] = r.cZ;
-            const DevSurface& s = sch->s[k];
-            f64::transform(s, r);
-            f64::normalize(r.cX, r.cY, r.cZ);
-            if (!s.non_aux) continue;
-            if (!f64::intersect(s, sch->fixes, r)) { stage = 3 * k; break; }
-            if (!f64::aperture_pass(s.type == RTB_SHADE, s.shape, s.size, s.center, r.X, r.Y)) {
-                stage = 3 * k + 1;
-                break;
-            }
-            int act = f64::action(s, a.knots, adj_order(s, a.beams, b), lam, r);
-            if (act == f64::ACT_RANGE) { atomicOr(err, DEV_ERR_OUT_OF_RANGE); stage = -2; break; }
-            if (act == f64::ACT_LOST) { stage = 3 * k + 2; break; }
-            f64::normalize(r.cX, r.cY, r.cZ);
-        }
-        a.flag[i] = (stage == -1) ? 1 : 0;
-        a.X[i] = r.X;
-        a.Y[i] = r.Y;
-        // one atomic per distinct counter in the warp (the rays of a beam
-        // mostly share theirs)
-        count_event(stage != -2, b * (n_stages + 1) + (stage >= 0 ? stage : n_stages), counts);
-    }
+    adj_forward<RtAdjForward>(a, in, counts, err);
 }
 
 // The dual-number surface constants of pass (k, d0) of the backward sweep:
@@ -363,7 +323,8 @@ struct rtb_adjoint {
     uint32_t fixes = 0;
     PreparedScheme ps;
     bool have_forward = false;
-    const void* rev_kernel = nullptr;              // the reverse sweep compiled for the scheme, or NULL
+    const void* fwd_kernel = nullptr;              // the forward and the reverse sweep compiled
+    const void* rev_kernel = nullptr;              // for the scheme's structure, or NULL
     // device
     void* mem = nullptr;
     DevScheme* d_sch = nullptr;
@@ -603,8 +564,11 @@ int rtb_adjoint_create(const rtb_surface* surfaces, size_t n_surfaces, const rtb
     // intersection kinds); the generic kernel when NVRTC is unavailable
     if (specialize_enabled()) {
         std::string why;
-        const void* k = nullptr;
-        if (adjoint_kernel(c->ps.sch, &k, &why) == RTB_OK) c->rev_kernel = k;
+        const void *f = nullptr, *r = nullptr;
+        if (adjoint_kernels(c->ps.sch, &f, &r, &why) == RTB_OK) {
+            c->fwd_kernel = f;
+            c->rev_kernel = r;
+        }
     }
     *out = c;
     return RTB_OK;
@@ -644,7 +608,15 @@ int rtb_adjoint_forward(rtb_adjoint* c, const double* theta, const rtb_rays* ray
     RTB_CUDA_TRY(cudaMemsetAsync(c->d_counts, 0, nb * ns1 * 8, s));
     RTB_CUDA_TRY(cudaMemsetAsync(c->d_err, 0, 4, s));
     AdjArgs a = adj_args(c);
-    k_adj_forward<<<adj_grid(c->n, 256), 256, 0, s>>>(a, dev_rays(rays), c->d_counts, c->d_err);
+    DevRays in = dev_rays(rays);
+    if (c->fwd_kernel) {
+        unsigned long long* counts = c->d_counts;
+        unsigned* err = c->d_err;
+        void* args[] = {&a, &in, &counts, &err};
+        RTB_CUDA_TRY(cudaLaunchKernel(c->fwd_kernel, dim3(adj_grid(c->n, 256)), dim3(256), args, 0, s));
+    } else {
+        k_adj_forward<<<adj_grid(c->n, 256), 256, 0, s>>>(a, in, c->d_counts, c->d_err);
+    }
     RTB_CUDA_TRY(cudaGetLastError());
     if (X) RTB_CUDA_TRY(cudaMemcpyAsync(X, c->d_X, c->n * 8, cudaMemcpyDeviceToDevice, s));
     if (Y) RTB_CUDA_TRY(cudaMemcpyAsync(Y, c->d_Y, c->n * 8, cudaMemcpyDeviceToDevice, s));

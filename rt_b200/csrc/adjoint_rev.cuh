@@ -1,6 +1,11 @@
-// adjoint_rev.cuh -- the adjoint's reverse sweep, as the body of the generic
-// kernel (k_adj_reverse, adjoint.cu) and of kernels compiled for one
-// scheme's structure (jit.cpp, rtb_adj_reverse_scheme).
+// adjoint_rev.cuh -- the adjoint's forward with checkpoints and its reverse
+// sweep, as the bodies of the generic kernels (k_adj_forward, k_adj_reverse,
+// adjoint.cu) and of kernels compiled for one scheme's structure (jit.cpp,
+// rtb_adj_forward_scheme, rtb_adj_reverse_scheme).
+//
+// Forward: the fused FP64 engine's per-ray loop (the same bits), storing each
+// ray's state (X Y Z cX cY cZ) at the input of every surface -- 48 bytes x
+// surfaces per ray.
 //
 // Per ray, surfaces last to first: surface k is recomputed from checkpoint k
 // and the adjoint of its output state is carried back through its stages in
@@ -65,6 +70,71 @@ struct AdjShape {
     __device__ __forceinline__ static bool rot32(const DevSurface& s) { return s.rot32 != 0; }
     __device__ __forceinline__ static bool first32(const DevSurface& s) { return s.first32 != 0; }
 };
+
+// Surface k (structure Sh) of the forward on one ray: its input state
+// stored as checkpoint k, then the plain FP64 engine's surface.  -1 while
+// the ray survives, the stage that lost it, or -2 (a wavelength outside a
+// table).
+template <class Sh>
+__device__ __forceinline__ int fwd_surface(const AdjArgs& a, int k, size_t i, int b, double lam, unsigned* err,
+                                           f64::Ray& r) {
+    double* c = a.ckpt + (size_t)k * 6 * a.n + i;
+    c[0] = r.X;
+    c[a.n] = r.Y;
+    c[2 * a.n] = r.Z;
+    c[3 * a.n] = r.cX;
+    c[4 * a.n] = r.cY;
+    c[5 * a.n] = r.cZ;
+    const DevScheme* sch = a.sch;
+    const DevSurface& s = sch->s[k];
+    f64::transform<Sh>(s, r);
+    f64::normalize(r.cX, r.cY, r.cZ);
+    if (!Sh::non_aux(s)) return -1;
+    if (!f64::intersect<Sh>(s, sch->fixes, r)) return 3 * k;
+    if (!f64::aperture_pass(Sh::type(s) == RTB_SHADE, Sh::shape(s), s.size, s.center, r.X, r.Y)) return 3 * k + 1;
+    const int act = f64::action<Sh>(s, a.knots, adj_order(s, a.beams, b), lam, r);
+    if (act == f64::ACT_RANGE) {
+        atomicOr(err, DEV_ERR_OUT_OF_RANGE);
+        return -2;
+    }
+    if (act == f64::ACT_LOST) return 3 * k + 2;
+    f64::normalize(r.cX, r.cY, r.cZ);
+    return -1;
+}
+
+// The forward through any scheme, its structure read at run time.
+struct RtAdjForward {
+    __device__ __forceinline__ static int run(const AdjArgs& a, size_t i, int b, double lam, unsigned* err,
+                                              f64::Ray& r) {
+        int stage = -1;
+        for (int k = 0; k < a.sch->n_surfaces && stage == -1; ++k) stage = fwd_surface<RtShape>(a, k, i, b, lam, err, r);
+        return stage;
+    }
+};
+
+// in: the rays; counts: [n_beams][3 n_surfaces + 1] loss and arrival counters.
+template <class Surfaces>
+__device__ __forceinline__ void adj_forward(const AdjArgs& a, const DevRays& in, unsigned long long* counts,
+                                            unsigned* err) {
+    const int n_stages = 3 * a.sch->n_surfaces;
+    for (size_t i = gtid(); i < a.n; i += gstride()) {
+        a.lambda[i] = in.lambda[i];
+        if (in.flag[i] != 1) {
+            a.flag[i] = 0;
+            continue;
+        }
+        f64::Ray r{in.X[i], in.Y[i], in.Z[i], in.cX[i], in.cY[i], in.cZ[i]};
+        const double lam = in.lambda[i];
+        const int b = beam_of(a.beams, a.n_beams, i);
+        const int stage = Surfaces::run(a, i, b, lam, err, r);
+        a.flag[i] = (stage == -1) ? 1 : 0;
+        a.X[i] = r.X;
+        a.Y[i] = r.Y;
+        // one atomic per distinct counter in the warp (the rays of a beam
+        // mostly share theirs)
+        count_event(stage != -2, b * (n_stages + 1) + (stage >= 0 ? stage : n_stages), counts);
+    }
+}
 
 // One lane's ray in the reverse sweep.
 struct RevRay {

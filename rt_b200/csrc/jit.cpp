@@ -371,7 +371,8 @@ static int load_kernel(const std::string& src, bool fmad, const char* name, cons
                        bool compile) {
     *kernel = nullptr;
     std::lock_guard<std::mutex> g(g_mu);
-    auto it = g_kernels.find(src);
+    const std::string kkey = src + '\0' + name;  // a source may hold several kernels
+    auto it = g_kernels.find(kkey);
     if (it != g_kernels.end()) {
         *kernel = reinterpret_cast<const void*>(it->second);
         return RTB_OK;
@@ -398,7 +399,7 @@ static int load_kernel(const std::string& src, bool fmad, const char* name, cons
         if (!compile) return RTB_OK;  // one-shot traces run the generic kernel
         return cuda_status(e);
     }
-    g_kernels.emplace(src, k);
+    g_kernels.emplace(kkey, k);
     *kernel = reinterpret_cast<const void*>(k);
     return RTB_OK;
 }
@@ -416,25 +417,43 @@ static std::string adj_shape(const DevSurface& s) {
     return t;
 }
 
+static const char* const kAdjForwardName = "rtb_adj_forward_scheme";
 static const char* const kAdjReverseName = "rtb_adj_reverse_scheme";
 
 std::string adjoint_source(const DevScheme& sch) {
     std::string src =
         "#include \"adjoint_rev.cuh\"\n"
         "namespace rtb {\n"
-        "struct SchemeAdjSurfaces {\n"
-        "    __device__ __forceinline__ static void sweep(const AdjArgs& a, RevRay& ray, int lane, double* acc_row) {\n";
+        "struct SchemeAdjForward {\n"
+        "    __device__ __forceinline__ static int run(const AdjArgs& a, size_t i, int b, double lam, unsigned* err,\n"
+        "                                              f64::Ray& r) {\n"
+        "        int stage = -1;\n";
+    for (int k = 0; k < sch.n_surfaces; ++k)
+        src += "        if (stage == -1) stage = fwd_surface<" + adj_shape(sch.s[k]) + ">(a, " + std::to_string(k) +
+               ", i, b, lam, err, r);\n";
+    src += "        return stage;\n    }\n};\n"
+           "struct SchemeAdjSurfaces {\n"
+           "    __device__ __forceinline__ static void sweep(const AdjArgs& a, RevRay& ray, int lane, double* acc_row) {\n";
     for (int k = sch.n_surfaces - 1; k >= 0; --k)
         src += "        rev_surface<" + adj_shape(sch.s[k]) + ">(a, " + std::to_string(k) + ", ray, lane, acc_row);\n";
     src += std::string("    }\n};\n}  // namespace rtb\n"
-                       "extern \"C\" __global__ void __launch_bounds__(rtb::kAdjThreads, 4) ") + kAdjReverseName +
+                       "extern \"C\" __global__ void __launch_bounds__(256) ") + kAdjForwardName +
+           "(rtb::AdjArgs a, rtb::DevRays in,\n        unsigned long long* counts, unsigned* err) {\n"
+           "    rtb::adj_forward<rtb::SchemeAdjForward>(a, in, counts, err);\n}\n"
+           "extern \"C\" __global__ void __launch_bounds__(rtb::kAdjThreads, 4) " + kAdjReverseName +
            "(rtb::AdjArgs a,\n        const double* gX, const double* gY, double* partial) {\n"
            "    rtb::adj_reverse<rtb::SchemeAdjSurfaces>(a, gX, gY, partial);\n}\n";
     return src;
 }
 
-int adjoint_kernel(const DevScheme& sch, const void** kernel, std::string* why) {
-    return load_kernel(adjoint_source(sch), false, kAdjReverseName, kernel, why, true);
+int adjoint_kernels(const DevScheme& sch, const void** forward, const void** reverse, std::string* why) {
+    const std::string src = adjoint_source(sch);
+    *reverse = nullptr;
+    int st = load_kernel(src, false, kAdjForwardName, forward, why, true);
+    if (st != RTB_OK || !*forward) return st;
+    st = load_kernel(src, false, kAdjReverseName, reverse, why, true);
+    if (!*reverse) *forward = nullptr;
+    return st;
 }
 
 int compile_adjoint(const DevScheme& sch, std::string* why) {

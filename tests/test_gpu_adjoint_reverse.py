@@ -109,9 +109,10 @@ def test_reverse_equals_passes_and_jvp_on_every_kind(name, fixes, monkeypatch):
 
 @pytest.mark.parametrize("name", ["c4", "mirrors", "lenses", "gratings"])
 def test_reverse_sweep_compiled_for_the_scheme_equals_generic(name, monkeypatch):
-    """rtb_adjoint_create compiles the reverse sweep for the scheme's
-    structure (RTB_SPECIALIZE=0: the generic kernel); both run the same
-    IEEE operations in the same order: the same gradient bits, also with
+    """rtb_adjoint_create compiles the forward and the reverse sweep for the
+    scheme's structure (RTB_SPECIALIZE=0: the generic kernels); both run the
+    same IEEE operations in the same order: the same positions and gradient
+    bits, also with
     the parameters moved off their create-time values (angles and distances
     away from zero change which transforms apply, which the compiled kernel
     reads at run time)."""
@@ -137,6 +138,7 @@ def test_reverse_sweep_compiled_for_the_scheme_equals_generic(name, monkeypatch)
                 th = np.where(theta > 0, np.maximum(th, 0.5 * theta), th)
             st, _ = adj.forward(th, rays)
             assert st == ffi.OK
+            out.append((adj.X.clone(), adj.Y.clone(), adj.flag.clone()))
             gen = torch.Generator(device="cuda").manual_seed(3)
             gX = torch.randn(n, dtype=torch.float64, device="cuda", generator=gen)
             gY = torch.randn(n, dtype=torch.float64, device="cuda", generator=gen)
@@ -147,4 +149,10 @@ def test_reverse_sweep_compiled_for_the_scheme_equals_generic(name, monkeypatch)
         grads.append(out)
         adj.destroy()
     for a, b in zip(*grads):
-        assert np.array_equal(a, b), np.max(np.abs(a - b))
+        if isinstance(a, tuple):  # the forward's outputs
+            assert torch.equal(a[2], b[2])
+            g = a[2] == 1
+            assert torch.equal(a[0][g].view(torch.int64), b[0][g].view(torch.int64))
+            assert torch.equal(a[1][g].view(torch.int64), b[1][g].view(torch.int64))
+        else:
+            assert np.array_equal(a, b), np.max(np.abs(a - b))

@@ -59,12 +59,14 @@ def test_c1_full_size_conservation_determinism_and_accuracy():
     outs = {}
     for prec in (ffi.FP64, ffi.MIXED):
         plan, counts, outside = _run_plan(cs, beams, prec, ccd)
+        torch.cuda.synchronize()  # the zeroed frame, before the library's stream uses it
         plan.run()
         stats = _conserved(plan, beams, counts, outside)
         first = _outputs(plan)
         frame = counts.clone()
         counts.zero_()
         outside.zero_()
+        torch.cuda.synchronize()  # the plan runs on the library's own stream
         plan.run()
         _conserved(plan, beams, counts, outside)
         again = _outputs(plan)
@@ -115,6 +117,7 @@ def test_c3_full_size_conservation():
     cs = S.to_c(S.echelle(), E.spline_init)
     ccd = S.ccd(S.C1_CCD)
     plan, counts, outside = _run_plan(cs, beams, ffi.MIXED, ccd, out_order=ffi.OUT_SLOT)
+    torch.cuda.synchronize()
     plan.run()
     stats = _conserved(plan, beams, counts, outside)
     assert stats.n_good > 0
