@@ -33,6 +33,20 @@
 namespace rtb {
 namespace rv {
 
+// Reciprocal and reciprocal square root for the derivative arithmetic (the
+// values the recomputation follows keep the plain engine's IEEE operations):
+// the hardware seed refined by Newton steps (two for 1/x, x (2 - x y); two
+// for 1/sqrt(x), y (3/2 - x y^2 / 2)), to about an ulp, in place of the
+// IEEE division and square-root sequences.
+__device__ __forceinline__ double rcp(double x) { return ad::tangent_rcp(x); }
+__device__ __forceinline__ double rsqrt(double x) {
+    double y;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    const double h = 0.5 * x;
+    y = y * fma(-h * y, y, 1.5);
+    return y * fma(-h * y, y, 1.5);
+}
+
 // Adjoints of the ray state.
 struct RayA {
     double X, Y, Z, cX, cY, cZ;
@@ -91,18 +105,10 @@ __device__ __forceinline__ void transform_rev(const DevSurface& s, const f64::Ra
 }
 
 // c -> c / |c| at the pre-normalisation cosines c: the adjoint of c is the
-// output adjoint's component orthogonal to the unit vector, over |c|.
+// output adjoint's component orthogonal to the unit vector, over |c| (the
+// derivative of Beam::Normalize's formula, which computes |c|).
 __device__ __forceinline__ void normalize_rev(double cX, double cY, double cZ, RayA& a) {
-    const double acX = fabs(cX), acY = fabs(cY), acZ = fabs(cZ);
-    double norm;
-    if (acX >= acY) {
-        if (acX >= acZ) norm = acX * sqrt(1.0 + acY * acY / acX / acX + acZ * acZ / acX / acX);
-        else norm = acZ * sqrt(1.0 + acX * acX / acZ / acZ + acY * acY / acZ / acZ);
-    } else {
-        if (acY >= acZ) norm = acY * sqrt(1.0 + acX * acX / acY / acY + acZ * acZ / acY / acY);
-        else norm = acZ * sqrt(1.0 + acX * acX / acZ / acZ + acY * acY / acZ / acZ);
-    }
-    const double in = ad::tangent_rcp(norm);
+    const double in = rsqrt(fma(cX, cX, fma(cY, cY, cZ * cZ)));
     const double uX = cX * in, uY = cY * in, uZ = cZ * in;
     const double d = a.cX * uX + a.cY * uY + a.cZ * uZ;
     a.cX = (a.cX - d * uX) * in;
@@ -120,7 +126,7 @@ __device__ __forceinline__ void conic_derivs_rev(const DevSurface& s, double X, 
                                                  RayA& a, SurfA& p) {
     const int n = Sh::n_poly(s);
     const double r2 = X * X + Y * Y;
-    const double iw = 1.0 / sqrt(1.0 - s.k1 * s.c * s.c * r2);
+    const double iw = rsqrt(1.0 - s.k1 * s.c * s.c * r2);
     const double iw3 = iw * iw * iw;
     const double gE = -(gX * X + gY * Y);
     double E = s.c * iw, dE = 0.5 * s.k1 * s.c * s.c * s.c * iw3;  // E and dE/dr2
@@ -149,9 +155,9 @@ __device__ __forceinline__ void toric_derivs_rev(const DevSurface& s, double X, 
                                                  double gY, double gZ, RayA& a, SurfA& p) {
     const int n = Sh::n_poly(s);
     const double c = s.c, k1 = s.k1, Y2 = Y * Y;
-    const double w = sqrt(1.0 - k1 * c * c * Y2);
-    const double iw = 1.0 / w, iw3 = iw * iw * iw, den = 1.0 + w, iden2 = 1.0 / (den * den);
-    double Fy = c * Y2 / den, dFy = c * Y * iw;
+    const double q = 1.0 - k1 * c * c * Y2;
+    const double iw = rsqrt(q), w = q * iw, iw3 = iw * iw * iw, iden = rcp(1.0 + w), iden2 = iden * iden;
+    double Fy = c * Y2 * iden, dFy = c * Y * iw;
     {
         double rr = Y2, rq = 1.0;
 #pragma unroll
@@ -169,8 +175,8 @@ __device__ __forceinline__ void toric_derivs_rev(const DevSurface& s, double X, 
     const double gFy = gY * s.cR * dFy;        // adjoint of Fy
     const double gdFy = gY * (s.cR * Fy - 1.0);  // adjoint of dFy
     // conic parts: Fy0 = c Y2 / (1 + w), dFy0 = c Y / w
-    double dY2 = gFy * (c / den + 0.5 * k1 * c * c * c * Y2 * iw * iden2) + gdFy * 0.5 * k1 * c * c * c * Y * iw3;
-    p.c += gFy * (Y2 / den + k1 * c * c * Y2 * Y2 * iw * iden2) + gdFy * (Y * iw + k1 * c * c * Y * Y2 * iw3);
+    double dY2 = gFy * (c * iden + 0.5 * k1 * c * c * c * Y2 * iw * iden2) + gdFy * 0.5 * k1 * c * c * c * Y * iw3;
+    p.c += gFy * (Y2 * iden + k1 * c * c * Y2 * Y2 * iw * iden2) + gdFy * (Y * iw + k1 * c * c * Y * Y2 * iw3);
     p.k1 += gFy * 0.5 * c * c * c * Y2 * Y2 * iw * iden2 + gdFy * 0.5 * c * c * c * Y * Y2 * iw3;
     {
         double rq = 1.0, rm = 0.0;  // Y2^i, Y2^(i-1)
@@ -221,7 +227,7 @@ __device__ __forceinline__ double along_rev(const f64::Ray& r, double t, RayA& a
 // B = 2 (k1 Z cZ + X cX + Y cY - cZ / c), C = k1 Z^2 + X^2 + Y^2 - 2 Z / c.
 __device__ __forceinline__ void quadric_BC_rev(const DevSurface& s, const f64::Ray& r, double gB, double gC, RayA& a,
                                                SurfA& p) {
-    const double b2 = 2.0 * gB, ic = 1.0 / s.c;
+    const double b2 = 2.0 * gB, ic = s.inv_c;
     p.k1 += b2 * r.Z * r.cZ + gC * r.Z * r.Z;
     p.c += (b2 * r.cZ + gC * 2.0 * r.Z) * ic * ic;
     a.X += b2 * r.cX + 2.0 * gC * r.X;
@@ -242,9 +248,10 @@ __device__ __forceinline__ void asphere_F_rev(const DevSurface& s, bool poly_onl
     double dsag = 0.0;  // d(sag + poly)/dr2
     if (!poly_only) {
         const double c = s.c, k1 = s.k1;
-        const double w = sqrt(1.0 - k1 * c * c * r2), iw = 1.0 / w, den = 1.0 + w, iden2 = 1.0 / (den * den);
-        dsag = c / den + 0.5 * k1 * c * c * c * r2 * iw * iden2;
-        p.c += -gF * (r2 / den + k1 * c * c * r2 * r2 * iw * iden2);
+        const double q = 1.0 - k1 * c * c * r2;
+        const double iw = rsqrt(q), w = q * iw, iden = rcp(1.0 + w), iden2 = iden * iden;
+        dsag = c * iden + 0.5 * k1 * c * c * c * r2 * iw * iden2;
+        p.c += -gF * (r2 * iden + k1 * c * c * r2 * r2 * iw * iden2);
         p.k1 += -gF * 0.5 * c * c * c * r2 * r2 * iw * iden2;
     }
     double rq = 1.0;  // r2^i
@@ -272,12 +279,13 @@ __device__ __forceinline__ void toric_F_rev(const DevSurface& s, bool fix_sign, 
                                             double gF, RayA& a, SurfA& p) {
     const double PX = r.X + t * r.cX, PY = r.Y + t * r.cY, PZ = r.Z + t * r.cZ;
     const double c = s.c, kk = fix_sign ? s.k1 : -s.k1, Y2 = PY * PY;
-    const double q = sqrt(1.0 - kk * c * c * Y2), iq = 1.0 / q, den = 1.0 + q, iden2 = 1.0 / (den * den);
-    const double FY = c * Y2 / den;
+    const double qq = 1.0 - kk * c * c * Y2;
+    const double iq = rsqrt(qq), q = qq * iq, iden = rcp(1.0 + q), iden2 = iden * iden;
+    const double FY = c * Y2 * iden;
     p.cR += gF * -0.5 * (PX * PX + PZ * PZ - FY * FY);
     const double gFY = gF * (s.cR * FY - 1.0);
-    const double gY2 = gFY * (c / den + 0.5 * kk * c * c * c * Y2 * iq * iden2);
-    p.c += gFY * (Y2 / den + kk * c * c * Y2 * Y2 * iq * iden2);
+    const double gY2 = gFY * (c * iden + 0.5 * kk * c * c * c * Y2 * iq * iden2);
+    p.c += gFY * (Y2 * iden + kk * c * c * Y2 * Y2 * iq * iden2);
     const double dk = gFY * 0.5 * c * c * c * Y2 * Y2 * iq * iden2;
     p.k1 += fix_sign ? dk : -dk;
     const double gPX = gF * -s.cR * PX, gPY = 2.0 * gY2 * PY, gPZ = gF * (1.0 - s.cR * PZ);
@@ -295,7 +303,7 @@ __device__ __forceinline__ double asphere_Ft(const DevSurface& s, bool poly_only
     const double X = r.X + t * r.cX, Y = r.Y + t * r.cY;
     const double r2 = X * X + Y * Y;
     double E = 0.0;
-    if (!poly_only) E = s.c / sqrt(1.0 - s.k1 * s.c * s.c * r2);
+    if (!poly_only) E = s.c * rsqrt(1.0 - s.k1 * s.c * s.c * r2);
     double sum = 0.0, rr = 1.0;
     for (int i = 1; i <= Sh::n_poly(s); ++i, rr *= r2) sum += (double)i * s.poly[i - 1] * rr;
     E += 2.0 * sum;
@@ -306,8 +314,9 @@ __device__ __forceinline__ double toric_Ft(const DevSurface& s, bool fix_sign, c
     const double X = r.X + t * r.cX, Y = r.Y + t * r.cY, Z = r.Z + t * r.cZ;
     const double sg = fix_sign ? -1.0 : 1.0;
     const double Y2 = Y * Y;
-    const double q = sqrt(1.0 + sg * s.k1 * s.c * s.c * Y2);
-    const double FY = s.c * Y2 / (1.0 + q), dFY = s.c * Y / q;
+    const double qq = 1.0 + sg * s.k1 * s.c * s.c * Y2;
+    const double iq = rsqrt(qq), q = qq * iq;
+    const double FY = s.c * Y2 * rcp(1.0 + q), dFY = s.c * Y * iq;
     return r.cZ - dFY * r.cY - s.cR * (X * r.cX + Z * r.cZ - FY * dFY * r.cY);
 }
 
@@ -346,35 +355,36 @@ __device__ __forceinline__ void isect_rev(const DevSurface& s, uint32_t fixes, c
                                           SurfA& p) {
     switch (Sh::kind(s)) {
         case IS_PLANE: {
-            const double s0 = -r.Z / r.cZ;
+            const double icZ = rcp(r.cZ);
+            const double s0 = -r.Z * icZ;
             const double g0 = a.X * r.cX + a.Y * r.cY;  // Z' = 0 carries nothing
             a.cX += a.X * s0;
             a.cY += a.Y * s0;
-            const double icZ = 1.0 / r.cZ;
             a.Z = -g0 * icZ;
             a.cZ += -g0 * s0 * icZ;
             return;
         }
         case IS_PARABOLOID: {
-            const double B = 2.0 * (s.k1 * r.Z * r.cZ + r.X * r.cX + r.Y * r.cY - r.cZ / s.c);
-            const double C = s.k1 * r.Z * r.Z + r.X * r.X + r.Y * r.Y - 2.0 * r.Z / s.c;
-            const double tt = -C / B;
+            const double B = 2.0 * (s.k1 * r.Z * r.cZ + r.X * r.cX + r.Y * r.cY - r.cZ * s.inv_c);
+            const double C = s.k1 * r.Z * r.Z + r.X * r.X + r.Y * r.Y - 2.0 * r.Z * s.inv_c;
+            const double iB = rcp(B);
+            const double tt = -C * iB;
             const double gt = along_rev(r, tt, a);
-            const double iB = 1.0 / B;
             quadric_BC_rev(s, r, -gt * tt * iB, -gt * iB, a, p);
             return;
         }
         case IS_CONIC: {
             const double A = s.k1 * r.cZ * r.cZ + r.cX * r.cX + r.cY * r.cY;
-            const double B = 2.0 * (s.k1 * r.Z * r.cZ + r.X * r.cX + r.Y * r.cY - r.cZ / s.c);
-            const double C = s.k1 * r.Z * r.Z + r.X * r.X + r.Y * r.Y - 2.0 * r.Z / s.c;
-            const double q = sqrt(B * B - 4.0 * A * C);
+            const double B = 2.0 * (s.k1 * r.Z * r.cZ + r.X * r.cX + r.Y * r.cY - r.cZ * s.inv_c);
+            const double C = s.k1 * r.Z * r.Z + r.X * r.X + r.Y * r.Y - 2.0 * r.Z * s.inv_c;
+            const double D = B * B - 4.0 * A * C;
+            const double iq = rsqrt(D), q = D * iq, iA = rcp(A);
             const double sg = (s.c > 0) ? -1.0 : 1.0;
-            const double tt = (-B + sg * q) / 2.0 / A;
+            const double tt = (-B + sg * q) * 0.5 * iA;
             const double gt = along_rev(r, tt, a);
-            const double gN = gt / (2.0 * A);
-            double gA = -gt * tt / A;
-            const double gD = sg * gN / (2.0 * q);
+            const double gN = gt * 0.5 * iA;
+            double gA = -gt * tt * iA;
+            const double gD = sg * gN * 0.5 * iq;
             const double gB = -gN + 2.0 * B * gD;
             gA += -4.0 * C * gD;
             const double gC = -4.0 * A * gD;
@@ -389,13 +399,13 @@ __device__ __forceinline__ void isect_rev(const DevSurface& s, uint32_t fixes, c
         case IS_ITER_CONIC: {
             const bool po = Sh::kind(s) == IS_ITER_POLY;
             const double gt = along_rev(r, t, a);
-            asphere_F_rev<Sh>(s, po, r, t, -gt / asphere_Ft<Sh>(s, po, r, t), a, p);
+            asphere_F_rev<Sh>(s, po, r, t, -gt * rcp(asphere_Ft<Sh>(s, po, r, t)), a, p);
             return;
         }
         case IS_TORIC: {
             const bool fs = (fixes & RTB_FIX_TORIC_SIGN) != 0;
             const double gt = along_rev(r, t, a);
-            toric_F_rev(s, fs, r, t, -gt / toric_Ft(s, fs, r, t), a, p);
+            toric_F_rev(s, fs, r, t, -gt * rcp(toric_Ft(s, fs, r, t)), a, p);
             return;
         }
         default: return;
@@ -450,10 +460,11 @@ __device__ __forceinline__ void reflect_rev(const DevSurface& s, bool tor, const
     slopes<Sh>(s, tor, r.X, r.Y, r.Z, dX, dY, dZ);
     const double num = r.cX * dX + r.cY * dY + r.cZ * dZ;
     const double den = dX * dX + dY * dY + dZ * dZ;
-    const double a2 = 2.0 * num / den;
+    const double iden = rcp(den);
+    const double a2 = 2.0 * num * iden;
     const double ga2 = -(a.cX * dX + a.cY * dY + a.cZ * dZ);
     double gX = -a.cX * a2, gY = -a.cY * a2, gZ = -a.cZ * a2;
-    const double gn = 2.0 * ga2 / den, gden = -ga2 * a2 / den;
+    const double gn = 2.0 * ga2 * iden, gden = -ga2 * a2 * iden;
     a.cX += gn * dX;
     a.cY += gn * dY;
     a.cZ += gn * dZ;
@@ -472,17 +483,18 @@ __device__ __forceinline__ void refract_rev(const DevSurface& s, bool tor, doubl
     slopes<Sh>(s, tor, r.X, r.Y, r.Z, dX, dY, dZ);
     const double G0 = dX * dX + dY * dY + dZ * dZ;
     const double num = r.cX * dX + r.cY * dY + r.cZ * dZ;
-    const double av = mu * num / G0, bv = (mu * mu - 1.0) / G0;
-    const double sq = sqrt(av * av - bv);
+    const double iG0 = rcp(G0);
+    const double av = mu * num * iG0, bv = (mu * mu - 1.0) * iG0;
+    const double d2 = av * av - bv, isq = rsqrt(d2), sq = d2 * isq;
     const double G = -av + sq;
     const double gG = a.cX * dX + a.cY * dY + a.cZ * dZ;
     double gX = a.cX * G, gY = a.cY * G, gZ = a.cZ * G;
     a.cX *= mu;
     a.cY *= mu;
     a.cZ *= mu;
-    const double ga = -gG + gG * av / sq, gb = -gG / (2.0 * sq);
-    const double gG0 = -(gb * bv + ga * av) / G0;
-    const double gn = ga * mu / G0;
+    const double ga = -gG + gG * av * isq, gb = -gG * 0.5 * isq;
+    const double gG0 = -(gb * bv + ga * av) * iG0;
+    const double gn = ga * mu * iG0;
     a.cX += gn * dX;
     a.cY += gn * dY;
     a.cZ += gn * dZ;
@@ -506,15 +518,17 @@ __device__ __forceinline__ double diffract_curved_rev(const DevSurface& s, bool 
     slopes<Sh>(s, tor, r.X, r.Y, r.Z, dX, dY, dZ);
     const double m = trans ? mu : 1.0, K = trans ? mu * mu - 1.0 : 0.0, sg = trans ? 1.0 : -1.0;
     const double den1 = tor ? dY * dY + dZ + dZ : dY * dY + 1.0;
-    const double g1 = dX / den1;
+    const double iden1 = rcp(den1);
+    const double g1 = dX * iden1;
     const double s1 = 1.0 + dX * g1;
-    const double u = 1.0 / sqrt(s1);
+    const double u = rsqrt(s1);
     const double v = -dY * u * g1, w = tor ? -dZ * u * g1 : -u * g1;
     const double G0 = dX * dX + dY * dY + dZ * dZ;
     const double num = r.cX * dX + r.cY * dY + r.cZ * dZ;
     const double dot = r.cX * u + r.cY * v + r.cZ * w;
-    const double av = m * num / G0, bv = (K + L * L - 2.0 * L * m * dot) / G0;
-    const double sq = sqrt(av * av - bv);
+    const double iG0 = rcp(G0);
+    const double av = m * num * iG0, bv = (K + L * L - 2.0 * L * m * dot) * iG0;
+    const double d2 = av * av - bv, isq = rsqrt(d2), sq = d2 * isq;
     const double G = -av + sg * sq;
     // c' = m c - L uvw + G dF
     const double gG = a.cX * dX + a.cY * dY + a.cZ * dZ;
@@ -524,9 +538,9 @@ __device__ __forceinline__ double diffract_curved_rev(const DevSurface& s, bool 
     a.cX *= m;
     a.cY *= m;
     a.cZ *= m;
-    const double ga = -gG + sg * gG * av / sq, gb = -sg * gG / (2.0 * sq);
-    const double gbn = gb / G0;
-    double gG0 = -gb * bv / G0;
+    const double ga = -gG + sg * gG * av * isq, gb = -sg * gG * 0.5 * isq;
+    const double gbn = gb * iG0;
+    double gG0 = -gb * bv * iG0;
     gL += gbn * (2.0 * L - 2.0 * m * dot);
     const double gdot = -2.0 * L * m * gbn;
     a.cX += gdot * u;
@@ -535,8 +549,8 @@ __device__ __forceinline__ double diffract_curved_rev(const DevSurface& s, bool 
     gu += gdot * r.cX;
     gv += gdot * r.cY;
     gw += gdot * r.cZ;
-    const double gn = ga * m / G0;
-    gG0 += -ga * av / G0;
+    const double gn = ga * m * iG0;
+    gG0 += -ga * av * iG0;
     a.cX += gn * dX;
     a.cY += gn * dY;
     a.cZ += gn * dZ;
@@ -559,8 +573,8 @@ __device__ __forceinline__ double diffract_curved_rev(const DevSurface& s, bool 
     const double gs1 = -0.5 * gu * u * u * u;
     gX += gs1 * g1;
     gg1 += gs1 * dX;
-    gX += gg1 / den1;
-    const double gden1 = -gg1 * g1 / den1;
+    gX += gg1 * iden1;
+    const double gden1 = -gg1 * g1 * iden1;
     gY += 2.0 * gden1 * dY;
     if (tor) gZ += 2.0 * gden1;
     slopes_rev<Sh>(s, tor, r.X, r.Y, r.Z, gX, gY, gZ, a, p);
@@ -580,11 +594,11 @@ __device__ __forceinline__ void action_rev(const DevSurface& s, double mu, doubl
     if (Sh::type(s) == RTB_LENS) {
         if (Sh::cls(s) == RTB_PLANE) {  // a = mu cZ, G = -a + sqrt(a^2 - (mu^2 - 1)), c' = (mu cX, mu cY, mu cZ + G)
             const double av = mu * r.cZ;
-            const double sq = sqrt(av * av - (mu * mu - 1.0));
+            const double isq = rsqrt(av * av - (mu * mu - 1.0));
             const double gG = a.cZ;
             a.cX *= mu;
             a.cY *= mu;
-            a.cZ = mu * a.cZ + mu * (-gG + gG * av / sq);
+            a.cZ = mu * a.cZ + mu * (-gG + gG * av * isq);
         } else if (Sh::cls(s) == RTB_CONIC || tor) {
             refract_rev<Sh>(s, tor, mu, r, a, p);
         }
@@ -599,20 +613,20 @@ __device__ __forceinline__ void action_rev(const DevSurface& s, double mu, doubl
         // reflective: a = cZ, b = L^2 - 2 L cX, G = -a - sqrt(a^2 - b), c' = (cX - L, cY, cZ + G)
         const double m = trans ? mu : 1.0, K = trans ? mu * mu - 1.0 : 0.0, sg = trans ? 1.0 : -1.0;
         const double av = m * r.cZ, bv = K + L * L - 2.0 * m * L * r.cX;
-        const double sq = sqrt(av * av - bv);
+        const double isq = rsqrt(av * av - bv);
         const double gG = a.cZ;
         gL = -a.cX;
         a.cX *= m;
         a.cY *= m;
         a.cZ *= m;
-        const double ga = -gG + sg * gG * av / sq, gb = -sg * gG / (2.0 * sq);
+        const double ga = -gG + sg * gG * av * isq, gb = -sg * gG * 0.5 * isq;
         gL += gb * (2.0 * L - 2.0 * m * r.cX);
         a.cX += gb * (-2.0 * m * L);
         a.cZ += ga * m;
     } else if (Sh::cls(s) == RTB_CONIC || tor) {
         gL = diffract_curved_rev<Sh>(s, tor, trans, mu, L, r, a, p);
     }
-    p.gr += gL * (-L / s.gr_const);  // L = (order lambda / n2) / gr
+    p.gr += gL * (-L * s.inv_gr);  // L = (order lambda / n2) / gr
 }
 
 // ---- one surface -----------------------------------------------------------------
