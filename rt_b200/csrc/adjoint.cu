@@ -582,6 +582,7 @@ int rtb_adjoint_theta(const rtb_adjoint* c, double* theta) {
 
 int rtb_adjoint_forward(rtb_adjoint* c, const double* theta, const rtb_rays* rays, double* X, double* Y, char* flag,
                         rtb_trace_stats* stats, void* stream) {
+    Range range("rtb_adjoint_forward");
     if (!c || !rays || rays->n != c->n || !rays->flag) return RTB_BAD_VALUE;
     DeviceGuard dg(c->device);
     Lock l;
@@ -631,6 +632,7 @@ int rtb_adjoint_forward(rtb_adjoint* c, const double* theta, const rtb_rays* ray
 }
 
 int rtb_adjoint_backward(rtb_adjoint* c, const double* gX, const double* gY, double* grad, void* stream) {
+    Range range("rtb_adjoint_backward");
     if (!c || !gX || !gY || (!grad && !c->params.empty()) || !c->have_forward) return RTB_BAD_VALUE;
     if (c->params.empty()) return RTB_OK;
     DeviceGuard dg(c->device);
@@ -691,6 +693,7 @@ int rtb_adjoint_backward(rtb_adjoint* c, const double* gX, const double* gY, dou
 }
 
 int rtb_adjoint_jvp(rtb_adjoint* c, const double* dtheta, double* dX, double* dY, void* stream) {
+    Range range("rtb_adjoint_jvp");
     if (!c || !dX || !dY || (!dtheta && !c->params.empty()) || !c->have_forward) return RTB_BAD_VALUE;
     DeviceGuard dg(c->device);
     Lock l;
@@ -713,6 +716,7 @@ int rtb_adjoint_jvp(rtb_adjoint* c, const double* dtheta, double* dX, double* dY
 
 int rtb_adjoint_spot_merit(rtb_adjoint* c, const double* target_x, double weight, double* merit, double* gX,
                            double* gY, void* stream) {
+    Range range("rtb_adjoint_spot_merit");
     if (!c || !target_x || !merit || !c->have_forward || ((gX == nullptr) != (gY == nullptr))) return RTB_BAD_VALUE;
     DeviceGuard dg(c->device);
     Lock l;

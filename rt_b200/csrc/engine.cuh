@@ -4,6 +4,8 @@
 #include <mutex>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "kernels.cuh"
 
 namespace rtb {
@@ -110,6 +112,26 @@ struct DevBuf {
 struct Lock {
     std::lock_guard<std::mutex> g;
     Lock() : g(engine().mu) {}
+};
+
+// A named range of a C ABI call on a profiler's timeline (NVTX, domain
+// "rt_b200"), from construction to destruction; a no-op when no tool is
+// attached.  Kernels and copies the call enqueues show under it.
+struct Range {
+    nvtxDomainHandle_t dom;
+    explicit Range(const char* name) {
+        static nvtxDomainHandle_t d = nvtxDomainCreateA("rt_b200");
+        dom = d;
+        nvtxEventAttributes_t a = {};
+        a.version = NVTX_VERSION;
+        a.size = NVTX_EVENT_ATTRIB_STRUCT_SIZE;
+        a.messageType = NVTX_MESSAGE_TYPE_ASCII;
+        a.message.ascii = name;
+        nvtxDomainRangePushEx(dom, &a);
+    }
+    ~Range() { nvtxDomainRangePop(dom); }
+    Range(const Range&) = delete;
+    Range& operator=(const Range&) = delete;
 };
 
 // Everything a trace launch reads, in one pool allocation.

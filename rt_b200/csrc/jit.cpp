@@ -110,6 +110,7 @@ std::map<std::string, std::vector<char>> g_cubins;  // compiled kernels, by sour
 std::map<std::string, cudaKernel_t> g_kernels;      // loaded kernels, by source
 
 int compile_to_cubin(const std::string& src, bool fmad, std::vector<char>& cubin, std::string& log) {
+    Range range("NVRTC compile");
     const Nvrtc& n = nvrtc();
     std::vector<const char*> names, texts;
     for (const char* t : {"cstdint", "stdint.h", "stddef.h"}) {

@@ -194,6 +194,7 @@ extern "C" {
 
 int rtb_plan_create(const rtb_surface* surfaces, size_t n_surfaces, const rtb_beam* beams, size_t n_beams,
                     const rtb_trace_opts* opts, rtb_plan** plan) {
+    Range range("rtb_plan_create");
     if (!plan || !opts || !beams || n_beams == 0) return RTB_BAD_VALUE;
     *plan = nullptr;
     if (opts->engine != RTB_ENGINE_FUSED) return RTB_BAD_VALUE;
@@ -351,6 +352,7 @@ int rtb_plan_create(const rtb_surface* surfaces, size_t n_surfaces, const rtb_be
 }
 
 int rtb_plan_run(rtb_plan* p, void* stream) {
+    Range range("rtb_plan_run");
     if (!p) return RTB_BAD_VALUE;
     DeviceGuard dg(p->device);
     Lock l;
@@ -414,6 +416,7 @@ int rtb_plan_config(const rtb_plan* p, int32_t* block, int32_t* rpt, uint64_t* n
 }
 
 int rtb_plan_autotune(rtb_plan* p, int reps, rtb_tune_entry* table, size_t capacity, size_t* n_entries) {
+    Range range("rtb_plan_autotune");
     if (!p || reps < 1) return RTB_BAD_VALUE;
     DeviceGuard dg(p->device);
     Lock l;

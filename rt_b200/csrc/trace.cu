@@ -223,6 +223,7 @@ int rtb_generate_beams(const rtb_beam* beams, size_t n_beams, const rtb_rays* ra
 
 int rtb_trace(const rtb_surface* surfaces, size_t n_surfaces, const rtb_beam* beams, size_t n_beams,
               const rtb_trace_opts* opts, const rtb_rays* rays, rtb_trace_stats* stats, void* stream) {
+    Range range("rtb_trace");
     if (!opts || !rays || !rays->flag || !rays->lost_stage) return RTB_BAD_VALUE;
     Lock l;
     int st = ensure_init();
@@ -250,6 +251,7 @@ int rtb_trace(const rtb_surface* surfaces, size_t n_surfaces, const rtb_beam* be
 int rtb_trace_out(const rtb_surface* surfaces, size_t n_surfaces, const rtb_beam* beams, size_t n_beams,
                   const rtb_trace_opts* opts, const rtb_rays* in, const rtb_rays* out, rtb_trace_stats* stats,
                   void* stream) {
+    Range range("rtb_trace_out");
     if (!opts || !in || !out || !in->flag || !out->flag || !out->lost_stage || in->n != out->n) return RTB_BAD_VALUE;
     Lock l;
     int st = ensure_init();
@@ -518,6 +520,7 @@ int trace_host_impl(const rtb_surface* surfaces, size_t n_surfaces, const rtb_be
 extern "C" RTB_API int rtb_trace_host(const rtb_surface* surfaces, size_t n_surfaces, const rtb_beam* beams,
                                       size_t n_beams, const rtb_trace_opts* opts, const rtb_rays* host_rays,
                                       rtb_trace_stats* stats) {
+    Range range("rtb_trace_host");
     if (!opts || !host_rays || !host_rays->flag) return RTB_BAD_VALUE;
     Lock l;
     int st = ensure_init();
