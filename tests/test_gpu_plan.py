@@ -291,7 +291,9 @@ def test_specialised_plan_equals_generic_kernel(name, precision, monkeypatch):
         assert abs(a[2] - b[2]) <= 1e-4 * a[3]["flag"].numel() + 1
         o, counts64, outside64 = frame_opts(ffi.FP64, ccd, state_out=1)  # the plan writes into these
         plan = E.Plan(cs.surfaces, beams, o)
+        torch.cuda.synchronize()  # the zeroed frame before the plan's own stream runs
         plan.run()
+        plan.result()  # waits for the run
         _, ref = plan_output(plan)
         ref = {k: v.clone() for k, v in ref.items()}
         plan.destroy()
