@@ -219,31 +219,7 @@ __global__ void k_adj_sum_partials(const double* partial, int n_blocks, int P, d
 // along that direction.
 __global__ void __launch_bounds__(kAdjThreads) k_adj_jvp(AdjArgs a, const ad::SurfD<1>* table, double* dX,
                                                          double* dY) {
-    const DevScheme* sch = a.sch;
-    const int ns = sch->n_surfaces;
-    for (size_t i = gtid(); i < a.n; i += gstride()) {
-        if (a.flag[i] != 1) {
-            dX[i] = 0.0;
-            dY[i] = 0.0;
-            continue;
-        }
-        const double lam = a.lambda[i];
-        const int b = beam_of(a.beams, a.n_beams, i);
-        ad::Seeds<1> sd;
-        sd.dense = nullptr;
-        sd.state[0] = -1;
-        sd.param[0] = -1;
-        double st[6];
-        for (int c = 0; c < 6; ++c) st[c] = a.ckpt[(size_t)c * a.n + i];
-        ad::RayD<1> r;
-        ad::load_state(st, sd, r);
-        for (int k = 0; k < ns; ++k) {
-            const DevSurface& s = sch->s[k];
-            ad::surface_step(s, table[k], sch->fixes, a.knots, adj_order(s, a.beams, b), lam, r);
-        }
-        dX[i] = r.X.d[0];
-        dY[i] = r.Y.d[0];
-    }
+    adj_jvp<RtAdjJvp>(a, table, dX, dY);
 }
 
 // One wavelength group of the spot merit: rays first + m * stride, m < count.
@@ -323,8 +299,9 @@ struct rtb_adjoint {
     uint32_t fixes = 0;
     PreparedScheme ps;
     bool have_forward = false;
-    const void* fwd_kernel = nullptr;              // the forward and the reverse sweep compiled
-    const void* rev_kernel = nullptr;              // for the scheme's structure, or NULL
+    const void* fwd_kernel = nullptr;              // the forward, the reverse sweep and the
+    const void* rev_kernel = nullptr;              // sensitivities compiled for the scheme's
+    const void* jvp_kernel = nullptr;              // structure, or NULL
     // device
     void* mem = nullptr;
     DevScheme* d_sch = nullptr;
@@ -564,10 +541,11 @@ int rtb_adjoint_create(const rtb_surface* surfaces, size_t n_surfaces, const rtb
     // intersection kinds); the generic kernel when NVRTC is unavailable
     if (specialize_enabled()) {
         std::string why;
-        const void *f = nullptr, *r = nullptr;
-        if (adjoint_kernels(c->ps.sch, &f, &r, &why) == RTB_OK) {
+        const void *f = nullptr, *r = nullptr, *j = nullptr;
+        if (adjoint_kernels(c->ps.sch, &f, &r, &j, &why) == RTB_OK) {
             c->fwd_kernel = f;
             c->rev_kernel = r;
+            c->jvp_kernel = j;
         }
     }
     *out = c;
@@ -708,7 +686,13 @@ int rtb_adjoint_jvp(rtb_adjoint* c, const double* dtheta, double* dX, double* dY
     if (st != RTB_OK) return st;
     k_build_surfd_dense<<<(unsigned)((ns + 31) / 32), 32, 0, s>>>(a, c->d_dtheta, table.as<ad::SurfD<1>>());
     RTB_CUDA_TRY(cudaGetLastError());
-    k_adj_jvp<<<adj_grid(c->n, kAdjThreads), kAdjThreads, 0, s>>>(a, table.as<ad::SurfD<1>>(), dX, dY);
+    const ad::SurfD<1>* tab = table.as<ad::SurfD<1>>();
+    if (c->jvp_kernel) {
+        void* args[] = {&a, &tab, &dX, &dY};
+        RTB_CUDA_TRY(cudaLaunchKernel(c->jvp_kernel, dim3(adj_grid(c->n, kAdjThreads)), dim3(kAdjThreads), args, 0, s));
+    } else {
+        k_adj_jvp<<<adj_grid(c->n, kAdjThreads), kAdjThreads, 0, s>>>(a, tab, dX, dY);
+    }
     RTB_CUDA_TRY(cudaGetLastError());
     RTB_CUDA_TRY(cudaStreamSynchronize(s));
     return RTB_OK;

@@ -1,7 +1,8 @@
-// adjoint_rev.cuh -- the adjoint's forward with checkpoints and its reverse
-// sweep, as the bodies of the generic kernels (k_adj_forward, k_adj_reverse,
-// adjoint.cu) and of kernels compiled for one scheme's structure (jit.cpp,
-// rtb_adj_forward_scheme, rtb_adj_reverse_scheme).
+// adjoint_rev.cuh -- the adjoint's forward with checkpoints, its reverse
+// sweep and its forward-mode sensitivities, as the bodies of the generic
+// kernels (k_adj_forward, k_adj_reverse, k_adj_jvp, adjoint.cu) and of
+// kernels compiled for one scheme's structure (jit.cpp,
+// rtb_adj_forward_scheme, rtb_adj_reverse_scheme, rtb_adj_jvp_scheme).
 //
 // Forward: the fused FP64 engine's per-ray loop (the same bits), storing each
 // ray's state (X Y Z cX cY cZ) at the input of every surface -- 48 bytes x
@@ -133,6 +134,50 @@ __device__ __forceinline__ void adj_forward(const AdjArgs& a, const DevRays& in,
         // one atomic per distinct counter in the warp (the rays of a beam
         // mostly share theirs)
         count_event(stage != -2, b * (n_stages + 1) + (stage >= 0 ? stage : n_stages), counts);
+    }
+}
+
+// Surface k (structure Sh) of the forward-mode sensitivities on one ray:
+// table[k] holds the surface's constants along the direction.
+template <class Sh>
+__device__ __forceinline__ void jvp_surface(const AdjArgs& a, int k, const ad::SurfD<1>* table, int b, double lam,
+                                            ad::RayD<1>& r) {
+    const DevSurface& s = a.sch->s[k];
+    ad::surface_step<1, Sh>(s, table[k], a.sch->fixes, a.knots, adj_order(s, a.beams, b), lam, r);
+}
+
+// The sensitivities through any scheme, its structure read at run time.
+struct RtAdjJvp {
+    __device__ __forceinline__ static void run(const AdjArgs& a, const ad::SurfD<1>* table, int b, double lam,
+                                               ad::RayD<1>& r) {
+        for (int k = 0; k < a.sch->n_surfaces; ++k) jvp_surface<RtShape>(a, k, table, b, lam, r);
+    }
+};
+
+// dX, dY: the rays' CCD-position sensitivities along the direction whose
+// surface constants table[k] holds, through the whole scheme from the
+// entrance rays (checkpoint 0); 0 for lost rays.
+template <class Surfaces>
+__device__ __forceinline__ void adj_jvp(const AdjArgs& a, const ad::SurfD<1>* table, double* dX, double* dY) {
+    for (size_t i = gtid(); i < a.n; i += gstride()) {
+        if (a.flag[i] != 1) {
+            dX[i] = 0.0;
+            dY[i] = 0.0;
+            continue;
+        }
+        const double lam = a.lambda[i];
+        const int b = beam_of(a.beams, a.n_beams, i);
+        ad::Seeds<1> sd;
+        sd.dense = nullptr;
+        sd.state[0] = -1;
+        sd.param[0] = -1;
+        double st[6];
+        for (int c = 0; c < 6; ++c) st[c] = a.ckpt[(size_t)c * a.n + i];
+        ad::RayD<1> r;
+        ad::load_state(st, sd, r);
+        Surfaces::run(a, table, b, lam, r);
+        dX[i] = r.X.d[0];
+        dY[i] = r.Y.d[0];
     }
 }
 

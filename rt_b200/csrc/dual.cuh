@@ -3,8 +3,9 @@
 // Dual<W> carries a value and W tangents.  The value is computed with the
 // same IEEE operation as plain double arithmetic (translation units that use
 // it are compiled with --fmad=false), so a trace in Dual<W> has exactly the
-// values of the plain FP64 engine; the tangents follow the chain rule, their
-// divisions as products with one refined reciprocal (tangent_rcp).
+// values of the plain FP64 engine; the tangents follow the chain rule with
+// explicit fused multiply-adds (a product rule is one FMA and one multiply),
+// their divisions as products with one refined reciprocal (tangent_rcp).
 #pragma once
 
 #ifndef __CUDACC_RTC__  // run-time compiled kernels take the device math built in
@@ -84,7 +85,7 @@ __device__ __forceinline__ Dual<W> operator*(const Dual<W>& a, const Dual<W>& b)
     Dual<W> r;
     r.v = a.v * b.v;
 #pragma unroll
-    for (int i = 0; i < W; ++i) r.d[i] = a.d[i] * b.v + a.v * b.d[i];
+    for (int i = 0; i < W; ++i) r.d[i] = fma(a.d[i], b.v, a.v * b.d[i]);
     return r;
 }
 template <int W>
@@ -121,7 +122,7 @@ __device__ __forceinline__ Dual<W> operator/(const Dual<W>& a, const Dual<W>& b)
     r.v = a.v / b.v;
     const double ib = tangent_rcp(b.v);
 #pragma unroll
-    for (int i = 0; i < W; ++i) r.d[i] = (a.d[i] - r.v * b.d[i]) * ib;
+    for (int i = 0; i < W; ++i) r.d[i] = fma(-r.v, b.d[i], a.d[i]) * ib;
     return r;
 }
 template <int W>

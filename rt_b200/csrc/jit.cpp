@@ -420,6 +420,7 @@ static std::string adj_shape(const DevSurface& s) {
 
 static const char* const kAdjForwardName = "rtb_adj_forward_scheme";
 static const char* const kAdjReverseName = "rtb_adj_reverse_scheme";
+static const char* const kAdjJvpName = "rtb_adj_jvp_scheme";
 
 std::string adjoint_source(const DevScheme& sch) {
     std::string src =
@@ -433,6 +434,12 @@ std::string adjoint_source(const DevScheme& sch) {
         src += "        if (stage == -1) stage = fwd_surface<" + adj_shape(sch.s[k]) + ">(a, " + std::to_string(k) +
                ", i, b, lam, err, r);\n";
     src += "        return stage;\n    }\n};\n"
+           "struct SchemeAdjJvp {\n"
+           "    __device__ __forceinline__ static void run(const AdjArgs& a, const ad::SurfD<1>* table, int b,\n"
+           "                                               double lam, ad::RayD<1>& r) {\n";
+    for (int k = 0; k < sch.n_surfaces; ++k)
+        src += "        jvp_surface<" + adj_shape(sch.s[k]) + ">(a, " + std::to_string(k) + ", table, b, lam, r);\n";
+    src += "    }\n};\n"
            "struct SchemeAdjSurfaces {\n"
            "    __device__ __forceinline__ static void sweep(const AdjArgs& a, RevRay& ray, int lane, double* acc_row) {\n";
     for (int k = sch.n_surfaces - 1; k >= 0; --k)
@@ -443,17 +450,22 @@ std::string adjoint_source(const DevScheme& sch) {
            "    rtb::adj_forward<rtb::SchemeAdjForward>(a, in, counts, err);\n}\n"
            "extern \"C\" __global__ void __launch_bounds__(rtb::kAdjThreads, 4) " + kAdjReverseName +
            "(rtb::AdjArgs a,\n        const double* gX, const double* gY, double* partial) {\n"
-           "    rtb::adj_reverse<rtb::SchemeAdjSurfaces>(a, gX, gY, partial);\n}\n";
+           "    rtb::adj_reverse<rtb::SchemeAdjSurfaces>(a, gX, gY, partial);\n}\n"
+           "extern \"C\" __global__ void __launch_bounds__(rtb::kAdjThreads) " + kAdjJvpName +
+           "(rtb::AdjArgs a,\n        const rtb::ad::SurfD<1>* table, double* dX, double* dY) {\n"
+           "    rtb::adj_jvp<rtb::SchemeAdjJvp>(a, table, dX, dY);\n}\n";
     return src;
 }
 
-int adjoint_kernels(const DevScheme& sch, const void** forward, const void** reverse, std::string* why) {
+int adjoint_kernels(const DevScheme& sch, const void** forward, const void** reverse, const void** jvp,
+                    std::string* why) {
     const std::string src = adjoint_source(sch);
-    *reverse = nullptr;
+    *reverse = *jvp = nullptr;
     int st = load_kernel(src, false, kAdjForwardName, forward, why, true);
     if (st != RTB_OK || !*forward) return st;
     st = load_kernel(src, false, kAdjReverseName, reverse, why, true);
-    if (!*reverse) *forward = nullptr;
+    if (st == RTB_OK && *reverse) st = load_kernel(src, false, kAdjJvpName, jvp, why, true);
+    if (!*reverse || !*jvp) *forward = *reverse = *jvp = nullptr;
     return st;
 }
 

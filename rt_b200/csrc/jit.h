@@ -33,14 +33,16 @@ int compile_scheme(const DevScheme& sch, int precision, std::string* why);
 // errors of loading a compiled kernel.
 int scheme_kernel(const DevScheme& sch, int precision, const void** kernel, std::string* why, bool compile = true);
 
-// The adjoint's forward with checkpoints and its reverse sweep
-// (adjoint_rev.cuh) compiled for the structure of `sch` (AdjShape per
-// surface: kinds, classes, types fixed; transforms and all numbers read at
-// run time, so the kernels serve every parameter value), compiled on first
-// use and cached, as function handles for cudaLaunchKernel; both NULL, with
-// `why`, when NVRTC is unavailable or fails.  Their parameters: (AdjArgs,
-// DevRays in, counts, err) and (AdjArgs, gX, gY, partial).
-int adjoint_kernels(const DevScheme& sch, const void** forward, const void** reverse, std::string* why);
+// The adjoint's forward with checkpoints, its reverse sweep and its
+// forward-mode sensitivities (adjoint_rev.cuh) compiled for the structure of
+// `sch` (AdjShape per surface: kinds, classes, types fixed; transforms and
+// all numbers read at run time, so the kernels serve every parameter value),
+// compiled on first use and cached, as function handles for
+// cudaLaunchKernel; all NULL, with `why`, when NVRTC is unavailable or
+// fails.  Their parameters: (AdjArgs, DevRays in, counts, err), (AdjArgs,
+// gX, gY, partial) and (AdjArgs, SurfD<1> table, dX, dY).
+int adjoint_kernels(const DevScheme& sch, const void** forward, const void** reverse, const void** jvp,
+                    std::string* why);
 
 // The CUDA source of those kernels, and its compilation alone (no device).
 std::string adjoint_source(const DevScheme& sch);

@@ -14,6 +14,7 @@
 
 #include "dual.cuh"
 #include "ray_fp64.cuh"
+#include "shape.cuh"
 
 namespace rtb {
 namespace ad {
@@ -415,9 +416,9 @@ __device__ __forceinline__ bool toric_isect(const DevSurface& ds, const SurfD<W>
     return true;
 }
 
-template <int W>
+template <int W, class Sh = RtShape>
 __device__ __forceinline__ bool intersect(const DevSurface& ds, const SurfD<W>& s, uint32_t fixes, RayD<W>& r) {
-    switch (ds.kind) {
+    switch (Sh::kind(ds)) {
         case IS_PLANE: return plane_isect(r);
         case IS_PARABOLOID: return paraboloid_isect(s, r);
         case IS_CONIC: return conic_isect(s, r);
@@ -430,20 +431,20 @@ __device__ __forceinline__ bool intersect(const DevSurface& ds, const SurfD<W>& 
 
 // ---- actions -------------------------------------------------------------------
 
-template <int W>
+template <int W, class Sh = RtShape>
 __device__ __forceinline__ void reflect(const DevSurface& ds, const SurfD<W>& s, RayD<W>& r) {
-    if (ds.cls == RTB_PLANE) {
+    if (Sh::cls(ds) == RTB_PLANE) {
         r.cZ = -r.cZ;
-    } else if (ds.cls == RTB_CONIC) {
+    } else if (Sh::cls(ds) == RTB_CONIC) {
         Dual<W> dFdX, dFdY;
-        conic_derivs(s, ds.n_poly, r.X, r.Y, dFdX, dFdY);
+        conic_derivs(s, Sh::n_poly(ds), r.X, r.Y, dFdX, dFdY);
         Dual<W> a2 = 2.0 * (r.cX * dFdX + r.cY * dFdY + r.cZ) / (dFdX * dFdX + dFdY * dFdY + 1.0);
         r.cX -= a2 * dFdX;
         r.cY -= a2 * dFdY;
         r.cZ -= a2;
-    } else if (ds.cls == RTB_TORIC) {
+    } else if (Sh::cls(ds) == RTB_TORIC) {
         Dual<W> dFdX, dFdY, dFdZ;
-        toric_derivs(s, ds.n_poly, r.X, r.Y, r.Z, dFdX, dFdY, dFdZ);
+        toric_derivs(s, Sh::n_poly(ds), r.X, r.Y, r.Z, dFdX, dFdY, dFdZ);
         Dual<W> a2 = 2.0 * (r.cX * dFdX + r.cY * dFdY + r.cZ * dFdZ) / (dFdX * dFdX + dFdY * dFdY + dFdZ * dFdZ);
         r.cX -= a2 * dFdX;
         r.cY -= a2 * dFdY;
@@ -451,9 +452,9 @@ __device__ __forceinline__ void reflect(const DevSurface& ds, const SurfD<W>& s,
     }
 }
 
-template <int W>
+template <int W, class Sh = RtShape>
 __device__ __forceinline__ bool refract(const DevSurface& ds, const SurfD<W>& s, double mu, RayD<W>& r) {
-    if (ds.cls == RTB_PLANE) {
+    if (Sh::cls(ds) == RTB_PLANE) {
         Dual<W> a = mu * r.cZ;
         double b = mu * mu - 1.0;
         Dual<W> a2 = a * a;
@@ -466,10 +467,10 @@ __device__ __forceinline__ bool refract(const DevSurface& ds, const SurfD<W>& s,
         return true;
     }
     Dual<W> dFdX, dFdY, dFdZ = cst<W>(1.0);
-    if (ds.cls == RTB_CONIC) conic_derivs(s, ds.n_poly, r.X, r.Y, dFdX, dFdY);
-    else toric_derivs(s, ds.n_poly, r.X, r.Y, r.Z, dFdX, dFdY, dFdZ);
-    Dual<W> G = (ds.cls == RTB_CONIC) ? dFdX * dFdX + dFdY * dFdY + 1.0 : dFdX * dFdX + dFdY * dFdY + dFdZ * dFdZ;
-    Dual<W> a = (ds.cls == RTB_CONIC) ? mu * (r.cX * dFdX + r.cY * dFdY + r.cZ) / G
+    if (Sh::cls(ds) == RTB_CONIC) conic_derivs(s, Sh::n_poly(ds), r.X, r.Y, dFdX, dFdY);
+    else toric_derivs(s, Sh::n_poly(ds), r.X, r.Y, r.Z, dFdX, dFdY, dFdZ);
+    Dual<W> G = (Sh::cls(ds) == RTB_CONIC) ? dFdX * dFdX + dFdY * dFdY + 1.0 : dFdX * dFdX + dFdY * dFdY + dFdZ * dFdZ;
+    Dual<W> a = (Sh::cls(ds) == RTB_CONIC) ? mu * (r.cX * dFdX + r.cY * dFdY + r.cZ) / G
                                       : mu * (r.cX * dFdX + r.cY * dFdY + r.cZ * dFdZ) / G;
     Dual<W> b = (mu * mu - 1.0) / G;
     Dual<W> a2 = a * a;
@@ -478,15 +479,15 @@ __device__ __forceinline__ bool refract(const DevSurface& ds, const SurfD<W>& s,
     G = -a + sqrt(b);
     r.cX = mu * r.cX + G * dFdX;
     r.cY = mu * r.cY + G * dFdY;
-    r.cZ = (ds.cls == RTB_CONIC) ? mu * r.cZ + G : mu * r.cZ + G * dFdZ;
+    r.cZ = (Sh::cls(ds) == RTB_CONIC) ? mu * r.cZ + G : mu * r.cZ + G * dFdZ;
     return true;
 }
 
-template <int W>
+template <int W, class Sh = RtShape>
 __device__ __forceinline__ bool diffract(const DevSurface& ds, const SurfD<W>& s, double mu, const Dual<W>& L,
                                          RayD<W>& r) {
-    if (ds.gr_type == RTB_TRANSPARENT) {
-        if (ds.cls == RTB_PLANE) {
+    if (Sh::gr_type(ds) == RTB_TRANSPARENT) {
+        if (Sh::cls(ds) == RTB_PLANE) {
             Dual<W> a = mu * r.cZ;
             Dual<W> b = mu * mu - 1.0 + L * L - 2.0 * mu * L * r.cX;
             Dual<W> a2 = a * a;
@@ -499,9 +500,9 @@ __device__ __forceinline__ bool diffract(const DevSurface& ds, const SurfD<W>& s
             return true;
         }
         Dual<W> dFdX, dFdY, dFdZ = cst<W>(1.0);
-        const bool tor = ds.cls == RTB_TORIC;
-        if (tor) toric_derivs(s, ds.n_poly, r.X, r.Y, r.Z, dFdX, dFdY, dFdZ);
-        else conic_derivs(s, ds.n_poly, r.X, r.Y, dFdX, dFdY);
+        const bool tor = Sh::cls(ds) == RTB_TORIC;
+        if (tor) toric_derivs(s, Sh::n_poly(ds), r.X, r.Y, r.Z, dFdX, dFdY, dFdZ);
+        else conic_derivs(s, Sh::n_poly(ds), r.X, r.Y, dFdX, dFdY);
         Dual<W> G = tor ? dFdX / (dFdY * dFdY + dFdZ + dFdZ) : dFdX / (dFdY * dFdY + 1.0);
         Dual<W> u = 1.0 / sqrt(1.0 + dFdX * G);
         Dual<W> v = -dFdY * u * G;
@@ -518,7 +519,7 @@ __device__ __forceinline__ bool diffract(const DevSurface& ds, const SurfD<W>& s
         r.cZ = tor ? mu * r.cZ - L * w + G * dFdZ : mu * r.cZ - L * w + G;
         return true;
     }
-    if (ds.cls == RTB_PLANE) {
+    if (Sh::cls(ds) == RTB_PLANE) {
         Dual<W> a = r.cZ;
         Dual<W> b = L * L - 2.0 * L * r.cX;
         Dual<W> a2 = a * a;
@@ -530,9 +531,9 @@ __device__ __forceinline__ bool diffract(const DevSurface& ds, const SurfD<W>& s
         return true;
     }
     Dual<W> dFdX, dFdY, dFdZ = cst<W>(1.0);
-    const bool tor = ds.cls == RTB_TORIC;
-    if (tor) toric_derivs(s, ds.n_poly, r.X, r.Y, r.Z, dFdX, dFdY, dFdZ);
-    else conic_derivs(s, ds.n_poly, r.X, r.Y, dFdX, dFdY);
+    const bool tor = Sh::cls(ds) == RTB_TORIC;
+    if (tor) toric_derivs(s, Sh::n_poly(ds), r.X, r.Y, r.Z, dFdX, dFdY, dFdZ);
+    else conic_derivs(s, Sh::n_poly(ds), r.X, r.Y, dFdX, dFdY);
     Dual<W> G = tor ? dFdX / (dFdY * dFdY + dFdZ + dFdZ) : dFdX / (dFdY * dFdY + 1.0);
     Dual<W> u = 1.0 / sqrt(1.0 + dFdX * G);
     Dual<W> v = -dFdY * u * G;
@@ -558,33 +559,33 @@ __device__ __forceinline__ bool diffract(const DevSurface& ds, const SurfD<W>& s
 
 // Mirror/Lens/Grating ::Action (f64::action); refractive indices depend on
 // the wavelength only, the grating constant on its groove density.
-template <int W>
+template <int W, class Sh = RtShape>
 __device__ __forceinline__ int action(const DevSurface& ds, const SurfD<W>& s, const double* knots, long long order,
                                       double lambda, RayD<W>& r) {
-    if (ds.type == RTB_MIRROR) {
-        reflect(ds, s, r);
+    if (Sh::type(ds) == RTB_MIRROR) {
+        reflect<W, Sh>(ds, s, r);
         return f64::ACT_OK;
     }
-    if (ds.type == RTB_LENS) {
+    if (Sh::type(ds) == RTB_LENS) {
         double a, b;
         if (!f64::table_eval(knots + ds.n1_off, ds.n1_n, lambda, a) ||
             !f64::table_eval(knots + ds.n2_off, ds.n2_n, lambda, b))
             return f64::ACT_RANGE;
         double mu = a;
         mu /= b;
-        return refract(ds, s, mu, r) ? f64::ACT_OK : f64::ACT_LOST;
+        return refract<W, Sh>(ds, s, mu, r) ? f64::ACT_OK : f64::ACT_LOST;
     }
-    if (ds.type == RTB_GRATING) {
+    if (Sh::type(ds) == RTB_GRATING) {
         double n2v, mu = 0.0;
         if (!f64::table_eval(knots + ds.n2_off, ds.n2_n, lambda, n2v)) return f64::ACT_RANGE;
-        if (ds.gr_type == RTB_TRANSPARENT) {
+        if (Sh::gr_type(ds) == RTB_TRANSPARENT) {
             double n1v;
             if (!f64::table_eval(knots + ds.n1_off, ds.n1_n, lambda, n1v)) return f64::ACT_RANGE;
             mu = n1v;
             mu /= n2v;
         }
         Dual<W> L = cst<W>((double)order * lambda / n2v) / s.gr;
-        return diffract(ds, s, mu, L, r) ? f64::ACT_OK : f64::ACT_LOST;
+        return diffract<W, Sh>(ds, s, mu, L, r) ? f64::ACT_OK : f64::ACT_LOST;
     }
     return f64::ACT_OK;
 }
@@ -592,15 +593,15 @@ __device__ __forceinline__ int action(const DevSurface& ds, const SurfD<W>& s, c
 // One surface on one ray, as the fused FP64 kernel runs it: transform,
 // normalise, and for a non-Aux surface intersection, aperture, action and
 // normalise.  True if the ray survives.
-template <int W>
+template <int W, class Sh = RtShape>
 __device__ __forceinline__ bool surface_step(const DevSurface& ds, const SurfD<W>& s, uint32_t fixes,
                                              const double* knots, long long order, double lambda, RayD<W>& r) {
     transform(ds, s, r);
     normalize(r.cX, r.cY, r.cZ);
-    if (!ds.non_aux) return true;
-    if (!intersect(ds, s, fixes, r)) return false;
-    if (!f64::aperture_pass(ds.type == RTB_SHADE, ds.shape, ds.size, ds.center, r.X.v, r.Y.v)) return false;
-    if (action(ds, s, knots, order, lambda, r) != f64::ACT_OK) return false;
+    if (!Sh::non_aux(ds)) return true;
+    if (!intersect<W, Sh>(ds, s, fixes, r)) return false;
+    if (!f64::aperture_pass(Sh::type(ds) == RTB_SHADE, Sh::shape(ds), ds.size, ds.center, r.X.v, r.Y.v)) return false;
+    if (action<W, Sh>(ds, s, knots, order, lambda, r) != f64::ACT_OK) return false;
     normalize(r.cX, r.cY, r.cZ);
     return true;
 }

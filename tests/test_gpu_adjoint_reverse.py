@@ -109,10 +109,10 @@ def test_reverse_equals_passes_and_jvp_on_every_kind(name, fixes, monkeypatch):
 
 @pytest.mark.parametrize("name", ["c4", "mirrors", "lenses", "gratings"])
 def test_reverse_sweep_compiled_for_the_scheme_equals_generic(name, monkeypatch):
-    """rtb_adjoint_create compiles the forward and the reverse sweep for the
-    scheme's structure (RTB_SPECIALIZE=0: the generic kernels); both run the
-    same IEEE operations in the same order: the same positions and gradient
-    bits, also with
+    """rtb_adjoint_create compiles the forward, the reverse sweep and the
+    sensitivities for the scheme's structure (RTB_SPECIALIZE=0: the generic
+    kernels); both run the same IEEE operations in the same order: the same
+    positions, gradient and sensitivity bits, also with
     the parameters moved off their create-time values (angles and distances
     away from zero change which transforms apply, which the compiled kernel
     reads at run time)."""
@@ -146,13 +146,19 @@ def test_reverse_sweep_compiled_for_the_scheme_equals_generic(name, monkeypatch)
             gX, gY = torch.where(finite, gX, 0.0), torch.where(finite, gY, 0.0)
             monkeypatch.delenv("RTB_ADJOINT_BACKWARD", raising=False)
             out.append(adj.backward(gX, gY))
+            d = np.random.default_rng(7).normal(size=len(theta))
+            dX, dY = adj.jvp(d)
+            out.append((dX.clone(), dY.clone()))
         grads.append(out)
         adj.destroy()
     for a, b in zip(*grads):
-        if isinstance(a, tuple):  # the forward's outputs
+        if isinstance(a, tuple) and len(a) == 3:  # the forward's outputs
             assert torch.equal(a[2], b[2])
             g = a[2] == 1
             assert torch.equal(a[0][g].view(torch.int64), b[0][g].view(torch.int64))
             assert torch.equal(a[1][g].view(torch.int64), b[1][g].view(torch.int64))
+        elif isinstance(a, tuple):  # the sensitivities along one direction
+            for x, y in zip(a, b):
+                assert torch.equal(torch.nan_to_num(x).view(torch.int64), torch.nan_to_num(y).view(torch.int64))
         else:
             assert np.array_equal(a, b), np.max(np.abs(a - b))
