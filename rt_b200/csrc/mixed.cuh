@@ -623,8 +623,8 @@ __device__ __forceinline__ void fused_mixed(const DevScheme* __restrict__ g_sch,
         int b = 0;
         if (valid && f == 1) {
             b = cur.at(beams, n_beams, bi);
-            const BeamCtx bc = beam_ctx(beams, b);
-            mx::normalize(r);
+            const BeamCtx& bc = cur.ctx;
+            if (!rows.packed) mx::normalize(r);  // row blocks hold normalised cosines
             mx::TableMemo memo;
             int stage = -1;
             Surfaces::run(sch, s_knots, bc, lam, memo, r, stage);

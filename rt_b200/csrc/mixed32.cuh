@@ -276,9 +276,9 @@ __device__ __forceinline__ void fused_mixed32(const DevScheme* __restrict__ g_sc
         int key = 0;
         double outX = 0, outY = 0;
         if (valid && f == 1) {
-            const BeamCtx bc = beam_ctx(beams, b);
+            const BeamCtx& bc = cur.ctx;
             const double off0[3] = {bc.bm->off0[0], bc.bm->off0[1], bc.bm->off0[2]};
-            m32::normalize(r);
+            if (!rows.packed) m32::normalize(r);  // row blocks hold normalised cosines
             mx::TableMemo memo;
             mx::Ray q{0, 0, 0, 0, 0, 0};
             int stage = -1;

@@ -13,6 +13,7 @@
 #include <cub/cub.cuh>
 
 #include "engine.cuh"
+#include "mixed32.cuh"
 #include "rowpipe.cuh"
 
 namespace rtb {
@@ -311,12 +312,15 @@ __global__ void k_gather_rows64(const uint32_t* order, uint64_t n, DevRays src, 
         const int l = (int)(t & 31);
         if (t < n) {
             const uint64_t i = order ? order[t] : t;
-            w.X[l] = src.X[i];
-            w.Y[l] = src.Y[i];
-            w.Z[l] = src.Z[i];
-            w.cX[l] = src.cX[i];
-            w.cY[l] = src.cY[i];
-            w.cZ[l] = src.cZ[i];
+            // the cosines normalised as the kernel would on load (mx::normalize)
+            mx::Ray r{src.X[i], src.Y[i], src.Z[i], src.cX[i], src.cY[i], src.cZ[i]};
+            mx::normalize(r);
+            w.X[l] = r.X;
+            w.Y[l] = r.Y;
+            w.Z[l] = r.Z;
+            w.cX[l] = r.cX;
+            w.cY[l] = r.cY;
+            w.cZ[l] = r.cZ;
             w.lambda[l] = src.lambda[i];
             w.flag[l] = src.flag[i];
         } else {
@@ -327,7 +331,8 @@ __global__ void k_gather_rows64(const uint32_t* order, uint64_t n, DevRays src, 
 }
 
 // The same with FP32 positions relative to the ray's beam's origin
-// (DevBeam::origin) and FP32 cosines; the wavelength stays FP64.
+// (DevBeam::origin) and FP32 cosines; the wavelength stays FP64.  Both
+// gathers store the cosines normalised, so the kernels skip that on rows.
 __global__ void k_gather_rows32(const uint32_t* order, uint64_t n, DevRays src, const DevBeam* beams, int n_beams,
                                 void* rows) {
     Row32* dst = static_cast<Row32*>(rows);
@@ -339,12 +344,16 @@ __global__ void k_gather_rows32(const uint32_t* order, uint64_t n, DevRays src, 
         if (t < n) {
             const uint64_t i = order ? order[t] : t;
             const DevBeam& b = beams[beam_of(beams, n_beams, i)];
-            w.X[l] = (float)(src.X[i] - b.origin[0]);
-            w.Y[l] = (float)(src.Y[i] - b.origin[1]);
-            w.Z[l] = (float)(src.Z[i] - b.origin[2]);
-            w.cX[l] = (float)src.cX[i];
-            w.cY[l] = (float)src.cY[i];
-            w.cZ[l] = (float)src.cZ[i];
+            // the FP32 cosines normalised as the kernel would on load (m32::normalize)
+            m32::Ray r{(float)(src.X[i] - b.origin[0]), (float)(src.Y[i] - b.origin[1]), (float)(src.Z[i] - b.origin[2]),
+                       (float)src.cX[i], (float)src.cY[i], (float)src.cZ[i]};
+            m32::normalize(r);
+            w.X[l] = r.X;
+            w.Y[l] = r.Y;
+            w.Z[l] = r.Z;
+            w.cX[l] = r.cX;
+            w.cY[l] = r.cY;
+            w.cZ[l] = r.cZ;
             w.lambda[l] = src.lambda[i];
             w.flag[l] = src.flag[i];
         } else {

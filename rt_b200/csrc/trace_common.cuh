@@ -42,28 +42,10 @@ __device__ __forceinline__ int beam_of(const DevBeam* beams, int n_beams, uint64
     return lo;
 }
 
-// The beam of the rays being traced, cached per thread: rays come in
-// increasing order (of index, or of slot in a plan's beam-major order), so
-// the beam of the previous ray is usually this one's, and the beam table is
-// searched only when a ray falls outside the cached beam's range.
-struct BeamCursor {
-    int b = 0;
-    uint64_t lo = 1, hi = 0;  // empty: the first ray searches
-    __device__ __forceinline__ int at(const DevBeam* beams, int n_beams, uint64_t i) {
-        if (i < lo || i >= hi) {
-            b = beam_of(beams, n_beams, i);
-            lo = (b == 0) ? 0ull : beams[b].first_ray;
-            hi = (b + 1 < n_beams) ? beams[b + 1].first_ray : ~0ull;
-        }
-        return b;
-    }
-};
-
-// What the surfaces need of a ray's beam, read once before its trace, so
-// that the loads overlap the first surfaces' arithmetic instead of stalling
-// a grating: whether the beam sets the gratings' orders, the orders of the
-// first two gratings (further ones are read from the table), and for the
-// FP32-state engine the first surface's offset.
+// What the surfaces need of a ray's beam, read once per beam (BeamCursor):
+// whether the beam sets the gratings' orders, the orders of the first two
+// gratings (further ones are read from the table), and the beam's entry for
+// the FP32-state engine's first-surface offset.
 struct BeamCtx {
     const DevBeam* bm;
     long long ord0, ord1;
@@ -79,6 +61,26 @@ __device__ __forceinline__ BeamCtx beam_ctx(const DevBeam* beams, int b) {
     const DevBeam& d = beams[b];
     return BeamCtx{&d, d.orders[0], d.orders[1], d.n_orders > 0};
 }
+
+// The beam of the rays being traced and what the surfaces need of it,
+// cached per thread: rays come in increasing order (of index, or of slot in
+// a plan's beam-major order), so the beam of the previous ray is usually
+// this one's, and the beam table is read only when a ray falls outside the
+// cached beam's range.
+struct BeamCursor {
+    int b = 0;
+    uint64_t lo = 1, hi = 0;  // empty: the first ray searches
+    BeamCtx ctx{nullptr, 0, 0, false};
+    __device__ __forceinline__ int at(const DevBeam* beams, int n_beams, uint64_t i) {
+        if (i < lo || i >= hi) {
+            b = beam_of(beams, n_beams, i);
+            lo = (b == 0) ? 0ull : beams[b].first_ray;
+            hi = (b + 1 < n_beams) ? beams[b + 1].first_ray : ~0ull;
+            ctx = beam_ctx(beams, b);
+        }
+        return b;
+    }
+};
 
 // Count one event per lane (a loss at a stage, or reaching the end), one
 // atomic per distinct counter in the warp.
