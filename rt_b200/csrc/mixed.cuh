@@ -9,10 +9,10 @@
 //     1e-5 mm, the root then good to ~1e-12 mm), the grating equation and the
 //     detector coordinate: FP64, contracted to FMA;
 //   * every division and square root: a MUFU seed (rcp/rsqrt.approx.f64)
-//     refined by Newton steps in FP64 instead of the IEEE FP64 division and
-//     square root sequences of the plain engine; the inverse of a Newton
-//     derivative from the seed alone; 1/c and 1/(grating constant) from the
-//     host;
+//     refined by one Newton step in FP64 (~2^-43 relative) instead of the
+//     IEEE FP64 division and square root sequences of the plain engine; the
+//     inverse of a Newton derivative from the seed alone; 1/c and
+//     1/(grating constant) from the host;
 //   * surface normals and their polynomial terms (the sqrt/div-heavy
 //     derivatives of conic_derivs / toric_derivs, surface.cu:45-94): FP32
 //     (from FP32 copies of the surface constants), promoted to FP64 before
@@ -36,13 +36,19 @@ struct Ray {
     double X, Y, Z, cX, cY, cZ;
 };
 
-// 1/x: rcp.approx.ftz.f64 seed (~2^-22) and two Newton steps.
+// Precision of the reciprocals and square roots.  Each comes from a MUFU seed
+// (~2^-22 relative) and one Newton step, which leaves ~2^-43 relative: a
+// ray parameter or distance of 1 m is then off by ~1e-10 mm, and a direction
+// by ~1e-13 rad, five orders of magnitude below the 0.05 um (5e-5 mm) budget
+// at the detector, whose error comes from the FP32 normals (~1e-8 rad).  A
+// second step (full FP64 precision) would cost two more FP64 instructions per
+// reciprocal and three per square root, ~70 per C1 ray.
+
+// 1/x: rcp.approx.ftz.f64 seed and one Newton step (~2^-43 relative).
 __device__ __forceinline__ double rcp(double x) {
     double r;
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
-    double e = fma(-x, r, 1.0);
-    r = fma(r, e, r);
-    e = fma(-x, r, 1.0);
+    const double e = fma(-x, r, 1.0);
     return fma(r, e, r);
 }
 
@@ -63,17 +69,20 @@ __device__ __forceinline__ double rsqrt_n(double x, int steps) {
     return y;
 }
 
-// sqrt(x) to FP64 accuracy; NaN for x < 0, 0 for x == 0.
+// sqrt(x) ~2^-43 relative: s = x * rsqrt seed, then one Newton correction
+// of the product, s + (x - s^2) / (2 sqrt x) with 1/sqrt x from the seed;
+// NaN for x < 0, 0 for x == 0.
 __device__ __forceinline__ double sqrt_(double x) {
     if (!(x > 0.0)) return (x == 0.0) ? 0.0 : __longlong_as_double(0x7ff8000000000000ll);
-    double y = rsqrt_n(x, 1);
-    double s = x * y;
-    return fma(0.5 * y, fma(-s, s, x), s);  // one correction of the product
+    const double y = rsqrt_n(x, 0);
+    const double s = x * y;
+    return fma(0.5 * y, fma(-s, s, x), s);
 }
 
+// Unit direction cosines: 1/|c| from the rsqrt seed and one Newton step.
 __device__ __forceinline__ void normalize(Ray& r) {
     double s = fma(r.cX, r.cX, fma(r.cY, r.cY, r.cZ * r.cZ));
-    double k = rsqrt_n(s, 2);
+    double k = rsqrt_n(s, 1);
     r.cX *= k;
     r.cY *= k;
     r.cZ *= k;
@@ -401,7 +410,7 @@ __device__ __forceinline__ bool diffract(const DevSurface& s, double mu, double 
     // L^2+M+M for the toric, surface.cu:1438,1487)
     double den = (cls == RTB_TORIC) ? fma(ny, ny, nz + nz) : fma(ny, ny, 1.0);
     double G = nx * rcp(den);
-    double u = rsqrt_n(fma(nx, G, 1.0), 2);
+    double u = rsqrt_n(fma(nx, G, 1.0), 1);
     double v = -ny * u * G;
     double w = (cls == RTB_TORIC) ? -nz * u * G : -u * G;
     double iG = rcp(fma(nx, nx, fma(ny, ny, nz * nz)));
