@@ -56,7 +56,7 @@ FIXES = 3  # RTB_FIX_TORIC_SIGN | RTB_FIX_TORIC_STEP: the toric fold's Steffense
 # 1.0e7 rays (31 x 64 x 5041; ncu op counters, FMA = 2, FFMA2 = 4).
 KERNEL_PROFILE = {
     "fused_mixed": {"traffic_per_ray": 76.92, "f64_flops_per_ray": 526.64, "f32_flops_per_ray": 52.17},
-    "fused_mixed32": {"traffic_per_ray": 52.06, "f64_flops_per_ray": 392.56, "f32_flops_per_ray": 225.15},
+    "fused_mixed32": {"traffic_per_ray": 52.06, "f64_flops_per_ray": 385.37, "f32_flops_per_ray": 237.10},
 }
 # bytes of input per ray the mixed kernels read: a plan's 32-ray row blocks
 # (Row64: 1824 B, Row32: 1056 B per 32 rays)

@@ -67,8 +67,10 @@ struct DevSurface {
     // Aux surfaces in between folded in, as P' = M P + off32 and D' = M D:
     // M in FP32 (rows), off32 in FP64.  rot32: M is not the identity;
     // first32: the first non-Aux surface, whose offset comes from the ray's
-    // beam (DevBeam::off0).  Set on non-Aux surfaces only.
-    float m32[9];
+    // beam (DevBeam::off0).  Set on non-Aux surfaces only.  Each entry of M is
+    // held twice, (m, m): the operand pair of the paired FP32 multiply-adds
+    // that rotate a position and a direction cosine together.
+    float2 m32[9];
     int32_t rot32, first32, pad32;
     double off32[3];
 };

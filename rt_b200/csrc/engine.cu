@@ -317,7 +317,7 @@ static void fp32_transforms(DevScheme& sch) {
         if (!s.non_aux) continue;
         bool ident = true;
         for (int i = 0; i < 9; ++i) {
-            s.m32[i] = (float)M[i];
+            s.m32[i] = make_float2((float)M[i], (float)M[i]);
             ident = ident && M[i] == ((i % 4 == 0) ? 1.0 : 0.0);
         }
         s.rot32 = ident ? 0 : 1;
