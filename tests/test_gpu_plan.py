@@ -410,3 +410,55 @@ def test_plan_outputs_by_slot(precision):
             x, y = x.view(torch.int64), y.view(torch.int64)
         assert torch.equal(x, y), f
     assert torch.equal(a[4], b[4]) and a[5] == b[5]
+
+
+def frame_histogram(out, ccd):
+    """The frame the mixed kernels accumulate, from a trace's own outputs: each
+    good ray's pixel as the kernels compute it (coordinate plus half the CCD
+    size, times the reciprocal pixel size, truncated with saturation)."""
+    X, Y = out["X"].cpu().numpy(), out["Y"].cpu().numpy()
+    good = out["flag"].cpu().numpy() == 1
+    fin = good & np.isfinite(X) & np.isfinite(Y)
+
+    def pix(v, size, p):
+        t = (v + 0.5 * size) * (1.0 / p)
+        return np.clip(np.nan_to_num(np.trunc(t), nan=0.0), 0, 2.0**32 - 1)
+
+    ix, iy = pix(X[fin], ccd.xsize, ccd.xpix), pix(Y[fin], ccd.ysize, ccd.ypix)
+    inside = (ix < ccd.xdim) & (iy < ccd.ydim)
+    p = iy[inside].astype(np.int64) * int(ccd.xdim) + ix[inside].astype(np.int64)
+    hist = np.bincount(p, minlength=int(ccd.xdim) * int(ccd.ydim)).astype(np.uint32)
+    return hist, int(good.sum() - inside.sum())
+
+
+@pytest.mark.parametrize("precision", [ffi.MIXED, ffi.MIXED32])
+def test_mixed_plan_frame_is_the_histogram_of_its_outputs(precision):
+    """A mixed plan's frame counts equal the histogram of the plan's own
+    detector coordinates, run after run, for a frame at any 4-byte alignment
+    and of any size, and it writes nothing outside the frame."""
+    beams = S.c1_beams(n_per_lambda=200)
+    cs = S.to_c(S.echelle(), E.spline_init)
+    c1 = S.ccd(S.C1_CCD)
+    odd = ffi.CCD(c1.xsize, c1.ysize, 4095, 4095, c1.xpix, c1.ypix)  # an odd number of pixels
+    for ccd, offset in ((c1, 0), (c1, 1), (odd, 0)):
+        n_pix = int(ccd.xdim) * int(ccd.ydim)
+        buf = torch.zeros(n_pix + 4, dtype=torch.int32, device="cuda")
+        counts = buf[offset:offset + n_pix]  # offset 1: 4-byte aligned only
+        outside = torch.zeros(1, dtype=torch.int64, device="cuda")
+        o = E.opts(engine=ffi.ENGINE_FUSED, precision=precision, fixes=FIXES, ccd=ccd, counts=counts,
+                   n_outside=outside)
+        plan = E.Plan(cs.surfaces, beams, o)
+        plan.run()
+        st, stats = plan.result()
+        assert st in TRACED and stats.n_good > 0
+        _, out = plan_output(plan)
+        hist, n_out = frame_histogram(out, ccd)
+        got = counts.cpu().numpy().view(np.uint32)
+        assert np.array_equal(got, hist), (ccd.xdim, offset, int((got != hist).sum()))
+        assert int(outside) == n_out
+        plan.run()
+        assert plan.result()[0] == st
+        assert np.array_equal(counts.cpu().numpy().view(np.uint32), 2 * hist)
+        # nothing written outside the frame
+        assert int(buf[:offset].abs().sum()) == 0 and int(buf[offset + n_pix:].abs().sum()) == 0
+        plan.destroy()
