@@ -241,6 +241,12 @@ def sgemm_tflops(n=8192, reps=5):
         torch.backends.cuda.matmul.allow_tf32 = prev
 
 
+def workload_config(n_rays, n_beams):
+    """The `config` of both arms' lines: the workload, not the engine."""
+    return {"workload": WORKLOAD, "n_rays": n_rays, "beams": n_beams, "l2": "inputs (3.3-5.7 GB) larger than L2",
+            "toric_fixes": FIXES}
+
+
 def reference_arm(args):
     # rank 0 alone runs (on the host cores) and prints; the other ranks exit
     from rt_b200 import replicas
@@ -253,8 +259,9 @@ def reference_arm(args):
     line = {"impl": "reference", "metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "engine": "CPU oracle (restatement of cuda_engine math; the reference's "
-                       "CPU engine simd_engine is a non-functional stub)"},
+            "config": workload_config(S.total_rays(beams), len(beams)),
+            "engine": "CPU oracle (restatement of cuda_engine math; the reference's CPU engine simd_engine is a "
+                      "non-functional stub), on a bounded sample of the workload (cpu_baseline.sample)",
             "cpu_baseline": res,
             "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -607,8 +614,7 @@ def main():
                 "warmup": args.warmup, "ms_per_step": hv["ms_per_step"], "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if head in MIXED_ENGINES else "f64",
                 "data": "synthetic",
-                "config": {"workload": WORKLOAD, "n_rays": n, "engine": head, "beams": len(beams),
-                           "l2": "inputs (3.3-5.7 GB) larger than L2", "toric_fixes": FIXES},
+                "config": workload_config(n, len(beams)), "engine": head,
                 "engines": engines,
                 "speedup_vs_plain_fp64": (hv["value"] / engines["per_surface"]["value"])
                 if "per_surface" in engines and "value" in engines["per_surface"] else None,
