@@ -4,7 +4,9 @@ The mixed plans (RTB_MIXED: FP64 ray state; RTB_MIXED32: FP32 ray state)
 trace a fixed sample of C1 -- every one of the 31 echelle orders, all 64
 wavelengths -- and of C3's beam draws, and the oracle traces the same
 generated rays on the CPU.  Checked: the CCD error of rays good in both
-(p99.9 <= 0.05 um), the pixel mismatch rate, and which rays are lost.
+(p99.9 <= 0.05 um; for the FP64-state engine also p99.9 <= 0.01 um and max
+<= 0.02 um, its own precision), the pixel mismatch rate, and which rays are
+lost.
 
 In the reference's own quirk mode (fixes = 0) the FP64 toric iteration
 divides 0/0 once converged (iter_toric, rt_cuda_engine_surface.cu:390) and
@@ -63,6 +65,10 @@ def test_mixed_plan_against_oracle(workload, precision, fixes):
           int(only_o.sum()))
     assert m["rays_compared"] > 0.05 * n
     assert m["p99_9_um"] <= 0.05
+    if precision == ffi.MIXED:
+        # the FP64-state engine's error comes from its FP32 normals (~0.005 um
+        # at p99.9 on C1): a guard on its precision, well inside the budget
+        assert m["p99_9_um"] <= 0.01 and m["max_um"] <= 0.02, m
     assert int(only_o.sum()) <= 2e-5 * n + 2  # aperture-edge rays
     if fixes & ffi.FIX_TORIC_STEP:
         assert m["pixel_mismatch_rate"] < 1e-3
