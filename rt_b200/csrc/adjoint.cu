@@ -228,11 +228,15 @@ struct Group {
 };
 
 // pass 0: count, sum X, sum Y; pass 1: sum of squared distances from the
-// centroid.  Block (part, g) sums a fixed slice of group g.
+// centroid.  Block (g, part) sums a fixed slice of group g.  The groups of a
+// composite beam interleave (group j holds rays j, j + n_lambda, ...), so the
+// blocks of all groups for one slice -- launched together, group index
+// fastest -- read the same stretch of the arrays, and a sector fetched for
+// one group is found in L2 by the others.
 __global__ void __launch_bounds__(kMeritThreads) k_group_moments(const Group* groups, const char* flag, const double* X,
                                                                  const double* Y, const double* centroid, int pass,
                                                                  double* partial) {
-    const int g = blockIdx.y, part = blockIdx.x;
+    const int g = blockIdx.x, part = blockIdx.y;
     const Group G = groups[g];
     const uint64_t per = (G.count + kMeritParts - 1) / kMeritParts;
     const uint64_t m0 = (uint64_t)part * per, m1 = (m0 + per < G.count) ? m0 + per : G.count;
@@ -263,14 +267,117 @@ __global__ void __launch_bounds__(kMeritThreads) k_group_moments(const Group* gr
 }
 
 // Seeds: gX = a_g (X - xbar) + b_g, gY = a_g (Y - ybar) for good rays.
+// Block (g, part), group index fastest, as in k_group_moments.
 __global__ void k_group_seeds(const Group* groups, int n_groups, const double* coef, const char* flag, const double* X,
                               const double* Y, double* gX, double* gY) {
-    const int g = blockIdx.y;
+    const int g = blockIdx.x;
     if (g >= n_groups) return;
     const Group G = groups[g];
     const double a = coef[4 * g], bx = coef[4 * g + 1], cx = coef[4 * g + 2], cy = coef[4 * g + 3];
-    for (uint64_t m = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; m < G.count; m += (uint64_t)gridDim.x * blockDim.x) {
+    for (uint64_t m = (uint64_t)blockIdx.y * blockDim.x + threadIdx.x; m < G.count; m += (uint64_t)gridDim.y * blockDim.x) {
         const uint64_t i = G.first + m * G.stride;
+        if (flag[i] == 1) {
+            gX[i] = a * (X[i] - cx) + bx;
+            gY[i] = a * (Y[i] - cy);
+        } else {
+            gX[i] = 0.0;
+            gY[i] = 0.0;
+        }
+    }
+}
+
+// The same moments and seeds read in index order, for beams of at most
+// kMeritThreads wavelengths (composite beams: ray first + j holds wavelength
+// j mod n_lambda).  Block c of a beam covers rays [start, end) of it, start a
+// multiple of the beam's width E = n_lambda * floor(kMeritThreads /
+// n_lambda) past its first ray; thread t < E takes rays start + t, start + t
+// + E, ..., all of one wavelength (t mod n_lambda), so the loads and stores
+// of a warp are consecutive and each thread keeps its group's sums in
+// registers.  The sums stay deterministic: each thread adds its rays in
+// order, the threads of a group are added in order, and k_dense_finish adds
+// the blocks of a beam in order.
+struct DenseBlock {
+    uint64_t start, end;  // rays of this block
+    int32_t nl, width;    // wavelengths of the beam, threads in use (E)
+    int32_t gbase;        // group of the beam's first wavelength
+    int32_t pbase;        // first partial of this block: (its index in the beam's blocks) * nl + the beam's offset
+};
+
+__global__ void __launch_bounds__(kMeritThreads) k_dense_moments(const DenseBlock* blocks, const char* flag,
+                                                                 const double* X, const double* Y,
+                                                                 const double* centroid, int pass, double* partial) {
+    const DenseBlock B = blocks[blockIdx.x];
+    const int t = threadIdx.x;
+    double v[3] = {0, 0, 0};
+    if (t < B.width) {
+        const int g = B.gbase + t % B.nl;
+        const double cx = pass ? centroid[2 * g] : 0.0, cy = pass ? centroid[2 * g + 1] : 0.0;
+        for (uint64_t i = B.start + t; i < B.end; i += B.width) {
+            if (flag[i] != 1) continue;
+            if (pass == 0) {
+                v[0] += 1.0;
+                v[1] += X[i];
+                v[2] += Y[i];
+            } else {
+                const double dx = X[i] - cx, dy = Y[i] - cy;
+                v[0] += dx * dx + dy * dy;
+            }
+        }
+    }
+    __shared__ double red[3][kMeritThreads];
+    for (int c = 0; c < 3; ++c) red[c][t] = v[c];
+    __syncthreads();
+    if (t < B.nl) {
+        double w[3] = {0, 0, 0};
+        for (int m = t; m < B.width; m += B.nl)
+            for (int c = 0; c < 3; ++c) w[c] += red[c][m];
+        for (int c = 0; c < 3; ++c) partial[((size_t)B.pbase + t) * 3 + c] = w[c];
+    }
+}
+
+// Per group (one block each): the partials of its beam's blocks, thread t
+// adding blocks t, t + kMeritThreads, ... in order, then the threads' sums by
+// a fixed tree.  pass 0 leaves count and centroid in out[4g .. 4g+2] and the
+// centroid in `centroid`; pass 1 the sum of squared distances in out[4g+3].
+struct DenseGroup {
+    int32_t pbase, nl, n_blocks, lg;  // the beam's first partial, wavelengths, blocks; this group's wavelength
+};
+
+__global__ void __launch_bounds__(kMeritThreads) k_dense_finish(const DenseGroup* groups, const double* partial,
+                                                                int pass, double* centroid, double* out) {
+    const int g = blockIdx.x;
+    const DenseGroup G = groups[g];
+    double v[3] = {0, 0, 0};
+    for (int c = threadIdx.x; c < G.n_blocks; c += blockDim.x)
+        for (int k = 0; k < 3; ++k) v[k] += partial[((size_t)G.pbase + (size_t)c * G.nl + G.lg) * 3 + k];
+    __shared__ double red[3][kMeritThreads];
+    for (int k = 0; k < 3; ++k) red[k][threadIdx.x] = v[k];
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w)
+            for (int k = 0; k < 3; ++k) red[k][threadIdx.x] += red[k][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x != 0) return;
+    for (int k = 0; k < 3; ++k) v[k] = red[k][0];
+    if (pass == 0) {
+        out[4 * g] = v[0];
+        centroid[2 * g] = out[4 * g + 1] = v[0] > 0 ? v[1] / v[0] : 0.0;
+        centroid[2 * g + 1] = out[4 * g + 2] = v[0] > 0 ? v[2] / v[0] : 0.0;
+    } else {
+        out[4 * g + 3] = v[0];
+    }
+}
+
+__global__ void __launch_bounds__(kMeritThreads) k_dense_seeds(const DenseBlock* blocks, const double* coef,
+                                                               const char* flag, const double* X, const double* Y,
+                                                               double* gX, double* gY) {
+    const DenseBlock B = blocks[blockIdx.x];
+    const int t = threadIdx.x;
+    if (t >= B.width) return;
+    const int g = B.gbase + t % B.nl;
+    const double a = coef[4 * g], bx = coef[4 * g + 1], cx = coef[4 * g + 2], cy = coef[4 * g + 3];
+    for (uint64_t i = B.start + t; i < B.end; i += B.width) {
         if (flag[i] == 1) {
             gX[i] = a * (X[i] - cx) + bx;
             gY[i] = a * (Y[i] - cy);
@@ -715,20 +822,77 @@ int rtb_adjoint_spot_merit(rtb_adjoint* c, const double* target_x, double weight
     }
     const int G = (int)groups.size();
     if (G == 0 || G > 65535) return RTB_BAD_VALUE;
+    std::vector<double> cen(2 * G, 0.0), nn(G, 0.0), ss(G, 0.0);
+    // index-order (dense) path: every beam of at most kMeritThreads wavelengths
+    bool dense = true;
+    for (const auto& b : c->beams_in) dense = dense && (b.n_lambda ? b.n_lambda : 1) <= (uint64_t)kMeritThreads;
+    std::vector<DenseBlock> dblocks;
+    std::vector<DenseGroup> dgroups;
+    if (dense) {
+        constexpr uint64_t kRaysPerThread = 8;
+        uint64_t pbase = 0;
+        int32_t gbase = 0;
+        for (const auto& b : c->beams_in) {
+            const int32_t nl = (int32_t)(b.n_lambda ? b.n_lambda : 1);
+            const int32_t width = nl * (kMeritThreads / nl);
+            const uint64_t chunk = (uint64_t)width * kRaysPerThread;
+            const uint64_t nblk = (b.n_rays + chunk - 1) / chunk;
+            for (uint64_t k = 0; k < nblk; ++k) {
+                const uint64_t start = b.first_ray + k * chunk;
+                const uint64_t end = std::min(b.first_ray + b.n_rays, start + chunk);
+                dblocks.push_back(DenseBlock{start, end, nl, width, gbase, (int32_t)(pbase + k * (uint64_t)nl)});
+            }
+            for (int32_t j = 0; j < nl; ++j) dgroups.push_back(DenseGroup{(int32_t)pbase, nl, (int32_t)nblk, j});
+            pbase += nblk * (uint64_t)nl;
+            gbase += nl;
+            if (pbase > (uint64_t)INT32_MAX || dblocks.size() > (size_t)INT32_MAX) dense = false;
+        }
+    }
+    const size_t n_part = dense ? (dgroups.empty() ? 0 : (size_t)dgroups.back().pbase +
+                                                         (size_t)dgroups.back().n_blocks * dgroups.back().nl)
+                                : (size_t)G * kMeritParts;
+    auto a256 = [](size_t b) { return (b + 255) / 256 * 256; };
+    const size_t tab_bytes = dense ? a256(dblocks.size() * sizeof(DenseBlock)) + a256(G * sizeof(DenseGroup))
+                                   : a256(G * sizeof(Group));
     DevBuf buf;
-    const size_t part_bytes = (size_t)G * kMeritParts * 3 * sizeof(double);
-    int st = buf.alloc(G * sizeof(Group) + part_bytes + (size_t)G * 4 * sizeof(double) + 256, s);
+    int st = buf.alloc(tab_bytes + a256(n_part * 3 * sizeof(double)) + (size_t)G * 10 * sizeof(double), s);
     if (st != RTB_OK) return st;
     char* p = buf.as<char>();
+    double* d_part = reinterpret_cast<double*>(p + tab_bytes);
+    double* d_coef = reinterpret_cast<double*>(p + tab_bytes + a256(n_part * 3 * sizeof(double)));  // 4G
+    double* d_cen = d_coef + 4 * (size_t)G;                                                         // 2G
+    double* d_out = d_cen + 2 * (size_t)G;                                                           // 4G
     Group* d_groups = reinterpret_cast<Group*>(p);
-    double* d_part = reinterpret_cast<double*>(p + (G * sizeof(Group) + 255) / 256 * 256);
-    double* d_coef = d_part + (size_t)G * kMeritParts * 3;
-    RTB_CUDA_TRY(cudaMemcpyAsync(d_groups, groups.data(), G * sizeof(Group), cudaMemcpyHostToDevice, s));
-    std::vector<double> part((size_t)G * kMeritParts * 3);
-    std::vector<double> cen(2 * G, 0.0), nn(G, 0.0), ss(G, 0.0);
-    for (int pass = 0; pass < 2; ++pass) {
+    DenseBlock* d_blocks = reinterpret_cast<DenseBlock*>(p);
+    DenseGroup* d_dgroups = reinterpret_cast<DenseGroup*>(p + a256(dblocks.size() * sizeof(DenseBlock)));
+    if (dense) {
+        if (!dblocks.empty())
+            RTB_CUDA_TRY(cudaMemcpyAsync(d_blocks, dblocks.data(), dblocks.size() * sizeof(DenseBlock),
+                                         cudaMemcpyHostToDevice, s));
+        RTB_CUDA_TRY(cudaMemcpyAsync(d_dgroups, dgroups.data(), G * sizeof(DenseGroup), cudaMemcpyHostToDevice, s));
+        for (int pass = 0; pass < 2; ++pass) {
+            if (!dblocks.empty())
+                k_dense_moments<<<(unsigned)dblocks.size(), kMeritThreads, 0, s>>>(d_blocks, c->d_flag, c->d_X, c->d_Y,
+                                                                                   d_cen, pass, d_part);
+            k_dense_finish<<<G, kMeritThreads, 0, s>>>(d_dgroups, d_part, pass, d_cen, d_out);
+            RTB_CUDA_TRY(cudaGetLastError());
+        }
+        std::vector<double> out(4 * (size_t)G);
+        RTB_CUDA_TRY(cudaMemcpyAsync(out.data(), d_out, out.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+        RTB_CUDA_TRY(cudaStreamSynchronize(s));
+        for (int g = 0; g < G; ++g) {
+            nn[g] = out[4 * g];
+            cen[2 * g] = out[4 * g + 1];
+            cen[2 * g + 1] = out[4 * g + 2];
+            ss[g] = out[4 * g + 3];
+        }
+    } else {
+        RTB_CUDA_TRY(cudaMemcpyAsync(d_groups, groups.data(), G * sizeof(Group), cudaMemcpyHostToDevice, s));
+    }
+    std::vector<double> part(dense ? 0 : (size_t)G * kMeritParts * 3);
+    for (int pass = 0; pass < (dense ? 0 : 2); ++pass) {
         if (pass == 1) RTB_CUDA_TRY(cudaMemcpyAsync(d_coef, cen.data(), 2 * G * sizeof(double), cudaMemcpyHostToDevice, s));
-        k_group_moments<<<dim3(kMeritParts, G), kMeritThreads, 0, s>>>(d_groups, c->d_flag, c->d_X, c->d_Y, d_coef, pass,
+        k_group_moments<<<dim3(G, kMeritParts), kMeritThreads, 0, s>>>(d_groups, c->d_flag, c->d_X, c->d_Y, d_coef, pass,
                                                                       d_part);
         RTB_CUDA_TRY(cudaGetLastError());
         RTB_CUDA_TRY(cudaMemcpyAsync(part.data(), d_part, part.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -760,10 +924,29 @@ int rtb_adjoint_spot_merit(rtb_adjoint* c, const double* target_x, double weight
     }
     *merit = M;
     if (gX) {
-        RTB_CUDA_TRY(cudaMemsetAsync(gX, 0, c->n * sizeof(double), s));  // rays outside every group
-        RTB_CUDA_TRY(cudaMemsetAsync(gY, 0, c->n * sizeof(double), s));
+        // rays outside every group get 0: all of them here, or (dense path,
+        // which writes every ray of every beam) those between the beams
+        uint64_t from = 0;
+        auto zero = [&](uint64_t a, uint64_t b) -> cudaError_t {
+            if (b <= a) return cudaSuccess;
+            cudaError_t e = cudaMemsetAsync(gX + a, 0, (b - a) * sizeof(double), s);
+            return e == cudaSuccess ? cudaMemsetAsync(gY + a, 0, (b - a) * sizeof(double), s) : e;
+        };
+        if (dense) {
+            for (const auto& b : c->beams_in) {
+                RTB_CUDA_TRY(zero(from, b.first_ray));
+                from = b.first_ray + b.n_rays;
+            }
+        }
+        RTB_CUDA_TRY(zero(from, c->n));
         RTB_CUDA_TRY(cudaMemcpyAsync(d_coef, coef.data(), coef.size() * sizeof(double), cudaMemcpyHostToDevice, s));
-        k_group_seeds<<<dim3(64, G), 256, 0, s>>>(d_groups, G, d_coef, c->d_flag, c->d_X, c->d_Y, gX, gY);
+        if (dense) {
+            if (!dblocks.empty())
+                k_dense_seeds<<<(unsigned)dblocks.size(), kMeritThreads, 0, s>>>(d_blocks, d_coef, c->d_flag, c->d_X,
+                                                                                 c->d_Y, gX, gY);
+        } else {
+            k_group_seeds<<<dim3(G, 64), 256, 0, s>>>(d_groups, G, d_coef, c->d_flag, c->d_X, c->d_Y, gX, gY);
+        }
         RTB_CUDA_TRY(cudaGetLastError());
         RTB_CUDA_TRY(cudaStreamSynchronize(s));
     }

@@ -235,3 +235,55 @@ def test_merit_gradient_matches_central_differences(n_per_lambda):
         g_lib = adj.backward(gX, gY)
         assert np.allclose(g_lib, g, rtol=1e-9, atol=0)
     adj.destroy()
+
+
+@pytest.mark.parametrize("n_lambda", [64, 300])
+def test_spot_merit_and_seeds_against_numpy(n_lambda):
+    """rtb_adjoint_spot_merit on two beams with rays outside both (before,
+    between, after): the merit and the per-ray seeds equal a numpy restatement
+    of sum_groups RMS + w (xbar - x_t)^2 over each beam's wavelength groups,
+    and the seeds of rays outside every beam are 0.  64 wavelengths take the
+    index-order path, 300 (more than a block's threads) the group-by-group one."""
+    specs = S.littrow_free_asphere()
+    cs = S.to_c(specs, E.spline_init)
+    a = S.make_beam(100, 40, n_lambda, S.C0_RADIUS, S.C4_LAMBDA, S.SEED + 41)
+    b = S.make_beam(100 + int(a.n_rays) + 77, 200, 5, S.C0_RADIUS, S.C4_LAMBDA, S.SEED + 42)
+    beams = [a, b]
+    n = int(b.first_ray + b.n_rays) + 50
+    groups = []
+    for bm in beams:
+        nl = int(bm.n_lambda) or 1
+        for j in range(nl):
+            groups.append(int(bm.first_ray) + j + nl * np.arange((int(bm.n_rays) - j + nl - 1) // nl))
+    outside = np.ones(n, bool)
+    for idx in groups:
+        outside[idx] = False
+    rays = E.generate(beams, n)
+    off = torch.as_tensor(outside, device="cuda")
+    rays.flag[off] = 0  # rays outside the beams: lost on entry, never traced
+    for f in E.FIELDS:
+        getattr(rays, f)[off] = 0.0
+    torch.cuda.synchronize()
+    adj = E.Adjoint(cs.surfaces, S.c4_params(), beams, n, fixes=FIXES)
+    st, _ = adj.forward(None, rays)
+    assert st == ffi.OK
+    X, Y = adj.X.cpu().numpy(), adj.Y.cpu().numpy()
+    good = adj.flag.cpu().numpy() == 1
+    target = np.linspace(-1.0, 1.0, len(groups))
+    m_lib, gX, gY = adj.spot_merit(target, WEIGHT)
+    M, rX, rY = 0.0, np.zeros(n), np.zeros(n)
+    for g, idx in enumerate(groups):
+        idx = idx[good[idx]]
+        if idx.size == 0:
+            continue
+        xb, yb = X[idx].mean(), Y[idx].mean()
+        rms = np.sqrt(np.mean((X[idx] - xb) ** 2 + (Y[idx] - yb) ** 2))
+        M += rms + WEIGHT * (xb - target[g]) ** 2
+        rX[idx] = (X[idx] - xb) / (idx.size * rms) + 2 * WEIGHT * (xb - target[g]) / idx.size
+        rY[idx] = (Y[idx] - yb) / (idx.size * rms)
+    assert abs(m_lib - M) <= 1e-12 * abs(M), (m_lib, M)
+    gX, gY = gX.cpu().numpy(), gY.cpu().numpy()
+    scale = max(np.abs(rX).max(), np.abs(rY).max())
+    assert np.abs(gX - rX).max() <= 1e-10 * scale and np.abs(gY - rY).max() <= 1e-10 * scale
+    assert outside.sum() == 100 + 77 + 50 and not gX[outside].any() and not gY[outside].any()
+    adj.destroy()
