@@ -199,21 +199,32 @@ def trace_host(surfaces, beams, host_rays, o: ffi.TraceOpts | None = None):
 
 
 def ccd_frame(rays: DeviceRays, ccd: ffi.CCD, counts=None, n_outside=None):
+    """Frame counts of the good rays (rtb_ccd_frame).  The call runs on the
+    library's own stream, which is not ordered with torch's: the device waits
+    for torch's work (the zeroed counters) before it and for the frame after
+    it, so the counts are complete when it returns."""
     import torch
     if counts is None:
         counts = torch.zeros(int(ccd.xdim) * int(ccd.ydim), dtype=torch.int32, device="cuda")
     if n_outside is None:
         n_outside = torch.zeros(1, dtype=torch.int64, device="cuda")
+    torch.cuda.synchronize()
     st = lib().rtb_ccd_frame(C.byref(rays.struct()), C.byref(ccd), ffi.vptr(counts), ffi.vptr(n_outside), None)
     ffi.check(st, "rtb_ccd_frame")
+    torch.cuda.synchronize()
     return counts, n_outside
 
 
 def reference_order(beams, n_stages: int, rays: DeviceRays):
+    """The reference's Rearrange order of each beam (rtb_reference_order), on
+    the library's own stream, waited for on both sides as in ccd_frame: the
+    order tensor is complete when it returns."""
     import torch
     order = torch.empty(rays.n, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
     st = lib().rtb_reference_order(_beams(beams), len(beams), n_stages, C.byref(rays.struct()), ffi.vptr(order), None)
     ffi.check(st, "rtb_reference_order")
+    torch.cuda.synchronize()
     return order
 
 
