@@ -150,7 +150,8 @@ def c4_adjoint(npl, reps=3):
     flattener, 64 wavelengths x npl rays, 24 parameters.  The merit
     sum_lambda RMS_spot + 10 (x_mean - x_t(lambda))^2 and its per-ray seeds
     come from rtb_adjoint_spot_merit; one forward with checkpoints, the merit
-    and one backward give its whole gradient.  Each call returns
+    and one backward give its whole gradient; likewise the spectral-resolution
+    merit (rtb_adjoint_resolution_merit).  Each call returns
     synchronised: wall-clock times, best of reps."""
     import torch
     from rt_b200 import engine as E
@@ -182,11 +183,17 @@ def c4_adjoint(npl, reps=3):
     d = np.zeros(len(theta))
     d[0] = 1.0
     t_jvp, _ = best(lambda: adj.jvp(d))
+    # the spectral-resolution merit (sum of inverse resolving powers along x)
+    # and its gradient by the same backward
+    t_res, (res_merit, rX, rY) = best(lambda: adj.resolution_merit(lam))
+    t_rbwd, rgrad = best(lambda: adj.backward(rX, rY))
     P = len(theta)
     res = {"n_rays": n, "n_good": stats.n_good, "n_params": P, "merit": merit,
            "forward_ms": t_fwd, "merit_ms": t_mer, "backward_ms": t_bwd, "jvp_ms_per_direction": t_jvp,
            "gradient_ms": t_fwd + t_mer + t_bwd, "central_differences_ms": 2 * P * t_fwd,
            "grad_norm": float(np.linalg.norm(grad)),
+           "resolution_merit": {"merit": res_merit, "merit_ms": t_res, "gradient_ms": t_fwd + t_res + t_rbwd,
+                                "grad_norm": float(np.linalg.norm(rgrad))},
            "how": "rtb_adjoint_forward (checkpoints at surface inputs), rtb_adjoint_spot_merit, "
                   "rtb_adjoint_backward (reverse sweep inside each surface, compiled for the scheme's structure), rtb_adjoint_jvp; "
                   "wall clock of synchronous calls, best of 3"}

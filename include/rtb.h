@@ -622,6 +622,19 @@ RTB_API int rtb_adjoint_jvp(rtb_adjoint* ctx, const double* dtheta, double* dX, 
  * order.  Deterministic. */
 RTB_API int rtb_adjoint_spot_merit(rtb_adjoint* ctx, const double* target_x, double weight, double* merit,
                                    double* gX, double* gY, void* stream);
+/* The spectral-resolution merit of the last forward: along the dispersion
+ * direction u = (ux, uy) on the CCD (normalised here), each group's spot has a
+ * centroid p_g and an RMS width s_g; for every pair of neighbouring
+ * wavelengths g, g+1 of a beam (both with good rays) the width of a resolution
+ * element in wavelength over its mean wavelength,
+ *   (s_g + s_g+1) / 2 * |lambda_g+1 - lambda_g| / |p_g+1 - p_g| / ((lambda_g + lambda_g+1) / 2),
+ * is summed: the sum of the inverse resolving powers.  lambda: host, the
+ * wavelength of each group (beams in order).  *merit, gX, gY as in
+ * rtb_adjoint_spot_merit.  RTB_BAD_VALUE for a zero direction, a wavelength
+ * that is not positive, or two neighbouring spots with one centroid.  No
+ * counterpart in the reference.  Deterministic. */
+RTB_API int rtb_adjoint_resolution_merit(rtb_adjoint* ctx, const double* lambda, double ux, double uy, double* merit,
+                                         double* gX, double* gY, void* stream);
 RTB_API int rtb_adjoint_destroy(rtb_adjoint* ctx);
 /* Compile the adjoint's reverse sweep for this scheme's structure ahead of
  * rtb_adjoint_create (which compiles it otherwise, once per structure and

@@ -22,6 +22,8 @@
 //
 // Translation unit compiled with --fmad=false: the dual numbers' values are
 // the plain engine's.
+#include <algorithm>
+#include <cmath>
 #include <cstdlib>
 #include <cstring>
 #include <vector>
@@ -227,8 +229,9 @@ struct Group {
     uint64_t first, stride, count;
 };
 
-// pass 0: count, sum X, sum Y; pass 1: sum of squared distances from the
-// centroid.  Block (g, part) sums a fixed slice of group g.  The groups of a
+// pass 0: count, sum X, sum Y; pass 1: the second moments about the
+// centroid, sum dX^2, sum dY^2, sum dX dY.  Block (g, part) sums a fixed
+// slice of group g.  The groups of a
 // composite beam interleave (group j holds rays j, j + n_lambda, ...), so the
 // blocks of all groups for one slice -- launched together, group index
 // fastest -- read the same stretch of the arrays, and a sector fetched for
@@ -251,7 +254,9 @@ __global__ void __launch_bounds__(kMeritThreads) k_group_moments(const Group* gr
             v[2] += Y[i];
         } else {
             const double dx = X[i] - cx, dy = Y[i] - cy;
-            v[0] += dx * dx + dy * dy;
+            v[0] += dx * dx;
+            v[1] += dy * dy;
+            v[2] += dx * dy;
         }
     }
     __shared__ double red[3][kMeritThreads];
@@ -266,19 +271,30 @@ __global__ void __launch_bounds__(kMeritThreads) k_group_moments(const Group* gr
         for (int c = 0; c < 3; ++c) partial[((size_t)g * kMeritParts + part) * 3 + c] = red[c][0];
 }
 
-// Seeds: gX = a_g (X - xbar) + b_g, gY = a_g (Y - ybar) for good rays.
-// Block (g, part), group index fastest, as in k_group_moments.
+// Seeds of a merit that depends on each group's centroid and second
+// moments: for a good ray of group g, with (dX, dY) its offset from the
+// centroid (cx, cy), gX = axx dX + axy dY + bx and gY = ayx dX + ayy dY + by;
+// coef holds (axx, axy, ayx, ayy, bx, by, cx, cy) per group.  Block (g, part),
+// group index fastest, as in k_group_moments.
+constexpr int kSeedCoef = 8;
+
+__device__ __forceinline__ void seed_of(const double* k, double x, double y, double& gx, double& gy) {
+    const double dx = x - k[6], dy = y - k[7];
+    gx = fma(k[0], dx, fma(k[1], dy, k[4]));
+    gy = fma(k[2], dx, fma(k[3], dy, k[5]));
+}
+
 __global__ void k_group_seeds(const Group* groups, int n_groups, const double* coef, const char* flag, const double* X,
                               const double* Y, double* gX, double* gY) {
     const int g = blockIdx.x;
     if (g >= n_groups) return;
     const Group G = groups[g];
-    const double a = coef[4 * g], bx = coef[4 * g + 1], cx = coef[4 * g + 2], cy = coef[4 * g + 3];
+    double k[kSeedCoef];
+    for (int j = 0; j < kSeedCoef; ++j) k[j] = coef[kSeedCoef * g + j];
     for (uint64_t m = (uint64_t)blockIdx.y * blockDim.x + threadIdx.x; m < G.count; m += (uint64_t)gridDim.y * blockDim.x) {
         const uint64_t i = G.first + m * G.stride;
         if (flag[i] == 1) {
-            gX[i] = a * (X[i] - cx) + bx;
-            gY[i] = a * (Y[i] - cy);
+            seed_of(k, X[i], Y[i], gX[i], gY[i]);
         } else {
             gX[i] = 0.0;
             gY[i] = 0.0;
@@ -320,7 +336,9 @@ __global__ void __launch_bounds__(kMeritThreads) k_dense_moments(const DenseBloc
                 v[2] += Y[i];
             } else {
                 const double dx = X[i] - cx, dy = Y[i] - cy;
-                v[0] += dx * dx + dy * dy;
+                v[0] += dx * dx;
+                v[1] += dy * dy;
+                v[2] += dx * dy;
             }
         }
     }
@@ -337,8 +355,8 @@ __global__ void __launch_bounds__(kMeritThreads) k_dense_moments(const DenseBloc
 
 // Per group (one block each): the partials of its beam's blocks, thread t
 // adding blocks t, t + kMeritThreads, ... in order, then the threads' sums by
-// a fixed tree.  pass 0 leaves count and centroid in out[4g .. 4g+2] and the
-// centroid in `centroid`; pass 1 the sum of squared distances in out[4g+3].
+// a fixed tree.  pass 0 leaves count and centroid in out[6g .. 6g+2] and the
+// centroid in `centroid`; pass 1 the second moments in out[6g+3 .. 6g+5].
 struct DenseGroup {
     int32_t pbase, nl, n_blocks, lg;  // the beam's first partial, wavelengths, blocks; this group's wavelength
 };
@@ -361,11 +379,11 @@ __global__ void __launch_bounds__(kMeritThreads) k_dense_finish(const DenseGroup
     if (threadIdx.x != 0) return;
     for (int k = 0; k < 3; ++k) v[k] = red[k][0];
     if (pass == 0) {
-        out[4 * g] = v[0];
-        centroid[2 * g] = out[4 * g + 1] = v[0] > 0 ? v[1] / v[0] : 0.0;
-        centroid[2 * g + 1] = out[4 * g + 2] = v[0] > 0 ? v[2] / v[0] : 0.0;
+        out[6 * g] = v[0];
+        centroid[2 * g] = out[6 * g + 1] = v[0] > 0 ? v[1] / v[0] : 0.0;
+        centroid[2 * g + 1] = out[6 * g + 2] = v[0] > 0 ? v[2] / v[0] : 0.0;
     } else {
-        out[4 * g + 3] = v[0];
+        for (int k = 0; k < 3; ++k) out[6 * g + 3 + k] = v[k];
     }
 }
 
@@ -376,11 +394,11 @@ __global__ void __launch_bounds__(kMeritThreads) k_dense_seeds(const DenseBlock*
     const int t = threadIdx.x;
     if (t >= B.width) return;
     const int g = B.gbase + t % B.nl;
-    const double a = coef[4 * g], bx = coef[4 * g + 1], cx = coef[4 * g + 2], cy = coef[4 * g + 3];
+    double k[kSeedCoef];
+    for (int j = 0; j < kSeedCoef; ++j) k[j] = coef[kSeedCoef * g + j];
     for (uint64_t i = B.start + t; i < B.end; i += B.width) {
         if (flag[i] == 1) {
-            gX[i] = a * (X[i] - cx) + bx;
-            gY[i] = a * (Y[i] - cy);
+            seed_of(k, X[i], Y[i], gX[i], gY[i]);
         } else {
             gX[i] = 0.0;
             gY[i] = 0.0;
@@ -805,152 +823,279 @@ int rtb_adjoint_jvp(rtb_adjoint* c, const double* dtheta, double* dX, double* dY
     return RTB_OK;
 }
 
-int rtb_adjoint_spot_merit(rtb_adjoint* c, const double* target_x, double weight, double* merit, double* gX,
-                           double* gY, void* stream) {
-    Range range("rtb_adjoint_spot_merit");
-    if (!c || !target_x || !merit || !c->have_forward || ((gX == nullptr) != (gY == nullptr))) return RTB_BAD_VALUE;
-    DeviceGuard dg(c->device);
-    Lock l;
-    cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
-    std::vector<Group> groups;
-    for (const auto& b : c->beams_in) {
-        const uint64_t nl = b.n_lambda ? b.n_lambda : 1;
-        for (uint64_t j = 0; j < nl; ++j) {
-            const uint64_t cnt = (b.n_rays > j) ? (b.n_rays - j + nl - 1) / nl : 0;
-            groups.push_back(Group{b.first_ray + j, nl, cnt});
-        }
-    }
-    const int G = (int)groups.size();
-    if (G == 0 || G > 65535) return RTB_BAD_VALUE;
-    std::vector<double> cen(2 * G, 0.0), nn(G, 0.0), ss(G, 0.0);
-    // index-order (dense) path: every beam of at most kMeritThreads wavelengths
-    bool dense = true;
-    for (const auto& b : c->beams_in) dense = dense && (b.n_lambda ? b.n_lambda : 1) <= (uint64_t)kMeritThreads;
-    std::vector<DenseBlock> dblocks;
-    std::vector<DenseGroup> dgroups;
-    if (dense) {
-        constexpr uint64_t kRaysPerThread = 8;
-        uint64_t pbase = 0;
-        int32_t gbase = 0;
-        for (const auto& b : c->beams_in) {
-            const int32_t nl = (int32_t)(b.n_lambda ? b.n_lambda : 1);
-            const int32_t width = nl * (kMeritThreads / nl);
-            const uint64_t chunk = (uint64_t)width * kRaysPerThread;
-            const uint64_t nblk = (b.n_rays + chunk - 1) / chunk;
-            for (uint64_t k = 0; k < nblk; ++k) {
-                const uint64_t start = b.first_ray + k * chunk;
-                const uint64_t end = std::min(b.first_ray + b.n_rays, start + chunk);
-                dblocks.push_back(DenseBlock{start, end, nl, width, gbase, (int32_t)(pbase + k * (uint64_t)nl)});
+}  // extern "C"
+
+namespace {
+
+// The moments of every wavelength group of the last forward (group g = beam
+// b, wavelength index j; rays first_ray + j + m * n_lambda, good rays only)
+// and the kernels that turn per-group seed coefficients into per-ray seeds.
+struct GroupMoments {
+    std::vector<double> n, cx, cy, sxx, syy, sxy;  // count, centroid, second moments about it
+};
+
+class MeritPass {
+  public:
+    MeritPass(rtb_adjoint* c, cudaStream_t s) : c_(c), s_(s) {}
+
+    int moments(GroupMoments& m) {
+        for (const auto& b : c_->beams_in) {
+            const uint64_t nl = b.n_lambda ? b.n_lambda : 1;
+            for (uint64_t j = 0; j < nl; ++j) {
+                const uint64_t cnt = (b.n_rays > j) ? (b.n_rays - j + nl - 1) / nl : 0;
+                groups_.push_back(Group{b.first_ray + j, nl, cnt});
             }
-            for (int32_t j = 0; j < nl; ++j) dgroups.push_back(DenseGroup{(int32_t)pbase, nl, (int32_t)nblk, j});
-            pbase += nblk * (uint64_t)nl;
-            gbase += nl;
-            if (pbase > (uint64_t)INT32_MAX || dblocks.size() > (size_t)INT32_MAX) dense = false;
         }
-    }
-    const size_t n_part = dense ? (dgroups.empty() ? 0 : (size_t)dgroups.back().pbase +
-                                                         (size_t)dgroups.back().n_blocks * dgroups.back().nl)
-                                : (size_t)G * kMeritParts;
-    auto a256 = [](size_t b) { return (b + 255) / 256 * 256; };
-    const size_t tab_bytes = dense ? a256(dblocks.size() * sizeof(DenseBlock)) + a256(G * sizeof(DenseGroup))
-                                   : a256(G * sizeof(Group));
-    DevBuf buf;
-    int st = buf.alloc(tab_bytes + a256(n_part * 3 * sizeof(double)) + (size_t)G * 10 * sizeof(double), s);
-    if (st != RTB_OK) return st;
-    char* p = buf.as<char>();
-    double* d_part = reinterpret_cast<double*>(p + tab_bytes);
-    double* d_coef = reinterpret_cast<double*>(p + tab_bytes + a256(n_part * 3 * sizeof(double)));  // 4G
-    double* d_cen = d_coef + 4 * (size_t)G;                                                         // 2G
-    double* d_out = d_cen + 2 * (size_t)G;                                                           // 4G
-    Group* d_groups = reinterpret_cast<Group*>(p);
-    DenseBlock* d_blocks = reinterpret_cast<DenseBlock*>(p);
-    DenseGroup* d_dgroups = reinterpret_cast<DenseGroup*>(p + a256(dblocks.size() * sizeof(DenseBlock)));
-    if (dense) {
-        if (!dblocks.empty())
-            RTB_CUDA_TRY(cudaMemcpyAsync(d_blocks, dblocks.data(), dblocks.size() * sizeof(DenseBlock),
-                                         cudaMemcpyHostToDevice, s));
-        RTB_CUDA_TRY(cudaMemcpyAsync(d_dgroups, dgroups.data(), G * sizeof(DenseGroup), cudaMemcpyHostToDevice, s));
+        G_ = (int)groups_.size();
+        if (G_ == 0 || G_ > 65535) return RTB_BAD_VALUE;
+        // index-order (dense) path: every beam of at most kMeritThreads wavelengths
+        dense_ = true;
+        for (const auto& b : c_->beams_in) dense_ = dense_ && (b.n_lambda ? b.n_lambda : 1) <= (uint64_t)kMeritThreads;
+        if (dense_) {
+            constexpr uint64_t kRaysPerThread = 8;
+            uint64_t pbase = 0;
+            int32_t gbase = 0;
+            for (const auto& b : c_->beams_in) {
+                const int32_t nl = (int32_t)(b.n_lambda ? b.n_lambda : 1);
+                const int32_t width = nl * (kMeritThreads / nl);
+                const uint64_t chunk = (uint64_t)width * kRaysPerThread;
+                const uint64_t nblk = (b.n_rays + chunk - 1) / chunk;
+                for (uint64_t k = 0; k < nblk; ++k) {
+                    const uint64_t start = b.first_ray + k * chunk;
+                    const uint64_t end = std::min(b.first_ray + b.n_rays, start + chunk);
+                    dblocks_.push_back(DenseBlock{start, end, nl, width, gbase, (int32_t)(pbase + k * (uint64_t)nl)});
+                }
+                for (int32_t j = 0; j < nl; ++j) dgroups_.push_back(DenseGroup{(int32_t)pbase, nl, (int32_t)nblk, j});
+                pbase += nblk * (uint64_t)nl;
+                gbase += nl;
+                if (pbase > (uint64_t)INT32_MAX || dblocks_.size() > (size_t)INT32_MAX) dense_ = false;
+            }
+        }
+        const size_t n_part = dense_ ? (size_t)dgroups_.back().pbase + (size_t)dgroups_.back().n_blocks * dgroups_.back().nl
+                                     : (size_t)G_ * kMeritParts;
+        const size_t tab_bytes = dense_ ? a256(dblocks_.size() * sizeof(DenseBlock)) + a256(G_ * sizeof(DenseGroup))
+                                        : a256(G_ * sizeof(Group));
+        const size_t part_bytes = a256(n_part * 3 * sizeof(double));
+        int st = buf_.alloc(tab_bytes + part_bytes + (size_t)G_ * (kSeedCoef + 2 + 6) * sizeof(double), s_);
+        if (st != RTB_OK) return st;
+        char* p = buf_.as<char>();
+        d_groups_ = reinterpret_cast<Group*>(p);
+        d_blocks_ = reinterpret_cast<DenseBlock*>(p);
+        DenseGroup* d_dgroups = reinterpret_cast<DenseGroup*>(p + a256(dblocks_.size() * sizeof(DenseBlock)));
+        double* d_part = reinterpret_cast<double*>(p + tab_bytes);
+        d_coef_ = reinterpret_cast<double*>(p + tab_bytes + part_bytes);  // kSeedCoef G
+        double* d_cen = d_coef_ + (size_t)kSeedCoef * G_;                    // 2 G
+        double* d_out = d_cen + 2 * (size_t)G_;                              // 6 G
+        m.n.assign(G_, 0.0);
+        m.cx.assign(G_, 0.0);
+        m.cy.assign(G_, 0.0);
+        m.sxx.assign(G_, 0.0);
+        m.syy.assign(G_, 0.0);
+        m.sxy.assign(G_, 0.0);
+        cudaStream_t s = s_;
+        if (dense_) {
+            if (!dblocks_.empty())
+                RTB_CUDA_TRY(cudaMemcpyAsync(d_blocks_, dblocks_.data(), dblocks_.size() * sizeof(DenseBlock),
+                                             cudaMemcpyHostToDevice, s));
+            RTB_CUDA_TRY(cudaMemcpyAsync(d_dgroups, dgroups_.data(), G_ * sizeof(DenseGroup), cudaMemcpyHostToDevice, s));
+            for (int pass = 0; pass < 2; ++pass) {
+                if (!dblocks_.empty())
+                    k_dense_moments<<<(unsigned)dblocks_.size(), kMeritThreads, 0, s>>>(d_blocks_, c_->d_flag, c_->d_X,
+                                                                                        c_->d_Y, d_cen, pass, d_part);
+                k_dense_finish<<<G_, kMeritThreads, 0, s>>>(d_dgroups, d_part, pass, d_cen, d_out);
+                RTB_CUDA_TRY(cudaGetLastError());
+            }
+            std::vector<double> out(6 * (size_t)G_);
+            RTB_CUDA_TRY(cudaMemcpyAsync(out.data(), d_out, out.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+            RTB_CUDA_TRY(cudaStreamSynchronize(s));
+            for (int g = 0; g < G_; ++g) {
+                m.n[g] = out[6 * g];
+                m.cx[g] = out[6 * g + 1];
+                m.cy[g] = out[6 * g + 2];
+                m.sxx[g] = out[6 * g + 3];
+                m.syy[g] = out[6 * g + 4];
+                m.sxy[g] = out[6 * g + 5];
+            }
+            return RTB_OK;
+        }
+        RTB_CUDA_TRY(cudaMemcpyAsync(d_groups_, groups_.data(), G_ * sizeof(Group), cudaMemcpyHostToDevice, s));
+        std::vector<double> part((size_t)G_ * kMeritParts * 3), cen(2 * (size_t)G_);
         for (int pass = 0; pass < 2; ++pass) {
-            if (!dblocks.empty())
-                k_dense_moments<<<(unsigned)dblocks.size(), kMeritThreads, 0, s>>>(d_blocks, c->d_flag, c->d_X, c->d_Y,
-                                                                                   d_cen, pass, d_part);
-            k_dense_finish<<<G, kMeritThreads, 0, s>>>(d_dgroups, d_part, pass, d_cen, d_out);
+            if (pass == 1)
+                RTB_CUDA_TRY(cudaMemcpyAsync(d_cen, cen.data(), cen.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+            k_group_moments<<<dim3(G_, kMeritParts), kMeritThreads, 0, s>>>(d_groups_, c_->d_flag, c_->d_X, c_->d_Y,
+                                                                           d_cen, pass, d_part);
             RTB_CUDA_TRY(cudaGetLastError());
-        }
-        std::vector<double> out(4 * (size_t)G);
-        RTB_CUDA_TRY(cudaMemcpyAsync(out.data(), d_out, out.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
-        RTB_CUDA_TRY(cudaStreamSynchronize(s));
-        for (int g = 0; g < G; ++g) {
-            nn[g] = out[4 * g];
-            cen[2 * g] = out[4 * g + 1];
-            cen[2 * g + 1] = out[4 * g + 2];
-            ss[g] = out[4 * g + 3];
-        }
-    } else {
-        RTB_CUDA_TRY(cudaMemcpyAsync(d_groups, groups.data(), G * sizeof(Group), cudaMemcpyHostToDevice, s));
-    }
-    std::vector<double> part(dense ? 0 : (size_t)G * kMeritParts * 3);
-    for (int pass = 0; pass < (dense ? 0 : 2); ++pass) {
-        if (pass == 1) RTB_CUDA_TRY(cudaMemcpyAsync(d_coef, cen.data(), 2 * G * sizeof(double), cudaMemcpyHostToDevice, s));
-        k_group_moments<<<dim3(G, kMeritParts), kMeritThreads, 0, s>>>(d_groups, c->d_flag, c->d_X, c->d_Y, d_coef, pass,
-                                                                      d_part);
-        RTB_CUDA_TRY(cudaGetLastError());
-        RTB_CUDA_TRY(cudaMemcpyAsync(part.data(), d_part, part.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
-        RTB_CUDA_TRY(cudaStreamSynchronize(s));
-        for (int g = 0; g < G; ++g) {
-            double v[3] = {0, 0, 0};
-            for (int q = 0; q < kMeritParts; ++q)
-                for (int k = 0; k < 3; ++k) v[k] += part[((size_t)g * kMeritParts + q) * 3 + k];
-            if (pass == 0) {
-                nn[g] = v[0];
-                cen[2 * g] = v[0] > 0 ? v[1] / v[0] : 0.0;
-                cen[2 * g + 1] = v[0] > 0 ? v[2] / v[0] : 0.0;
-            } else {
-                ss[g] = v[0];
+            RTB_CUDA_TRY(cudaMemcpyAsync(part.data(), d_part, part.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+            RTB_CUDA_TRY(cudaStreamSynchronize(s));
+            for (int g = 0; g < G_; ++g) {
+                double v[3] = {0, 0, 0};
+                for (int q = 0; q < kMeritParts; ++q)
+                    for (int k = 0; k < 3; ++k) v[k] += part[((size_t)g * kMeritParts + q) * 3 + k];
+                if (pass == 0) {
+                    m.n[g] = v[0];
+                    cen[2 * g] = m.cx[g] = v[0] > 0 ? v[1] / v[0] : 0.0;
+                    cen[2 * g + 1] = m.cy[g] = v[0] > 0 ? v[2] / v[0] : 0.0;
+                } else {
+                    m.sxx[g] = v[0];
+                    m.syy[g] = v[1];
+                    m.sxy[g] = v[2];
+                }
             }
         }
+        return RTB_OK;
     }
-    double M = 0.0;
-    std::vector<double> coef(4 * G, 0.0);
-    for (int g = 0; g < G; ++g) {
-        if (!(nn[g] > 0)) continue;
-        const double rms = std::sqrt(ss[g] / nn[g]);
-        const double dx = cen[2 * g] - target_x[g];
-        M += rms + weight * dx * dx;
-        coef[4 * g] = rms > 0 ? 1.0 / (nn[g] * rms) : 0.0;  // d rms / dX_i = (X_i - xbar) / (N rms)
-        coef[4 * g + 1] = 2.0 * weight * dx / nn[g];        // d w (xbar - t)^2 / dX_i
-        coef[4 * g + 2] = cen[2 * g];
-        coef[4 * g + 3] = cen[2 * g + 1];
-    }
-    *merit = M;
-    if (gX) {
-        // rays outside every group get 0: all of them here, or (dense path,
-        // which writes every ray of every beam) those between the beams
+
+    // Per-ray seeds from kSeedCoef coefficients per group (see seed_of); rays
+    // outside every group get 0.
+    int seeds(const std::vector<double>& coef, double* gX, double* gY) {
+        cudaStream_t s = s_;
+        // rays outside every group: all of them here, or (dense path, which
+        // writes every ray of every beam) those between the beams
         uint64_t from = 0;
         auto zero = [&](uint64_t a, uint64_t b) -> cudaError_t {
             if (b <= a) return cudaSuccess;
             cudaError_t e = cudaMemsetAsync(gX + a, 0, (b - a) * sizeof(double), s);
             return e == cudaSuccess ? cudaMemsetAsync(gY + a, 0, (b - a) * sizeof(double), s) : e;
         };
-        if (dense) {
-            for (const auto& b : c->beams_in) {
+        if (dense_) {
+            for (const auto& b : c_->beams_in) {
                 RTB_CUDA_TRY(zero(from, b.first_ray));
                 from = b.first_ray + b.n_rays;
             }
         }
-        RTB_CUDA_TRY(zero(from, c->n));
-        RTB_CUDA_TRY(cudaMemcpyAsync(d_coef, coef.data(), coef.size() * sizeof(double), cudaMemcpyHostToDevice, s));
-        if (dense) {
-            if (!dblocks.empty())
-                k_dense_seeds<<<(unsigned)dblocks.size(), kMeritThreads, 0, s>>>(d_blocks, d_coef, c->d_flag, c->d_X,
-                                                                                 c->d_Y, gX, gY);
+        RTB_CUDA_TRY(zero(from, c_->n));
+        RTB_CUDA_TRY(cudaMemcpyAsync(d_coef_, coef.data(), coef.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+        if (dense_) {
+            if (!dblocks_.empty())
+                k_dense_seeds<<<(unsigned)dblocks_.size(), kMeritThreads, 0, s>>>(d_blocks_, d_coef_, c_->d_flag,
+                                                                                  c_->d_X, c_->d_Y, gX, gY);
         } else {
-            k_group_seeds<<<dim3(G, 64), 256, 0, s>>>(d_groups, G, d_coef, c->d_flag, c->d_X, c->d_Y, gX, gY);
+            k_group_seeds<<<dim3(G_, 64), 256, 0, s>>>(d_groups_, G_, d_coef_, c_->d_flag, c_->d_X, c_->d_Y, gX, gY);
         }
         RTB_CUDA_TRY(cudaGetLastError());
         RTB_CUDA_TRY(cudaStreamSynchronize(s));
+        return RTB_OK;
     }
-    return RTB_OK;
+
+    int n_groups() const { return G_; }
+
+  private:
+    static size_t a256(size_t b) { return (b + 255) / 256 * 256; }
+    rtb_adjoint* c_;
+    cudaStream_t s_;
+    std::vector<Group> groups_;
+    std::vector<DenseBlock> dblocks_;
+    std::vector<DenseGroup> dgroups_;
+    int G_ = 0;
+    bool dense_ = false;
+    DevBuf buf_;
+    Group* d_groups_ = nullptr;
+    DenseBlock* d_blocks_ = nullptr;
+    double* d_coef_ = nullptr;
+};
+
+}  // namespace
+
+extern "C" {
+
+int rtb_adjoint_spot_merit(rtb_adjoint* c, const double* target_x, double weight, double* merit, double* gX,
+                           double* gY, void* stream) {
+    Range range("rtb_adjoint_spot_merit");
+    if (!c || !target_x || !merit || !c->have_forward || ((gX == nullptr) != (gY == nullptr))) return RTB_BAD_VALUE;
+    DeviceGuard dg(c->device);
+    Lock l;
+    MeritPass mp(c, stream ? (cudaStream_t)stream : c->stream);
+    GroupMoments m;
+    int st = mp.moments(m);
+    if (st != RTB_OK) return st;
+    const int G = mp.n_groups();
+    double M = 0.0;
+    std::vector<double> coef((size_t)kSeedCoef * G, 0.0);
+    for (int g = 0; g < G; ++g) {
+        if (!(m.n[g] > 0)) continue;
+        const double rms = std::sqrt((m.sxx[g] + m.syy[g]) / m.n[g]);
+        const double dx = m.cx[g] - target_x[g];
+        M += rms + weight * dx * dx;
+        double* k = &coef[(size_t)kSeedCoef * g];
+        const double a = rms > 0 ? 1.0 / (m.n[g] * rms) : 0.0;  // d rms / dX_i = (X_i - xbar) / (N rms)
+        k[0] = k[3] = a;
+        k[4] = 2.0 * weight * dx / m.n[g];  // d w (xbar - t)^2 / dX_i
+        k[6] = m.cx[g];
+        k[7] = m.cy[g];
+    }
+    *merit = M;
+    return gX ? mp.seeds(coef, gX, gY) : RTB_OK;
+}
+
+int rtb_adjoint_resolution_merit(rtb_adjoint* c, const double* lambda, double ux, double uy, double* merit,
+                                 double* gX, double* gY, void* stream) {
+    Range range("rtb_adjoint_resolution_merit");
+    if (!c || !lambda || !merit || !c->have_forward || ((gX == nullptr) != (gY == nullptr))) return RTB_BAD_VALUE;
+    const double un = std::hypot(ux, uy);
+    if (!(un > 0.0) || !std::isfinite(un)) return RTB_BAD_VALUE;
+    ux /= un;
+    uy /= un;
+    DeviceGuard dg(c->device);
+    Lock l;
+    MeritPass mp(c, stream ? (cudaStream_t)stream : c->stream);
+    GroupMoments m;
+    int st = mp.moments(m);
+    if (st != RTB_OK) return st;
+    const int G = mp.n_groups();
+    for (int g = 0; g < G; ++g)
+        if (!std::isfinite(lambda[g]) || !(lambda[g] > 0.0)) return RTB_BAD_VALUE;
+    // along the dispersion direction u: the centroid p_g and RMS width s_g of
+    // each group's spot
+    std::vector<double> p(G, 0.0), sg(G, 0.0), dM_dp(G, 0.0), dM_ds(G, 0.0);
+    for (int g = 0; g < G; ++g) {
+        if (!(m.n[g] > 0)) continue;
+        p[g] = ux * m.cx[g] + uy * m.cy[g];
+        const double v = (ux * ux * m.sxx[g] + 2.0 * ux * uy * m.sxy[g] + uy * uy * m.syy[g]) / m.n[g];
+        sg[g] = std::sqrt(std::max(v, 0.0));
+    }
+    // pairs of neighbouring wavelengths of a beam, both with good rays: the
+    // width of a resolution element in wavelength over its mean wavelength,
+    // (s_g + s_h) / 2 * |lambda_h - lambda_g| / |p_h - p_g| / ((lambda_g + lambda_h) / 2)
+    double M = 0.0;
+    int g0 = 0;
+    for (const auto& b : c->beams_in) {
+        const int nl = (int)(b.n_lambda ? b.n_lambda : 1);
+        for (int j = 0; j + 1 < nl; ++j) {
+            const int g = g0 + j, h = g + 1;
+            if (!(m.n[g] > 0) || !(m.n[h] > 0)) continue;
+            const double d = p[h] - p[g];
+            if (d == 0.0) return RTB_BAD_VALUE;  // two wavelengths on one spot: no resolution to speak of
+            const double w = std::fabs(lambda[h] - lambda[g]) / (0.5 * (lambda[g] + lambda[h]));
+            const double ad = std::fabs(d), sbar = 0.5 * (sg[g] + sg[h]);
+            M += w * sbar / ad;
+            dM_ds[g] += 0.5 * w / ad;
+            dM_ds[h] += 0.5 * w / ad;
+            const double dd = -w * sbar / (ad * d);  // d(w sbar / |d|) / dd
+            dM_dp[h] += dd;
+            dM_dp[g] -= dd;
+        }
+        g0 += nl;
+    }
+    *merit = M;
+    if (!gX) return RTB_OK;
+    // d/dq_i of p_g = 1 / N_g, of s_g = (q_i - p_g) / (N_g s_g), q_i = u . (X_i, Y_i):
+    // dM/dX_i = ux (dM/dp_g / N_g + dM/ds_g (q_i - p_g) / (N_g s_g)), likewise Y
+    std::vector<double> coef((size_t)kSeedCoef * G, 0.0);
+    for (int g = 0; g < G; ++g) {
+        if (!(m.n[g] > 0)) continue;
+        double* k = &coef[(size_t)kSeedCoef * g];
+        const double a = sg[g] > 0 ? dM_ds[g] / (m.n[g] * sg[g]) : 0.0, bp = dM_dp[g] / m.n[g];
+        k[0] = a * ux * ux;
+        k[1] = a * ux * uy;
+        k[2] = a * ux * uy;
+        k[3] = a * uy * uy;
+        k[4] = bp * ux;
+        k[5] = bp * uy;
+        k[6] = m.cx[g];
+        k[7] = m.cy[g];
+    }
+    return mp.seeds(coef, gX, gY);
 }
 
 int rtb_adjoint_destroy(rtb_adjoint* c) {

@@ -55,6 +55,7 @@ def lib() -> C.CDLL:
         L.rtb_adjoint_backward.argtypes = [vp, vp, vp, vp, vp]
         L.rtb_adjoint_jvp.argtypes = [vp, vp, vp, vp, vp]
         L.rtb_adjoint_spot_merit.argtypes = [vp, vp, C.c_double, P(C.c_double), vp, vp, vp]
+        L.rtb_adjoint_resolution_merit.argtypes = [vp, vp, C.c_double, C.c_double, P(C.c_double), vp, vp, vp]
         L.rtb_adjoint_destroy.argtypes = [vp]
         L.rtb_qe_curves.argtypes = [P(ffi.QeSurface), C.c_size_t, vp, C.c_size_t, C.c_size_t, C.c_size_t, vp, vp]
         L.rtb_grating_energy_distr.argtypes = [C.c_size_t, vp, C.c_long] + [C.c_double] * 6 + [vp]
@@ -388,6 +389,19 @@ class Adjoint:
         self._sync()
         ffi.check(lib().rtb_adjoint_spot_merit(self.h, t.ctypes.data, weight, C.byref(m), ffi.vptr(gX), ffi.vptr(gY),
                                                None), "rtb_adjoint_spot_merit")
+        return m.value, gX, gY
+
+    def resolution_merit(self, lambdas, direction=(1.0, 0.0)):
+        """rtb_adjoint_resolution_merit: (merit, gX, gY), the seeds on the device."""
+        import torch
+        lam = np.ascontiguousarray(lambdas, dtype=np.float64)
+        m = C.c_double(0.0)
+        gX = torch.empty(self.n, dtype=torch.float64, device="cuda")
+        gY = torch.empty(self.n, dtype=torch.float64, device="cuda")
+        self._sync()
+        ffi.check(lib().rtb_adjoint_resolution_merit(self.h, lam.ctypes.data, float(direction[0]), float(direction[1]),
+                                                     C.byref(m), ffi.vptr(gX), ffi.vptr(gY), None),
+                  "rtb_adjoint_resolution_merit")
         return m.value, gX, gY
 
     def destroy(self):

@@ -237,24 +237,23 @@ def test_merit_gradient_matches_central_differences(n_per_lambda):
     adj.destroy()
 
 
-@pytest.mark.parametrize("n_lambda", [64, 300])
-def test_spot_merit_and_seeds_against_numpy(n_lambda):
-    """rtb_adjoint_spot_merit on two beams with rays outside both (before,
-    between, after): the merit and the per-ray seeds equal a numpy restatement
-    of sum_groups RMS + w (xbar - x_t)^2 over each beam's wavelength groups,
-    and the seeds of rays outside every beam are 0.  64 wavelengths take the
-    index-order path, 300 (more than a block's threads) the group-by-group one."""
+def _two_beam_forward(n_lambda):
+    """C4's scheme traced for two beams (n_lambda and 5 wavelengths) with rays
+    outside both (before, between, after): the adjoint, the forward's X, Y
+    and good flags (numpy), each wavelength group's ray indices and the mask
+    of the rays outside every beam."""
     specs = S.littrow_free_asphere()
     cs = S.to_c(specs, E.spline_init)
     a = S.make_beam(100, 40, n_lambda, S.C0_RADIUS, S.C4_LAMBDA, S.SEED + 41)
     b = S.make_beam(100 + int(a.n_rays) + 77, 200, 5, S.C0_RADIUS, S.C4_LAMBDA, S.SEED + 42)
     beams = [a, b]
     n = int(b.first_ray + b.n_rays) + 50
-    groups = []
+    groups, lams = [], []
     for bm in beams:
         nl = int(bm.n_lambda) or 1
         for j in range(nl):
             groups.append(int(bm.first_ray) + j + nl * np.arange((int(bm.n_rays) - j + nl - 1) // nl))
+            lams.append(bm.range[0] + j * (bm.range[1] - bm.range[0]) / max(1, nl - 1))
     outside = np.ones(n, bool)
     for idx in groups:
         outside[idx] = False
@@ -269,6 +268,25 @@ def test_spot_merit_and_seeds_against_numpy(n_lambda):
     assert st == ffi.OK
     X, Y = adj.X.cpu().numpy(), adj.Y.cpu().numpy()
     good = adj.flag.cpu().numpy() == 1
+    return adj, X, Y, good, groups, np.array(lams), outside, [int(bm.n_lambda) or 1 for bm in beams]
+
+
+def _check_seeds(gX, gY, rX, rY, outside):
+    gX, gY = gX.cpu().numpy(), gY.cpu().numpy()
+    scale = max(np.abs(rX).max(), np.abs(rY).max())
+    assert np.abs(gX - rX).max() <= 1e-10 * scale and np.abs(gY - rY).max() <= 1e-10 * scale
+    assert outside.sum() == 100 + 77 + 50 and not gX[outside].any() and not gY[outside].any()
+
+
+@pytest.mark.parametrize("n_lambda", [64, 300])
+def test_spot_merit_and_seeds_against_numpy(n_lambda):
+    """rtb_adjoint_spot_merit on two beams with rays outside both: the merit
+    and the per-ray seeds equal a numpy restatement of sum_groups RMS + w
+    (xbar - x_t)^2 over each beam's wavelength groups, and the seeds of rays
+    outside every beam are 0.  64 wavelengths take the index-order path, 300
+    (more than a block's threads) the group-by-group one."""
+    adj, X, Y, good, groups, _, outside, _ = _two_beam_forward(n_lambda)
+    n = X.size
     target = np.linspace(-1.0, 1.0, len(groups))
     m_lib, gX, gY = adj.spot_merit(target, WEIGHT)
     M, rX, rY = 0.0, np.zeros(n), np.zeros(n)
@@ -282,8 +300,124 @@ def test_spot_merit_and_seeds_against_numpy(n_lambda):
         rX[idx] = (X[idx] - xb) / (idx.size * rms) + 2 * WEIGHT * (xb - target[g]) / idx.size
         rY[idx] = (Y[idx] - yb) / (idx.size * rms)
     assert abs(m_lib - M) <= 1e-12 * abs(M), (m_lib, M)
-    gX, gY = gX.cpu().numpy(), gY.cpu().numpy()
-    scale = max(np.abs(rX).max(), np.abs(rY).max())
-    assert np.abs(gX - rX).max() <= 1e-10 * scale and np.abs(gY - rY).max() <= 1e-10 * scale
-    assert outside.sum() == 100 + 77 + 50 and not gX[outside].any() and not gY[outside].any()
+    _check_seeds(gX, gY, rX, rY, outside)
+    adj.destroy()
+
+
+def resolution_np(X, Y, groups, lams, nls, u):
+    """The spectral-resolution merit (rtb_adjoint_resolution_merit) in numpy:
+    per group, the centroid p and RMS width s of u.(X, Y); summed over the
+    neighbouring wavelengths of each beam, s-bar |dlambda| / |dp| / lambda-bar.
+    Also returns its derivatives in each ray's X and Y (autograd by hand)."""
+    u = np.asarray(u, dtype=np.float64) / np.hypot(*u)
+    q = u[0] * X + u[1] * Y
+    p = np.array([q[i].mean() for i in groups])
+    s = np.array([np.sqrt(np.mean((q[i] - q[i].mean()) ** 2)) for i in groups])
+    M, dp, ds = 0.0, np.zeros(len(groups)), np.zeros(len(groups))
+    g0 = 0
+    for nl in nls:
+        for j in range(nl - 1):
+            g, h = g0 + j, g0 + j + 1
+            d = p[h] - p[g]
+            w = abs(lams[h] - lams[g]) / (0.5 * (lams[g] + lams[h]))
+            sb = 0.5 * (s[g] + s[h])
+            M += w * sb / abs(d)
+            ds[g] += 0.5 * w / abs(d)
+            ds[h] += 0.5 * w / abs(d)
+            dp[h] += -w * sb / (abs(d) * d)
+            dp[g] -= -w * sb / (abs(d) * d)
+        g0 += nl
+    rX, rY = np.zeros(X.size), np.zeros(X.size)
+    for g, i in enumerate(groups):
+        dq = dp[g] / i.size + ds[g] * (q[i] - p[g]) / (i.size * s[g])
+        rX[i], rY[i] = u[0] * dq, u[1] * dq
+    return M, rX, rY
+
+
+@pytest.mark.parametrize("n_lambda", [64, 300])
+def test_resolution_merit_and_seeds_against_numpy(n_lambda):
+    """rtb_adjoint_resolution_merit on the same two beams, along a tilted
+    dispersion direction: merit and seeds equal the numpy restatement; rays
+    outside every beam get 0; a zero direction is refused."""
+    adj, X, Y, good, groups, lams, outside, nls = _two_beam_forward(n_lambda)
+    u = (0.8, -0.35)
+    m_lib, gX, gY = adj.resolution_merit(lams, u)
+    M, rX, rY = resolution_np(X, Y, [i[good[i]] for i in groups], lams, nls, u)
+    assert abs(m_lib - M) <= 1e-11 * abs(M), (m_lib, M)
+    _check_seeds(gX, gY, rX, rY, outside)
+    with pytest.raises(RuntimeError):
+        adj.resolution_merit(lams, (0.0, 0.0))
+    adj.destroy()
+
+
+def resolution_difference(Xp, Yp, Xm, Ym, groups, lams):
+    """M(+) - M(-) of the resolution merit along x for two forwards on the same
+    rays, from per-ray differences (Xp - Xm is exact for nearby doubles) so
+    that it keeps its digits where M is far larger than the difference:
+    per pair, s/|d| moves by (ds |d-| - s- d|d|) / (|d+| |d-|), with the width
+    difference ds = (s+^2 - s-^2) / (s+ + s-) from the products of the
+    per-ray differences and sums."""
+    p, s, dp, ds = [], [], [], []
+    for i in groups:
+        xp, xm = Xp[i], Xm[i]
+        dx = xp - xm
+        pp, pm, dmean = xp.mean(), xm.mean(), dx.mean()
+        up, um = xp - pp, xm - pm
+        sp, sm = np.sqrt(np.mean(up * up)), np.sqrt(np.mean(um * um))
+        dvar = np.mean((dx - dmean) * (up + um))  # s+^2 - s-^2
+        p.append(pm)
+        s.append(sm)
+        dp.append(dmean)
+        ds.append(dvar / (sp + sm))
+    dM = 0.0
+    for g in range(len(groups) - 1):
+        h = g + 1
+        w = abs(lams[h] - lams[g]) / (0.5 * (lams[g] + lams[h]))
+        dm_, dd = p[h] - p[g], dp[h] - dp[g]
+        dpl = dm_ + dd
+        sbar_m, dsbar = 0.5 * (s[g] + s[h]), 0.5 * (ds[g] + ds[h])
+        dM += w * (dsbar * abs(dm_) - sbar_m * np.sign(dm_) * dd) / (abs(dpl) * abs(dm_))
+    return dM
+
+
+def test_resolution_merit_gradient_matches_central_differences():
+    """The gradient of the spectral-resolution merit by one forward, the
+    merit's seeds and one backward against central differences of the FP64
+    forward (relative step 1e-6) on C4 at 1e5 rays, both over the rays good at
+    theta0 and at every difference point: within 1e-6 relative.  Where no ray
+    changes its fate between those points, the library's own seeds
+    (rtb_adjoint_resolution_merit) give the same gradient."""
+    _, _, beams, n, rays, adj = setup(1600)
+    theta0 = adj.theta()
+    P = len(theta0)
+    h = steps(theta0)
+    lam = np.linspace(S.C4_LAMBDA[0], S.C4_LAMBDA[1], S.C4_NLAMBDA)
+    groups = [np.arange(j, n, S.C4_NLAMBDA) for j in range(S.C4_NLAMBDA)]
+    adj.forward(None, rays)
+    good0 = adj.flag.cpu().numpy() == 1
+    mask = good0.copy()
+    pts = []
+    for j in range(P):
+        for sgn in (1.0, -1.0):
+            t = theta0.copy()
+            t[j] += sgn * h[j]
+            st, _ = adj.forward(t, rays)
+            assert st == ffi.OK
+            mask &= adj.flag.cpu().numpy() == 1
+            pts.append((adj.X.cpu().numpy(), adj.Y.cpu().numpy()))
+    gm = [i[mask[i]] for i in groups]
+    merit = lambda X, Y: resolution_np(X, Y, gm, lam, [S.C4_NLAMBDA], (1.0, 0.0))  # noqa: E731
+    fd = np.array([resolution_difference(*pts[2 * j], *pts[2 * j + 1], gm, lam) / (2 * h[j]) for j in range(P)])
+    del pts
+    adj.forward(None, rays)
+    M, rX, rY = merit(adj.X.cpu().numpy(), adj.Y.cpu().numpy())
+    g = adj.backward(torch.as_tensor(rX, device="cuda"), torch.as_tensor(rY, device="cuda"))
+    rel = np.abs(g - fd) / np.abs(fd)
+    print("resolution merit", M, "rays changing fate", int((good0 & ~mask).sum()), "rel err", rel.max())
+    assert np.all(np.abs(fd) > 0)
+    assert rel.max() <= 1e-6, (int(np.argmax(rel)), rel.max())
+    if np.array_equal(mask, good0):
+        m_lib, gX, gY = adj.resolution_merit(lam)
+        assert abs(m_lib - M) <= 1e-11 * abs(M)
+        assert np.allclose(adj.backward(gX, gY), g, rtol=1e-9, atol=0)
     adj.destroy()
