@@ -77,3 +77,10 @@ def test_reference_arm_under_torchrun_two_ranks():
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
     assert d["e2e"]["value"] == d["value"] and d["cpu_baseline"]["kind"] == "port"
+    # the same workload config as the GPU arm's line (bench.workload_config)
+    sys.path.insert(0, ROOT)
+    import bench
+    from rt_b200 import schemes as S
+    beams = S.c1_beams()
+    assert d["config"] == bench.workload_config(S.total_rays(beams), len(beams))
+    assert d["metric"] == bench.METRIC and d["unit"] == bench.UNIT and d["higher_is_better"] is True
